@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark: implicit time steps of the 3D lens problem on B200 (plain FP64 path by default).
+
+A step is one implicit-Euler time step (dt = 250 s): a full Newton solve (ECFV+AD linearization,
+BiCGStab + red-black block ILU(0), FP64 update) of the 256 x 256 x 128 lens problem (8.39 M
+cells), starting from the hydrostatic state. W warm-up steps advance the simulation, then K steps
+are timed with CUDA events on the library's stream, bracketed by a barrier and a synchronize.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--precision mixed]
+
+Prints one JSON line. value = Mcells per second of implicit time steps (cells x steps / time);
+ms_per_step and s_per_step carry the time per step. Under torchrun every rank runs its own
+permeability realization (independent problems, no data-path collective: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ewoms-numerics_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "s per implicit time step, plain FP64 vs learned+mixed (same Newton tol); Mcells/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic bytes per kernel launch (FP64 s = 8, FP32 s = 4); see DESIGN.md
+
+
+def geometry(n):
+    nx, ny, nz = n
+    N = nx * ny * nz
+    F = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1)
+    return N, F
+
+
+def kernel_bytes(name, N, F, s_mat=8, s_vec=8):
+    """Bytes a launch must move at minimum in the band / red-black layout (no index arrays):
+    every matrix block and vector entry it needs read once, every output written once."""
+    Nh = N // 2
+    blk, vec = 4 * s_mat, 2 * s_vec
+    table = {
+        # linearization: x, storage(old), K, lens flag in; the iq cache out (6 doubles)
+        "intensive": N * (16 + 1) + N * 48,
+        # x, S_old, K, lens, iq (6) in; r and the Jacobian column (diag + 2 per face) out
+        "assemble": N * (16 + 16 + 8 + 1 + 48) + N * (16 + 32) + F * 64,
+        # black rows: own d, red d, L blocks (one per face), Dinv; y_b out
+        "ilu_black_apply": Nh * (vec + blk + vec) + Nh * vec + F * blk,
+        # red rows: own d, black y, A_rb blocks (one per face), Dinv; y_r out
+        "ilu_red_apply": Nh * (vec + blk + vec) + Nh * vec + F * blk,
+        "jacobi_apply": N * (vec + blk + vec),
+        # v = A y (all blocks, y) + r0hat for the dot; v out
+        "bicg_spmv_alpha": (N + 2 * F) * blk + N * vec * 3,
+        "bicg_spmv_omega": (N + 2 * F) * blk + N * vec * 3,
+        "spmv": (N + 2 * F) * blk + N * vec * 2,
+        "bicg_p": N * vec * 4,
+        "bicg_hs": N * vec * 6,
+        "bicg_xr": N * vec * 7,
+        "bicg_init": N * vec * 6,
+        "newton_update": N * 16 * 3,
+        "diag_inverse": N * blk * 2,
+        "ilu_black_factor": Nh * (2 * blk) + F * blk * 3 + Nh * blk,
+    }
+    return table.get(name)
+
+
+def lin_bytes(N, F, s=8):
+    """B_lin of the linearization (both kernels): N (2s x + 2s S_old + 8 K + 1 + 2s r + 4s J_ii)
+    + F (2 x 4s J_ij)."""
+    return N * (2 * s + 2 * s + 8 + 1 + 2 * s + 4 * s) + F * (8 * s)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ncu dram bytes (read + write) per launch at the full 256x256x128 workload, from the captures
+# summarised in profiles/ (scaled from the captured case by cell count where noted there).
+NCU_TRAFFIC = {}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline: the oracle restatement on the host cores
+
+
+def cpu_sample_run(nx, ny, nz, steps, seed=0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ewg
+    import oracle
+    oracle.build()
+    case = ewg.lens3d_case(nx, ny, nz, seed=seed)
+    cores = os.cpu_count() or 1
+    o = oracle.Oracle(case, nthreads=cores)
+    o.apply_initial_solution()
+    t0 = time.perf_counter()
+    its = o.run(steps, 250.0)
+    el = time.perf_counter() - t0
+    return case.n_cells, el, cores, its
+
+
+def cpu_baseline_block(nx=64, ny=64, nz=32):
+    n, el, cores, its = cpu_sample_run(nx, ny, nz, 1)
+    return {"value": n / el / 1e6, "unit": "Mcells/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (CPU restatement, element loop on {cores} threads, natural-order ILU0 "
+                      f"and BiCGStab sequential) on a {nx}x{ny}x{nz} sub-grid of the same 3D lens "
+                      f"problem, first implicit step (Newton {its[0][0]} its, BiCGStab {its[0][1]} its): "
+                      f"{el:.2f} s for {n} cells",
+            "s_per_step": el}
+
+
+# ---------------------------------------------------------------------------------------------
+
+
+def run_reference(args, rank, world, pg):
+    """The reference's CPU path: the oracle restatement on the host cores (the reference itself
+    needs DUNE / ewoms-material, absent here)."""
+    if rank != 0:
+        return
+    nx, ny, nz = 48, 48, 24
+    import ewg
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    case = ewg.lens3d_case(nx, ny, nz, seed=0)
+    cores = os.cpu_count() or 1
+    o = oracle.Oracle(case, nthreads=cores)
+    o.apply_initial_solution()
+    for _ in range(args.warmup):
+        o.run(1, 250.0)
+    t0 = time.perf_counter()
+    its = o.run(args.steps, 250.0)
+    el = time.perf_counter() - t0
+    value = case.n_cells * args.steps / el / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mcells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "s_per_step": el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"lens3d {nx}x{ny}x{nz} sample of the 256x256x128 lens problem",
+                                        "dt": 250.0, "newton_tol": 1e-8, "linear_tol": 1e-10},
+        "newton_its": [a for a, _ in its], "linear_its": [b for _, b in its],
+        "cpu_baseline": {"value": value, "unit": "Mcells/s", "cores": cores, "kind": "port",
+                         "sample": f"oracle restatement on a {nx}x{ny}x{nz} sub-grid, {args.steps} implicit steps after "
+                                   f"{args.warmup} warm-up steps, element loop on {cores} threads"},
+        "e2e": {"value": value, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local, pg):
+    import torch
+
+    import ewg
+    dev = local if torch.cuda.is_available() else 0
+    torch.cuda.set_device(dev)
+    nx, ny, nz = args.nx, args.ny, args.nz
+    case = ewg.lens3d_case(nx, ny, nz, seed=rank)
+    N, F = geometry((nx, ny, nz))
+    mixed = args.precision == "mixed"
+    sopts = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED if mixed else ewg.PRECISION_FP64)
+    nopts = ewg.default_newton_opts()
+    ctx = ewg.Context(case)
+    ctx.apply_initial_solution()
+
+    def one_step(dt=250.0):
+        h = dt
+        for _ in range(10):
+            st, rep = ctx.newton_apply(h, nopts, sopts)
+            if st == ewg.EWG_OK:
+                ctx.advance_time_level()
+                return rep
+            ctx.restore_time_level()
+            h /= 2
+        raise RuntimeError("time step failed after 10 halvings")
+
+    for _ in range(args.warmup):
+        one_step()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    torch.cuda.synchronize()
+    ctx.profile_reset()
+    ctx.profile_enable(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps = []
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            reps.append(one_step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg)
+    torch.cuda.synchronize()
+    ms_local = ev0.elapsed_time(ev1)
+    prof = ctx.profile()
+    ctx.profile_enable(False)
+    ms = max_over_ranks(pg, ms_local)
+    total_cells = sum_over_ranks(pg, float(N))
+    value = total_cells * args.steps / (ms * 1e-3) / 1e6
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.empty((N, 2), dtype=torch.float64, pin_memory=True)
+        xn = xh.numpy()
+        xn[:] = ctx.get_solution(0)
+        barrier(pg)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.set_solution(1, xn)
+            ctx.set_solution(0, xn)
+            h = 250.0
+            for _ in range(10):
+                st, _rep = ctx.newton_apply(h, nopts, sopts)
+                if st == ewg.EWG_OK:
+                    break
+                ctx.restore_time_level()
+                h /= 2
+            ctx.get_solution(0, out=xn)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(pg)
+        e_ms = max_over_ranks(pg, e0.elapsed_time(e1))
+        e2e = {"value": total_cells * args.steps / (e_ms * 1e-3) / 1e6, "unit": "Mcells/s",
+               "h2d_bytes_per_step": 2 * N * 16, "d2h_bytes_per_step": N * 16,
+               "ms_per_step": e_ms / args.steps}
+
+    if rank != 0:
+        ctx.close()
+        return
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak()
+    s = 4 if mixed else 8
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dn) = dom
+    db = kernel_bytes(dname, N, F, s_mat=s, s_vec=s)
+    avg_ms = dms / dn
+    achieved = db / (avg_ms * 1e-3) / 1e9 if db else None
+    traffic = NCU_TRAFFIC.get(dname)
+    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": traffic,
+                "algorithmic_bytes_per_launch": db, "avg_launch_ms": avg_ms, "launches": dn,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback"}
+    # linearization and BiCGStab-iteration rooflines
+    t_lin = sum(prof.get(k, (0, 0))[0] for k in ("intensive", "assemble"))
+    n_lin = prof.get("assemble", (0, 0))[1]
+    lin = None
+    if n_lin:
+        lin_avg = t_lin / n_lin
+        lb = lin_bytes(N, F, 8)
+        lin = {"ms_per_linearization": lin_avg, "mcells_per_s": N / (lin_avg * 1e-3) / 1e6,
+               "algorithmic_bytes": lb, "achieved_gbs": lb / (lin_avg * 1e-3) / 1e9,
+               "frac": lb / (lin_avg * 1e-3) / 1e9 / peak, "launches": n_lin}
+    it_kernels = ("bicg_p", "ilu_black_apply", "ilu_red_apply", "jacobi_apply", "bicg_spmv_alpha",
+                  "bicg_hs", "bicg_spmv_omega", "bicg_xr")
+    n_it = prof.get("bicg_xr", (0, 0))[1]
+    bicg = None
+    if n_it:
+        t_it = sum(prof.get(k, (0, 0))[0] for k in it_kernels) / n_it
+        b_it = sum((kernel_bytes(k, N, F, s, s) or 0) * prof.get(k, (0, 0))[1] for k in it_kernels) / n_it
+        bicg = {"ms_per_iteration": t_it, "iterations_per_s": 1e3 / t_it, "algorithmic_bytes": b_it,
+                "achieved_gbs": b_it / (t_it * 1e-3) / 1e9, "frac": b_it / (t_it * 1e-3) / 1e9 / peak,
+                "iterations": n_it}
+    launches = int(sum(v[1] for v in prof.values()))
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_block()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "s_per_step": ms / args.steps / 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if not mixed else "f64/f32",
+        "data": "synthetic (seeded log-normal permeability per rank, hydrostatic initial state)",
+        "config": {"workload": f"lens3d {nx}x{ny}x{nz} ({N} cells) plain {'FP64' if not mixed else 'mixed'} path, "
+                               f"implicit Euler dt=250 s, Newton tol 1e-8, BiCGStab+ILU0 rel 1e-10",
+                   "cells": N, "interior_faces": F, "precision": args.precision,
+                   "l2": "working set (> 4 GB) larger than L2 (126 MB); no flush needed"},
+        "newton_its": [r.iterations for r in reps], "linear_its": [r.linear_iterations for r in reps],
+        "phase_s": {"linearize": sum(r.t_linearize for r in reps) / len(reps),
+                    "solve": sum(r.t_solve for r in reps) / len(reps),
+                    "update": sum(r.t_update for r in reps) / len(reps)},
+        "roofline": roofline, "linearization": lin, "bicgstab": bicg,
+        "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        "gpu_launches": launches, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # the host-core reference arm: rank 0 alone runs it, other ranks exit without work
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")), None)
+        return
+    rank, world, local, pg = dist_init(args)
+    try:
+        run_ours(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

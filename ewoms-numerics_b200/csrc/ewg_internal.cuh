@@ -1,0 +1,206 @@
+// Internal declarations of the B200 ECFV linearizer / BiCGStab solver (libewg.so).
+//
+// Device storage order ("red-black split"): cell c = i + nx*(j + ny*k) has colour
+// col(c) = (i + j + k) & 1 and half index h(c) = c >> 1; it lives at s(c) = col*Nh + h with
+// Nh = N/2. nx is even, so the pair {2h, 2h+1} always holds one red and one black cell of the same
+// x-row, every colour holds exactly Nh cells, and a cell's face neighbours (all of the other
+// colour) sit at half indices h-1+b / h+b (x), h -/+ nx/2 (y), h -/+ nx*ny/2 (z) where b is the
+// cell's position in its pair. A warp of consecutive h therefore reads and writes contiguous
+// 8/16-byte words in every array and every neighbour stream.
+//
+// Jacobian: the reference's BCRS pattern (fvbaselinearizer.hh:303-340) is, on a structured grid,
+// the 5-point (2D) / 7-point (3D) block stencil, so it is stored band-major with implicit columns:
+// plane (band*4 + q)[s] holds entry q = 2*eq + pv of the block of row s in band
+//   0 diagonal, 1 -x, 2 +x, 3 -y, 4 +y, 5 -z, 6 +z.
+// Bands of missing neighbours (boundary rows) stay zero forever.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ewg.h"
+
+namespace ewg {
+
+constexpr int kMaxBands = 7;
+
+// Regularised material law of one region with the constants RegularizedVanGenuchtenParams /
+// RegularizedBrooksCoreyParams derive in finalize().
+struct LawDev {
+    int kind;
+    double swr, snr, den;           // den = 1 - (swr + snr)
+    // van Genuchten
+    double alpha, n, m, negInvM, invN, invM, twoM;
+    double pcLowSw, pcHighSw, pcLow, pcSlopeLow, m1High;
+    double spX0, spH, spY0, spY1, spHM0, spHM1;  // Hermite segment on [x0, x0 + h]
+    // Brooks-Corey
+    double pe, negInvLambda, krwExp, krnExp, bcLowSw, bcPcLow, bcSlopeLow, bcSlopeOne;
+};
+
+// Everything a kernel needs about the problem, passed by value.
+struct Phys {
+    int dim, nx, ny, nz;
+    int64_t N, Nh;
+    int nxh;                 // nx / 2
+    int64_t planeh;          // nx * ny / 2
+    int nb;                  // number of bands: 1 + 2*dim
+    double h[3], L[3];
+    double vol, area[3];
+    double porosity, rho[2], mu[2], g;  // gravity vector (0, -g, 0)
+    double pRef, leftScale;
+    double inletXlo, inletXhi, inletZlo, inletZhi, inletRate;
+    double lensLo[3], lensHi[3], eps;
+    LawDev law[2];           // 0 outer, 1 lens
+};
+
+struct CellIdx {
+    int64_t c;               // natural index
+    int i, j, k;
+    int b;                   // position inside the pair (c & 1)
+};
+
+__host__ __device__ inline CellIdx cell_of(const Phys& P, int col, int64_t h) {
+    CellIdx r;
+    int64_t row = h / P.nxh;              // x-row index j + ny*k
+    int64_t hx = h - row * P.nxh;
+    r.j = (int)(row % P.ny);
+    r.k = (int)(row / P.ny);
+    r.b = col ^ ((r.j + r.k) & 1);
+    r.i = (int)(2 * hx + r.b);
+    r.c = row * P.nx + r.i;
+    return r;
+}
+
+__host__ __device__ inline int64_t split_of(const Phys& P, int64_t c) {
+    int i = (int)(c % P.nx);
+    int64_t row = c / P.nx;
+    int j = (int)(row % P.ny), k = (int)(row / P.ny);
+    int col = (i + j + k) & 1;
+    return col * P.Nh + (c >> 1);
+}
+
+// Band of the face in direction (axis, side): 1 + 2*axis + side.
+__host__ __device__ inline int band_of(int axis, int side) { return 1 + 2 * axis + side; }
+__host__ __device__ inline int opposite_band(int band) { return band == 0 ? 0 : (((band - 1) ^ 1) + 1); }
+
+// Split-order position of the neighbour of cell (col, h, b) across face (axis, side), or -1.
+__host__ __device__ inline int64_t neighbour_split(const Phys& P, int col, int64_t h, const CellIdx& ci,
+                                                   int axis, int side) {
+    int64_t base = (int64_t)(col ^ 1) * P.Nh;
+    if (axis == 0) {
+        if (side == 0) return ci.i > 0 ? base + h - 1 + ci.b : -1;
+        return ci.i < P.nx - 1 ? base + h + ci.b : -1;
+    }
+    if (axis == 1) {
+        if (side == 0) return ci.j > 0 ? base + h - P.nxh : -1;
+        return ci.j < P.ny - 1 ? base + h + P.nxh : -1;
+    }
+    if (side == 0) return ci.k > 0 ? base + h - P.planeh : -1;
+    return ci.k < P.nz - 1 ? base + h + P.planeh : -1;
+}
+
+// ---- kernel profiling ----------------------------------------------------------------------
+
+// Kernel classes counted on every launch and, with profiling on, timed with a CUDA event pair on
+// the context stream (the device-side analogue of the reference's linearize / solve / update
+// timers, newtonmethod.hh:488-500).
+enum KernelId {
+    K_INTENSIVE = 0, K_ASSEMBLE, K_STORAGE, K_INITIAL, K_LAYOUT,
+    K_DIAG_INVERSE, K_ILU_BLACK_FACTOR, K_ILU_BLACK_APPLY, K_ILU_RED_APPLY, K_JACOBI_APPLY,
+    K_SPMV, K_BICG_INIT, K_BICG_P, K_BICG_SPMV_ALPHA, K_BICG_HS, K_BICG_SPMV_OMEGA, K_BICG_XR,
+    K_TO_FLOAT, K_DEFECT_ACCUMULATE, K_DEFECT_RESIDUAL, K_NEWTON_UPDATE, K_BCRS,
+    K_NUM_KERNELS
+};
+extern const char* const kKernelNames[K_NUM_KERNELS];
+
+struct Profiler {
+    static constexpr int kPool = 1024;
+    bool on = false;
+    cudaEvent_t ev[2 * kPool] = {};
+    int pendId[kPool] = {};
+    int npend = 0;
+    bool created = false;
+    double ms[K_NUM_KERNELS] = {};
+    long long launches[K_NUM_KERNELS] = {};
+};
+
+}  // namespace ewg
+
+struct ewg_ctx {
+    ewg::Phys P;
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    int jacPrecision = EWG_PRECISION_FP64;   // what ewg_linearize writes
+    bool jacFromLinearizer = false;          // J/r valid
+    bool iluValid = false;
+    int iluKind = -1, iluPrecision = -1;
+    // host copy of the reference BCRS pattern
+    int64_t nnzb = 0;
+    int32_t* d_rowPtr = nullptr;             // device BCRS pattern (for export / import)
+    int32_t* d_colIdx = nullptr;
+    // state (split order)
+    double2* x0 = nullptr;      // solution(0)
+    double2* x1 = nullptr;      // solution(1)
+    double2* sold = nullptr;    // storage of solution(1) per unit volume
+    double* perm = nullptr;
+    uint8_t* lens = nullptr;
+    double* iq = nullptr;       // 6 planes: pc, dpc, lw, dlw, ln, dln
+    double2* r = nullptr;       // residual
+    double* J = nullptr;        // nb*4 planes, FP64
+    float* J32 = nullptr;       // nb*4 planes, FP32 (mixed precision)
+    unsigned long long* d_errmax = nullptr;  // max|r| as ordered bits
+    int* d_flags = nullptr;                  // [0] nonfinite
+    // solver
+    double2* dx = nullptr;      // solution update
+    double2* d_stage = nullptr; // natural-order staging for host transfers
+    void* sv = nullptr;         // solver workspace (vectors, ILU factors), owned by the solver
+    size_t svBytes = 0;
+    // host staging
+    double* h_pinned = nullptr;
+    size_t h_pinnedBytes = 0;
+    ewg::Profiler prof;
+};
+
+namespace ewg {
+
+// ---- host helpers implemented across the .cu files --------------------------------------
+void prof_begin(ewg_ctx* ctx, int id);
+void prof_end(ewg_ctx* ctx, int id);
+void prof_flush(ewg_ctx* ctx);  // call after the stream is synchronised
+
+// Launch a kernel on the context stream, counted and (with profiling on) timed.
+#define EWG_LAUNCH(ctx, id, kernel, grid, block, ...)                      \
+    do {                                                                 \
+        ::ewg::prof_begin((ctx), (id));                                  \
+        kernel<<<(grid), (block), 0, (ctx)->stream>>>(__VA_ARGS__);      \
+        ::ewg::prof_end((ctx), (id));                                    \
+    } while (0)
+
+void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p);
+ewg_status cuda_fail(ewg_ctx* ctx, cudaError_t e, const char* what);
+int grid_size_for(ewg_ctx* ctx, const void* kernel, int block, size_t smem = 0);
+
+// linearization (ewg_linearize.cu)
+ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold);
+ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const double2* x,
+                            double2* r, double* maxOut, int* nonfinite);
+ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x);
+
+// solver (ewg_solver.cu)
+ewg_status solver_solve(ewg_ctx* ctx, const ewg_solve_opts* o, ewg_solve_report* rep);
+ewg_status solver_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* o, const double2* b,
+                                       double2* y);
+ewg_status solver_spmv(ewg_ctx* ctx, const double2* x, double2* y);
+ewg_status solver_newton_update(ewg_ctx* ctx, int* nonfinite);
+void solver_free(ewg_ctx* ctx);
+
+// layout conversion (ewg_api.cu)
+ewg_status to_split(ewg_ctx* ctx, const double* host_natural, double2* dev_split);
+ewg_status from_split(ewg_ctx* ctx, const double2* dev_split, double* host_natural);
+
+}  // namespace ewg

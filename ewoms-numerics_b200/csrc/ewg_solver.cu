@@ -1,0 +1,974 @@
+// Preconditioned BiCGStab on the band-stored block Jacobian (linear/bicgstabsolver.hh:116-326,
+// linear/combinedcriterion.hh:112-205, linear/parallelbasebackend.hh:301-338).
+//
+// Device design
+//   * All vectors are 2-blocks per cell in red-black split order (see ewg_internal.cuh).
+//   * Every BiCGStab scalar (rho, alpha, omega, the criterion errors, the status) lives in a
+//     device-side state word. Each kernel ends with a deterministic grid reduction (fixed grid,
+//     per-block partials, the last block to finish sums the partials in block order) and that
+//     last block updates the scalars, so the host never sits between two kernels of an iteration.
+//     The host reads the status only every few iterations; kernels launched after convergence
+//     return immediately.
+//   * Block ILU(0) in red-black order (colour 0 first). Red rows have only black neighbours, so
+//     the factorisation only changes black rows: L_bk = A_bk inv(D_k), D_b' = A_bb - sum L_bk A_kb
+//     (dune-istl bilu0_decomposition restricted to this ordering). Each sweep of
+//     bilu_backsolve becomes one fully parallel phase: black rows
+//     y_b = inv(D_b') (d_b - sum_k L_bk d_k), then red rows y_r = inv(D_r) (d_r - sum_b A_rb y_b).
+//   * FP32 instances of the same kernels run the inner solve of the mixed-precision mode.
+#include <math_constants.h>
+
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+
+#include "ewg_internal.cuh"
+
+namespace ewg {
+
+constexpr int kSolBlock = 256;
+constexpr int kMaxRed = 4;
+
+enum BiStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_FAILED = 2, ST_BREAKDOWN = 3, ST_MAXITER = 4 };
+
+struct BiState {
+    double rho, alpha, omega, rho_i, beta;
+    double r0r0;
+    double resErr, lastResErr, initResErr;
+    double relTol, absTol, maxRes;
+    double w;           // preconditioner relaxation
+    int status;
+    int iter;
+    int restarts;
+    int maxIter;
+    int restartOnBreakdown;
+    int restartPending;
+    int stagnates;
+    int pad;
+};
+
+template <typename T> struct V2T;
+template <> struct V2T<double> { using type = double2; };
+template <> struct V2T<float> { using type = float2; };
+
+// ---- deterministic grid reduction -----------------------------------------------------------
+
+template <int NS, int NM>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NS + NM], double* partials, unsigned* counter,
+                                            double (&out)[NS + NM]) {
+    constexpr int NV = NS + NM;
+    __shared__ double sh[NV][kSolBlock / 32];
+    __shared__ int amLast;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            double u = __shfl_xor_sync(0xffffffffu, v[k], o);
+            v[k] = k < NS ? v[k] + u : fmax(v[k], u);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NV; ++k) {
+            double a = sh[k][0];
+            for (int w = 1; w < nw; ++w) a = k < NS ? a + sh[k][w] : fmax(a, sh[k][w]);
+            partials[(size_t)blockIdx.x * NV + k] = a;
+        }
+        __threadfence();
+        amLast = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!amLast) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double u = __ldcg(&partials[(size_t)b * NV + k]);
+            acc[k] = k < NS ? acc[k] + u : fmax(acc[k], u);
+        }
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            double u = __shfl_xor_sync(0xffffffffu, acc[k], o);
+            acc[k] = k < NS ? acc[k] + u : fmax(acc[k], u);
+        }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NV; ++k) {
+            double a = sh[k][0];
+            for (int w = 1; w < nw; ++w) a = k < NS ? a + sh[k][w] : fmax(a, sh[k][w]);
+            out[k] = a;
+        }
+        *counter = 0u;
+    }
+    return true;
+}
+
+// NaN-propagating |x| for max reductions: NaN compares false, so map it to +inf
+__device__ __forceinline__ double absn(double x) { return x == x ? fabs(x) : CUDART_INF; }
+
+// ---- 2x2 helpers --------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ void load_block(const T* __restrict__ A, int64_t stride, int band, int64_t s, double b[4]) {
+    const T* p = A + (int64_t)band * 4 * stride + s;
+    b[0] = (double)p[0];
+    b[1] = (double)p[stride];
+    b[2] = (double)p[2 * stride];
+    b[3] = (double)p[3 * stride];
+}
+template <typename T>
+__device__ __forceinline__ void store4(T* __restrict__ A, int64_t stride, int plane4, int64_t s, const double b[4]) {
+    T* p = A + (int64_t)plane4 * 4 * stride + s;
+    p[0] = (T)b[0];
+    p[stride] = (T)b[1];
+    p[2 * stride] = (T)b[2];
+    p[3 * stride] = (T)b[3];
+}
+__device__ __forceinline__ bool inv2(const double a[4], double o[4]) {
+    double det = a[0] * a[3] - a[1] * a[2];
+    if (det == 0.0 || !isfinite(det)) return false;
+    double di = 1.0 / det;
+    o[0] = a[3] * di;
+    o[1] = -a[1] * di;
+    o[2] = -a[2] * di;
+    o[3] = a[0] * di;
+    return true;
+}
+__device__ __forceinline__ void mul2(const double a[4], const double b[4], double o[4]) {
+    double t0 = a[0] * b[0] + a[1] * b[2], t1 = a[0] * b[1] + a[1] * b[3];
+    double t2 = a[2] * b[0] + a[3] * b[2], t3 = a[2] * b[1] + a[3] * b[3];
+    o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+}
+
+// bands in ascending column order of a natural-order BCRS row, without the diagonal
+__host__ __device__ inline int lower_upper_band(int dim, int q) {
+    // 3D: -z -y -x +x +y +z ; 2D: -y -x +x +y
+    return dim == 3 ? (q == 0 ? 5 : q == 1 ? 3 : q == 2 ? 1 : q == 3 ? 2 : q == 4 ? 4 : 6)
+                    : (q == 0 ? 3 : q == 1 ? 1 : q == 2 ? 2 : 4);
+}
+
+__device__ __forceinline__ int64_t nbr_of_band(const Phys& P, int col, int64_t h, const CellIdx& ci, int band) {
+    return neighbour_split(P, col, h, ci, (band - 1) >> 1, (band - 1) & 1);
+}
+
+// ---- preconditioner setup -------------------------------------------------------------------
+
+// colour 0 (red) rows and, for block Jacobi, all rows: Dinv = inv(A_ii)
+template <typename TM>
+__global__ void k_diag_inverse(const __grid_constant__ Phys P, const TM* __restrict__ A, TM* __restrict__ Dinv,
+                               int64_t count, int* bad) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < count;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a[4], o[4];
+        load_block(A, P.N, 0, s, a);
+        if (!inv2(a, o)) { atomicOr(bad, 1); o[0] = o[1] = o[2] = o[3] = 0.0; }
+        store4(Dinv, P.N, 0, s, o);
+    }
+}
+
+// black rows: L_bk = A_bk inv(D_k) in ascending column order, D_b' = A_bb - sum L_bk A_kb
+template <typename TM>
+__global__ void k_ilu_black_factor(const __grid_constant__ Phys P, const TM* __restrict__ A, TM* __restrict__ Dinv,
+                                   TM* __restrict__ L, int* bad) {
+    const int nOff = 2 * P.dim;
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < P.Nh;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = P.Nh + h;
+        const CellIdx ci = cell_of(P, 1, h);
+        double D[4];
+        load_block(A, P.N, 0, s, D);
+        for (int q = 0; q < nOff; ++q) {
+            const int band = lower_upper_band(P.dim, q);
+            const int64_t sk = nbr_of_band(P, 1, h, ci, band);
+            double Lb[4] = {0.0, 0.0, 0.0, 0.0};
+            if (sk >= 0) {
+                double Abk[4], Dk[4], Akb[4], B[4];
+                load_block(A, P.N, band, s, Abk);
+                load_block(Dinv, P.N, 0, sk, Dk);
+                mul2(Abk, Dk, Lb);
+                load_block(A, P.N, opposite_band(band), sk, Akb);
+                mul2(Lb, Akb, B);
+                for (int t = 0; t < 4; ++t) D[t] -= B[t];
+            }
+            store4(L, P.Nh, band - 1, h, Lb);
+        }
+        double o[4];
+        if (!inv2(D, o)) { atomicOr(bad, 1); o[0] = o[1] = o[2] = o[3] = 0.0; }
+        store4(Dinv, P.N, 0, s, o);
+    }
+}
+
+// ---- preconditioner application -----------------------------------------------------------
+
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_ilu_black_apply(const __grid_constant__ Phys P, const TM* __restrict__ Dinv,
+                                                                const TM* __restrict__ L,
+                                                                const typename V2T<TV>::type* __restrict__ d,
+                                                                typename V2T<TV>::type* __restrict__ y,
+                                                                const int* __restrict__ status, double w) {
+    if (status && *status != ST_RUNNING) return;
+    const int nOff = 2 * P.dim;
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < P.Nh;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = P.Nh + h;
+        const CellIdx ci = cell_of(P, 1, h);
+        auto ds = d[s];
+        double r0 = (double)ds.x, r1 = (double)ds.y;
+        for (int q = 0; q < nOff; ++q) {
+            const int band = lower_upper_band(P.dim, q);
+            const int64_t sk = nbr_of_band(P, 1, h, ci, band);
+            if (sk < 0) continue;
+            double Lb[4];
+            load_block(L, P.Nh, band - 1, h, Lb);
+            auto dk = d[sk];
+            const double x0 = (double)dk.x, x1 = (double)dk.y;
+            r0 -= Lb[0] * x0; r0 -= Lb[1] * x1;
+            r1 -= Lb[2] * x0; r1 -= Lb[3] * x1;
+        }
+        double Di[4];
+        load_block(Dinv, P.N, 0, s, Di);
+        typename V2T<TV>::type out;
+        out.x = (TV)(w * (Di[0] * r0 + Di[1] * r1));
+        out.y = (TV)(w * (Di[2] * r0 + Di[3] * r1));
+        y[s] = out;
+    }
+}
+
+// red rows after the black phase: y_r = inv(D_r) (d_r - sum_b A_rb y_b), columns descending.
+// With relaxation w != 1 the black values were scaled by w; the backward sweep of the reference
+// runs on unscaled values and scales at the end, so undo it for the coupling term.
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_ilu_red_apply(const __grid_constant__ Phys P, const TM* __restrict__ A,
+                                                              const TM* __restrict__ Dinv,
+                                                              const typename V2T<TV>::type* __restrict__ d,
+                                                              typename V2T<TV>::type* __restrict__ y,
+                                                              const int* __restrict__ status, double w) {
+    if (status && *status != ST_RUNNING) return;
+    const int nOff = 2 * P.dim;
+    const double winv = 1.0 / w;
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < P.Nh;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = h;
+        const CellIdx ci = cell_of(P, 0, h);
+        auto ds = d[s];
+        double r0 = (double)ds.x, r1 = (double)ds.y;
+        for (int q = nOff - 1; q >= 0; --q) {
+            const int band = lower_upper_band(P.dim, q);
+            const int64_t sk = nbr_of_band(P, 0, h, ci, band);
+            if (sk < 0) continue;
+            double Ab[4];
+            load_block(A, P.N, band, s, Ab);
+            auto yk = y[sk];
+            double x0 = (double)yk.x, x1 = (double)yk.y;
+            if (w != 1.0) { x0 *= winv; x1 *= winv; }
+            r0 -= Ab[0] * x0; r0 -= Ab[1] * x1;
+            r1 -= Ab[2] * x0; r1 -= Ab[3] * x1;
+        }
+        double Di[4];
+        load_block(Dinv, P.N, 0, s, Di);
+        typename V2T<TV>::type out;
+        out.x = (TV)(w * (Di[0] * r0 + Di[1] * r1));
+        out.y = (TV)(w * (Di[2] * r0 + Di[3] * r1));
+        y[s] = out;
+    }
+}
+
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_jacobi_apply(const __grid_constant__ Phys P, const TM* __restrict__ Dinv,
+                                                             const typename V2T<TV>::type* __restrict__ d,
+                                                             typename V2T<TV>::type* __restrict__ y,
+                                                             const int* __restrict__ status, double w) {
+    if (status && *status != ST_RUNNING) return;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        auto ds = d[s];
+        const double r0 = (double)ds.x, r1 = (double)ds.y;
+        double Di[4];
+        load_block(Dinv, P.N, 0, s, Di);
+        typename V2T<TV>::type out;
+        out.x = (TV)(w * (Di[0] * r0 + Di[1] * r1));
+        out.y = (TV)(w * (Di[2] * r0 + Di[3] * r1));
+        y[s] = out;
+    }
+}
+
+// ---- SpMV ----------------------------------------------------------------------------------
+
+template <typename TM, typename TV>
+__device__ __forceinline__ void spmv_row(const Phys& P, const TM* __restrict__ A,
+                                         const typename V2T<TV>::type* __restrict__ x, int64_t s,
+                                         double& a0, double& a1) {
+    const int col = s >= P.Nh ? 1 : 0;
+    const int64_t h = s - col * P.Nh;
+    const CellIdx ci = cell_of(P, col, h);
+    const int nOff = 2 * P.dim;
+    a0 = 0.0; a1 = 0.0;
+    // ascending columns: lower bands, diagonal, upper bands
+    for (int q = 0; q <= nOff; ++q) {
+        int band;
+        int64_t sk;
+        if (q == P.dim) { band = 0; sk = s; }
+        else {
+            band = lower_upper_band(P.dim, q < P.dim ? q : q - 1);
+            sk = nbr_of_band(P, col, h, ci, band);
+            if (sk < 0) continue;
+        }
+        double B[4];
+        load_block(A, P.N, band, s, B);
+        auto xk = x[sk];
+        const double x0 = (double)xk.x, x1 = (double)xk.y;
+        a0 += B[0] * x0; a0 += B[1] * x1;
+        a1 += B[2] * x0; a1 += B[3] * x1;
+    }
+}
+
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_spmv(const __grid_constant__ Phys P, const TM* __restrict__ A,
+                                                     const typename V2T<TV>::type* __restrict__ x,
+                                                     typename V2T<TV>::type* __restrict__ y) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1;
+        spmv_row<TM, TV>(P, A, x, s, a0, a1);
+        typename V2T<TV>::type o;
+        o.x = (TV)a0; o.y = (TV)a1;
+        y[s] = o;
+    }
+}
+
+// ---- BiCGStab kernels ------------------------------------------------------------------------
+
+__device__ __forceinline__ void criterion_check(BiState* st) {
+    // CombinedCriterion::converged / failed
+    double red = st->resErr / fmax(1e-20, st->initResErr);
+    bool conv = red <= st->relTol || st->resErr <= st->absTol;
+    if (conv) { st->status = ST_CONVERGED; return; }
+    if (st->stagnates || st->resErr > st->maxRes) st->status = ST_FAILED;
+}
+
+// top of a BiCGStab iteration: shadow restart, breakdown test, beta, rho
+__device__ __forceinline__ void iteration_top(BiState* st, double rho_i, double rr) {
+    const double breakdownEps = DBL_MIN * 1e10;
+    if (st->iter >= st->maxIter) { st->status = ST_MAXITER; return; }
+    if (st->restartOnBreakdown && fabs(rho_i) <= 1e-12 * sqrt(st->r0r0) * sqrt(rr)) {
+        st->restartPending = 1;
+        st->r0r0 = rr;
+        rho_i = rr;
+        st->rho = 1.0; st->alpha = 1.0; st->omega = 1.0;
+        st->restarts += 1;
+    }
+    if (fabs(st->rho) <= breakdownEps || fabs(st->omega) <= breakdownEps) { st->status = ST_BREAKDOWN; return; }
+    st->beta = (rho_i / st->rho) * (st->alpha / st->omega);
+    st->rho = rho_i;
+    st->rho_i = rho_i;
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_init(const __grid_constant__ Phys P,
+                                                          const typename V2T<TV>::type* __restrict__ b,
+                                                          typename V2T<TV>::type* __restrict__ x,
+                                                          typename V2T<TV>::type* __restrict__ r,
+                                                          typename V2T<TV>::type* __restrict__ r0,
+                                                          typename V2T<TV>::type* __restrict__ v,
+                                                          typename V2T<TV>::type* __restrict__ p,
+                                                          BiState* st, double* partials, unsigned* counter) {
+    double red[2] = {0.0, 0.0};  // sum b.b, max |b|
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        auto bs = b[s];
+        typename V2T<TV>::type z;
+        z.x = (TV)0; z.y = (TV)0;
+        x[s] = z; v[s] = z; p[s] = z;
+        r[s] = bs; r0[s] = bs;
+        const double b0 = (double)bs.x, b1 = (double)bs.y;
+        red[0] += b0 * b0 + b1 * b1;
+        red[1] = fmax(red[1], fmax(absn(b0), absn(b1)));
+    }
+    double out[2];
+    if (grid_reduce<1, 1>(red, partials, counter, out) && threadIdx.x == 0) {
+        // CombinedCriterion::setInitial
+        st->resErr = fmax(out[1], DBL_MIN * 1e10);
+        st->initResErr = st->resErr;
+        st->lastResErr = st->resErr;
+        st->stagnates = 0;
+        st->iter = 0;
+        st->restarts = 0;
+        st->restartPending = 0;
+        st->rho = 1.0; st->alpha = 1.0; st->omega = 1.0;
+        st->r0r0 = out[0];
+        st->status = ST_RUNNING;
+        double rel = st->resErr / fmax(1e-20, st->initResErr);
+        if (rel <= st->relTol || st->resErr <= st->absTol) { st->status = ST_CONVERGED; return; }
+        iteration_top(st, out[0], out[0]);
+    }
+}
+
+// p = r + (-beta) (omega v - p); on a restart r0hat = r, v = p = 0 first
+template <typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_p(const __grid_constant__ Phys P,
+                                                       const typename V2T<TV>::type* __restrict__ r,
+                                                       typename V2T<TV>::type* __restrict__ r0,
+                                                       typename V2T<TV>::type* __restrict__ v,
+                                                       typename V2T<TV>::type* __restrict__ p,
+                                                       const BiState* __restrict__ st) {
+    if (st->status != ST_RUNNING) return;
+    const bool restart = st->restartPending != 0;
+    const double beta = st->beta, omega = st->omega;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        auto rs = r[s];
+        typename V2T<TV>::type vs = v[s], ps = p[s];
+        if (restart) {
+            r0[s] = rs;
+            vs.x = (TV)0; vs.y = (TV)0;
+            ps = vs;
+            v[s] = vs;
+        }
+        double t0 = (double)vs.x * omega, t1 = (double)vs.y * omega;
+        t0 -= (double)ps.x; t1 -= (double)ps.y;
+        t0 *= -beta; t1 *= -beta;
+        typename V2T<TV>::type o;
+        o.x = (TV)((double)rs.x + t0);
+        o.y = (TV)((double)rs.y + t1);
+        p[s] = o;
+    }
+}
+
+// v = A y; alpha = rho_i / (r0hat . v)
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_alpha(const __grid_constant__ Phys P, const TM* __restrict__ A,
+                                                                const typename V2T<TV>::type* __restrict__ y,
+                                                                const typename V2T<TV>::type* __restrict__ r0,
+                                                                typename V2T<TV>::type* __restrict__ v,
+                                                                BiState* st, double* partials, unsigned* counter) {
+    if (st->status != ST_RUNNING) return;
+    double red[1] = {0.0};
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1;
+        spmv_row<TM, TV>(P, A, y, s, a0, a1);
+        typename V2T<TV>::type o;
+        o.x = (TV)a0; o.y = (TV)a1;
+        v[s] = o;
+        auto rh = r0[s];
+        red[0] += (double)rh.x * (double)o.x + (double)rh.y * (double)o.y;
+    }
+    double out[1];
+    if (grid_reduce<1, 0>(red, partials, counter, out) && threadIdx.x == 0) {
+        const double breakdownEps = DBL_MIN * 1e10;
+        st->restartPending = 0;
+        double denom = out[0];
+        if (fabs(denom) <= breakdownEps) { st->status = ST_BREAKDOWN; return; }
+        st->alpha = st->rho_i / denom;
+        if (fabs(st->alpha) <= breakdownEps) st->status = ST_BREAKDOWN;
+    }
+}
+
+// h = x + alpha y (in x), s = r - alpha v (in r); criterion on s with y as change indicator
+template <typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_hs(const __grid_constant__ Phys P,
+                                                        typename V2T<TV>::type* __restrict__ x,
+                                                        const typename V2T<TV>::type* __restrict__ y,
+                                                        typename V2T<TV>::type* __restrict__ r,
+                                                        const typename V2T<TV>::type* __restrict__ v,
+                                                        BiState* st, double* partials, unsigned* counter) {
+    if (st->status != ST_RUNNING) return;
+    const double alpha = st->alpha;
+    double red[2] = {0.0, 0.0};  // max |s|, any y != 0
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        auto ys = y[s], xs = x[s], rs = r[s], vs = v[s];
+        typename V2T<TV>::type hx, sx;
+        hx.x = (TV)((double)ys.x * alpha + (double)xs.x);
+        hx.y = (TV)((double)ys.y * alpha + (double)xs.y);
+        sx.x = (TV)((double)rs.x - (double)vs.x * alpha);
+        sx.y = (TV)((double)rs.y - (double)vs.y * alpha);
+        x[s] = hx;
+        r[s] = sx;
+        red[0] = fmax(red[0], fmax(absn((double)sx.x), absn((double)sx.y)));
+        if (ys.x != (TV)0 || ys.y != (TV)0) red[1] = 1.0;
+    }
+    double out[2];
+    if (grid_reduce<0, 2>(red, partials, counter, out) && threadIdx.x == 0) {
+        st->lastResErr = st->resErr;
+        st->resErr = out[0];
+        st->stagnates = out[1] == 0.0;
+        criterion_check(st);
+    }
+}
+
+// t = A z; omega = (t . s) / (t . t)
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_omega(const __grid_constant__ Phys P, const TM* __restrict__ A,
+                                                                const typename V2T<TV>::type* __restrict__ z,
+                                                                const typename V2T<TV>::type* __restrict__ sres,
+                                                                typename V2T<TV>::type* __restrict__ t,
+                                                                BiState* st, double* partials, unsigned* counter) {
+    if (st->status != ST_RUNNING) return;
+    double red[2] = {0.0, 0.0};
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1;
+        spmv_row<TM, TV>(P, A, z, s, a0, a1);
+        typename V2T<TV>::type o;
+        o.x = (TV)a0; o.y = (TV)a1;
+        t[s] = o;
+        auto ss = sres[s];
+        const double t0 = (double)o.x, t1 = (double)o.y;
+        red[0] += t0 * t0 + t1 * t1;
+        red[1] += t0 * (double)ss.x + t1 * (double)ss.y;
+    }
+    double out[2];
+    if (grid_reduce<2, 0>(red, partials, counter, out) && threadIdx.x == 0) {
+        const double breakdownEps = DBL_MIN * 1e10;
+        if (fabs(out[0]) <= breakdownEps) { st->status = ST_BREAKDOWN; return; }
+        st->omega = out[1] / out[0];
+        if (fabs(st->omega) <= breakdownEps) st->status = ST_BREAKDOWN;
+    }
+}
+
+// x += omega z; criterion on r (still s) with z as change indicator; r += -omega t;
+// then the next iteration's r0hat . r and r . r
+template <typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_xr(const __grid_constant__ Phys P,
+                                                        typename V2T<TV>::type* __restrict__ x,
+                                                        const typename V2T<TV>::type* __restrict__ z,
+                                                        typename V2T<TV>::type* __restrict__ r,
+                                                        const typename V2T<TV>::type* __restrict__ t,
+                                                        const typename V2T<TV>::type* __restrict__ r0,
+                                                        BiState* st, double* partials, unsigned* counter) {
+    if (st->status != ST_RUNNING) return;
+    const double omega = st->omega;
+    double red[4] = {0.0, 0.0, 0.0, 0.0};  // sum r0.r', sum r'.r', max |s|, any z != 0
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        auto xs = x[s], zs = z[s], rs = r[s], ts = t[s], rh = r0[s];
+        typename V2T<TV>::type xn, rn;
+        xn.x = (TV)((double)xs.x + omega * (double)zs.x);
+        xn.y = (TV)((double)xs.y + omega * (double)zs.y);
+        x[s] = xn;
+        red[2] = fmax(red[2], fmax(absn((double)rs.x), absn((double)rs.y)));
+        if (zs.x != (TV)0 || zs.y != (TV)0) red[3] = 1.0;
+        rn.x = (TV)((double)rs.x + (-omega) * (double)ts.x);
+        rn.y = (TV)((double)rs.y + (-omega) * (double)ts.y);
+        r[s] = rn;
+        const double r0v = (double)rn.x, r1v = (double)rn.y;
+        red[0] += (double)rh.x * r0v + (double)rh.y * r1v;
+        red[1] += r0v * r0v + r1v * r1v;
+    }
+    double out[4];
+    if (grid_reduce<2, 2>(red, partials, counter, out) && threadIdx.x == 0) {
+        st->lastResErr = st->resErr;
+        st->resErr = out[2];
+        st->stagnates = out[3] == 0.0;
+        criterion_check(st);
+        if (st->status != ST_RUNNING) return;
+        st->iter += 1;
+        iteration_top(st, out[0], out[1]);
+    }
+}
+
+// ---- mixed precision: defect correction ----------------------------------------------------
+
+__global__ void k_to_float(const __grid_constant__ Phys P, const double2* __restrict__ a, float2* __restrict__ b) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = a[s];
+        b[s] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+// x64 += dx32; r64 = b - A32 x64 (FP64 arithmetic); max |r64| into *maxOut (ordered bits)
+__global__ void k_defect_accumulate(const __grid_constant__ Phys P, double2* __restrict__ x64, const float2* __restrict__ dx32) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        float2 d = dx32[s];
+        double2 x = x64[s];
+        x.x += (double)d.x;
+        x.y += (double)d.y;
+        x64[s] = x;
+    }
+}
+
+__global__ void __launch_bounds__(kSolBlock) k_defect_residual(const __grid_constant__ Phys P, const float* __restrict__ A,
+                                                                const double2* __restrict__ b,
+                                                                const double2* __restrict__ x64,
+                                                                double2* __restrict__ r64, double* partials,
+                                                                unsigned* counter, double* maxOut) {
+    double red[1] = {0.0};
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1;
+        spmv_row<float, double>(P, A, x64, s, a0, a1);
+        double2 bs = b[s];
+        double2 o = make_double2(bs.x - a0, bs.y - a1);
+        r64[s] = o;
+        red[0] = fmax(red[0], fmax(absn(o.x), absn(o.y)));
+    }
+    double out[1];
+    if (grid_reduce<0, 1>(red, partials, counter, out) && threadIdx.x == 0) *maxOut = out[0];
+}
+
+// ---- Newton update --------------------------------------------------------------------------
+
+__global__ void k_newton_update(const __grid_constant__ Phys P, double2* __restrict__ x, const double2* __restrict__ dx, int* bad) {
+    int b = 0;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double2 d = dx[s];
+        if (!isfinite(d.x) || !isfinite(d.y)) b = 1;
+        double2 v = x[s];
+        v.x -= d.x;
+        v.y -= d.y;
+        x[s] = v;
+    }
+    if (b) atomicOr(bad, 1);
+}
+
+// ---- host side ------------------------------------------------------------------------------
+
+// Workspace for one precision: Krylov vectors, ILU factors, reduction scratch.
+template <typename T>
+struct KrylovWs {
+    using V = typename V2T<T>::type;
+    V *x = nullptr, *r = nullptr, *r0 = nullptr, *v = nullptr, *p = nullptr, *y = nullptr, *z = nullptr, *b = nullptr;
+    T* Dinv = nullptr;   // 4 planes x N
+    T* L = nullptr;      // (2*dim*4) planes x Nh (black rows)
+};
+
+struct SolverWs {
+    KrylovWs<double> d;
+    KrylovWs<float> f;
+    double2* x64 = nullptr;   // mixed: accumulated solution
+    double2* r64 = nullptr;   // mixed: FP64 defect
+    double* partials = nullptr;
+    unsigned* counter = nullptr;
+    BiState* st = nullptr;
+    int* flags = nullptr;     // [0] singular block
+    double* dmax = nullptr;
+    BiState* h_st = nullptr;  // pinned mirror
+    int gridRed = 0;
+    bool haveF = false;
+};
+
+template <typename T>
+static cudaError_t alloc_ws(KrylovWs<T>& w, const Phys& P) {
+    using V = typename V2T<T>::type;
+    cudaError_t e;
+    V** vs[] = {&w.x, &w.r, &w.r0, &w.v, &w.p, &w.y, &w.z, &w.b};
+    for (V** q : vs)
+        if ((e = cudaMalloc(q, sizeof(V) * P.N)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.Dinv, sizeof(T) * 4 * P.N)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.L, sizeof(T) * 4 * 2 * P.dim * P.Nh)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+template <typename T>
+static void free_ws(KrylovWs<T>& w) {
+    void* ps[] = {w.x, w.r, w.r0, w.v, w.p, w.y, w.z, w.b, w.Dinv, w.L};
+    for (void* q : ps) if (q) cudaFree(q);
+    w = KrylovWs<T>();
+}
+
+static SolverWs* ws_of(ewg_ctx* ctx) { return (SolverWs*)ctx->sv; }
+
+static ewg_status ensure_ws(ewg_ctx* ctx, bool needFloat) {
+    cudaError_t e;
+    if (!ctx->sv) {
+        SolverWs* w = new SolverWs();
+        ctx->sv = w;
+        if ((e = alloc_ws(w->d, ctx->P)) != cudaSuccess) return cuda_fail(ctx, e, "alloc solver vectors");
+        w->gridRed = ctx->numSMs * 4;
+        if ((e = cudaMalloc(&w->partials, sizeof(double) * kMaxRed * w->gridRed * 2)) != cudaSuccess) return cuda_fail(ctx, e, "alloc partials");
+        if ((e = cudaMalloc(&w->counter, sizeof(unsigned) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc counter");
+        if ((e = cudaMemset(w->counter, 0, sizeof(unsigned) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "memset counter");
+        if ((e = cudaMalloc(&w->st, sizeof(BiState))) != cudaSuccess) return cuda_fail(ctx, e, "alloc state");
+        if ((e = cudaMalloc(&w->flags, sizeof(int) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc flags");
+        if ((e = cudaMalloc(&w->dmax, sizeof(double) * 2)) != cudaSuccess) return cuda_fail(ctx, e, "alloc dmax");
+        if ((e = cudaMallocHost(&w->h_st, sizeof(BiState))) != cudaSuccess) return cuda_fail(ctx, e, "alloc pinned state");
+    }
+    SolverWs* w = ws_of(ctx);
+    if (needFloat && !w->haveF) {
+        if ((e = alloc_ws(w->f, ctx->P)) != cudaSuccess) return cuda_fail(ctx, e, "alloc fp32 solver vectors");
+        if ((e = cudaMalloc(&w->x64, sizeof(double2) * ctx->P.N)) != cudaSuccess) return cuda_fail(ctx, e, "alloc x64");
+        if ((e = cudaMalloc(&w->r64, sizeof(double2) * ctx->P.N)) != cudaSuccess) return cuda_fail(ctx, e, "alloc r64");
+        w->haveF = true;
+    }
+    return EWG_OK;
+}
+
+void solver_free(ewg_ctx* ctx) {
+    SolverWs* w = ws_of(ctx);
+    if (!w) return;
+    free_ws(w->d);
+    free_ws(w->f);
+    void* ps[] = {w->x64, w->r64, w->partials, w->counter, w->st, w->flags, w->dmax};
+    for (void* q : ps) if (q) cudaFree(q);
+    if (w->h_st) cudaFreeHost(w->h_st);
+    delete w;
+    ctx->sv = nullptr;
+}
+
+template <typename T>
+static const T* jac_of(ewg_ctx* ctx);
+template <> const double* jac_of<double>(ewg_ctx* ctx) { return ctx->J; }
+template <> const float* jac_of<float>(ewg_ctx* ctx) { return ctx->J32; }
+
+template <typename T>
+static ewg_status setup_precond(ewg_ctx* ctx, KrylovWs<T>& w, int kind) {
+    const Phys& P = ctx->P;
+    SolverWs* sw = ws_of(ctx);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(sw->flags, 0, sizeof(int), ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "memset flags");
+    const T* A = jac_of<T>(ctx);
+    if (kind == EWG_PRECOND_JACOBI) {
+        int g = grid_size_for(ctx, (const void*)k_diag_inverse<T>, kSolBlock);
+        EWG_LAUNCH(ctx, K_DIAG_INVERSE, k_diag_inverse<T>, g, kSolBlock, P, A, w.Dinv, P.N, sw->flags);
+    } else {
+        int g = grid_size_for(ctx, (const void*)k_diag_inverse<T>, kSolBlock);
+        EWG_LAUNCH(ctx, K_DIAG_INVERSE, k_diag_inverse<T>, g, kSolBlock, P, A, w.Dinv, P.Nh, sw->flags);
+        int g2 = grid_size_for(ctx, (const void*)k_ilu_black_factor<T>, kSolBlock);
+        EWG_LAUNCH(ctx, K_ILU_BLACK_FACTOR, k_ilu_black_factor<T>, g2, kSolBlock, P, A, w.Dinv, w.L, sw->flags);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "preconditioner setup");
+    int bad = 0;
+    if ((e = cudaMemcpyAsync(&bad, sw->flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "read flags");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync precond");
+    if (bad) {
+        ctx->err = "preconditioner: singular 2x2 diagonal block";
+        return EWG_ERR_BREAKDOWN;
+    }
+    return EWG_OK;
+}
+
+template <typename T>
+static void launch_precond(ewg_ctx* ctx, KrylovWs<T>& w, int kind, double relax,
+                           const typename V2T<T>::type* d, typename V2T<T>::type* y, const int* status) {
+    const Phys& P = ctx->P;
+    const T* A = jac_of<T>(ctx);
+    if (kind == EWG_PRECOND_JACOBI) {
+        int g = grid_size_for(ctx, (const void*)k_jacobi_apply<T, T>, kSolBlock);
+        {
+            auto kfn = k_jacobi_apply<T, T>;
+            EWG_LAUNCH(ctx, K_JACOBI_APPLY, kfn, g, kSolBlock, P, w.Dinv, d, y, status, relax);
+        }
+    } else {
+        int g = grid_size_for(ctx, (const void*)k_ilu_black_apply<T, T>, kSolBlock);
+        {
+            auto kfn = k_ilu_black_apply<T, T>;
+            EWG_LAUNCH(ctx, K_ILU_BLACK_APPLY, kfn, g, kSolBlock, P, w.Dinv, w.L, d, y, status, relax);
+        }
+        int g2 = grid_size_for(ctx, (const void*)k_ilu_red_apply<T, T>, kSolBlock);
+        {
+            auto kfn = k_ilu_red_apply<T, T>;
+            EWG_LAUNCH(ctx, K_ILU_RED_APPLY, kfn, g2, kSolBlock, P, A, w.Dinv, d, y, status, relax);
+        }
+    }
+}
+
+// One BiCGStab solve of A x = b for the precision T; b must already be in w.b.
+template <typename T>
+static ewg_status bicgstab(ewg_ctx* ctx, KrylovWs<T>& w, const ewg_solve_opts* o, double relTol, double absTol,
+                           int maxIter, int* itersOut, int* restartsOut, double* resOut, int* statusOut,
+                           double* initOut = nullptr) {
+    const Phys& P = ctx->P;
+    SolverWs* sw = ws_of(ctx);
+    const T* A = jac_of<T>(ctx);
+    cudaError_t e;
+    BiState init;
+    memset(&init, 0, sizeof(init));
+    init.relTol = relTol;
+    init.absTol = absTol;
+    init.maxRes = o->linear_solver_max_error;
+    init.maxIter = maxIter;
+    init.restartOnBreakdown = o->restart_on_breakdown;
+    init.w = o->preconditioner_relaxation;
+    if ((e = cudaMemcpyAsync(sw->st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return cuda_fail(ctx, e, "upload state");
+    const int G = sw->gridRed;
+    double* part = sw->partials;
+    unsigned* cnt = sw->counter;
+    EWG_LAUNCH(ctx, K_BICG_INIT, k_bicg_init<T>, G, kSolBlock, P, w.b, w.x, w.r, w.r0, w.v, w.p, sw->st, part, cnt);
+    int interval = o->check_interval > 0 ? o->check_interval : (P.N >= (1 << 20) ? 1 : 8);
+    const int* status = &sw->st->status;
+    const double relax = o->preconditioner_relaxation;
+    int guard = 0;
+    for (;;) {
+        for (int k = 0; k < interval; ++k) {
+            EWG_LAUNCH(ctx, K_BICG_P, k_bicg_p<T>, G, kSolBlock, P, w.r, w.r0, w.v, w.p, sw->st);
+            launch_precond<T>(ctx, w, o->precond, relax, w.p, w.y, status);
+            {
+                auto kfn = k_bicg_spmv_alpha<T, T>;
+                EWG_LAUNCH(ctx, K_BICG_SPMV_ALPHA, kfn, G, kSolBlock, P, A, w.y, w.r0, w.v, sw->st, part, cnt);
+            }
+            EWG_LAUNCH(ctx, K_BICG_HS, k_bicg_hs<T>, G, kSolBlock, P, w.x, w.y, w.r, w.v, sw->st, part, cnt);
+            launch_precond<T>(ctx, w, o->precond, relax, w.r, w.z, status);
+            {
+                auto kfn = k_bicg_spmv_omega<T, T>;
+                EWG_LAUNCH(ctx, K_BICG_SPMV_OMEGA, kfn, G, kSolBlock, P, A, w.z, w.r, w.y, sw->st, part, cnt);
+            }
+            EWG_LAUNCH(ctx, K_BICG_XR, k_bicg_xr<T>, G, kSolBlock, P, w.x, w.z, w.r, w.y, w.r0, sw->st, part, cnt);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "bicgstab launch");
+        if ((e = cudaMemcpyAsync(sw->h_st, sw->st, sizeof(BiState), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+            return cuda_fail(ctx, e, "read state");
+        if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync bicgstab");
+        if (sw->h_st->status != ST_RUNNING) break;
+        if (++guard > maxIter + 2) { ctx->err = "bicgstab: status never left RUNNING"; return EWG_ERR_TIMEOUT; }
+    }
+    const BiState& hs = *sw->h_st;
+    *itersOut = hs.iter;
+    *restartsOut = hs.restarts;
+    *resOut = hs.resErr;
+    *statusOut = hs.status;
+    if (initOut) *initOut = hs.initResErr;
+    switch (hs.status) {
+        case ST_CONVERGED: return EWG_OK;
+        case ST_BREAKDOWN: ctx->err = "Breakdown of the BiCGStab solver"; return EWG_ERR_BREAKDOWN;
+        default: ctx->err = "BiCGStab did not converge"; return EWG_ERR_NOT_CONVERGED;
+    }
+}
+
+ewg_status solver_solve(ewg_ctx* ctx, const ewg_solve_opts* o, ewg_solve_report* rep) {
+    const Phys& P = ctx->P;
+    const bool mixed = o->precision == EWG_PRECISION_MIXED;
+    if (mixed != (ctx->jacPrecision == EWG_PRECISION_MIXED)) {
+        ctx->err = "solve precision does not match the precision of the stored Jacobian";
+        return EWG_ERR_INVALID;
+    }
+    ewg_status st = ensure_ws(ctx, mixed);
+    if (st) return st;
+    SolverWs* sw = ws_of(ctx);
+    cudaError_t e;
+    memset(rep, 0, sizeof(*rep));
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    int status = 0;
+    if (!mixed) {
+        if (!ctx->iluValid || ctx->iluKind != o->precond || ctx->iluPrecision != EWG_PRECISION_FP64) {
+            if ((st = setup_precond<double>(ctx, sw->d, o->precond))) return st;
+            ctx->iluValid = true; ctx->iluKind = o->precond; ctx->iluPrecision = EWG_PRECISION_FP64;
+        }
+        if ((e = cudaMemcpyAsync(sw->d.b, ctx->r, sizeof(double2) * P.N, cudaMemcpyDeviceToDevice, ctx->stream)) != cudaSuccess)
+            return cuda_fail(ctx, e, "copy rhs");
+        int it = 0, rs = 0;
+        double res = 0, ini = 0;
+        st = bicgstab<double>(ctx, sw->d, o, o->linear_solver_tolerance, o->linear_solver_abs_tolerance,
+                              o->linear_solver_max_iterations, &it, &rs, &res, &status, &ini);
+        if (st == EWG_ERR_CUDA || st == EWG_ERR_TIMEOUT) return st;
+        rep->iterations = it;
+        rep->restarts = rs;
+        rep->outer_iterations = 1;
+        rep->final_residual = res;
+        rep->initial_residual = ini;
+        if ((e = cudaMemcpyAsync(ctx->dx, sw->d.x, sizeof(double2) * P.N, cudaMemcpyDeviceToDevice, ctx->stream)) != cudaSuccess)
+            return cuda_fail(ctx, e, "copy dx");
+    } else {
+        if (!ctx->iluValid || ctx->iluKind != o->precond || ctx->iluPrecision != EWG_PRECISION_MIXED) {
+            if ((st = setup_precond<float>(ctx, sw->f, o->precond))) return st;
+            ctx->iluValid = true; ctx->iluKind = o->precond; ctx->iluPrecision = EWG_PRECISION_MIXED;
+        }
+        const int G = sw->gridRed;
+        int gs = grid_size_for(ctx, (const void*)k_to_float, kSolBlock);
+        // x64 = 0, r64 = b
+        if ((e = cudaMemsetAsync(sw->x64, 0, sizeof(double2) * P.N, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "zero x64");
+        if ((e = cudaMemcpyAsync(sw->r64, ctx->r, sizeof(double2) * P.N, cudaMemcpyDeviceToDevice, ctx->stream)) != cudaSuccess)
+            return cuda_fail(ctx, e, "copy r64");
+        // initial max |b|
+        EWG_LAUNCH(ctx, K_DEFECT_RESIDUAL, k_defect_residual, G, kSolBlock, P, ctx->J32, ctx->r, sw->x64, sw->r64, sw->partials, sw->counter, sw->dmax);
+        double bmax = 0;
+        if ((e = cudaMemcpyAsync(&bmax, sw->dmax, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "read bmax");
+        if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync");
+        rep->initial_residual = bmax;
+        double init = fmax(bmax, DBL_MIN * 1e10);
+        double absTol = o->defect_tolerance > 0 ? o->defect_tolerance : o->linear_solver_abs_tolerance;
+        double res = bmax;
+        int totalIt = 0, totalRs = 0, outer = 0;
+        st = EWG_ERR_NOT_CONVERGED;
+        if (res / fmax(1e-20, init) <= o->linear_solver_tolerance || res <= absTol) st = EWG_OK;
+        while (st != EWG_OK && outer < o->max_defect_iterations) {
+            EWG_LAUNCH(ctx, K_TO_FLOAT, k_to_float, gs, kSolBlock, P, sw->r64, sw->f.b);
+            int it = 0, rs = 0, istat = 0;
+            double ires = 0;
+            ewg_status ist = bicgstab<float>(ctx, sw->f, o, o->inner_tolerance, 0.0,
+                                             o->linear_solver_max_iterations, &it, &rs, &ires, &istat);
+            if (ist == EWG_ERR_CUDA || ist == EWG_ERR_TIMEOUT) return ist;
+            totalIt += it;
+            totalRs += rs;
+            ++outer;
+            if (ist == EWG_ERR_BREAKDOWN && it == 0) { st = EWG_ERR_BREAKDOWN; break; }
+            EWG_LAUNCH(ctx, K_DEFECT_ACCUMULATE, k_defect_accumulate, gs, kSolBlock, P, sw->x64, sw->f.x);
+            EWG_LAUNCH(ctx, K_DEFECT_RESIDUAL, k_defect_residual, G, kSolBlock, P, ctx->J32, ctx->r, sw->x64, sw->r64, sw->partials, sw->counter, sw->dmax);
+            if ((e = cudaMemcpyAsync(&res, sw->dmax, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "read defect");
+            if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync defect");
+            if (!(res == res)) { st = EWG_ERR_NONFINITE; ctx->err = "non-finite defect"; break; }
+            if (res / fmax(1e-20, init) <= o->linear_solver_tolerance || res <= absTol) st = EWG_OK;
+        }
+        if (st == EWG_ERR_NOT_CONVERGED) ctx->err = "defect correction did not converge";
+        rep->iterations = totalIt;
+        rep->restarts = totalRs;
+        rep->outer_iterations = outer;
+        rep->final_residual = res;
+        if ((e = cudaMemcpyAsync(ctx->dx, sw->x64, sizeof(double2) * P.N, cudaMemcpyDeviceToDevice, ctx->stream)) != cudaSuccess)
+            return cuda_fail(ctx, e, "copy dx");
+        status = st == EWG_OK ? ST_CONVERGED : ST_FAILED;
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    if ((e = cudaEventSynchronize(ctx->ev1)) != cudaSuccess) return cuda_fail(ctx, e, "sync solve");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    rep->seconds = ms * 1e-3;
+    rep->converged = status == ST_CONVERGED;
+    rep->status = status == ST_CONVERGED ? EWG_OK : (status == ST_BREAKDOWN ? EWG_ERR_BREAKDOWN : EWG_ERR_NOT_CONVERGED);
+    return (ewg_status)rep->status;
+}
+
+ewg_status solver_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* o, const double2* b, double2* y) {
+    if (o->precision != EWG_PRECISION_FP64 || ctx->jacPrecision != EWG_PRECISION_FP64) {
+        ctx->err = "apply_preconditioner is available for the FP64 Jacobian";
+        return EWG_ERR_INVALID;
+    }
+    ewg_status st = ensure_ws(ctx, false);
+    if (st) return st;
+    SolverWs* sw = ws_of(ctx);
+    if (!ctx->iluValid || ctx->iluKind != o->precond || ctx->iluPrecision != EWG_PRECISION_FP64) {
+        if ((st = setup_precond<double>(ctx, sw->d, o->precond))) return st;
+        ctx->iluValid = true; ctx->iluKind = o->precond; ctx->iluPrecision = EWG_PRECISION_FP64;
+    }
+    launch_precond<double>(ctx, sw->d, o->precond, o->preconditioner_relaxation, b, y, nullptr);
+    return cuda_fail(ctx, cudaGetLastError(), "apply preconditioner");
+}
+
+ewg_status solver_spmv(ewg_ctx* ctx, const double2* x, double2* y) {
+    int g = grid_size_for(ctx, (const void*)k_spmv<double, double>, kSolBlock);
+    {
+        auto kfn = k_spmv<double, double>;
+        EWG_LAUNCH(ctx, K_SPMV, kfn, g, kSolBlock, ctx->P, ctx->J, x, y);
+    }
+    return cuda_fail(ctx, cudaGetLastError(), "spmv");
+}
+
+ewg_status solver_newton_update(ewg_ctx* ctx, int* nonfinite) {
+    ewg_status st = ensure_ws(ctx, false);
+    if (st) return st;
+    SolverWs* sw = ws_of(ctx);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(sw->flags + 1, 0, sizeof(int), ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "memset");
+    int g = grid_size_for(ctx, (const void*)k_newton_update, kSolBlock);
+    EWG_LAUNCH(ctx, K_NEWTON_UPDATE, k_newton_update, g, kSolBlock, ctx->P, ctx->x0, ctx->dx, sw->flags + 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "newton update");
+    int bad = 0;
+    if ((e = cudaMemcpyAsync(&bad, sw->flags + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "read");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync update");
+    *nonfinite = bad;
+    return EWG_OK;
+}
+
+}  // namespace ewg

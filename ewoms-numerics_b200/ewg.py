@@ -1,0 +1,503 @@
+"""ctypes plumbing for the C ABI in include/ewg.h (libewg.so) and the lens-problem presets.
+
+The product is the CUDA library; this module only declares the ABI structs, loads the in-tree
+``libewg.so`` and builds problem definitions (grid, material regions, permeability fields) on the
+host. There is no CPU fallback: ``load()`` raises if the library is missing and ``Context``
+raises if no sm_100 device is usable.
+
+Problem presets follow ``tests/problems/lensproblem.hh``:
+  * ``reference``  -- the reference's own parameters (lensproblem.hh:248-288, 464-533)
+  * ``baseline``   -- the graded 2D parameter set (48x32, K 9.05e-12 / 9.05e-13, VG alpha
+                      3.7e-4 / 4.5e-4, inlet x in (2.25, 3.75), hydrostatic left and right)
+  * ``lens3d``     -- the 3D extrusion (256x256x128 at full size, any even nx) with a seeded
+                      log-normal permeability field
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libewg.so")
+
+EWG_OK = 0
+STATUS_NAMES = {0: "EWG_OK", 1: "EWG_ERR_INVALID", 2: "EWG_ERR_CUDA", 3: "EWG_ERR_NONFINITE",
+                4: "EWG_ERR_BREAKDOWN", 5: "EWG_ERR_NOT_CONVERGED", 6: "EWG_ERR_TIMEOUT",
+                7: "EWG_ERR_NO_DEVICE", 8: "EWG_ERR_MAX_ERROR"}
+
+LAW_VG, LAW_BC = 0, 1
+PRECOND_ILU0, PRECOND_JACOBI = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class Grid(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double)]
+
+    @property
+    def n_cells(self) -> int:
+        return self.nx * self.ny * (self.nz if self.dim == 3 else 1)
+
+    @property
+    def shape(self):
+        """numpy shape of a natural-order cell field (x fastest): (nz, ny, nx)."""
+        return (self.nz if self.dim == 3 else 1, self.ny, self.nx)
+
+
+class Material(C.Structure):
+    _fields_ = [("law", C.c_int32), ("swr", C.c_double), ("snr", C.c_double),
+                ("vg_alpha", C.c_double), ("vg_n", C.c_double),
+                ("bc_entry_pressure", C.c_double), ("bc_lambda", C.c_double)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("lens_lo", C.c_double * 3), ("lens_hi", C.c_double * 3), ("eps", C.c_double),
+                ("porosity", C.c_double), ("temperature", C.c_double),
+                ("rho_w", C.c_double), ("mu_w", C.c_double), ("rho_n", C.c_double),
+                ("mu_n", C.c_double), ("gravity", C.c_double), ("p_ref", C.c_double),
+                ("left_pressure_scale", C.c_double),
+                ("inlet_x_lo", C.c_double), ("inlet_x_hi", C.c_double),
+                ("inlet_z_lo", C.c_double), ("inlet_z_hi", C.c_double),
+                ("inlet_rate", C.c_double), ("outer", Material), ("lens", Material)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precond", C.c_int32), ("precision", C.c_int32),
+                ("linear_solver_tolerance", C.c_double),
+                ("linear_solver_abs_tolerance", C.c_double),
+                ("linear_solver_max_error", C.c_double),
+                ("linear_solver_max_iterations", C.c_int32),
+                ("preconditioner_relaxation", C.c_double),
+                ("defect_tolerance", C.c_double), ("inner_tolerance", C.c_double),
+                ("max_defect_iterations", C.c_int32), ("check_interval", C.c_int32),
+                ("restart_on_breakdown", C.c_int32)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("restarts", C.c_int32), ("iterations", C.c_int32),
+                ("outer_iterations", C.c_int32), ("status", C.c_int32),
+                ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("seconds", C.c_double)]
+
+
+class LinReport(C.Structure):
+    _fields_ = [("error", C.c_double), ("nonfinite", C.c_int32), ("seconds", C.c_double)]
+
+
+class NewtonOpts(C.Structure):
+    _fields_ = [("newton_tolerance", C.c_double), ("newton_max_error", C.c_double),
+                ("newton_max_iterations", C.c_int32), ("newton_target_iterations", C.c_int32),
+                ("verbose", C.c_int32)]
+
+
+class NewtonReport(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32),
+                ("linear_iterations", C.c_int32), ("status", C.c_int32), ("error", C.c_double),
+                ("t_linearize", C.c_double), ("t_solve", C.c_double), ("t_update", C.c_double)]
+
+
+def default_solve_opts(**kw) -> SolveOpts:
+    """Reference defaults (fvbasediscretization.hh:249-252, parallelbicgstabbackend.hh:48,
+    parallelbasebackend.hh:514) with the graded linear tolerance 1e-10 unless overridden."""
+    o = SolveOpts(precond=PRECOND_ILU0, precision=PRECISION_FP64,
+                  linear_solver_tolerance=1e-10, linear_solver_abs_tolerance=1e-10,
+                  linear_solver_max_error=1e7, linear_solver_max_iterations=1000,
+                  preconditioner_relaxation=1.0, defect_tolerance=0.0, inner_tolerance=1e-4,
+                  max_defect_iterations=50, check_interval=0, restart_on_breakdown=1)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def default_newton_opts(**kw) -> NewtonOpts:
+    """NewtonTolerance 1e-8, NewtonMaxError 1e100, max 18, target 10 (newtonmethod.hh:150-155)."""
+    o = NewtonOpts(newton_tolerance=1e-8, newton_max_error=1e100, newton_max_iterations=18,
+                   newton_target_iterations=10, verbose=0)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+# ------------------------------------------------------------------------------------------
+# problem presets
+
+
+def _vg(swr, snr, alpha, n) -> Material:
+    return Material(law=LAW_VG, swr=swr, snr=snr, vg_alpha=alpha, vg_n=n,
+                    bc_entry_pressure=0.0, bc_lambda=0.0)
+
+
+def _bc(swr, snr, pe, lam) -> Material:
+    return Material(law=LAW_BC, swr=swr, snr=snr, vg_alpha=0.0, vg_n=0.0,
+                    bc_entry_pressure=pe, bc_lambda=lam)
+
+
+@dataclass
+class LensCase:
+    """A complete lens-problem definition: grid, problem constants and permeability field."""
+    name: str
+    grid: Grid
+    problem: Problem
+    perm: np.ndarray          # natural order, float64, N
+    dt: float = 250.0
+    n_steps: int = 10
+
+    @property
+    def n_cells(self) -> int:
+        return self.grid.n_cells
+
+
+def cell_centers(grid: Grid):
+    """Cell centres (x, y, z) as natural-order flat arrays: (i + 0.5) * h per axis."""
+    nz = grid.nz if grid.dim == 3 else 1
+    hx, hy = grid.lx / grid.nx, grid.ly / grid.ny
+    hz = grid.lz / nz if grid.dim == 3 else 0.0
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(grid.ny), np.arange(grid.nx), indexing="ij")
+    x = (i + 0.5) * hx
+    y = (j + 0.5) * hy
+    z = (k + 0.5) * hz if grid.dim == 3 else np.zeros_like(x, dtype=float)
+    return x.ravel(), y.ravel(), z.ravel()
+
+
+def in_lens(grid: Grid, problem: Problem) -> np.ndarray:
+    """isInLens_ (lensproblem.hh:596-604) at the cell centres."""
+    x, y, z = cell_centers(grid)
+    pos = [x, y, z]
+    m = np.ones(grid.n_cells, dtype=bool)
+    for a in range(grid.dim):
+        m &= (pos[a] >= problem.lens_lo[a] - problem.eps) & (pos[a] <= problem.lens_hi[a] + problem.eps)
+    return m
+
+
+def _base_problem() -> Problem:
+    p = Problem()
+    p.eps = 3e-6
+    p.porosity = 0.4
+    p.temperature = 293.15
+    p.rho_w, p.mu_w = 1000.0, 1e-3      # SimpleH2O as a liquid
+    p.rho_n, p.mu_n = 1460.0, 5.7e-4    # DNAPL (TCE)
+    p.gravity = 9.81
+    p.p_ref = 1e5
+    p.inlet_rate = -0.04
+    p.inlet_z_lo, p.inlet_z_hi = -1e30, 1e30
+    return p
+
+
+def reference_case(nx=48, ny=32) -> LensCase:
+    """The reference's lensproblem.hh parameters in 2D (6 m x 4 m)."""
+    g = Grid(dim=2, nx=nx, ny=ny, nz=1, lx=6.0, ly=4.0, lz=1.0)
+    p = _base_problem()
+    p.lens_lo[:] = [1.0, 2.0, 0.0]
+    p.lens_hi[:] = [4.0, 3.0, 1.0]
+    p.outer = _vg(0.05, 0.0, 0.0037, 4.7)
+    p.lens = _vg(0.18, 0.0, 0.00045, 7.3)
+    p.left_pressure_scale = 1.0 + 1.5 / 4.0
+    p.inlet_x_lo, p.inlet_x_hi = 2.0, 3.0     # 0.5 < (xmax - x)/width < 2/3
+    lens = in_lens(g, p)
+    perm = np.where(lens, 9.05e-12, 4.6e-10).astype(np.float64)
+    return LensCase("reference", g, p, perm)
+
+
+def baseline_case(nx=48, ny=32) -> LensCase:
+    """The graded 2D lens preset (Dirichlet-like hydrostatic free flow on left and right)."""
+    g = Grid(dim=2, nx=nx, ny=ny, nz=1, lx=6.0, ly=4.0, lz=1.0)
+    p = _base_problem()
+    p.lens_lo[:] = [1.0, 2.0, 0.0]
+    p.lens_hi[:] = [4.0, 3.0, 1.0]
+    p.outer = _vg(0.05, 0.0, 3.7e-4, 4.7)
+    p.lens = _vg(0.18, 0.0, 4.5e-4, 7.3)
+    p.left_pressure_scale = 1.0
+    p.inlet_x_lo, p.inlet_x_hi = 2.25, 3.75
+    lens = in_lens(g, p)
+    perm = np.where(lens, 9.05e-13, 9.05e-12).astype(np.float64)
+    return LensCase("baseline", g, p, perm)
+
+
+def brooks_corey_case(nx=48, ny=32) -> LensCase:
+    """The baseline geometry with EffToAbsLaw<RegularizedBrooksCorey> (entry pressure 500 Pa,
+    lambda 2 as in tutorial/tutorial1problem.hh:182-183; lens entry pressure 1500 Pa)."""
+    c = baseline_case(nx, ny)
+    c.problem.outer = _bc(0.05, 0.0, 500.0, 2.0)
+    c.problem.lens = _bc(0.18, 0.0, 1500.0, 2.0)
+    c.name = "brooks_corey"
+    return c
+
+
+def gaussian_log_field(shape, sigma=1.0, corr_cells=8.0, seed=0) -> np.ndarray:
+    """Seeded stationary Gaussian field with exponential covariance exp(-r / corr_cells), zero
+    mean and standard deviation sigma, by spectral synthesis on the periodic grid: white noise
+    filtered with the square root of the covariance's discrete spectrum, then rescaled so the
+    sample standard deviation is exactly sigma."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    axes = [np.fft.fftfreq(s) * s for s in shape]  # integer lags on the torus
+    grids = np.meshgrid(*[np.minimum(np.abs(a), s - np.abs(a)) for a, s in zip(axes, shape)],
+                        indexing="ij")
+    r = np.sqrt(sum(g.astype(np.float64) ** 2 for g in grids))
+    cov = np.exp(-r / corr_cells)
+    spec = np.fft.rfftn(cov).real
+    spec = np.maximum(spec, 0.0)
+    noise = rng.standard_normal(shape)
+    f = np.fft.irfftn(np.fft.rfftn(noise) * np.sqrt(spec), s=shape)
+    f -= f.mean()
+    f *= sigma / f.std()
+    return f
+
+
+def lens3d_case(nx=256, ny=256, nz=128, seed=0, sigma=1.0, corr_cells=8.0,
+                extents=(6.0, 4.0, 3.0)) -> LensCase:
+    """3D extrusion of the graded lens problem: centred lens box of 40 % of each extent, ln K a
+    seeded Gaussian field (mean ln 9.05e-12, exponential covariance), K x 0.1 in the lens,
+    DNAPL inlet on the top face over x in (2.25, 3.75) m and the middle 40 % in z."""
+    lx, ly, lz = extents
+    g = Grid(dim=3, nx=nx, ny=ny, nz=nz, lx=lx, ly=ly, lz=lz)
+    p = _base_problem()
+    p.lens_lo[:] = [0.3 * lx, 0.3 * ly, 0.3 * lz]
+    p.lens_hi[:] = [0.7 * lx, 0.7 * ly, 0.7 * lz]
+    p.outer = _vg(0.05, 0.0, 3.7e-4, 4.7)
+    p.lens = _vg(0.18, 0.0, 4.5e-4, 7.3)
+    p.left_pressure_scale = 1.0
+    p.inlet_x_lo, p.inlet_x_hi = 2.25 * lx / 6.0, 3.75 * lx / 6.0
+    p.inlet_z_lo, p.inlet_z_hi = 0.3 * lz, 0.7 * lz
+    f = gaussian_log_field((nz, ny, nx), sigma=sigma, corr_cells=corr_cells, seed=seed).ravel()
+    lnk = np.log(9.05e-12) + f
+    lens = in_lens(g, p)
+    lnk = np.where(lens, lnk + np.log(0.1), lnk)
+    return LensCase("lens3d", g, p, np.exp(lnk).astype(np.float64))
+
+
+# ------------------------------------------------------------------------------------------
+# library loading
+
+_lib = None
+
+
+def _ptr(a: np.ndarray, ctype=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def load(path: str = LIB_PATH):
+    """Load the in-tree libewg.so and declare its signatures. Raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libewg.so not built at {path}: run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    d = C.c_double
+    sig = {
+        "ewg_create": (C.c_int, [P(Grid), P(Problem), P(d), P(C.c_void_p)]),
+        "ewg_destroy": (None, [C.c_void_p]),
+        "ewg_last_error": (C.c_char_p, [C.c_void_p]),
+        "ewg_create_error": (C.c_char_p, []),
+        "ewg_num_cells": (C.c_int64, [C.c_void_p]),
+        "ewg_num_blocks": (C.c_int64, [C.c_void_p]),
+        "ewg_abi_version": (C.c_int32, []),
+        "ewg_set_solution": (C.c_int, [C.c_void_p, C.c_int32, P(d)]),
+        "ewg_get_solution": (C.c_int, [C.c_void_p, C.c_int32, P(d)]),
+        "ewg_apply_initial_solution": (C.c_int, [C.c_void_p]),
+        "ewg_advance_time_level": (C.c_int, [C.c_void_p]),
+        "ewg_restore_time_level": (C.c_int, [C.c_void_p]),
+        "ewg_linearize": (C.c_int, [C.c_void_p, d, P(LinReport)]),
+        "ewg_get_residual": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(d)]),
+        "ewg_residual_norm": (C.c_int, [C.c_void_p, P(d), d, P(d)]),
+        "ewg_set_matrix_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(d)]),
+        "ewg_set_residual": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_solve": (C.c_int, [C.c_void_p, P(SolveOpts), P(SolveReport)]),
+        "ewg_get_update": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_apply_preconditioner": (C.c_int, [C.c_void_p, P(SolveOpts), P(d), P(d)]),
+        "ewg_apply_jacobian": (C.c_int, [C.c_void_p, P(d), P(d)]),
+        "ewg_newton_update": (C.c_int, [C.c_void_p]),
+        "ewg_newton_apply": (C.c_int, [C.c_void_p, d, P(NewtonOpts), P(SolveOpts), P(NewtonReport)]),
+        "ewg_default_solve_opts": (None, [P(SolveOpts)]),
+        "ewg_default_newton_opts": (None, [P(NewtonOpts)]),
+        "ewg_get_stream": (C.c_void_p, [C.c_void_p]),
+        "ewg_profile_num_kernels": (C.c_int32, []),
+        "ewg_profile_kernel_name": (C.c_char_p, [C.c_int32]),
+        "ewg_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
+        "ewg_profile_reset": (C.c_int, [C.c_void_p]),
+        "ewg_profile_get": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class EwgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Context:
+    """One device problem (ewg_ctx). Host arrays are natural order, N x 2 float64."""
+
+    def __init__(self, case: LensCase):
+        lib = load()
+        self.lib = lib
+        self.case = case
+        self.n = case.grid.n_cells
+        h = C.c_void_p()
+        perm = np.ascontiguousarray(case.perm, dtype=np.float64)
+        st = lib.ewg_create(C.byref(case.grid), C.byref(case.problem), _ptr(perm), C.byref(h))
+        if st != EWG_OK:
+            raise EwgError(st, lib.ewg_create_error().decode())
+        self.h = h
+        self.nnzb = lib.ewg_num_blocks(h)
+
+    def _check(self, st, what=""):
+        if st != EWG_OK:
+            raise EwgError(st, f"{what}: {self.lib.ewg_last_error(self.h).decode()}")
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ewg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def vec(self):
+        return np.zeros((self.n, 2), dtype=np.float64)
+
+    def set_solution(self, time_idx, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)
+        self._check(self.lib.ewg_set_solution(self.h, time_idx, _ptr(x)), "set_solution")
+
+    def get_solution(self, time_idx=0, out=None):
+        x = self.vec() if out is None else out
+        assert x.dtype == np.float64 and x.shape == (self.n, 2) and x.flags.c_contiguous
+        self._check(self.lib.ewg_get_solution(self.h, time_idx, _ptr(x)), "get_solution")
+        return x
+
+    def apply_initial_solution(self):
+        self._check(self.lib.ewg_apply_initial_solution(self.h), "apply_initial_solution")
+
+    def advance_time_level(self):
+        self._check(self.lib.ewg_advance_time_level(self.h), "advance_time_level")
+
+    def restore_time_level(self):
+        self._check(self.lib.ewg_restore_time_level(self.h), "restore_time_level")
+
+    def linearize(self, dt) -> LinReport:
+        rep = LinReport()
+        self._check(self.lib.ewg_linearize(self.h, dt, C.byref(rep)), "linearize")
+        return rep
+
+    def residual(self):
+        r = self.vec()
+        self._check(self.lib.ewg_get_residual(self.h, _ptr(r)), "get_residual")
+        return r
+
+    def jacobian_bcrs(self):
+        rp = np.zeros(self.n + 1, dtype=np.int32)
+        ci = np.zeros(self.nnzb, dtype=np.int32)
+        b = np.zeros((self.nnzb, 2, 2), dtype=np.float64)
+        self._check(self.lib.ewg_get_jacobian_bcrs(self.h, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32),
+                                                   _ptr(b)), "get_jacobian_bcrs")
+        return rp, ci, b
+
+    def set_matrix_bcrs(self, rp, ci, b):
+        rp = np.ascontiguousarray(rp, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self._check(self.lib.ewg_set_matrix_bcrs(self.h, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32),
+                                                 _ptr(b)), "set_matrix_bcrs")
+
+    def set_residual(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(self.n, 2)
+        self._check(self.lib.ewg_set_residual(self.h, _ptr(r)), "set_residual")
+
+    def residual_norm(self, x, dt):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)
+        out = C.c_double()
+        self._check(self.lib.ewg_residual_norm(self.h, _ptr(x), dt, C.byref(out)), "residual_norm")
+        return out.value
+
+    def solve(self, opts: SolveOpts | None = None, check=False) -> SolveReport:
+        opts = opts or default_solve_opts()
+        rep = SolveReport()
+        st = self.lib.ewg_solve(self.h, C.byref(opts), C.byref(rep))
+        if check:
+            self._check(st, "solve")
+        return rep
+
+    def update(self):
+        dx = self.vec()
+        self._check(self.lib.ewg_get_update(self.h, _ptr(dx)), "get_update")
+        return dx
+
+    def apply_preconditioner(self, b, opts: SolveOpts | None = None):
+        opts = opts or default_solve_opts()
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(self.n, 2)
+        y = self.vec()
+        self._check(self.lib.ewg_apply_preconditioner(self.h, C.byref(opts), _ptr(b), _ptr(y)),
+                    "apply_preconditioner")
+        return y
+
+    def apply_jacobian(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)
+        y = self.vec()
+        self._check(self.lib.ewg_apply_jacobian(self.h, _ptr(x), _ptr(y)), "apply_jacobian")
+        return y
+
+    def newton_update(self):
+        self._check(self.lib.ewg_newton_update(self.h), "newton_update")
+
+    def newton_apply(self, dt, nopts=None, sopts=None) -> tuple[int, NewtonReport]:
+        nopts = nopts or default_newton_opts()
+        sopts = sopts or default_solve_opts()
+        rep = NewtonReport()
+        st = self.lib.ewg_newton_apply(self.h, dt, C.byref(nopts), C.byref(sopts), C.byref(rep))
+        return st, rep
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer handle) all work of this context runs on."""
+        return self.lib.ewg_get_stream(self.h)
+
+    def profile_enable(self, on=True):
+        self._check(self.lib.ewg_profile_enable(self.h, int(on)), "profile_enable")
+
+    def profile_reset(self):
+        self._check(self.lib.ewg_profile_reset(self.h), "profile_reset")
+
+    def profile(self) -> dict:
+        """{kernel class: (milliseconds, launches)} accumulated since the last reset."""
+        out = {}
+        ms = C.c_double()
+        n = C.c_int64()
+        for k in range(self.lib.ewg_profile_num_kernels()):
+            self._check(self.lib.ewg_profile_get(self.h, k, C.byref(ms), C.byref(n)), "profile_get")
+            if n.value:
+                out[self.lib.ewg_profile_kernel_name(k).decode()] = (ms.value, n.value)
+        return out
+
+    def run(self, n_steps, dt, nopts=None, sopts=None, max_divisions=10):
+        """Simulator time loop at a fixed step size with FvBaseProblem::timeIntegration's halving
+        retry (fvbaseproblem.hh:507-550). Returns the per-step Newton reports."""
+        reports = []
+        for _ in range(n_steps):
+            h = dt
+            for _attempt in range(max_divisions):
+                st, rep = self.newton_apply(h, nopts, sopts)
+                if st == EWG_OK:
+                    break
+                self.restore_time_level()
+                h /= 2.0
+            else:
+                raise EwgError(st, "time integration did not converge")
+            self.advance_time_level()
+            reports.append(rep)
+        return reports

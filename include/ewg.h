@@ -1,0 +1,260 @@
+/*
+ * ewg.h -- C ABI of the B200 element-centred finite-volume (ECFV) linearizer and the
+ * BiCGStab / block-ILU0 / block-Jacobi solver for the immiscible two-phase model.
+ *
+ * The entry points replace, one for one, the pieces of eWoms' hot path that a Problem/Model
+ * reaches through the property system:
+ *
+ *   FvBaseLinearizer            discretizations/common/fvbaselinearizer.hh
+ *   FvBaseAdLocalLinearizer     discretizations/common/fvbaseadlocallinearizer.hh
+ *   ParallelBiCGStabSolverBackend / ParallelBaseBackend
+ *                               linear/parallelbicgstabbackend.hh, linear/parallelbasebackend.hh
+ *   BiCGStabSolver + CombinedCriterion
+ *                               linear/bicgstabsolver.hh, linear/combinedcriterion.hh
+ *   NewtonMethod::apply         nonlinear/newtonmethod.hh
+ *
+ * Conventions
+ *   - Plain C types only. Host pointers are borrowed for the duration of a call and copied.
+ *   - Cell vectors on the host are in the reference's natural (lexicographic, x fastest) order,
+ *     one 2-block per cell: {p_w, S_w} for primary variables, {conti_w, conti_n} for residuals
+ *     (pressure0Idx = 0, saturation0Idx = 1, conti0EqIdx = 0; models/immiscible/immiscibleindices.hh).
+ *   - Jacobian blocks are 2x2, row-major [eqIdx][pvIdx]; J[row j][col i] = dR_j / dx_i, the layout
+ *     FvBaseLinearizer::linearizeElement_ scatters (fvbaselinearizer.hh:496-508).
+ *   - Every function returns an ewg_status. Non-zero means failure; ewg_last_error() explains.
+ *     A caller mapping non-zero to Ewoms::NumericalIssue keeps the reference's time-step halving
+ *     (fvbaseproblem.hh:507-550) unchanged.
+ *   - One context owns all device buffers and one CUDA stream. Calls on one context are not
+ *     reentrant. There is no CPU fallback: without a usable CUDA device ewg_create fails with
+ *     EWG_ERR_NO_DEVICE.
+ */
+#ifndef EWG_H
+#define EWG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EWG_ABI_VERSION 1
+
+typedef enum ewg_status {
+    EWG_OK = 0,
+    EWG_ERR_INVALID = 1,        /* bad argument or unsupported configuration */
+    EWG_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    EWG_ERR_NONFINITE = 3,      /* NaN/Inf in residual, gradient or Newton update */
+    EWG_ERR_BREAKDOWN = 4,      /* BiCGStab breakdown / stagnation (bicgstabsolver.hh:196,228,284) */
+    EWG_ERR_NOT_CONVERGED = 5,  /* linear or Newton iteration did not converge */
+    EWG_ERR_TIMEOUT = 6,        /* a bounded device wait gave up */
+    EWG_ERR_NO_DEVICE = 7,      /* no CUDA device, or the device is not sm_100 */
+    EWG_ERR_MAX_ERROR = 8       /* Newton error above NewtonMaxError (newtonmethod.hh:681-684) */
+} ewg_status;
+
+/* Structured grid (StructuredGridVanguard, io/structuredgridvanguard.hh:136-175). The domain is
+ * [0,lx] x [0,ly] (x [0,lz]) with uniform cells; gravity acts along -y in 2D and 3D
+ * (multiphasebaseproblem.hh:393-398, lensproblem.hh:284-287). nx must be even: the device stores
+ * cells in red-black split order. */
+typedef struct ewg_grid {
+    int32_t dim;                /* 2 or 3 */
+    int32_t nx, ny, nz;         /* nz is ignored (treated as 1) for dim == 2 */
+    double lx, ly, lz;          /* extents [m]; lz ignored for dim == 2 */
+} ewg_grid;
+
+typedef enum ewg_law_kind {
+    EWG_LAW_VAN_GENUCHTEN = 0,  /* EffToAbsLaw<RegularizedVanGenuchten> (lensproblem.hh:107-126) */
+    EWG_LAW_BROOKS_COREY = 1    /* EffToAbsLaw<RegularizedBrooksCorey> (tutorial/tutorial1problem.hh:86-104) */
+} ewg_law_kind;
+
+/* Material-law parameters of one region (lensproblem.hh:266-279). */
+typedef struct ewg_material {
+    int32_t law;                /* ewg_law_kind */
+    double swr, snr;            /* residual saturations of the wetting / non-wetting phase */
+    double vg_alpha, vg_n;      /* van Genuchten alpha [1/Pa] and n */
+    double bc_entry_pressure;   /* Brooks-Corey entry pressure [Pa] */
+    double bc_lambda;           /* Brooks-Corey shape parameter */
+} ewg_material;
+
+/* Boundary-face kinds of the lens problem (LensProblem::boundary, lensproblem.hh:464-533). */
+typedef struct ewg_problem {
+    double lens_lo[3], lens_hi[3];  /* lens box (isInLens_, lensproblem.hh:596-604) */
+    double eps;                     /* geometric tolerance, 3e-6 in the reference */
+    double porosity;                /* 0.4 */
+    double temperature;             /* 293.15 K; carried for completeness (liquids are constant) */
+    double rho_w, mu_w;             /* wetting liquid density [kg/m^3], viscosity [Pa s] */
+    double rho_n, mu_n;             /* non-wetting liquid */
+    double gravity;                 /* magnitude [m/s^2]; the vector is (0,-g[,0]) */
+    double p_ref;                   /* pressure at the top (y = ly), 1e5 Pa */
+    double left_pressure_scale;     /* hydrostatic factor on the left boundary: 1 + 1.5/H in the
+                                       reference (lensproblem.hh:481-488), 1 for plain Dirichlet */
+    double inlet_x_lo, inlet_x_hi;  /* inlet on the top face for inlet_x_lo < x < inlet_x_hi */
+    double inlet_z_lo, inlet_z_hi;  /* 3D only: and inlet_z_lo < z < inlet_z_hi */
+    double inlet_rate;              /* mass rate on the non-wetting equation [kg/(m^2 s)], -0.04 */
+    ewg_material outer;             /* material outside the lens */
+    ewg_material lens;              /* material inside the lens */
+} ewg_problem;
+
+typedef enum ewg_precond_kind {
+    EWG_PRECOND_ILU0 = 0,       /* block ILU(0), red-black (2-colour) ordering on the device */
+    EWG_PRECOND_JACOBI = 1      /* block Jacobi, one sweep with relaxation */
+} ewg_precond_kind;
+
+typedef enum ewg_precision {
+    EWG_PRECISION_FP64 = 0,     /* Jacobian, preconditioner and BiCGStab in FP64 */
+    EWG_PRECISION_MIXED = 1     /* FP32 Jacobian copy, FP32 preconditioner and BiCGStab inside an
+                                   FP64 defect-correction loop */
+} ewg_precision;
+
+/* Linear-solver parameters; names follow the reference's runtime parameters. */
+typedef struct ewg_solve_opts {
+    int32_t precond;                  /* ewg_precond_kind */
+    int32_t precision;                /* ewg_precision */
+    double linear_solver_tolerance;   /* LinearSolverTolerance (relative max-norm reduction) */
+    double linear_solver_abs_tolerance; /* LinearSolverAbsTolerance (max-norm) */
+    double linear_solver_max_error;   /* LinearSolverMaxError, 1e7 */
+    int32_t linear_solver_max_iterations; /* LinearSolverMaxIterations, 1000 */
+    double preconditioner_relaxation; /* PreconditionerRelaxation, 1.0 */
+    /* mixed precision only: FP64 defect-correction loop */
+    double defect_tolerance;          /* stop when max|b - A x| <= this (FP64); <= 0: same as abs tol */
+    double inner_tolerance;           /* relative reduction asked of each FP32 inner solve */
+    int32_t max_defect_iterations;
+    int32_t check_interval;           /* BiCGStab iterations between host status reads; 0 = auto */
+    int32_t restart_on_breakdown;     /* 1: when |r0hat . r| <= 1e-12 |r0hat| |r| at the top of an
+                                         iteration, restart with r0hat = r (x kept). 0: exactly the
+                                         reference, which then breaks down (EWG_ERR_BREAKDOWN) */
+} ewg_solve_opts;
+
+typedef struct ewg_solve_report {
+    int32_t converged;
+    int32_t restarts;                 /* shadow-residual restarts taken */
+    int32_t iterations;               /* BiCGStab iterations (sum over defect-correction passes) */
+    int32_t outer_iterations;         /* defect-correction passes (1 for FP64) */
+    int32_t status;                   /* ewg_status of the solve */
+    double initial_residual;          /* max|b| */
+    double final_residual;            /* max-norm of the last checked residual */
+    double seconds;                   /* device time of the solve */
+} ewg_solve_report;
+
+typedef struct ewg_lin_report {
+    double error;                     /* max over cells and equations of |r| (newtonmethod.hh:659-674) */
+    int32_t nonfinite;                /* 1 if any residual entry is NaN/Inf */
+    double seconds;                   /* device time of the linearization */
+} ewg_lin_report;
+
+typedef struct ewg_newton_opts {
+    double newton_tolerance;          /* NewtonTolerance, 1e-8 */
+    double newton_max_error;          /* NewtonMaxError, 1e100 */
+    int32_t newton_max_iterations;    /* NewtonMaxIterations, 18 */
+    int32_t newton_target_iterations; /* NewtonTargetIterations, 10 */
+    int32_t verbose;
+} ewg_newton_opts;
+
+typedef struct ewg_newton_report {
+    int32_t converged;
+    int32_t iterations;               /* Newton iterations (numIterations_) */
+    int32_t linear_iterations;        /* BiCGStab iterations summed over the Newton iterations */
+    int32_t status;
+    double error;                     /* last Newton error */
+    double t_linearize, t_solve, t_update;  /* device seconds per phase (newtonmethod.hh:488-500) */
+} ewg_newton_report;
+
+typedef struct ewg_ctx ewg_ctx;
+
+/* ---- context ------------------------------------------------------------------------ */
+
+/* Build the device problem: geometry, per-cell permeability (natural order, N doubles, isotropic
+ * K [m^2]; NULL = lens/outer constants are not given here, so perm is required) and the
+ * precomputed 7-band (3D) / 5-band (2D) block pattern of the Jacobian. Replaces
+ * FvBaseLinearizer::init + createMatrix_ (fvbaselinearizer.hh:284-340). */
+ewg_status ewg_create(const ewg_grid* grid, const ewg_problem* problem, const double* perm,
+                      ewg_ctx** out);
+void ewg_destroy(ewg_ctx* ctx);
+const char* ewg_last_error(const ewg_ctx* ctx);
+/* Last error of a failed ewg_create (no context exists yet). */
+const char* ewg_create_error(void);
+int64_t ewg_num_cells(const ewg_ctx* ctx);
+/* Number of 2x2 blocks of the reference's BCRS pattern: N + 2 * interior faces. */
+int64_t ewg_num_blocks(const ewg_ctx* ctx);
+int32_t ewg_abi_version(void);
+
+/* ---- solution history (FvBaseDiscretization::solution(timeIdx)) -------------------- */
+
+/* time_idx 0: current Newton iterate; time_idx 1: solution of the previous time level. x is
+ * N x {p_w, S_w}. Setting time_idx 1 also recomputes the old-time storage term from it
+ * (fvbaselocalresidual.hh:538-575 with the storage cache). */
+ewg_status ewg_set_solution(ewg_ctx* ctx, int32_t time_idx, const double* x);
+ewg_status ewg_get_solution(ewg_ctx* ctx, int32_t time_idx, double* x);
+/* Hydrostatic initial condition of LensProblem::initial (lensproblem.hh:545-578) into both levels. */
+ewg_status ewg_apply_initial_solution(ewg_ctx* ctx);
+/* advanceTimeLevel (fvbasediscretization.hh:1396-1407): solution(1) = solution(0). */
+ewg_status ewg_advance_time_level(ewg_ctx* ctx);
+/* updateFailed (fvbasediscretization.hh:1370-1387): solution(0) = solution(1). */
+ewg_status ewg_restore_time_level(ewg_ctx* ctx);
+
+/* ---- FvBaseLinearizer ---------------------------------------------------------------- */
+
+/* linearizeDomain() at the current iterate with time-step size dt: residual r(x) and Jacobian
+ * dr/dx into device buffers (fvbaselinearizer.hh:166-197, 401-512). */
+ewg_status ewg_linearize(ewg_ctx* ctx, double dt, ewg_lin_report* report);
+/* residual() (N x 2, natural order). */
+ewg_status ewg_get_residual(ewg_ctx* ctx, double* r);
+/* jacobian() as the reference's BCRS: row_ptr[N+1], col_idx[nnzb] (sorted per row), blocks
+ * [nnzb][2][2]. Any pointer may be NULL to skip it. */
+ewg_status ewg_get_jacobian_bcrs(ewg_ctx* ctx, int32_t* row_ptr, int32_t* col_idx, double* blocks);
+/* Residual-only evaluation at x (natural order, N x 2) without touching the Jacobian or the
+ * stored iterate: max-norm of r(x). Used by the Newton initial-guess fallback. */
+ewg_status ewg_residual_norm(ewg_ctx* ctx, const double* x, double dt, double* max_norm);
+
+/* ---- linear solver backend (ParallelBaseBackend::prepare/setResidual/setMatrix/solve) -- */
+
+/* setMatrix(M) from a host BCRS with the structured pattern (same layout as
+ * ewg_get_jacobian_bcrs). Overrides the Jacobian of the last linearization. */
+ewg_status ewg_set_matrix_bcrs(ewg_ctx* ctx, const int32_t* row_ptr, const int32_t* col_idx,
+                               const double* blocks);
+/* setResidual(b) (N x 2, natural). Overrides the residual of the last linearization. */
+ewg_status ewg_set_residual(ewg_ctx* ctx, const double* b);
+/* solve(x): preconditioned BiCGStab on J dx = r, x0 = 0 (parallelbasebackend.hh:301-338,
+ * bicgstabsolver.hh:116-326). dx stays on the device; the report carries the outcome.
+ * Returns EWG_OK when converged, EWG_ERR_NOT_CONVERGED / EWG_ERR_BREAKDOWN otherwise. */
+ewg_status ewg_solve(ewg_ctx* ctx, const ewg_solve_opts* opts, ewg_solve_report* report);
+/* The last solution update dx (N x 2, natural). */
+ewg_status ewg_get_update(ewg_ctx* ctx, double* dx);
+/* Apply the preconditioner once, y = M^-1 b (natural order host vectors). For parity tests. */
+ewg_status ewg_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* opts, const double* b,
+                                    double* y);
+/* y = J x with the current Jacobian (natural order host vectors). */
+ewg_status ewg_apply_jacobian(ewg_ctx* ctx, const double* x, double* y);
+
+/* ---- Newton (NewtonMethod::apply, newtonmethod.hh:308-517) -------------------------- */
+
+/* x(0) -= dx after checking that dx is finite (newtonmethod.hh:743-809). */
+ewg_status ewg_newton_update(ewg_ctx* ctx);
+/* One full Newton solve of the implicit-Euler step of size dt, starting at solution(0) and with
+ * the old storage of solution(1). Mirrors proceed_/preSolve_/update_ exactly; returns EWG_OK if
+ * converged. On failure solution(0) holds the last iterate (callers restore it). */
+ewg_status ewg_newton_apply(ewg_ctx* ctx, double dt, const ewg_newton_opts* nopts,
+                            const ewg_solve_opts* sopts, ewg_newton_report* report);
+
+/* ---- instrumentation (no reference counterpart; the analogue of the reference's phase timers,
+ * newtonmethod.hh:488-500) --------------------------------------------------------------- */
+
+/* The CUDA stream (cudaStream_t) all work of the context is launched on. */
+void* ewg_get_stream(ewg_ctx* ctx);
+/* Kernel classes: count and names. */
+int32_t ewg_profile_num_kernels(void);
+const char* ewg_profile_kernel_name(int32_t id);
+/* Per-kernel-class device time: with profiling on, every launch is bracketed by a CUDA event pair
+ * on the context stream. Launches are always counted. */
+ewg_status ewg_profile_enable(ewg_ctx* ctx, int32_t on);
+ewg_status ewg_profile_reset(ewg_ctx* ctx);
+ewg_status ewg_profile_get(ewg_ctx* ctx, int32_t id, double* ms_total, int64_t* launches);
+
+/* Default option values of the reference (fvbasediscretization.hh:249-252,
+ * parallelbicgstabbackend.hh:48, parallelbasebackend.hh:514, newtonmethod.hh:150-155). */
+void ewg_default_solve_opts(ewg_solve_opts* o);
+void ewg_default_newton_opts(ewg_newton_opts* o);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EWG_H */

@@ -1,0 +1,1087 @@
+// TEST INFRASTRUCTURE ONLY: parity checker and timed CPU baseline. The product never links this.
+//
+// CPU restatement of eWoms' ECFV + AD linearization (immiscible two-phase, lens problem) and of
+// the BiCGStab / block ILU(0) / block Jacobi solve. The structure follows the reference:
+//   element loop, focus = the element's own DOF   fvbaselinearizer.hh:401-512
+//   local residual (flux, volume terms, boundary)  fvbaselocalresidual.hh:154-629
+//   AD column scatter J[globJ][globI] += dR_j/dx_i fvbaseadlocallinearizer.hh:178-297
+//   intensive quantities                           immiscibleintensivequantities.hh:87-145
+//   TPFA Darcy flux with gravity and upwinding     darcyfluxmodule.hh:185-527
+//   two-point gradients                            fvbasegradientcalculator.hh:194-312
+//   free-flow boundary                             immiscibleboundaryratevector.hh:91-153
+//   lens problem                                   tests/problems/lensproblem.hh:248-623
+//   Newton                                         nonlinear/newtonmethod.hh:308-909
+//   BiCGStab + CombinedCriterion                   linear/bicgstabsolver.hh:116-326,
+//                                                  linear/combinedcriterion.hh:112-205
+// PARITY UNPINNED: the third-party arithmetic (ewoms-material laws, DenseAd, harmonicMean,
+// dune-istl ILU) is restated from the published algorithms; no reference binary or golden vector
+// exists to pin it.
+
+#include "ewoms_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// ---------------------------------------------------------------------------------------------
+// Forward-mode AD value with two derivatives: restates ewoms-common DenseAd::Evaluation<double,2>
+// (value + d/d(p_w), d/d(S_w)); comparisons use the value only.
+struct Eval {
+    double v = 0.0;
+    double d[2] = {0.0, 0.0};
+    Eval() = default;
+    Eval(double x) : v(x) {}
+    static Eval variable(double x, int i) { Eval e(x); e.d[i] = 1.0; return e; }
+};
+static inline Eval operator+(const Eval& a, const Eval& b) { Eval r; r.v = a.v + b.v; r.d[0] = a.d[0] + b.d[0]; r.d[1] = a.d[1] + b.d[1]; return r; }
+static inline Eval operator-(const Eval& a, const Eval& b) { Eval r; r.v = a.v - b.v; r.d[0] = a.d[0] - b.d[0]; r.d[1] = a.d[1] - b.d[1]; return r; }
+static inline Eval operator-(const Eval& a) { Eval r; r.v = -a.v; r.d[0] = -a.d[0]; r.d[1] = -a.d[1]; return r; }
+static inline Eval operator*(const Eval& a, const Eval& b) {
+    Eval r; r.v = a.v * b.v;
+    r.d[0] = a.d[0] * b.v + b.d[0] * a.v;
+    r.d[1] = a.d[1] * b.v + b.d[1] * a.v;
+    return r;
+}
+static inline Eval operator/(const Eval& a, const Eval& b) {
+    // (u/v)' = (v u' - u v') / v^2
+    Eval r;
+    r.d[0] = (b.v * a.d[0] - a.v * b.d[0]) / (b.v * b.v);
+    r.d[1] = (b.v * a.d[1] - a.v * b.d[1]) / (b.v * b.v);
+    r.v = a.v / b.v;
+    return r;
+}
+static inline Eval operator+(const Eval& a, double b) { Eval r = a; r.v += b; return r; }
+static inline Eval operator+(double a, const Eval& b) { Eval r = b; r.v = a + b.v; return r; }
+static inline Eval operator-(const Eval& a, double b) { Eval r = a; r.v -= b; return r; }
+static inline Eval operator-(double a, const Eval& b) { Eval r; r.v = a - b.v; r.d[0] = -b.d[0]; r.d[1] = -b.d[1]; return r; }
+static inline Eval operator*(const Eval& a, double b) { Eval r; r.v = a.v * b; r.d[0] = a.d[0] * b; r.d[1] = a.d[1] * b; return r; }
+static inline Eval operator*(double a, const Eval& b) { Eval r; r.v = a * b.v; r.d[0] = a * b.d[0]; r.d[1] = a * b.d[1]; return r; }
+static inline Eval operator/(const Eval& a, double b) { Eval r; r.v = a.v / b; r.d[0] = a.d[0] / b; r.d[1] = a.d[1] / b; return r; }
+static inline Eval operator/(double a, const Eval& b) {
+    Eval r; r.v = a / b.v;
+    r.d[0] = -a * b.d[0] / (b.v * b.v);
+    r.d[1] = -a * b.d[1] / (b.v * b.v);
+    return r;
+}
+static inline Eval& operator+=(Eval& a, const Eval& b) { a = a + b; return a; }
+static inline Eval& operator-=(Eval& a, const Eval& b) { a = a - b; return a; }
+static inline Eval& operator*=(Eval& a, const Eval& b) { a = a * b; return a; }
+static inline Eval& operator/=(Eval& a, double b) { a = a / b; return a; }
+static inline Eval pow(const Eval& x, double e) {
+    Eval r;
+    double px = std::pow(x.v, e);
+    if (x.v == 0.0) return Eval(0.0);  // DenseAd special-cases base 0
+    double df = px / x.v * e;
+    r.v = px; r.d[0] = df * x.d[0]; r.d[1] = df * x.d[1];
+    return r;
+}
+static inline Eval sqrt(const Eval& x) {
+    Eval r; double s = std::sqrt(x.v); double df = 0.5 / s;
+    r.v = s; r.d[0] = df * x.d[0]; r.d[1] = df * x.d[1];
+    return r;
+}
+static inline double val(const Eval& e) { return e.v; }
+static inline double val(double e) { return e; }
+static inline double pow(double x, double e) { return std::pow(x, e); }
+static inline double sqrt(double x) { return std::sqrt(x); }
+
+// ewoms-common harmonicMean: 0 if x*y <= 0, else 2xy/(y+x)
+static inline double harmonicMean(double x, double y) {
+    if (x * y <= 0) return 0.0;
+    return (2 * x * y) / (y + x);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Material laws (ewoms-material, restated). One region's parameters, finalized like
+// RegularizedVanGenuchtenParams::finalize / RegularizedBrooksCoreyParams.
+struct Law {
+    int kind = EWG_LAW_VAN_GENUCHTEN;
+    double swr = 0, snr = 0;
+    // van Genuchten
+    double alpha = 0, n = 0, m = 0;
+    double pcLowSw = 0.01, pcHighSw = 0.99;
+    double pcLow = 0, pcSlopeLow = 0, pcHigh = 0, pcSlopeHigh = 0;
+    double spX0 = 0, spX1 = 1, spY0 = 0, spY1 = 0, spM0 = 0, spM1 = 0;
+    // Brooks-Corey
+    double pe = 0, lambda = 0;
+};
+
+template <class E> static E vgPcnw(const Law& p, const E& Sw) {
+    return pow(pow(Sw, -1.0 / p.m) - 1.0, 1.0 / p.n) / p.alpha;
+}
+template <class E> static E vgKrw(const Law& p, const E& Sw) {
+    E r = 1.0 - pow(1.0 - pow(Sw, 1.0 / p.m), p.m);
+    return sqrt(Sw) * r * r;
+}
+template <class E> static E vgKrn(const Law& p, const E& Sw) {
+    return pow(1.0 - Sw, 1.0 / 3) * pow(1.0 - pow(Sw, 1.0 / p.m), 2 * p.m);
+}
+// cubic Hermite segment through (x0,y0,m0), (x1,y1,m1): a two-point spline with given slopes
+template <class E> static E hermite(const Law& p, const E& x) {
+    double h = p.spX1 - p.spX0;
+    E t = (x - p.spX0) / h;
+    E t2 = t * t;
+    E t3 = t2 * t;
+    E h00 = 2.0 * t3 - 3.0 * t2 + 1.0;
+    E h10 = t3 - 2.0 * t2 + t;
+    E h01 = -2.0 * t3 + 3.0 * t2;
+    E h11 = t3 - t2;
+    return h00 * p.spY0 + h10 * (h * p.spM0) + h01 * p.spY1 + h11 * (h * p.spM1);
+}
+template <class E> static E regVgPcnw(const Law& p, const E& Sw) {
+    if (val(Sw) < p.pcLowSw) return p.pcLow + p.pcSlopeLow * (Sw - p.pcLowSw);
+    if (val(Sw) > p.pcHighSw) {
+        double yTh = p.pcHigh;
+        double m1 = (0.0 - yTh) / (1.0 - p.pcHighSw) * 2;
+        if (val(Sw) < 1.0) return hermite(p, Sw);
+        return m1 * (Sw - 1.0) + 0.0;
+    }
+    return vgPcnw(p, Sw);
+}
+template <class E> static E regVgKrw(const Law& p, const E& Sw) {
+    if (val(Sw) <= 0) return E(0.0);
+    if (val(Sw) >= 1) return E(1.0);
+    return vgKrw(p, Sw);
+}
+template <class E> static E regVgKrn(const Law& p, const E& Sw) {
+    if (val(Sw) <= 0) return E(1.0);
+    if (val(Sw) >= 1) return E(0.0);
+    return vgKrn(p, Sw);
+}
+static double bcDPc(const Law& p, double Sw) { return -p.pe / p.lambda * std::pow(Sw, -1.0 / p.lambda - 1.0); }
+template <class E> static E regBcPcnw(const Law& p, const E& Sw) {
+    const double th = p.pcLowSw;
+    if (val(Sw) <= th) {
+        double m = bcDPc(p, th);
+        double pcTh = p.pe * std::pow(th, -1.0 / p.lambda);
+        return pcTh + m * (Sw - th);
+    }
+    if (val(Sw) >= 1.0) {
+        double m = bcDPc(p, 1.0);
+        return p.pe + m * (Sw - 1.0);
+    }
+    return p.pe * pow(Sw, -1.0 / p.lambda);
+}
+template <class E> static E regBcKrw(const Law& p, const E& Sw) {
+    if (val(Sw) <= 0) return E(0.0);
+    if (val(Sw) >= 1) return E(1.0);
+    return pow(Sw, 2.0 / p.lambda + 3);
+}
+template <class E> static E regBcKrn(const Law& p, const E& Sw) {
+    if (val(Sw) >= 1) return E(0.0);
+    if (val(Sw) <= 0) return E(1.0);
+    return pow(1.0 - Sw, 2) * (1.0 - pow(Sw, 2.0 / p.lambda + 1));
+}
+// RegularizedVanGenuchtenParams::dPcnw_dSw_: central finite difference, eps 1e-7
+static double vgDPcFd(const Law& p, double Sw) {
+    const double eps = 1e-7;
+    double delta = 0.0, pc1, pc2;
+    if (Sw + eps < 1.0) { pc2 = vgPcnw(p, Sw + eps); delta += eps; } else pc2 = vgPcnw(p, Sw);
+    if (Sw - eps > 0.0) { pc1 = vgPcnw(p, Sw - eps); delta += eps; } else pc1 = vgPcnw(p, Sw);
+    return (pc2 - pc1) / delta;
+}
+static Law makeLaw(const ewg_material& m) {
+    Law p;
+    p.kind = m.law;
+    p.swr = m.swr; p.snr = m.snr;
+    if (m.law == EWG_LAW_VAN_GENUCHTEN) {
+        p.alpha = m.vg_alpha; p.n = m.vg_n; p.m = 1.0 - 1.0 / m.vg_n;
+        p.pcLowSw = 0.01; p.pcHighSw = 0.99;
+        p.pcLow = vgPcnw(p, p.pcLowSw);
+        p.pcSlopeLow = vgDPcFd(p, p.pcLowSw);
+        p.pcHigh = vgPcnw(p, p.pcHighSw);
+        p.pcSlopeHigh = 2 * (0.0 - p.pcHigh) / (1.0 - p.pcHighSw);
+        double mTh = vgDPcFd(p, p.pcHighSw);
+        p.spX0 = p.pcHighSw; p.spX1 = 1.0; p.spY0 = p.pcHigh; p.spY1 = 0.0;
+        p.spM0 = mTh; p.spM1 = p.pcSlopeHigh;
+    } else {
+        p.pe = m.bc_entry_pressure; p.lambda = m.bc_lambda; p.pcLowSw = 0.01;
+    }
+    return p;
+}
+// EffToAbsLaw: effective saturation (S - Sr)/(1 - sum Sr); krn reads 1 - S_n,eff
+template <class E> static void capillaryPressures(E pc[2], const Law& p, const E& Sw) {
+    E Se = (Sw - p.swr) / (1.0 - (p.swr + p.snr));
+    pc[0] = E(0.0);
+    pc[1] = (p.kind == EWG_LAW_VAN_GENUCHTEN) ? regVgPcnw(p, Se) : regBcPcnw(p, Se);
+}
+template <class E> static void relativePermeabilities(E kr[2], const Law& p, const E& Sw) {
+    E Sn = 1.0 - Sw;
+    E Sew = (Sw - p.swr) / (1.0 - (p.swr + p.snr));
+    E Sen = (Sn - p.snr) / (1.0 - (p.swr + p.snr));
+    E Swn = 1.0 - Sen;
+    if (p.kind == EWG_LAW_VAN_GENUCHTEN) { kr[0] = regVgKrw(p, Sew); kr[1] = regVgKrn(p, Swn); }
+    else { kr[0] = regBcKrw(p, Sew); kr[1] = regBcKrn(p, Swn); }
+}
+
+// ---------------------------------------------------------------------------------------------
+struct IQ {  // ImmiscibleIntensiveQuantities
+    Eval p[2], S[2], rho[2], mu[2], kr[2], mob[2];
+    double porosity = 0, K = 0;
+};
+
+struct Face {            // one intersection of a cell (YaspGrid order: -x,+x,-y,+y,-z,+z)
+    int axis, side;      // side 0: lower face (normal -e_axis), 1: upper face
+    int64_t nbr;         // neighbour cell or -1 on the boundary
+};
+
+struct Ctx {
+    int dim = 2, n[3] = {1, 1, 1};
+    double L[3] = {1, 1, 1}, h[3] = {1, 1, 1};
+    int64_t N = 0;
+    ewg_problem prob{};
+    Law law[2];                      // 0 outer, 1 lens
+    std::vector<double> perm;
+    std::vector<unsigned char> inLens;
+    std::vector<double> sol[2];      // solution(timeIdx), N x 2
+    std::vector<double> storageOld;  // cached storage of timeIdx 1 (per unit volume), N x 2
+    std::vector<double> resid;       // N x 2
+    std::vector<int32_t> rowPtr, colIdx;
+    std::vector<double> blocks;      // nnzb x 4
+    std::vector<IQ> iqCache;
+    bool recycleStorage = true;
+    int nthreads = 1;
+    std::string err;
+
+    double vol() const { return dim == 2 ? h[0] * h[1] : h[0] * h[1] * h[2]; }
+    double area(int axis) const {
+        if (dim == 2) return axis == 0 ? h[1] : h[0];
+        return axis == 0 ? h[1] * h[2] : (axis == 1 ? h[0] * h[2] : h[0] * h[1]);
+    }
+    void ijk(int64_t c, int64_t& i, int64_t& j, int64_t& k) const {
+        i = c % n[0]; j = (c / n[0]) % n[1]; k = c / ((int64_t)n[0] * n[1]);
+    }
+    void center(int64_t c, double x[3]) const {
+        int64_t id[3]; ijk(c, id[0], id[1], id[2]);
+        for (int a = 0; a < 3; ++a) x[a] = (a < dim) ? (id[a] + 0.5) * h[a] : 0.0;
+    }
+    void faceCenter(int64_t c, int axis, int side, double x[3]) const {
+        int64_t id[3]; ijk(c, id[0], id[1], id[2]);
+        center(c, x);
+        x[axis] = (id[axis] + side) * h[axis];
+    }
+    int numFaces() const { return 2 * dim; }
+    void faces(int64_t c, Face f[6]) const {
+        int64_t id[3]; ijk(c, id[0], id[1], id[2]);
+        int64_t stride[3] = {1, n[0], (int64_t)n[0] * n[1]};
+        for (int a = 0; a < dim; ++a)
+            for (int s = 0; s < 2; ++s) {
+                Face& F = f[2 * a + s];
+                F.axis = a; F.side = s;
+                bool has = s == 0 ? id[a] > 0 : id[a] < n[a] - 1;
+                F.nbr = has ? c + (s == 0 ? -stride[a] : stride[a]) : -1;
+            }
+    }
+    bool isInLens(const double x[3]) const {
+        for (int a = 0; a < dim; ++a)
+            if (x[a] < prob.lens_lo[a] - prob.eps || x[a] > prob.lens_hi[a] + prob.eps) return false;
+        return true;
+    }
+    double gravity(int a) const { return a == 1 ? -prob.gravity : 0.0; }
+};
+
+static IQ computeIQ(const Ctx& C, int64_t c, const double* x, bool variable) {
+    IQ q;
+    const Law& L = C.law[C.inLens[c]];
+    Eval Sw = variable ? Eval::variable(x[2 * c + 1], 1) : Eval(x[2 * c + 1]);
+    q.S[0] = Sw;
+    q.S[1] = 1.0 - (Eval(0.0) + Sw);
+    Eval pC[2];
+    capillaryPressures(pC, L, q.S[0]);
+    relativePermeabilities(q.kr, L, q.S[0]);
+    Eval p0 = variable ? Eval::variable(x[2 * c + 0], 0) : Eval(x[2 * c + 0]);
+    for (int a = 0; a < 2; ++a) q.p[a] = p0 + (pC[a] - pC[0]);
+    q.mu[0] = Eval(C.prob.mu_w); q.mu[1] = Eval(C.prob.mu_n);
+    q.rho[0] = Eval(C.prob.rho_w); q.rho[1] = Eval(C.prob.rho_n);
+    for (int a = 0; a < 2; ++a) q.mob[a] = q.kr[a] / q.mu[a];
+    q.porosity = C.prob.porosity;
+    q.K = C.perm[c];
+    return q;
+}
+
+// ImmiscibleLocalResidual::computeStorage: phi * S_a * rho_a
+template <class E> static void storageOf(const IQ& q, E out[2]);
+template <> void storageOf<Eval>(const IQ& q, Eval out[2]) {
+    for (int a = 0; a < 2; ++a) out[a] = Eval(q.porosity) * q.S[a] * q.rho[a];
+}
+template <> void storageOf<double>(const IQ& q, double out[2]) {
+    for (int a = 0; a < 2; ++a) out[a] = q.porosity * q.S[a].v * q.rho[a].v;
+}
+
+// Interior-face flux (mass per area) seen from the focus cell i = interior DOF (ECFV: focus is
+// always the element's own DOF): darcyfluxmodule.hh:185-324, 461-527, immisciblelocalresidual.hh:123-149.
+static void interiorFlux(const Ctx& C, int64_t ci, int64_t cj, const Face& f, const IQ& qi,
+                         const IQ& qj, Eval flux[2]) {
+    double xi[3], xj[3], xf[3];
+    C.center(ci, xi); C.center(cj, xj); C.faceCenter(ci, f.axis, f.side, xf);
+    double nrm[3] = {0, 0, 0};
+    nrm[f.axis] = f.side == 0 ? -1.0 : 1.0;
+    const int dim = C.dim;
+    double distSq = 0.0;
+    for (int d = 0; d < dim; ++d) { double t = xj[d] - xi[d]; distSq += t * t; }
+    Eval grad[2][3];
+    for (int a = 0; a < 2; ++a) {
+        Eval deltay = Eval(qj.p[a].v) - qi.p[a];  // i is the focus
+        for (int d = 0; d < dim; ++d) { double t = xj[d] - xi[d]; grad[a][d] = deltay * (t / distSq); }
+    }
+    // gravity correction
+    double distIn[3], distEx[3], distTot[3];
+    for (int d = 0; d < 3; ++d) { distIn[d] = xi[d] - xf[d]; distEx[d] = xj[d] - xf[d]; distTot[d] = xj[d] - xi[d]; }
+    double absDistTotSq = 0.0;
+    for (int d = 0; d < dim; ++d) absDistTotSq += distTot[d] * distTot[d];
+    double gIn = 0.0, gEx = 0.0;
+    for (int d = 0; d < dim; ++d) { gIn += C.gravity(d) * distIn[d]; gEx += C.gravity(d) * distEx[d]; }
+    for (int a = 0; a < 2; ++a) {
+        Eval pStatIn = -qi.rho[a] * gIn;           // focus: carries rho derivatives
+        Eval pStatEx = Eval(-(qj.rho[a].v * gEx));  // exterior: value only
+        Eval q = (pStatEx - pStatIn) / absDistTotSq;
+        for (int d = 0; d < dim; ++d) grad[a][d] += distTot[d] * q;
+        for (int d = 0; d < dim; ++d)
+            if (!std::isfinite(grad[a][d].v)) throw std::runtime_error("Non-finite potential gradient");
+    }
+    // face permeability: entry-wise harmonic mean of isotropic tensors
+    double Kf[3][3];
+    for (int r = 0; r < dim; ++r)
+        for (int s = 0; s < dim; ++s)
+            Kf[r][s] = harmonicMean(r == s ? qi.K : 0.0, r == s ? qj.K : 0.0);
+    for (int a = 0; a < 2; ++a) {
+        Eval tmp(0.0);
+        for (int d = 0; d < dim; ++d) tmp += grad[a][d] * nrm[d];
+        bool upIsExterior = tmp.v > 0;
+        Eval mob = upIsExterior ? Eval(qj.mob[a].v) : qi.mob[a];
+        // filter velocity v = -mob * K grad; volume flux = v . n
+        Eval vel[3];
+        for (int r = 0; r < dim; ++r) {
+            Eval s(0.0);
+            for (int c2 = 0; c2 < dim; ++c2) s += Kf[r][c2] * grad[a][c2];
+            vel[r] = s * (-mob);
+        }
+        Eval volFlux(0.0);
+        for (int d = 0; d < dim; ++d) volFlux += vel[d] * nrm[d];
+        Eval rho = upIsExterior ? Eval(qj.rho[a].v) : qi.rho[a];
+        flux[a] = volFlux * rho;
+    }
+}
+
+// LensProblem::boundary + ImmiscibleBoundaryRateVector, returned as a mass rate per area
+// (positive = leaving through the face). kind: 0 no-flow, 1 free-flow, 2 inlet.
+static void boundaryRate(const Ctx& C, int64_t ci, const Face& f, const IQ& qi, Eval rate[2],
+                         int* kind) {
+    double xf[3], xi[3];
+    C.faceCenter(ci, f.axis, f.side, xf);
+    C.center(ci, xi);
+    const ewg_problem& P = C.prob;
+    const int dim = C.dim;
+    double xmin = 0.0, xmax = C.L[0], ymax = C.L[1], ymin = 0.0;
+    bool left = xf[0] < xmin + P.eps, right = xf[0] > xmax - P.eps;
+    rate[0] = Eval(0.0); rate[1] = Eval(0.0);
+    if (left || right) {
+        *kind = 1;
+        double densityW = P.rho_w, densityN = P.rho_n;
+        double pw, Sw = 1.0;
+        double depth = ymax - xf[1];
+        if (left) {
+            double alpha = P.left_pressure_scale;
+            pw = P.p_ref - alpha * densityW * C.gravity(1) * depth;
+        } else {
+            pw = P.p_ref - densityW * C.gravity(1) * depth;
+        }
+        (void)ymin;
+        const Law& Lf = C.law[C.isInLens(xf) ? 1 : 0];
+        double pC[2];
+        capillaryPressures(pC, Lf, Sw);
+        double pB[2] = {pw, pw + pC[1] - pC[0]};
+        double rhoB[2] = {densityW, densityN};
+        double muB[2] = {P.mu_w, P.mu_n};
+        // boundary gradient (fvbasegradientcalculator.hh:277-312), i is the focus
+        double distSq = 0.0;
+        for (int d = 0; d < dim; ++d) { double t = xf[d] - xi[d]; distSq += t * t; }
+        Eval grad[2][3];
+        for (int a = 0; a < 2; ++a) {
+            Eval deltay = Eval(pB[a]) - qi.p[a];
+            for (int d = 0; d < dim; ++d) { double t = xf[d] - xi[d]; grad[a][d] = deltay * (t / distSq); }
+        }
+        double distIn[3];
+        for (int d = 0; d < 3; ++d) distIn[d] = xi[d] - xf[d];
+        double absDistSq = 0.0, gTimesDist = 0.0;
+        for (int d = 0; d < dim; ++d) { absDistSq += distIn[d] * distIn[d]; gTimesDist += C.gravity(d) * distIn[d]; }
+        for (int a = 0; a < 2; ++a) {
+            Eval rhoIn = qi.rho[a];
+            Eval pStatIn = -gTimesDist * rhoIn;
+            Eval q = pStatIn / absDistSq;
+            for (int d = 0; d < dim; ++d) grad[a][d] += distIn[d] * q;
+            for (int d = 0; d < dim; ++d)
+                if (!std::isfinite(grad[a][d].v)) throw std::runtime_error("Non finite potential gradient");
+        }
+        double nrm[3] = {0, 0, 0};
+        nrm[f.axis] = f.side == 0 ? -1.0 : 1.0;
+        const Law& Li = C.law[C.inLens[ci]];
+        double krB[2];
+        relativePermeabilities(krB, Li, Sw);
+        for (int a = 0; a < 2; ++a) {
+            Eval tmp(0.0);
+            for (int d = 0; d < dim; ++d) tmp += grad[a][d] * nrm[d];
+            Eval mob = (tmp.v > 0) ? Eval(krB[a] / muB[a]) : qi.mob[a];
+            Eval volFlux(0.0);
+            for (int d = 0; d < dim; ++d) {
+                Eval s(0.0);
+                for (int c2 = 0; c2 < dim; ++c2) s += (d == c2 ? qi.K : 0.0) * grad[a][c2];
+                Eval v = s * (-mob);
+                volFlux += v * nrm[d];
+            }
+            Eval density = (pB[a] > qi.p[a].v) ? Eval(rhoB[a]) : qi.rho[a];
+            rate[a] = rate[a] + volFlux * density;
+        }
+        return;
+    }
+    bool upper = xf[1] > ymax - P.eps;
+    bool inlet = upper && xf[0] > P.inlet_x_lo && xf[0] < P.inlet_x_hi;
+    if (inlet && dim == 3) inlet = xf[2] > P.inlet_z_lo && xf[2] < P.inlet_z_hi;
+    if (inlet) {
+        *kind = 2;
+        rate[1] = Eval(P.inlet_rate);
+        return;
+    }
+    *kind = 0;
+}
+
+// FvBaseAdLocalLinearizer::linearize + FvBaseLocalResidual::eval for one element, then the
+// column scatter of FvBaseLinearizer::linearizeElement_.
+static void linearizeElement(Ctx& C, int64_t e, double dt, int newtonIteration,
+                             const std::vector<int32_t>& diagPos, double* errOut) {
+    Face f[6];
+    C.faces(e, f);
+    const int nf = C.numFaces();
+    // stencil DOFs: the element, then one DOF per neighbouring element (intersection order)
+    int64_t dofs[7]; int ndof = 0;
+    dofs[ndof++] = e;
+    int faceDof[6];
+    for (int k = 0; k < nf; ++k) { faceDof[k] = -1; if (f[k].nbr >= 0) { faceDof[k] = ndof; dofs[ndof++] = f[k].nbr; } }
+    const IQ& qi = C.iqCache[e];
+    // local residual: one 2-vector of AD values per stencil DOF (eq index == phase index)
+    Eval R[7][2];
+    for (int d = 0; d < ndof; ++d) { R[d][0] = Eval(0.0); R[d][1] = Eval(0.0); }
+    // evalFluxes: residual[i] += flux, residual[j] -= flux
+    for (int k = 0; k < nf; ++k) {
+        if (f[k].nbr < 0) continue;
+        Eval flux[2];
+        interiorFlux(C, e, f[k].nbr, f[k], qi, C.iqCache[f[k].nbr], flux);
+        double alpha = 1.0;  // extrusion factor
+        alpha *= C.area(f[k].axis);
+        for (int a = 0; a < 2; ++a) flux[a] = flux[a] * alpha;
+        int j = faceDof[k];
+        for (int a = 0; a < 2; ++a) { R[0][a] += flux[a]; R[j][a] -= flux[a]; }
+    }
+    // evalVolumeTerms_ (focus DOF only; numPrimaryDof == 1)
+    {
+        double V = C.vol() * 1.0;
+        Eval tmp[2];
+        storageOf<Eval>(qi, tmp);
+        double tmp2[2];
+        if (newtonIteration == 0) {
+            if (!C.recycleStorage) {
+                IQ qold = computeIQ(C, e, C.sol[1].data(), false);
+                storageOf<double>(qold, tmp2);
+            } else {
+                tmp2[0] = tmp[0].v; tmp2[1] = tmp[1].v;
+            }
+            C.storageOld[2 * e] = tmp2[0]; C.storageOld[2 * e + 1] = tmp2[1];
+        } else {
+            tmp2[0] = C.storageOld[2 * e]; tmp2[1] = C.storageOld[2 * e + 1];
+        }
+        for (int a = 0; a < 2; ++a) {
+            tmp[a] -= Eval(tmp2[a]);
+            tmp[a] *= Eval(V / dt);
+            R[0][a] += tmp[a];
+        }
+        // source term: LensProblem::source is zero
+        for (int a = 0; a < 2; ++a) { Eval src(0.0); src = src * V; R[0][a] -= src; }
+    }
+    // evalBoundary_
+    for (int k = 0; k < nf; ++k) {
+        if (f[k].nbr >= 0) continue;
+        Eval rate[2]; int kind;
+        boundaryRate(C, e, f[k], qi, rate, &kind);
+        for (int a = 0; a < 2; ++a) { rate[a] = rate[a] * (C.area(f[k].axis) * 1.0); R[0][a] += rate[a]; }
+    }
+    // volumetric residual
+    for (int d = 0; d < ndof; ++d) {
+        double V = C.vol();
+        for (int a = 0; a < 2; ++a) R[d][a] /= V;
+    }
+    // scatter: residual row of the focus DOF and the Jacobian column of the focus DOF
+    C.resid[2 * e] = R[0][0].v; C.resid[2 * e + 1] = R[0][1].v;
+    double err = std::max(std::abs(R[0][0].v), std::abs(R[0][1].v));
+    if (!std::isfinite(R[0][0].v) || !std::isfinite(R[0][1].v)) err = std::numeric_limits<double>::infinity();
+    *errOut = std::max(*errOut, err);
+    for (int d = 0; d < ndof; ++d) {
+        int64_t row = dofs[d];
+        // locate block (row, e)
+        int32_t pos = -1;
+        if (row == e) pos = diagPos[e];
+        else {
+            for (int32_t q = C.rowPtr[row]; q < C.rowPtr[row + 1]; ++q) if (C.colIdx[q] == e) { pos = q; break; }
+        }
+        double* B = &C.blocks[4 * (size_t)pos];
+        for (int eq = 0; eq < 2; ++eq)
+            for (int pv = 0; pv < 2; ++pv) B[2 * eq + pv] = R[d][eq].d[pv];
+    }
+}
+
+static void parallelFor(int nthreads, int64_t n, const std::function<void(int64_t, int64_t, int)>& fn) {
+    if (nthreads <= 1 || n < 4096) { fn(0, n, 0); return; }
+    std::vector<std::thread> th;
+    int64_t chunk = (n + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; ++t) {
+        int64_t b = t * chunk, e = std::min<int64_t>(n, b + chunk);
+        if (b >= e) break;
+        th.emplace_back(fn, b, e, t);
+    }
+    for (auto& t : th) t.join();
+}
+
+static void buildPattern(Ctx& C) {
+    // createMatrix_: row i holds {i} and its face neighbours, columns sorted (std::set)
+    C.rowPtr.assign(C.N + 1, 0);
+    std::vector<int32_t> cols;
+    cols.reserve((size_t)C.N * (2 * C.dim + 1));
+    Face f[6];
+    for (int64_t c = 0; c < C.N; ++c) {
+        std::set<int64_t> s;
+        s.insert(c);
+        C.faces(c, f);
+        for (int k = 0; k < C.numFaces(); ++k) if (f[k].nbr >= 0) s.insert(f[k].nbr);
+        for (int64_t v : s) cols.push_back((int32_t)v);
+        C.rowPtr[c + 1] = (int32_t)cols.size();
+    }
+    C.colIdx = std::move(cols);
+    C.blocks.assign(C.colIdx.size() * 4, 0.0);
+}
+
+static std::vector<int32_t> diagPositions(const Ctx& C) {
+    std::vector<int32_t> d(C.N);
+    for (int64_t r = 0; r < C.N; ++r)
+        for (int32_t q = C.rowPtr[r]; q < C.rowPtr[r + 1]; ++q) if (C.colIdx[q] == r) { d[r] = q; break; }
+    return d;
+}
+
+static double linearize(Ctx& C, double dt, int newtonIteration) {
+    // resetSystem_
+    std::fill(C.resid.begin(), C.resid.end(), 0.0);
+    std::fill(C.blocks.begin(), C.blocks.end(), 0.0);
+    std::vector<int32_t> diag = diagPositions(C);
+    // intensive-quantity cache (EnableIntensiveQuantityCache): one evaluation per DOF
+    C.iqCache.resize(C.N);
+    const double* x = C.sol[0].data();
+    parallelFor(C.nthreads, C.N, [&](int64_t b, int64_t e, int) {
+        for (int64_t c = b; c < e; ++c) C.iqCache[c] = computeIQ(C, c, x, true);
+    });
+    std::vector<double> errs(std::max(1, C.nthreads), 0.0);
+    std::vector<std::string> exc(std::max(1, C.nthreads));
+    parallelFor(C.nthreads, C.N, [&](int64_t b, int64_t e, int t) {
+        try {
+            for (int64_t c = b; c < e; ++c) linearizeElement(C, c, dt, newtonIteration, diag, &errs[t]);
+        } catch (const std::exception& ex) { exc[t] = ex.what(); }
+    });
+    for (auto& s : exc) if (!s.empty()) throw std::runtime_error(s);
+    double err = 0.0;
+    for (double v : errs) err = std::max(err, v);
+    return err;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2x2 block helpers (row-major [eq][pv])
+static inline void inv2(const double* A, double* out) {
+    double det = A[0] * A[3] - A[1] * A[2];
+    if (det == 0.0 || !std::isfinite(det)) throw std::runtime_error("singular diagonal block");
+    double di = 1.0 / det;
+    out[0] = A[3] * di; out[1] = -A[1] * di; out[2] = -A[2] * di; out[3] = A[0] * di;
+}
+static inline void mul2(const double* A, const double* B, double* out) {
+    double o[4];
+    o[0] = A[0] * B[0] + A[1] * B[2]; o[1] = A[0] * B[1] + A[1] * B[3];
+    o[2] = A[2] * B[0] + A[3] * B[2]; o[3] = A[2] * B[1] + A[3] * B[3];
+    std::memcpy(out, o, sizeof(o));
+}
+static inline void mmv2(const double* A, const double* x, double* y) {  // y -= A x
+    y[0] -= A[0] * x[0]; y[0] -= A[1] * x[1];
+    y[1] -= A[2] * x[0]; y[1] -= A[3] * x[1];
+}
+
+// A block-sparse matrix in BCRS with sorted columns (a dune BCRSMatrix<FieldMatrix<double,2,2>>).
+struct Bcrs {
+    int64_t n = 0;
+    std::vector<int32_t> rp, ci;
+    std::vector<double> v;
+    std::vector<int32_t> diag;
+    void findDiag() {
+        diag.assign(n, -1);
+        for (int64_t r = 0; r < n; ++r)
+            for (int32_t q = rp[r]; q < rp[r + 1]; ++q) if (ci[q] == r) diag[r] = q;
+    }
+    void mv(const double* x, double* y) const {
+        for (int64_t r = 0; r < n; ++r) {
+            double a0 = 0.0, a1 = 0.0;
+            for (int32_t q = rp[r]; q < rp[r + 1]; ++q) {
+                const double* B = &v[4 * (size_t)q]; const double* xx = &x[2 * (size_t)ci[q]];
+                a0 += B[0] * xx[0]; a0 += B[1] * xx[1];
+                a1 += B[2] * xx[0]; a1 += B[3] * xx[1];
+            }
+            y[2 * r] = a0; y[2 * r + 1] = a1;
+        }
+    }
+};
+
+// dune-istl bilu0_decomposition: left-looking, stored inverse diagonal
+static void bilu0(Bcrs& A) {
+    for (int64_t i = 0; i < A.n; ++i) {
+        int32_t ij = A.rp[i];
+        for (; ij < A.rp[i + 1] && A.ci[ij] < i; ++ij) {
+            int32_t j = A.ci[ij];
+            int32_t jj = A.diag[j];
+            double* Lij = &A.v[4 * (size_t)ij];
+            mul2(Lij, &A.v[4 * (size_t)jj], Lij);  // A_ij * inv(A_jj)
+            int32_t jk = jj + 1, ik = ij + 1;
+            while (ik < A.rp[i + 1] && jk < A.rp[j + 1]) {
+                if (A.ci[ik] == A.ci[jk]) {
+                    double B[4];
+                    mul2(Lij, &A.v[4 * (size_t)jk], B);
+                    double* Aik = &A.v[4 * (size_t)ik];
+                    for (int t = 0; t < 4; ++t) Aik[t] -= B[t];
+                    ++ik; ++jk;
+                } else if (A.ci[ik] < A.ci[jk]) ++ik; else ++jk;
+            }
+        }
+        if (ij >= A.rp[i + 1] || A.ci[ij] != i) throw std::runtime_error("diagonal entry missing");
+        double inv[4];
+        inv2(&A.v[4 * (size_t)ij], inv);
+        std::memcpy(&A.v[4 * (size_t)ij], inv, sizeof(inv));
+    }
+}
+// dune-istl bilu_backsolve
+static void biluApply(const Bcrs& A, const double* d, double* v) {
+    for (int64_t i = 0; i < A.n; ++i) {
+        double rhs[2] = {d[2 * i], d[2 * i + 1]};
+        for (int32_t q = A.rp[i]; q < A.rp[i + 1] && A.ci[q] < i; ++q) mmv2(&A.v[4 * (size_t)q], &v[2 * (size_t)A.ci[q]], rhs);
+        v[2 * i] = rhs[0]; v[2 * i + 1] = rhs[1];
+    }
+    for (int64_t i = A.n - 1; i >= 0; --i) {
+        double rhs[2] = {v[2 * i], v[2 * i + 1]};
+        int32_t q = A.rp[i + 1] - 1;
+        for (; A.ci[q] > i; --q) mmv2(&A.v[4 * (size_t)q], &v[2 * (size_t)A.ci[q]], rhs);
+        const double* D = &A.v[4 * (size_t)q];
+        v[2 * i] = D[0] * rhs[0] + D[1] * rhs[1];
+        v[2 * i + 1] = D[2] * rhs[0] + D[3] * rhs[1];
+    }
+}
+
+struct Precond {
+    int kind = EWG_PRECOND_ILU0;
+    int ordering = ORC_ORDER_NATURAL;
+    double w = 1.0;
+    Bcrs F;                         // factor (ILU) in the chosen ordering
+    std::vector<int64_t> perm, iperm;  // new index -> old, old -> new
+    std::vector<double> Dinv;        // Jacobi
+    std::vector<double> tin, tout;
+    void setup(const Ctx& C, const Bcrs& A) {
+        if (kind == EWG_PRECOND_JACOBI) {
+            Dinv.assign(4 * (size_t)A.n, 0.0);
+            for (int64_t i = 0; i < A.n; ++i) inv2(&A.v[4 * (size_t)A.diag[i]], &Dinv[4 * (size_t)i]);
+            return;
+        }
+        perm.resize(A.n); iperm.resize(A.n);
+        if (ordering == ORC_ORDER_NATURAL) {
+            for (int64_t i = 0; i < A.n; ++i) perm[i] = iperm[i] = i;
+        } else {
+            int64_t k = 0;
+            for (int color = 0; color < 2; ++color)
+                for (int64_t c = 0; c < A.n; ++c) {
+                    int64_t i, j, kk; C.ijk(c, i, j, kk);
+                    if (((i + j + kk) & 1) == color) { perm[k] = c; iperm[c] = k; ++k; }
+                }
+        }
+        F.n = A.n; F.rp.assign(A.n + 1, 0); F.ci.clear(); F.v.clear();
+        for (int64_t r = 0; r < A.n; ++r) {
+            int64_t o = perm[r];
+            std::vector<std::pair<int32_t, int32_t>> row;
+            for (int32_t q = A.rp[o]; q < A.rp[o + 1]; ++q) row.push_back({(int32_t)iperm[A.ci[q]], q});
+            std::sort(row.begin(), row.end());
+            for (auto& pr : row) {
+                F.ci.push_back(pr.first);
+                for (int t = 0; t < 4; ++t) F.v.push_back(A.v[4 * (size_t)pr.second + t]);
+            }
+            F.rp[r + 1] = (int32_t)F.ci.size();
+        }
+        F.findDiag();
+        bilu0(F);
+        tin.resize(2 * A.n); tout.resize(2 * A.n);
+    }
+    void apply(const double* d, double* v) {
+        if (kind == EWG_PRECOND_JACOBI) {
+            for (int64_t i = 0; i < (int64_t)(Dinv.size() / 4); ++i) {
+                const double* D = &Dinv[4 * (size_t)i];
+                v[2 * i] = w * (D[0] * d[2 * i] + D[1] * d[2 * i + 1]);
+                v[2 * i + 1] = w * (D[2] * d[2 * i] + D[3] * d[2 * i + 1]);
+            }
+            return;
+        }
+        for (int64_t r = 0; r < F.n; ++r) { tin[2 * r] = d[2 * perm[r]]; tin[2 * r + 1] = d[2 * perm[r] + 1]; }
+        biluApply(F, tin.data(), tout.data());
+        for (int64_t r = 0; r < F.n; ++r) { v[2 * perm[r]] = w * tout[2 * r]; v[2 * perm[r] + 1] = w * tout[2 * r + 1]; }
+    }
+};
+
+struct BreakdownError : std::runtime_error { using std::runtime_error::runtime_error; };
+
+// CombinedCriterion (combinedcriterion.hh:112-205)
+struct Criterion {
+    double relTol, absTol, maxRes;
+    double resErr = 0, lastResErr = 0, initResErr = 0;
+    bool stagnates = false;
+    void updateErrors(const double* change, const double* resid, int64_t n2) {
+        lastResErr = resErr;
+        resErr = 0.0;
+        stagnates = true;
+        for (int64_t i = 0; i < n2; ++i) {
+            resErr = std::max(resErr, std::abs(resid[i]));
+            if (stagnates && change[i] != 0.0) stagnates = false;
+        }
+    }
+    void setInitial(const double* x, const double* r, int64_t n2) {
+        updateErrors(x, r, n2);
+        stagnates = false;
+        resErr = std::max(resErr, std::numeric_limits<double>::min() * 1e10);
+        initResErr = resErr; lastResErr = resErr;
+    }
+    double reduction() const { return resErr / std::max(1e-20, initResErr); }
+    bool converged() const { return reduction() <= relTol || resErr <= absTol; }
+    bool failed() const { return !converged() && (stagnates || resErr > maxRes); }
+};
+
+static double dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    return s;
+}
+
+// BiCGStabSolver::apply (bicgstabsolver.hh:116-326), including its aliasing (h == x, s == r,
+// t == y) and the criterion update order.
+// Extension (off = exactly the reference): when the shadow residual has become orthogonal to
+// the residual (|r0hat . r| <= 1e-12 |r0hat| |r|), restart with r0hat = r, keeping x.
+static bool bicgstab(const Bcrs& A, Precond& M, const std::vector<double>& b, std::vector<double>& x,
+                     Criterion& crit, int maxIter, bool restartOnBreakdown, int* iters,
+                     int* restarts) {
+    const double breakdownEps = std::numeric_limits<double>::min() * 1e10;
+    const int64_t n2 = (int64_t)b.size();
+    x.assign(n2, 0.0);
+    std::vector<double> r = b;
+    crit.setInitial(x.data(), r.data(), n2);
+    *iters = 0;
+    *restarts = 0;
+    if (crit.converged()) return true;
+    std::vector<double> r0hat = b;
+    double r0r0 = dot(r0hat, r0hat);
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    std::vector<double> v(n2, 0.0), p(n2, 0.0), y(n2, 0.0), z(n2, 0.0);
+    std::vector<double>& h = x; std::vector<double>& s = r; std::vector<double>& t = y;
+    int it = 0;
+    for (; it < maxIter; ++it) {
+        double rho_i = dot(r0hat, r);
+        if (restartOnBreakdown) {
+            double rr = dot(r, r);
+            if (std::abs(rho_i) <= 1e-12 * std::sqrt(r0r0) * std::sqrt(rr)) {
+                r0hat = r; r0r0 = rr; rho_i = rr;
+                rho = 1.0; alpha = 1.0; omega = 1.0;
+                std::fill(v.begin(), v.end(), 0.0); std::fill(p.begin(), p.end(), 0.0);
+                ++*restarts;
+            }
+        }
+        if (std::abs(rho) <= breakdownEps || std::abs(omega) <= breakdownEps)
+            throw BreakdownError("Breakdown of the BiCGStab solver (division by zero)");
+        double beta = (rho_i / rho) * (alpha / omega);
+        rho = rho_i;
+        for (int64_t i = 0; i < n2; ++i) {
+            double tmp = v[i];
+            tmp *= omega; tmp -= p[i]; tmp *= -beta;
+            p[i] = r[i]; p[i] += tmp;
+        }
+        M.apply(p.data(), y.data());
+        A.mv(y.data(), v.data());
+        double denom = dot(r0hat, v);
+        if (std::abs(denom) <= breakdownEps) throw BreakdownError("Breakdown of the BiCGStab solver (division by zero)");
+        alpha = rho_i / denom;
+        if (std::abs(alpha) <= breakdownEps) throw BreakdownError("Breakdown of the BiCGStab solver (stagnation detected)");
+        for (int64_t i = 0; i < n2; ++i) {
+            double tmp = y[i]; tmp *= alpha; tmp += x[i]; h[i] = tmp;
+            tmp = v[i]; tmp *= alpha; s[i] -= tmp;
+        }
+        crit.updateErrors(y.data(), s.data(), n2);
+        if (crit.converged()) { *iters = it; return true; }
+        if (crit.failed()) { *iters = it; return false; }
+        z = s;
+        M.apply(s.data(), z.data());
+        A.mv(z.data(), t.data());
+        denom = dot(t, t);
+        if (std::abs(denom) <= breakdownEps) throw BreakdownError("Breakdown of the BiCGStab solver (division by zero)");
+        omega = dot(t, s) / denom;
+        if (std::abs(omega) <= breakdownEps) throw BreakdownError("Breakdown of the BiCGStab solver (stagnation detected)");
+        for (int64_t i = 0; i < n2; ++i) x[i] += omega * z[i];
+        crit.updateErrors(z.data(), r.data(), n2);
+        if (crit.converged()) { *iters = it; return true; }
+        if (crit.failed()) { *iters = it; return false; }
+        for (int64_t i = 0; i < n2; ++i) r[i] += -omega * t[i];
+    }
+    *iters = it;
+    return false;
+}
+
+static Bcrs systemMatrix(const Ctx& C) {
+    Bcrs A; A.n = C.N; A.rp = C.rowPtr; A.ci = C.colIdx; A.v = C.blocks; A.findDiag();
+    return A;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+struct orc_ctx { Ctx C; };
+
+extern "C" {
+
+orc_ctx* orc_create(const ewg_grid* g, const ewg_problem* p, const double* perm, int nthreads) {
+    orc_ctx* o = new orc_ctx();
+    Ctx& C = o->C;
+    C.dim = g->dim;
+    C.n[0] = g->nx; C.n[1] = g->ny; C.n[2] = g->dim == 3 ? g->nz : 1;
+    C.L[0] = g->lx; C.L[1] = g->ly; C.L[2] = g->dim == 3 ? g->lz : 1.0;
+    for (int a = 0; a < 3; ++a) C.h[a] = C.L[a] / C.n[a];
+    C.N = (int64_t)C.n[0] * C.n[1] * C.n[2];
+    C.prob = *p;
+    C.law[0] = makeLaw(p->outer);
+    C.law[1] = makeLaw(p->lens);
+    C.perm.assign(perm, perm + C.N);
+    C.inLens.resize(C.N);
+    for (int64_t c = 0; c < C.N; ++c) { double x[3]; C.center(c, x); C.inLens[c] = C.isInLens(x) ? 1 : 0; }
+    C.sol[0].assign(2 * C.N, 0.0); C.sol[1].assign(2 * C.N, 0.0);
+    C.storageOld.assign(2 * C.N, 0.0);
+    C.resid.assign(2 * C.N, 0.0);
+    C.nthreads = std::max(1, nthreads);
+    buildPattern(C);
+    return o;
+}
+void orc_destroy(orc_ctx* c) { delete c; }
+const char* orc_last_error(const orc_ctx* c) { return c->C.err.c_str(); }
+int64_t orc_num_cells(const orc_ctx* c) { return c->C.N; }
+int64_t orc_num_blocks(const orc_ctx* c) { return (int64_t)c->C.colIdx.size(); }
+void orc_set_recycle_first_iteration_storage(orc_ctx* c, int on) { c->C.recycleStorage = on != 0; }
+
+void orc_set_solution(orc_ctx* c, int t, const double* x) { c->C.sol[t].assign(x, x + 2 * c->C.N); }
+void orc_get_solution(const orc_ctx* c, int t, double* x) { std::memcpy(x, c->C.sol[t].data(), sizeof(double) * 2 * c->C.N); }
+
+// LensProblem::initial (lensproblem.hh:545-578) + assignNaive
+void orc_apply_initial_solution(orc_ctx* o) {
+    Ctx& C = o->C;
+    double ymax = C.L[1];
+    for (int64_t c = 0; c < C.N; ++c) {
+        double x[3]; C.center(c, x);
+        double depth = ymax - x[1];
+        double densityW = C.prob.rho_w;
+        double pw = C.prob.p_ref - densityW * C.gravity(1) * depth;
+        C.sol[0][2 * c] = pw; C.sol[0][2 * c + 1] = 1.0;
+    }
+    C.sol[1] = C.sol[0];
+}
+void orc_advance_time_level(orc_ctx* o) { o->C.sol[1] = o->C.sol[0]; }
+
+int orc_linearize(orc_ctx* o, double dt, int it, double* error) {
+    try {
+        double e = linearize(o->C, dt, it);
+        if (error) *error = e;
+        return 0;
+    } catch (const std::exception& ex) { o->C.err = ex.what(); return 1; }
+}
+void orc_get_residual(const orc_ctx* o, double* r) { std::memcpy(r, o->C.resid.data(), sizeof(double) * 2 * o->C.N); }
+void orc_get_jacobian_bcrs(const orc_ctx* o, int32_t* rp, int32_t* ci, double* b) {
+    const Ctx& C = o->C;
+    if (rp) std::memcpy(rp, C.rowPtr.data(), sizeof(int32_t) * C.rowPtr.size());
+    if (ci) std::memcpy(ci, C.colIdx.data(), sizeof(int32_t) * C.colIdx.size());
+    if (b) std::memcpy(b, C.blocks.data(), sizeof(double) * C.blocks.size());
+}
+void orc_set_jacobian_blocks(orc_ctx* o, const double* b) { o->C.blocks.assign(b, b + o->C.blocks.size()); }
+void orc_set_residual(orc_ctx* o, const double* r) { o->C.resid.assign(r, r + 2 * o->C.N); }
+
+int orc_fd_jacobian(orc_ctx* o, double dt, double* out) {
+    Ctx& C = o->C;
+    try {
+        std::vector<double> x0 = C.sol[0];
+        std::vector<double> so = C.storageOld;
+        linearize(C, dt, 1);  // storage cache already filled by the caller
+        std::vector<double> r0 = C.resid;
+        std::vector<double> blocks(C.blocks.size(), 0.0);
+        for (int64_t col = 0; col < C.N; ++col) {
+            for (int pv = 0; pv < 2; ++pv) {
+                double base = x0[2 * col + pv];
+                double eps = pv == 0 ? 1e-2 : 1e-8;  // pressure ~1e5 Pa, saturation ~1
+                std::vector<double>& x = C.sol[0];
+                x[2 * col + pv] = base + eps;
+                linearize(C, dt, 1);
+                std::vector<double> rp = C.resid;
+                x[2 * col + pv] = base - eps;
+                linearize(C, dt, 1);
+                std::vector<double> rm = C.resid;
+                x[2 * col + pv] = base;
+                // rows that see this column: the column's own row and its neighbours' rows
+                for (int64_t row = 0; row < C.N; ++row) {
+                    for (int32_t q = C.rowPtr[row]; q < C.rowPtr[row + 1]; ++q) {
+                        if (C.colIdx[q] != col) continue;
+                        for (int eq = 0; eq < 2; ++eq)
+                            blocks[4 * (size_t)q + 2 * eq + pv] = (rp[2 * row + eq] - rm[2 * row + eq]) / (2 * eps);
+                    }
+                }
+            }
+        }
+        C.sol[0] = x0;
+        C.storageOld = so;
+        linearize(C, dt, 1);
+        std::memcpy(out, blocks.data(), sizeof(double) * blocks.size());
+        return 0;
+    } catch (const std::exception& ex) { C.err = ex.what(); return 1; }
+}
+
+int orc_solve(orc_ctx* o, const ewg_solve_opts* so, int ordering, double* dx, int* iterations, double* finalRes) {
+    Ctx& C = o->C;
+    try {
+        Bcrs A = systemMatrix(C);
+        Precond M; M.kind = so->precond; M.ordering = ordering; M.w = so->preconditioner_relaxation;
+        M.setup(C, A);
+        Criterion crit{so->linear_solver_tolerance, so->linear_solver_abs_tolerance, so->linear_solver_max_error};
+        std::vector<double> x;
+        int it = 0, restarts = 0;
+        bool ok = bicgstab(A, M, C.resid, x, crit, so->linear_solver_max_iterations,
+                           so->restart_on_breakdown != 0, &it, &restarts);
+        if (dx) std::memcpy(dx, x.data(), sizeof(double) * x.size());
+        if (iterations) *iterations = it;
+        if (finalRes) *finalRes = crit.resErr;
+        return ok ? 0 : EWG_ERR_NOT_CONVERGED;
+    } catch (const BreakdownError& ex) { C.err = ex.what(); return EWG_ERR_BREAKDOWN; }
+    catch (const std::exception& ex) { C.err = ex.what(); return EWG_ERR_INVALID; }
+}
+
+int orc_apply_preconditioner(orc_ctx* o, const ewg_solve_opts* so, int ordering, const double* b, double* y) {
+    Ctx& C = o->C;
+    try {
+        Bcrs A = systemMatrix(C);
+        Precond M; M.kind = so->precond; M.ordering = ordering; M.w = so->preconditioner_relaxation;
+        M.setup(C, A);
+        M.apply(b, y);
+        return 0;
+    } catch (const std::exception& ex) { C.err = ex.what(); return 1; }
+}
+
+void orc_apply_jacobian(const orc_ctx* o, const double* x, double* y) {
+    Bcrs A = systemMatrix(o->C);
+    A.mv(x, y);
+}
+
+// NewtonMethod::apply at a fixed time-step size
+int orc_newton_apply(orc_ctx* o, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
+                     int ordering, int* newtonIts, int* linIts, double* errorOut) {
+    Ctx& C = o->C;
+    int numIterations = 0, linTotal = 0;
+    double error = 1e100, lastError = 1e100;
+    auto converged = [&]() { return error <= no->newton_tolerance; };
+    auto proceed = [&]() {
+        if (numIterations < 1) return true;
+        if (converged()) return false;
+        if (numIterations >= no->newton_max_iterations) return error * 4.0 < lastError;
+        return true;
+    };
+    int status = 0;
+    try {
+        while (proceed()) {
+            lastError = error;
+            double e = linearize(C, dt, numIterations);
+            // preSolve_: max-norm of the residual, eqWeight == 1
+            lastError = error;
+            error = e;
+            if (error > no->newton_max_error) throw std::runtime_error("Newton: error above NewtonMaxError");
+            if (!proceed()) { ++numIterations; break; }
+            std::vector<double> dx(2 * C.N);
+            int it = 0;
+            double fr = 0;
+            int rc = orc_solve(o, so, ordering, dx.data(), &it, &fr);
+            linTotal += it;
+            if (rc != 0) { status = rc; break; }
+            double one = 0.0;
+            for (double v : dx) one += std::abs(v);
+            if (!std::isfinite(one)) throw std::runtime_error("Non-finite update!");
+            for (int64_t i = 0; i < 2 * C.N; ++i) C.sol[0][i] -= dx[i];
+            ++numIterations;
+        }
+    } catch (const std::exception& ex) { C.err = ex.what(); status = EWG_ERR_NONFINITE; }
+    if (newtonIts) *newtonIts = numIterations;
+    if (linIts) *linIts = linTotal;
+    if (errorOut) *errorOut = error;
+    if (status) return status;
+    return converged() ? 0 : EWG_ERR_NOT_CONVERGED;
+}
+
+double orc_residual_norm(orc_ctx* o, const double* x, double dt) {
+    Ctx& C = o->C;
+    std::vector<double> keep = C.sol[0];
+    std::vector<double> r = C.resid; std::vector<double> b = C.blocks;
+    C.sol[0].assign(x, x + 2 * C.N);
+    double e = 0.0;
+    try { e = linearize(C, dt, 1); } catch (...) { e = std::numeric_limits<double>::infinity(); }
+    C.sol[0] = keep; C.resid = r; C.blocks = b;
+    return e;
+}
+
+void orc_material_eval(const ewg_material* m, double sw, double* out) {
+    Law L = makeLaw(*m);
+    Eval S = Eval::variable(sw, 1);
+    Eval pc[2], kr[2];
+    capillaryPressures(pc, L, S);
+    relativePermeabilities(kr, L, S);
+    out[0] = pc[1].v; out[1] = pc[1].d[1];
+    out[2] = kr[0].v; out[3] = kr[0].d[1];
+    out[4] = kr[1].v; out[5] = kr[1].d[1];
+}
+
+void orc_global_storage(const orc_ctx* o, int t, double* out) {
+    const Ctx& C = o->C;
+    out[0] = out[1] = 0.0;
+    for (int64_t c = 0; c < C.N; ++c) {
+        IQ q = computeIQ(C, c, C.sol[t].data(), false);
+        double s[2]; storageOf<double>(q, s);
+        out[0] += s[0] * C.vol(); out[1] += s[1] * C.vol();
+    }
+}
+
+void orc_boundary_rates(orc_ctx* o, double* out) {
+    Ctx& C = o->C;
+    out[0] = out[1] = 0.0;
+    Face f[6];
+    for (int64_t c = 0; c < C.N; ++c) {
+        C.faces(c, f);
+        IQ q = computeIQ(C, c, C.sol[0].data(), true);
+        for (int k = 0; k < C.numFaces(); ++k) {
+            if (f[k].nbr >= 0) continue;
+            Eval rate[2]; int kind;
+            boundaryRate(C, c, f[k], q, rate, &kind);
+            out[0] += rate[0].v * C.area(f[k].axis);
+            out[1] += rate[1].v * C.area(f[k].axis);
+        }
+    }
+}
+
+}  // extern "C"

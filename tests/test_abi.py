@@ -1,0 +1,79 @@
+"""CPU checks of the C-ABI library: it loads, exports every entry point include/ewg.h declares,
+its structs have the C layout, and it fails loudly (no CPU fallback) without a device."""
+import ctypes as C
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT, PKG
+
+HEADER = os.path.join(ROOT, "include", "ewg.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ewg_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import ewg
+    if not os.path.exists(ewg.LIB_PATH):
+        sys.path.insert(0, PKG)
+        import build
+        build.build()
+    return ewg.load()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = _declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(lib):
+    assert lib.ewg_abi_version() == 1
+
+
+def test_struct_layout_matches_c(tmp_path):
+    """sizeof/offsetof of the ABI structs from a C compiler equal the ctypes mirrors."""
+    import ewg
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ewg.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+                   'sizeof(ewg_grid),sizeof(ewg_material),sizeof(ewg_problem),sizeof(ewg_solve_opts),'
+                   'sizeof(ewg_solve_report),sizeof(ewg_lin_report),sizeof(ewg_newton_opts),'
+                   'sizeof(ewg_newton_report),offsetof(ewg_problem,lens),offsetof(ewg_solve_opts,restart_on_breakdown));}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = [int(v) for v in subprocess.check_output([str(exe)]).split()]
+    want = [C.sizeof(ewg.Grid), C.sizeof(ewg.Material), C.sizeof(ewg.Problem), C.sizeof(ewg.SolveOpts),
+            C.sizeof(ewg.SolveReport), C.sizeof(ewg.LinReport), C.sizeof(ewg.NewtonOpts),
+            C.sizeof(ewg.NewtonReport), ewg.Problem.lens.offset, ewg.SolveOpts.restart_on_breakdown.offset]
+    assert got == want
+
+
+def test_create_without_device_fails_loudly(lib):
+    """On a machine without a usable B200 ewg_create reports EWG_ERR_NO_DEVICE instead of
+    falling back to the CPU."""
+    import ewg
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    case = ewg.baseline_case()
+    with pytest.raises(ewg.EwgError) as ei:
+        ewg.Context(case)
+    assert ei.value.status == 7
+
+
+def test_invalid_grid_rejected(lib):
+    import ewg
+    case = ewg.baseline_case(nx=47, ny=32)
+    with pytest.raises(ewg.EwgError) as ei:
+        ewg.Context(case)
+    assert ei.value.status in (1, 7)

@@ -1,0 +1,251 @@
+"""GPU parity tests: the CUDA path (through the C ABI of libewg.so) against the CPU oracle.
+
+Tolerances (FP64): residual and every Jacobian entry within 1e-12 relative to the field's maximum
+magnitude per (equation, primary variable) component; preconditioner and SpMV within 1e-11;
+after 10 implicit-Euler steps p_w within 1e-8 relative and S_w within 1e-8 absolute of the oracle
+with identical Newton iteration counts.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_close
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(ROOT, "tests", "golden", "lens2d_golden.npz")
+LIN_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def _cases(ewg):
+    return {
+        "baseline": lambda: ewg.baseline_case(),
+        "reference": lambda: ewg.reference_case(),
+        "brooks_corey": lambda: ewg.brooks_corey_case(),
+        "lens3d_4x3x3": lambda: ewg.lens3d_case(4, 3, 3, seed=1),
+        "lens3d_8x6x4": lambda: ewg.lens3d_case(8, 6, 4, seed=2),
+        "lens3d_16x12x10": lambda: ewg.lens3d_case(16, 12, 10, seed=3, corr_cells=3.0),
+    }
+
+
+def _perturb(ewg, case, x, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x = x.copy()
+    xc, yc, zc = ewg.cell_centers(case.grid)
+    plume = np.exp(-((xc - 0.5 * case.grid.lx) ** 2) / 0.8 - ((yc - 0.8 * case.grid.ly) ** 2) / 0.5)
+    x[:, 1] = 1.0 - 0.7 * plume * rng.uniform(0.3, 1.0, size=len(xc))
+    x[:, 1] = np.where(rng.uniform(size=len(xc)) < 0.05, rng.uniform(-0.02, 1.02, size=len(xc)), x[:, 1])
+    x[:, 0] += rng.normal(0.0, 80.0, size=len(xc))
+    return x
+
+
+def _compare_linearization(ewg, oracle_mod, case, x, xold=None, dt=250.0):
+    xold = x if xold is None else xold
+    ctx = ewg.Context(case)
+    ctx.set_solution(1, xold)
+    ctx.set_solution(0, x)
+    rep = ctx.linearize(dt)
+    o = oracle_mod.Oracle(case)
+    o.set_solution(1, xold)
+    o.set_solution(0, x)
+    o.set_recycle_first_iteration_storage(False)
+    err = o.linearize(dt, 0)
+    r_g, r_o = ctx.residual(), o.residual()
+    rp_g, ci_g, b_g = ctx.jacobian_bcrs()
+    rp_o, ci_o, b_o = o.jacobian_bcrs()
+    assert np.array_equal(rp_g, rp_o) and np.array_equal(ci_g, ci_o)
+    for eq in range(2):
+        ok, e, s = rel_close(r_g[:, eq], r_o[:, eq], LIN_RTOL, scale=np.max(np.abs(r_o)))
+        assert ok, ("residual", eq, e, s)
+        for pv in range(2):
+            ok, e, s = rel_close(b_g[:, eq, pv], b_o[:, eq, pv], LIN_RTOL)
+            assert ok, ("jacobian", eq, pv, e, s)
+    assert rep.error == pytest.approx(err, rel=1e-12)
+    return ctx, o
+
+
+@pytest.mark.parametrize("name", ["baseline", "reference", "brooks_corey", "lens3d_4x3x3",
+                                  "lens3d_8x6x4", "lens3d_16x12x10"])
+@pytest.mark.parametrize("state", ["initial", "perturbed", "old_differs"])
+def test_linearization_matches_oracle(ewg_mod, oracle_mod, name, state):
+    case = _cases(ewg_mod)[name]()
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x0 = o.get_solution(0)
+    if state == "initial":
+        _compare_linearization(ewg_mod, oracle_mod, case, x0)
+    elif state == "perturbed":
+        _compare_linearization(ewg_mod, oracle_mod, case, _perturb(ewg_mod, case, x0, 11))
+    else:
+        x = _perturb(ewg_mod, case, x0, 12)
+        _compare_linearization(ewg_mod, oracle_mod, case, x, xold=_perturb(ewg_mod, case, x0, 13), dt=100.0)
+
+
+@pytest.mark.parametrize("name", ["baseline", "reference"])
+@pytest.mark.parametrize("tag", ["init", "pert"])
+def test_linearization_matches_golden(ewg_mod, gold, name, tag):
+    case = {"baseline": ewg_mod.baseline_case, "reference": ewg_mod.reference_case}[name]()
+    ctx = ewg_mod.Context(case)
+    x = gold[f"{name}_{tag}_x"]
+    ctx.set_solution(1, x)
+    ctx.set_solution(0, x)
+    ctx.linearize(250.0)
+    _, _, b = ctx.jacobian_bcrs()
+    assert rel_close(ctx.residual(), gold[f"{name}_{tag}_r"], LIN_RTOL)[0]
+    for eq in range(2):
+        for pv in range(2):
+            assert rel_close(b[:, eq, pv], gold[f"{name}_{tag}_blocks"][:, eq, pv], LIN_RTOL)[0]
+
+
+def test_linearization_is_deterministic(ewg_mod):
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=5, corr_cells=3.0)
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x = _perturb(ewg_mod, case, ctx.get_solution(0), 3)
+    ctx.set_solution(0, x)
+    outs = []
+    for _ in range(2):
+        ctx.linearize(250.0)
+        outs.append((ctx.residual(), ctx.jacobian_bcrs()[2]))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def _system(ewg, oracle_mod, case, seed):
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x = _perturb(ewg, case, o.get_solution(0), seed)
+    o.set_solution(0, x)
+    o.set_solution(1, x)
+    o.linearize(250.0, 0)
+    ctx = ewg.Context(case)
+    rp, ci, b = o.jacobian_bcrs()
+    ctx.set_matrix_bcrs(rp, ci, b)
+    ctx.set_residual(o.residual())
+    return ctx, o
+
+
+@pytest.mark.parametrize("name", ["baseline", "lens3d_8x6x4", "lens3d_16x12x10"])
+def test_spmv_and_preconditioners_match_oracle(ewg_mod, oracle_mod, name):
+    case = _cases(ewg_mod)[name]()
+    ctx, o = _system(ewg_mod, oracle_mod, case, 21)
+    rng = np.random.Generator(np.random.PCG64(5))
+    v = rng.standard_normal((o.n, 2))
+    assert rel_close(ctx.apply_jacobian(v), o.apply_jacobian(v), 1e-13)[0]
+    ilu = ewg_mod.default_solve_opts(precond=ewg_mod.PRECOND_ILU0)
+    y_g = ctx.apply_preconditioner(v, ilu)
+    y_o = o.apply_preconditioner(v, ilu, ordering=oracle_mod.ORDER_REDBLACK)
+    assert rel_close(y_g, y_o, 1e-11)[0]
+    jac = ewg_mod.default_solve_opts(precond=ewg_mod.PRECOND_JACOBI, preconditioner_relaxation=0.9)
+    assert rel_close(ctx.apply_preconditioner(v, jac), o.apply_preconditioner(v, jac), 1e-13)[0]
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+@pytest.mark.parametrize("name", ["baseline", "reference", "lens3d_16x12x10"])
+def test_bicgstab_matches_oracle(ewg_mod, oracle_mod, name, precond):
+    case = _cases(ewg_mod)[name]()
+    ctx, o = _system(ewg_mod, oracle_mod, case, 31)
+    opts = ewg_mod.default_solve_opts(precond=precond, linear_solver_max_iterations=2000)
+    rep = ctx.solve(opts, check=True)
+    dx_g = ctx.update()
+    rc, dx_o, it_o, fr_o = o.solve(opts, ordering=oracle_mod.ORDER_REDBLACK)
+    assert rc == 0 and rep.converged
+    # same algorithm, same ordering: same iteration count up to reduction rounding
+    assert abs(rep.iterations - it_o) <= 2, (rep.iterations, it_o)
+    # both satisfy the linear tolerance on the oracle's operator
+    res = o.apply_jacobian(dx_g) - o.residual()
+    assert np.max(np.abs(res)) <= 1.01e-10 + 1e-10 * np.max(np.abs(o.residual()))
+    assert rel_close(dx_g, dx_o, 1e-6)[0]
+
+
+def test_bicgstab_reference_breakdown_is_reported(ewg_mod):
+    """Without the shadow restart the reference algorithm breaks down on the initial state; the
+    device reports EWG_ERR_BREAKDOWN (bicgstabsolver.hh:228-232) instead of hanging or faulting."""
+    case = ewg_mod.baseline_case()
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    ctx.linearize(250.0)
+    rep = ctx.solve(ewg_mod.default_solve_opts(restart_on_breakdown=0))
+    assert rep.status == 4 and not rep.converged
+    rep = ctx.solve(ewg_mod.default_solve_opts(restart_on_breakdown=1))
+    assert rep.converged and rep.restarts >= 1
+
+
+def test_nonfinite_state_is_reported(ewg_mod):
+    case = ewg_mod.baseline_case()
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x = ctx.get_solution(0)
+    x[100, 0] = np.nan
+    ctx.set_solution(0, x)
+    with pytest.raises(ewg_mod.EwgError) as ei:
+        ctx.linearize(250.0)
+    assert ei.value.status == 3
+    assert np.isinf(ctx.residual_norm(x, 250.0))
+
+
+def test_residual_norm_entry_point(ewg_mod):
+    case = ewg_mod.lens3d_case(8, 6, 4, seed=2)
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x = _perturb(ewg_mod, case, ctx.get_solution(0), 4)
+    n = ctx.residual_norm(x, 250.0)
+    ctx.set_solution(0, x)
+    rep = ctx.linearize(250.0)
+    assert n == rep.error
+    # the stored iterate was not touched by the residual-only call
+    assert np.array_equal(ctx.get_solution(0), x)
+
+
+@pytest.mark.parametrize("name", ["baseline", "reference"])
+def test_ten_steps_match_oracle(ewg_mod, oracle_mod, gold, name):
+    """10 implicit-Euler steps, dt = 250 s, Newton tol 1e-8: fields within 1e-8 of the oracle and
+    identical Newton iteration counts per step."""
+    case = {"baseline": ewg_mod.baseline_case, "reference": ewg_mod.reference_case}[name]()
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    reps = ctx.run(10, 250.0)
+    x_g = ctx.get_solution(0)
+    x_o = gold[f"{name}_run10_x"]
+    steps_o = gold[f"{name}_run10_steps"]
+    assert [r.iterations for r in reps] == list(steps_o[:, 0])
+    assert rel_close(x_g[:, 0], x_o[:, 0], 1e-8)[0]
+    assert np.max(np.abs(x_g[:, 1] - x_o[:, 1])) <= 1e-8
+
+
+def test_time_step_halving_on_newton_failure(ewg_mod):
+    """A Newton failure restores solution(0) from solution(1) (updateFailed) and the step is
+    retried with half the size (FvBaseProblem::timeIntegration)."""
+    case = ewg_mod.baseline_case()
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x_init = ctx.get_solution(0)
+    nopts = ewg_mod.default_newton_opts(newton_max_iterations=2)
+    st, rep = ctx.newton_apply(250.0, nopts)
+    assert st == 5 and not rep.converged
+    ctx.restore_time_level()
+    assert np.array_equal(ctx.get_solution(0), x_init)
+    reps = ctx.run(1, 250.0, nopts=ewg_mod.default_newton_opts(newton_max_iterations=4))
+    assert reps[0].converged
+
+
+def test_mixed_precision_newton(ewg_mod):
+    """FP32 Jacobian / ILU / BiCGStab inside FP64 defect correction reaches the same Newton
+    tolerance; the fields stay within 1e-6 of the FP64 path after 3 steps."""
+    case = ewg_mod.baseline_case()
+    c64 = ewg_mod.Context(case)
+    c64.apply_initial_solution()
+    c64.run(3, 250.0)
+    c32 = ewg_mod.Context(case)
+    c32.apply_initial_solution()
+    mixed = ewg_mod.default_solve_opts(precision=ewg_mod.PRECISION_MIXED)
+    reps = c32.run(3, 250.0, sopts=mixed)
+    assert all(r.converged and r.error <= 1e-8 for r in reps)
+    a, b = c64.get_solution(0), c32.get_solution(0)
+    assert rel_close(b[:, 0], a[:, 0], 1e-8)[0]
+    assert np.max(np.abs(b[:, 1] - a[:, 1])) <= 1e-6
