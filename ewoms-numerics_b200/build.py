@@ -43,6 +43,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
+    # the C++ host driver over the C ABI
+    drv_src = os.path.join(HERE, "host", "lens_gpu.cc")
+    drv = os.path.join(HERE, "lens_gpu")
+    if force or _stale(drv, [drv_src, os.path.join(HERE, "host", "ewg.hh"), OUT]):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-o", drv, drv_src, "-L", HERE, "-lewg",
+               "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
     return OUT
 
 

@@ -237,10 +237,11 @@ def gaussian_log_field(shape, sigma=1.0, corr_cells=8.0, seed=0) -> np.ndarray:
                         indexing="ij")
     r = np.sqrt(sum(g.astype(np.float64) ** 2 for g in grids))
     cov = np.exp(-r / corr_cells)
-    spec = np.fft.rfftn(cov).real
+    axes = tuple(range(len(shape)))
+    spec = np.fft.rfftn(cov, axes=axes).real
     spec = np.maximum(spec, 0.0)
     noise = rng.standard_normal(shape)
-    f = np.fft.irfftn(np.fft.rfftn(noise) * np.sqrt(spec), s=shape)
+    f = np.fft.irfftn(np.fft.rfftn(noise, axes=axes) * np.sqrt(spec), s=shape, axes=axes)
     f -= f.mean()
     f *= sigma / f.std()
     return f

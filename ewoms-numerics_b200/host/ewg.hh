@@ -1,0 +1,87 @@
+// C++ host interface over the C ABI of libewg.so (include/ewg.h).
+//
+// ewg::Context owns one device problem; every failing call throws ewg::Error carrying the
+// ewg_status, which eWoms' host code maps to Ewoms::NumericalIssue so FvBaseProblem::
+// timeIntegration's time-step halving (fvbaseproblem.hh:507-550) works unchanged.
+#ifndef EWG_HOST_EWG_HH
+#define EWG_HOST_EWG_HH
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ewg.h"
+
+namespace ewg {
+
+class Error : public std::runtime_error {
+public:
+    Error(ewg_status st, const std::string& what) : std::runtime_error(what), status_(st) {}
+    ewg_status status() const { return status_; }
+
+private:
+    ewg_status status_;
+};
+
+class Context {
+public:
+    Context(const ewg_grid& grid, const ewg_problem& problem, const std::vector<double>& perm) {
+        ewg_status st = ewg_create(&grid, &problem, perm.data(), &ctx_);
+        if (st != EWG_OK) throw Error(st, std::string("ewg_create: ") + ewg_create_error());
+    }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    ~Context() { ewg_destroy(ctx_); }
+
+    ewg_ctx* raw() const { return ctx_; }
+    int64_t numCells() const { return ewg_num_cells(ctx_); }
+    int64_t numBlocks() const { return ewg_num_blocks(ctx_); }
+
+    void check(ewg_status st, const char* what) const {
+        if (st != EWG_OK) throw Error(st, std::string(what) + ": " + ewg_last_error(ctx_));
+    }
+
+    void setSolution(int timeIdx, const double* x) { check(ewg_set_solution(ctx_, timeIdx, x), "ewg_set_solution"); }
+    void getSolution(int timeIdx, double* x) const { check(ewg_get_solution(ctx_, timeIdx, x), "ewg_get_solution"); }
+    void applyInitialSolution() { check(ewg_apply_initial_solution(ctx_), "ewg_apply_initial_solution"); }
+    void advanceTimeLevel() { check(ewg_advance_time_level(ctx_), "ewg_advance_time_level"); }
+    void restoreTimeLevel() { check(ewg_restore_time_level(ctx_), "ewg_restore_time_level"); }
+
+    ewg_lin_report linearize(double dt) {
+        ewg_lin_report rep{};
+        check(ewg_linearize(ctx_, dt, &rep), "ewg_linearize");
+        return rep;
+    }
+    void getResidual(double* r) const { check(ewg_get_residual(ctx_, r), "ewg_get_residual"); }
+    void getJacobianBcrs(int32_t* rowPtr, int32_t* colIdx, double* blocks) const {
+        check(ewg_get_jacobian_bcrs(ctx_, rowPtr, colIdx, blocks), "ewg_get_jacobian_bcrs");
+    }
+    void setMatrixBcrs(const int32_t* rowPtr, const int32_t* colIdx, const double* blocks) {
+        check(ewg_set_matrix_bcrs(ctx_, rowPtr, colIdx, blocks), "ewg_set_matrix_bcrs");
+    }
+    void setResidual(const double* b) { check(ewg_set_residual(ctx_, b), "ewg_set_residual"); }
+
+    // Returns the report; does not throw on non-convergence (the backend's solve() returns false).
+    ewg_solve_report solve(const ewg_solve_opts& o, ewg_status* status) {
+        ewg_solve_report rep{};
+        *status = ewg_solve(ctx_, &o, &rep);
+        if (*status == EWG_ERR_CUDA || *status == EWG_ERR_INVALID || *status == EWG_ERR_TIMEOUT)
+            check(*status, "ewg_solve");
+        return rep;
+    }
+    void getUpdate(double* dx) const { check(ewg_get_update(ctx_, dx), "ewg_get_update"); }
+    void newtonUpdate() { check(ewg_newton_update(ctx_), "ewg_newton_update"); }
+    double residualNorm(const double* x, double dt) {
+        double v = 0;
+        check(ewg_residual_norm(ctx_, x, dt, &v), "ewg_residual_norm");
+        return v;
+    }
+
+private:
+    ewg_ctx* ctx_ = nullptr;
+};
+
+}  // namespace ewg
+
+#endif
