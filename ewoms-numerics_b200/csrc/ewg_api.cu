@@ -26,7 +26,8 @@ const char* const kKernelNames[K_NUM_KERNELS] = {
     "intensive", "assemble", "storage", "initial", "layout",
     "diag_inverse", "ilu_black_factor", "ilu_black_apply", "ilu_red_apply", "jacobi_apply",
     "spmv", "bicg_init", "bicg_p", "bicg_spmv_alpha", "bicg_hs", "bicg_spmv_omega", "bicg_xr",
-    "to_float", "defect_accumulate", "defect_residual", "newton_update", "bcrs"};
+    "to_float", "defect_accumulate", "defect_residual", "newton_update", "bcrs",
+    "bicg_true_residual"};
 
 void prof_flush(ewg_ctx* ctx) {
     Profiler& pr = ctx->prof;
@@ -39,7 +40,8 @@ void prof_flush(ewg_ctx* ctx) {
 
 void prof_begin(ewg_ctx* ctx, int id) {
     Profiler& pr = ctx->prof;
-    if (!pr.on) return;
+    pr.pendingTimed = pr.on && (pr.launches[id] % pr.period) == 0;
+    if (!pr.pendingTimed) return;
     if (pr.npend == Profiler::kPool) {
         cudaStreamSynchronize(ctx->stream);
         prof_flush(ctx);
@@ -51,7 +53,9 @@ void prof_begin(ewg_ctx* ctx, int id) {
 void prof_end(ewg_ctx* ctx, int id) {
     Profiler& pr = ctx->prof;
     pr.launches[id] += 1;
-    if (!pr.on) return;
+    if (!pr.pendingTimed) return;
+    pr.pendingTimed = false;
+    pr.sampled[id] += 1;
     cudaEventRecord(pr.ev[2 * pr.npend + 1], ctx->stream);
     pr.npend += 1;
 }
@@ -311,6 +315,7 @@ void ewg_default_solve_opts(ewg_solve_opts* o) {
     o->max_defect_iterations = 50;
     o->check_interval = 0;
     o->restart_on_breakdown = 1;
+    o->verify_true_residual = 1;
 }
 
 void* ewg_get_stream(ewg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -330,6 +335,7 @@ ewg_status ewg_profile_enable(ewg_ctx* ctx, int32_t on) {
     cudaStreamSynchronize(ctx->stream);
     prof_flush(ctx);
     pr.on = on != 0;
+    pr.period = on > 1 ? on : 1;
     return EWG_OK;
 }
 
@@ -337,7 +343,11 @@ ewg_status ewg_profile_reset(ewg_ctx* ctx) {
     if (!ctx) return EWG_ERR_INVALID;
     cudaStreamSynchronize(ctx->stream);
     prof_flush(ctx);
-    for (int k = 0; k < K_NUM_KERNELS; ++k) { ctx->prof.ms[k] = 0.0; ctx->prof.launches[k] = 0; }
+    for (int k = 0; k < K_NUM_KERNELS; ++k) {
+        ctx->prof.ms[k] = 0.0;
+        ctx->prof.launches[k] = 0;
+        ctx->prof.sampled[k] = 0;
+    }
     return EWG_OK;
 }
 
@@ -346,7 +356,9 @@ ewg_status ewg_profile_get(ewg_ctx* ctx, int32_t id, double* msTotal, int64_t* l
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "profile sync");
     prof_flush(ctx);
-    if (msTotal) *msTotal = ctx->prof.ms[id];
+    // with a sampling period the timed launches stand for all launches of the class
+    const Profiler& pr = ctx->prof;
+    if (msTotal) *msTotal = pr.sampled[id] ? pr.ms[id] * (double)pr.launches[id] / (double)pr.sampled[id] : 0.0;
     if (launches) *launches = ctx->prof.launches[id];
     return EWG_OK;
 }
@@ -409,18 +421,18 @@ ewg_status ewg_create(const ewg_grid* grid, const ewg_problem* problem, const do
     if ((e = cudaMalloc(&ctx->lens, P.N)) != cudaSuccess) return fail("alloc lens");
     if ((e = cudaMalloc(&ctx->iq, sizeof(double) * 6 * P.N)) != cudaSuccess) return fail("alloc iq");
     if ((e = cudaMalloc(&ctx->J, sizeof(double) * 4 * P.nb * P.N)) != cudaSuccess) return fail("alloc J");
-    if ((e = cudaMemset(ctx->J, 0, sizeof(double) * 4 * P.nb * P.N)) != cudaSuccess) return fail("zero J");
+    if ((e = cudaMemsetAsync(ctx->J, 0, sizeof(double) * 4 * P.nb * P.N, ctx->stream)) != cudaSuccess) return fail("zero J");
     if ((e = cudaMalloc(&ctx->d_errmax, sizeof(unsigned long long))) != cudaSuccess) return fail("alloc errmax");
     if ((e = cudaMalloc(&ctx->d_flags, sizeof(int) * 4)) != cudaSuccess) return fail("alloc flags");
-    if ((e = cudaMemset(ctx->x0, 0, nv)) != cudaSuccess) return fail("zero");
-    if ((e = cudaMemset(ctx->x1, 0, nv)) != cudaSuccess) return fail("zero");
-    if ((e = cudaMemset(ctx->sold, 0, nv)) != cudaSuccess) return fail("zero");
-    if ((e = cudaMemset(ctx->r, 0, nv)) != cudaSuccess) return fail("zero");
-    if ((e = cudaMemset(ctx->dx, 0, nv)) != cudaSuccess) return fail("zero");
+    if ((e = cudaMemsetAsync(ctx->x0, 0, nv, ctx->stream)) != cudaSuccess) return fail("zero");
+    if ((e = cudaMemsetAsync(ctx->x1, 0, nv, ctx->stream)) != cudaSuccess) return fail("zero");
+    if ((e = cudaMemsetAsync(ctx->sold, 0, nv, ctx->stream)) != cudaSuccess) return fail("zero");
+    if ((e = cudaMemsetAsync(ctx->r, 0, nv, ctx->stream)) != cudaSuccess) return fail("zero");
+    if ((e = cudaMemsetAsync(ctx->dx, 0, nv, ctx->stream)) != cudaSuccess) return fail("zero");
     // permeability (natural -> split) and lens flags
     double* stage = nullptr;
     if ((e = cudaMalloc(&stage, sizeof(double) * P.N)) != cudaSuccess) return fail("alloc stage");
-    e = cudaMemcpy(stage, perm, sizeof(double) * P.N, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(stage, perm, sizeof(double) * P.N, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         EWG_LAUNCH(ctx, K_LAYOUT, k_scalar_to_split, lgrid(ctx, (const void*)k_scalar_to_split), kApiBlock, P, stage, ctx->perm);
         EWG_LAUNCH(ctx, K_LAYOUT, k_lens_flags, lgrid(ctx, (const void*)k_lens_flags), kApiBlock, P, ctx->lens);
@@ -429,14 +441,20 @@ ewg_status ewg_create(const ewg_grid* grid, const ewg_problem* problem, const do
     }
     cudaFree(stage);
     if (e != cudaSuccess) return fail("upload permeability");
+    {
+        ewg_status bst = compute_boundary_constants(ctx);
+        if (bst != EWG_OK) { g_createError = ctx->err; ewg_destroy(ctx); return bst; }
+    }
     // reference BCRS pattern
     std::vector<int32_t> rp, ci;
     host_pattern(P, rp, ci);
     ctx->nnzb = (int64_t)ci.size();
     if ((e = cudaMalloc(&ctx->d_rowPtr, sizeof(int32_t) * rp.size())) != cudaSuccess) return fail("alloc rowptr");
     if ((e = cudaMalloc(&ctx->d_colIdx, sizeof(int32_t) * ci.size())) != cudaSuccess) return fail("alloc colidx");
-    if ((e = cudaMemcpy(ctx->d_rowPtr, rp.data(), sizeof(int32_t) * rp.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return fail("upload rowptr");
-    if ((e = cudaMemcpy(ctx->d_colIdx, ci.data(), sizeof(int32_t) * ci.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return fail("upload colidx");
+    if ((e = cudaMemcpyAsync(ctx->d_rowPtr, rp.data(), sizeof(int32_t) * rp.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail("upload rowptr");
+    if ((e = cudaMemcpyAsync(ctx->d_colIdx, ci.data(), sizeof(int32_t) * ci.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail("upload colidx");
+    // everything above is ordered on the context stream; finish it before returning
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail("sync create");
     *out = ctx;
     return EWG_OK;
 }
@@ -504,7 +522,9 @@ static ewg_status ensure_j32(ewg_ctx* ctx) {
     const size_t bytes = sizeof(float) * 4 * ctx->P.nb * ctx->P.N;
     cudaError_t e = cudaMalloc(&ctx->J32, bytes);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "alloc J32");
-    return cuda_fail(ctx, cudaMemset(ctx->J32, 0, bytes), "zero J32");
+    e = cudaMemsetAsync(ctx->J32, 0, bytes, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return cuda_fail(ctx, e, "zero J32");
 }
 
 static ewg_status linearize_impl(ewg_ctx* ctx, double dt, ewg_lin_report* rep) {
@@ -547,11 +567,11 @@ ewg_status ewg_get_jacobian_bcrs(ewg_ctx* ctx, int32_t* rowPtr, int32_t* colIdx,
     if (check_ctx(ctx)) return EWG_ERR_INVALID;
     cudaError_t e;
     const Phys& P = ctx->P;
-    if (rowPtr && (e = cudaMemcpy(rowPtr, ctx->d_rowPtr, sizeof(int32_t) * (P.N + 1), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if (rowPtr && (e = cudaMemcpyAsync(rowPtr, ctx->d_rowPtr, sizeof(int32_t) * (P.N + 1), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "rowptr");
-    if (colIdx && (e = cudaMemcpy(colIdx, ctx->d_colIdx, sizeof(int32_t) * ctx->nnzb, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if (colIdx && (e = cudaMemcpyAsync(colIdx, ctx->d_colIdx, sizeof(int32_t) * ctx->nnzb, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "colidx");
-    if (!blocks) return EWG_OK;
+    if (!blocks) return cuda_fail(ctx, cudaStreamSynchronize(ctx->stream), "sync pattern");
     if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "BCRS export needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
     double* tmp = nullptr;
     if ((e = cudaMalloc(&tmp, sizeof(double) * 4 * ctx->nnzb)) != cudaSuccess) return cuda_fail(ctx, e, "alloc export");
@@ -577,7 +597,9 @@ ewg_status ewg_set_matrix_bcrs(ewg_ctx* ctx, const int32_t* rowPtr, const int32_
     cudaError_t e;
     double* tmp = nullptr;
     if ((e = cudaMalloc(&tmp, sizeof(double) * 4 * ctx->nnzb)) != cudaSuccess) return cuda_fail(ctx, e, "alloc import");
-    e = cudaMemcpy(tmp, blocks, sizeof(double) * 4 * ctx->nnzb, cudaMemcpyHostToDevice);
+    // stream-ordered: a plain cudaMemcpy from pageable memory may return before its DMA lands,
+    // and the legacy stream does not order the non-blocking context stream
+    e = cudaMemcpyAsync(tmp, blocks, sizeof(double) * 4 * ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         EWG_LAUNCH(ctx, K_BCRS, k_bcrs_blocks<false>, lgrid(ctx, (const void*)k_bcrs_blocks<false>), kApiBlock, P, ctx->d_rowPtr, ctx->d_colIdx, ctx->J, tmp, ctx->d_flags);
         e = cudaGetLastError();

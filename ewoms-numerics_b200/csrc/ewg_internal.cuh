@@ -53,6 +53,10 @@ struct Phys {
     double inletXlo, inletXhi, inletZlo, inletZhi, inletRate;
     double lensLo[3], lensHi[3], eps;
     LawDev law[2];           // 0 outer, 1 lens
+    // free-flow boundary state S_w = 1 per region (filled on the device at context creation):
+    // p_cnw and the phase mobilities k_r / mu
+    double bndPc[2];
+    double bndLam[2][2];
 };
 
 struct CellIdx {
@@ -111,6 +115,7 @@ enum KernelId {
     K_DIAG_INVERSE, K_ILU_BLACK_FACTOR, K_ILU_BLACK_APPLY, K_ILU_RED_APPLY, K_JACOBI_APPLY,
     K_SPMV, K_BICG_INIT, K_BICG_P, K_BICG_SPMV_ALPHA, K_BICG_HS, K_BICG_SPMV_OMEGA, K_BICG_XR,
     K_TO_FLOAT, K_DEFECT_ACCUMULATE, K_DEFECT_RESIDUAL, K_NEWTON_UPDATE, K_BCRS,
+    K_BICG_TRUE_RESIDUAL,
     K_NUM_KERNELS
 };
 extern const char* const kKernelNames[K_NUM_KERNELS];
@@ -118,6 +123,9 @@ extern const char* const kKernelNames[K_NUM_KERNELS];
 struct Profiler {
     static constexpr int kPool = 1024;
     bool on = false;
+    int period = 1;                     // time every period-th launch of each class
+    bool pendingTimed = false;
+    long long sampled[K_NUM_KERNELS] = {};
     cudaEvent_t ev[2 * kPool] = {};
     int pendId[kPool] = {};
     int npend = 0;
@@ -190,6 +198,7 @@ ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold);
 ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const double2* x,
                             double2* r, double* maxOut, int* nonfinite);
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x);
+ewg_status compute_boundary_constants(ewg_ctx* ctx);
 
 // solver (ewg_solver.cu)
 ewg_status solver_solve(ewg_ctx* ctx, const ewg_solve_opts* o, ewg_solve_report* rep);

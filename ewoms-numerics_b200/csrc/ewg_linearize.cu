@@ -75,7 +75,115 @@ __device__ __forceinline__ void block_max_publish(double v, unsigned long long* 
     }
 }
 
-template <typename JT, bool WITH_J>
+// One interior face seen from the focus cell i (darcyfluxmodule.hh:185-324, 461-527;
+// immisciblelocalresidual.hh:123-149): adds the mass fluxes to R_i and dR_i/dx_i and returns the
+// block dR_j/dx_i of the neighbour's local residual (already divided by the neighbour's volume).
+template <int AXIS>
+__device__ __forceinline__ void interior_face(const Phys& P, int side, int idxA, double Ki, const double pI[2],
+                                              double dpcI, const double lam[2], const double dlam[2],
+                                              double2 xj, double Kj, double pcj, const double lamj[2],
+                                              double R[2], double D[2][2], double Dj[4]) {
+    const double h = P.h[AXIS];
+    const double xc = (idxA + 0.5) * h;
+    const double xcj = (idxA + (side ? 1 : -1) + 0.5) * h;
+    const double dA = xcj - xc;
+    const double distSq = dA * dA;
+    const double coef = dA / distSq;
+    const double nA = side ? 1.0 : -1.0;
+    const double Kf = harmonic_mean(Ki, Kj);
+    const double area = P.area[AXIS];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const double pJ = a == 0 ? xj.x : xj.x + (pcj - 0.0);
+        const double deltay = pJ - pI[a];
+        double grad = deltay * coef;
+        const double dgP = -coef;
+        const double dgS = a == 0 ? 0.0 : -dpcI * coef;
+        if (AXIS == 1) {
+            // gravity correction; for the other axes the hydrostatic terms are exactly zero
+            const double xf = (idxA + side) * h;
+            const double gIn = -P.g * (xc - xf), gEx = -P.g * (xcj - xf);
+            const double rho = P.rho[a];
+            const double pStatIn = -rho * gIn;
+            const double pStatEx = -(rho * gEx);
+            grad = grad + dA * ((pStatEx - pStatIn) / distSq);
+        }
+        const bool upExt = grad * nA > 0;
+        const double lamU = upExt ? lamj[a] : lam[a];
+        const double dlamU = upExt ? 0.0 : dlam[a];
+        const double sK = Kf * grad;
+        const double vel = sK * (-lamU);
+        const double dvelP = (Kf * dgP) * (-lamU);
+        const double dvelS = (Kf * dgS) * (-lamU) + (-dlamU) * sK;
+        const double rho = P.rho[a];
+        const double F = vel * nA * rho * area;
+        const double dFP = dvelP * nA * rho * area;
+        const double dFS = dvelS * nA * rho * area;
+        R[a] += F;
+        D[a][0] += dFP;
+        D[a][1] += dFS;
+        Dj[2 * a] = -dFP / P.vol;
+        Dj[2 * a + 1] = -dFS / P.vol;
+    }
+}
+
+// One boundary face of the lens problem (lensproblem.hh:464-533): free flow with the hydrostatic
+// S_w = 1 state on the left / right faces (immiscibleboundaryratevector.hh:91-153, boundary
+// gradient fvbasegradientcalculator.hh:277-312, darcyfluxmodule.hh:333-453), the DNAPL inlet on
+// the top face, no flow elsewhere.
+template <int DIM, int AXIS>
+__device__ __forceinline__ void boundary_face(const Phys& P, int side, const int idx[3], int lensI, double Ki,
+                                              const double pI[2], double dpcI, const double lam[2],
+                                              const double dlam[2], double R[2], double D[2][2]) {
+    double xc[3], xf[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xc[d] = d < DIM ? (idx[d] + 0.5) * P.h[d] : 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xf[d] = xc[d];
+    xf[AXIS] = (idx[AXIS] + side) * P.h[AXIS];
+    const double area = P.area[AXIS];
+    const bool left = xf[0] < 0.0 + P.eps, right = xf[0] > P.L[0] - P.eps;
+    if (left || right) {
+        const double g1 = -P.g;
+        const double depth = P.L[1] - xf[1];
+        const double pw = left ? P.pRef - P.leftScale * P.rho[0] * g1 * depth : P.pRef - P.rho[0] * g1 * depth;
+        const double pB[2] = {pw, pw + P.bndPc[in_lens(P, xf) ? 1 : 0] - 0.0};
+        const double dA = xf[AXIS] - xc[AXIS];
+        const double distSq = dA * dA;
+        const double distIn = xc[AXIS] - xf[AXIS];
+        const double absDistSq = distIn * distIn;
+        const double gTimesDist = AXIS == 1 ? g1 * distIn : 0.0;
+        const double coef = dA / distSq;
+        const double nA = side ? 1.0 : -1.0;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const double deltay = pB[a] - pI[a];
+            double grad = deltay * coef;
+            const double dgP = -coef;
+            const double dgS = a == 0 ? 0.0 : -dpcI * coef;
+            const double rho = P.rho[a];
+            const double pStatIn = -gTimesDist * rho;
+            grad = grad + distIn * (pStatIn / absDistSq);
+            const bool upB = grad * nA > 0;
+            const double lamU = upB ? P.bndLam[lensI][a] : lam[a];
+            const double dlamU = upB ? 0.0 : dlam[a];
+            const double sK = Ki * grad;
+            const double vel = sK * (-lamU);
+            const double dvelP = (Ki * dgP) * (-lamU);
+            const double dvelS = (Ki * dgS) * (-lamU) + (-dlamU) * sK;
+            R[a] += vel * nA * rho * area;
+            D[a][0] += dvelP * nA * rho * area;
+            D[a][1] += dvelS * nA * rho * area;
+        }
+        return;
+    }
+    const bool upper = xf[1] > P.L[1] - P.eps;
+    bool inlet = upper && xf[0] > P.inletXlo && xf[0] < P.inletXhi;
+    if (DIM == 3) inlet = inlet && xf[2] > P.inletZlo && xf[2] < P.inletZhi;
+    if (inlet) R[1] += P.inletRate * area;
+}
+
+template <int DIM, typename JT, bool WITH_J>
 __global__ void __launch_bounds__(kLinBlock) k_assemble(
     const __grid_constant__ Phys P, const double2* __restrict__ x, const double2* __restrict__ sold,
     const double* __restrict__ perm, const uint8_t* __restrict__ lens, const double* __restrict__ iq,
@@ -91,24 +199,62 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
         const int64_t h = s - col * P.Nh;
         const CellIdx ci = cell_of(P, col, h);
         const int idx[3] = {ci.i, ci.j, ci.k};
+        const int nAx[3] = {P.nx, P.ny, P.nz};
         const double2 xi = x[s];
         const double Ki = perm[s];
         const double pci = iq[s], dpci = iq[N + s];
         const double lam[2] = {iq[2 * N + s], iq[4 * N + s]};
         const double dlam[2] = {iq[3 * N + s], iq[5 * N + s]};
         // p_alpha = p_w + (pC[alpha] - pC[0]) with pC[0] = 0
-        const double pI[2] = {xi.x + (0.0 - 0.0), xi.x + (pci - 0.0)};
-        const double dpIdS[2] = {0.0, dpci};
-        double xc[3];
-        for (int a = 0; a < 3; ++a) xc[a] = a < P.dim ? (idx[a] + 0.5) * P.h[a] : 0.0;
-        const double g[3] = {0.0, -P.g, 0.0};
+        const double pI[2] = {xi.x, xi.x + (pci - 0.0)};
 
-        // residual of the focus DOF and its derivatives [eq][pv]
         double R[2] = {0.0, 0.0};
         double D[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 
-        // ---- fluxes over interior faces (YaspGrid intersection order) ----
-        for (int axis = 0; axis < P.dim; ++axis) {
+        const bool interior = ci.i > 0 && ci.i < P.nx - 1 && ci.j > 0 && ci.j < P.ny - 1 &&
+                              (DIM == 2 || (ci.k > 0 && ci.k < P.nz - 1));
+        if (interior) {
+            // every face has a neighbour: issue all neighbour loads before the flux arithmetic
+            constexpr int NF = 2 * DIM;
+            const int64_t base = (int64_t)(col ^ 1) * P.Nh;
+            int64_t nb[NF];
+            nb[0] = base + h - 1 + ci.b;
+            nb[1] = base + h + ci.b;
+            nb[2] = base + h - P.nxh;
+            nb[3] = base + h + P.nxh;
+            if (DIM == 3) {
+                nb[NF - 2] = base + h - P.planeh;
+                nb[NF - 1] = base + h + P.planeh;
+            }
+            const double* xs = reinterpret_cast<const double*>(x);
+            double pwj[NF], Kj[NF], pcj[NF], lwj[NF], lnj[NF];
+#pragma unroll
+            for (int q = 0; q < NF; ++q) {
+                pwj[q] = xs[2 * nb[q]];
+                Kj[q] = perm[nb[q]];
+                pcj[q] = iq[nb[q]];
+                lwj[q] = iq[2 * N + nb[q]];
+                lnj[q] = iq[4 * N + nb[q]];
+            }
+#pragma unroll
+            for (int q = 0; q < NF; ++q) {
+                const int axis = q >> 1, side = q & 1;
+                const double lamj[2] = {lwj[q], lnj[q]};
+                const double2 xj = make_double2(pwj[q], 0.0);
+                double Dj[4];
+                if (axis == 0)
+                    interior_face<0>(P, side, idx[0], Ki, pI, dpci, lam, dlam, xj, Kj[q], pcj[q], lamj, R, D, Dj);
+                else if (axis == 1)
+                    interior_face<1>(P, side, idx[1], Ki, pI, dpci, lam, dlam, xj, Kj[q], pcj[q], lamj, R, D, Dj);
+                else
+                    interior_face<2>(P, side, idx[2], Ki, pI, dpci, lam, dlam, xj, Kj[q], pcj[q], lamj, R, D, Dj);
+                if (WITH_J) store_block(J, N, opposite_band(band_of(axis, side)), nb[q], Dj);
+            }
+        } else {
+        // ---- fluxes over interior faces in intersection order (-x, +x, -y, +y, -z, +z) ----
+#pragma unroll
+        for (int axis = 0; axis < DIM; ++axis) {
+#pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const int64_t sj = neighbour_split(P, col, h, ci, axis, side);
                 if (sj < 0) continue;
@@ -116,60 +262,16 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
                 const double Kj = perm[sj];
                 const double pcj = iq[sj];
                 const double lamj[2] = {iq[2 * N + sj], iq[4 * N + sj]};
-                double xcj[3] = {xc[0], xc[1], xc[2]};
-                xcj[axis] = (idx[axis] + (side ? 1 : -1) + 0.5) * P.h[axis];
-                double xf[3] = {xc[0], xc[1], xc[2]};
-                xf[axis] = (idx[axis] + side) * P.h[axis];
-                double distSq = 0.0, gIn = 0.0, gEx = 0.0;
-                for (int d = 0; d < P.dim; ++d) {
-                    double t = xcj[d] - xc[d];
-                    distSq += t * t;
-                }
-                for (int d = 0; d < P.dim; ++d) {
-                    gIn += g[d] * (xc[d] - xf[d]);
-                    gEx += g[d] * (xcj[d] - xf[d]);
-                }
-                const double dA = xcj[axis] - xc[axis];
-                const double coef = dA / distSq;
-                const double nA = side ? 1.0 : -1.0;
-                const double Kf = harmonic_mean(Ki, Kj);
-                const double area = P.area[axis];
-                double Dj[2][2];
-                for (int a = 0; a < 2; ++a) {
-                    const double pJ = a == 0 ? xj.x + (0.0 - 0.0) : xj.x + (pcj - 0.0);
-                    // raw two-point gradient along the face axis, derivatives from the focus only
-                    const double deltay = pJ - pI[a];
-                    double grad = deltay * coef;
-                    const double dgP = -1.0 * coef;
-                    const double dgS = -dpIdS[a] * coef;
-                    // gravity correction with the phase densities of both sides
-                    const double rho = P.rho[a];
-                    const double pStatIn = -rho * gIn;
-                    const double pStatEx = -(rho * gEx);
-                    grad = grad + dA * ((pStatEx - pStatIn) / distSq);
-                    const double tmp = grad * nA;
-                    const bool upExt = tmp > 0;
-                    const double lamU = upExt ? lamj[a] : lam[a];
-                    const double dlamU = upExt ? 0.0 : dlam[a];
-                    // filter velocity -lambda K grad, volume flux v.n, mass flux * rho_up * area
-                    const double sK = Kf * grad;
-                    const double vel = sK * (-lamU);
-                    const double dvelP = (Kf * dgP) * (-lamU);
-                    const double dvelS = (Kf * dgS) * (-lamU) + (-dlamU) * sK;
-                    const double F = vel * nA * rho * area;
-                    const double dFP = dvelP * nA * rho * area;
-                    const double dFS = dvelS * nA * rho * area;
-                    R[a] += F;
-                    D[a][0] += dFP;
-                    D[a][1] += dFS;
-                    Dj[a][0] = -dFP / V;
-                    Dj[a][1] = -dFS / V;
-                }
-                if (WITH_J) {
-                    const double blk[4] = {Dj[0][0], Dj[0][1], Dj[1][0], Dj[1][1]};
-                    store_block(J, N, opposite_band(band_of(axis, side)), sj, blk);
-                }
+                double Dj[4];
+                if (axis == 0)
+                    interior_face<0>(P, side, idx[0], Ki, pI, dpci, lam, dlam, xj, Kj, pcj, lamj, R, D, Dj);
+                else if (axis == 1)
+                    interior_face<1>(P, side, idx[1], Ki, pI, dpci, lam, dlam, xj, Kj, pcj, lamj, R, D, Dj);
+                else
+                    interior_face<2>(P, side, idx[2], Ki, pI, dpci, lam, dlam, xj, Kj, pcj, lamj, R, D, Dj);
+                if (WITH_J) store_block(J, N, opposite_band(band_of(axis, side)), sj, Dj);
             }
+        }
         }
 
         // ---- storage: (phi S rho - storage(x_old)) V / dt ----
@@ -186,60 +288,20 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
         }
 
         // ---- boundary faces ----
-        for (int axis = 0; axis < P.dim; ++axis) {
+        if (!interior)
+#pragma unroll
+        for (int axis = 0; axis < DIM; ++axis) {
+#pragma unroll
             for (int side = 0; side < 2; ++side) {
-                const bool has = side == 0 ? idx[axis] > 0 : idx[axis] < (axis == 0 ? P.nx : (axis == 1 ? P.ny : P.nz)) - 1;
+                const bool has = side == 0 ? idx[axis] > 0 : idx[axis] < nAx[axis] - 1;
                 if (has) continue;
-                double xf[3] = {xc[0], xc[1], xc[2]};
-                xf[axis] = (idx[axis] + side) * P.h[axis];
-                const double area = P.area[axis];
-                const bool left = xf[0] < 0.0 + P.eps, right = xf[0] > P.L[0] - P.eps;
-                if (left || right) {
-                    // free-flow boundary with a hydrostatic fluid state at S_w = 1
-                    const double depth = P.L[1] - xf[1];
-                    const double pw = left ? P.pRef - P.leftScale * P.rho[0] * g[1] * depth
-                                           : P.pRef - P.rho[0] * g[1] * depth;
-                    const MatOut mf = material(P.law[in_lens(P, xf) ? 1 : 0], 1.0);
-                    const MatOut mi = material(P.law[lens[s]], 1.0);
-                    const double pB[2] = {pw, pw + mf.pc.v - 0.0};
-                    const double lamB[2] = {mi.krw.v / P.mu[0], mi.krn.v / P.mu[1]};
-                    double distSq = 0.0, absDistSq = 0.0, gTimesDist = 0.0;
-                    for (int d = 0; d < P.dim; ++d) {
-                        double t = xf[d] - xc[d];
-                        distSq += t * t;
-                        double u = xc[d] - xf[d];
-                        absDistSq += u * u;
-                        gTimesDist += g[d] * u;
-                    }
-                    const double coef = (xf[axis] - xc[axis]) / distSq;
-                    const double distIn = xc[axis] - xf[axis];
-                    const double nA = side ? 1.0 : -1.0;
-                    for (int a = 0; a < 2; ++a) {
-                        const double deltay = pB[a] - pI[a];
-                        double grad = deltay * coef;
-                        const double dgP = -1.0 * coef;
-                        const double dgS = -dpIdS[a] * coef;
-                        const double rho = P.rho[a];
-                        const double pStatIn = -gTimesDist * rho;
-                        grad = grad + distIn * (pStatIn / absDistSq);
-                        const double tmp = grad * nA;
-                        const bool upB = tmp > 0;
-                        const double lamU = upB ? lamB[a] : lam[a];
-                        const double dlamU = upB ? 0.0 : dlam[a];
-                        const double sK = Ki * grad;
-                        const double vel = sK * (-lamU);
-                        const double dvelP = (Ki * dgP) * (-lamU);
-                        const double dvelS = (Ki * dgS) * (-lamU) + (-dlamU) * sK;
-                        R[a] += vel * nA * rho * area;
-                        D[a][0] += dvelP * nA * rho * area;
-                        D[a][1] += dvelS * nA * rho * area;
-                    }
-                    continue;
-                }
-                const bool upper = xf[1] > P.L[1] - P.eps;
-                bool inlet = upper && xf[0] > P.inletXlo && xf[0] < P.inletXhi;
-                if (inlet && P.dim == 3) inlet = xf[2] > P.inletZlo && xf[2] < P.inletZhi;
-                if (inlet) R[1] += P.inletRate * area;
+                const int li = lens[s];
+                if (axis == 0)
+                    boundary_face<DIM, 0>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
+                else if (axis == 1)
+                    boundary_face<DIM, 1>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
+                else
+                    boundary_face<DIM, 2>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
             }
         }
 
@@ -257,6 +319,17 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
     }
     if (bad) atomicOr(flags, 1);
     block_max_publish(localMax, errmax);
+}
+
+// S_w = 1 state of the free-flow boundary per region: p_cnw and k_r / mu of both phases
+__global__ void k_boundary_constants(const __grid_constant__ Phys P, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int r = 0; r < 2; ++r) {
+        MatOut m = material(P.law[r], 1.0);
+        out[3 * r] = m.pc.v;
+        out[3 * r + 1] = m.krw.v / P.mu[0];
+        out[3 * r + 2] = m.krn.v / P.mu[1];
+    }
 }
 
 __global__ void k_storage(const __grid_constant__ Phys P, const double2* __restrict__ x,
@@ -287,6 +360,25 @@ ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold) {
     return cuda_fail(ctx, cudaGetLastError(), "k_storage");
 }
 
+ewg_status compute_boundary_constants(ewg_ctx* ctx) {
+    double* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(double) * 6);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "alloc boundary constants");
+    k_boundary_constants<<<1, 32, 0, ctx->stream>>>(ctx->P, d);
+    double h[6] = {0, 0, 0, 0, 0, 0};
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "boundary constants");
+    for (int r = 0; r < 2; ++r) {
+        ctx->P.bndPc[r] = h[3 * r];
+        ctx->P.bndLam[r][0] = h[3 * r + 1];
+        ctx->P.bndLam[r][1] = h[3 * r + 2];
+    }
+    return EWG_OK;
+}
+
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x) {
     int grid = grid_size_for(ctx, (const void*)k_initial, kLinBlock);
     EWG_LAUNCH(ctx, K_INITIAL, k_initial, grid, kLinBlock, ctx->P, x);
@@ -303,18 +395,19 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
     int g1 = grid_size_for(ctx, (const void*)k_intensive, kLinBlock);
     EWG_LAUNCH(ctx, K_INTENSIVE, k_intensive, g1, kLinBlock, ctx->P, x, ctx->lens, ctx->iq);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_intensive");
+    const bool three = ctx->P.dim == 3;
     if (!withJacobian) {
-        auto k = k_assemble<double, false>;
+        auto k = three ? k_assemble<3, double, false> : k_assemble<2, double, false>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
                                              nullptr, ctx->d_errmax, ctx->d_flags);
     } else if (ctx->jacPrecision == EWG_PRECISION_MIXED) {
-        auto k = k_assemble<float, true>;
+        auto k = three ? k_assemble<3, float, true> : k_assemble<2, float, true>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
                                              ctx->J32, ctx->d_errmax, ctx->d_flags);
     } else {
-        auto k = k_assemble<double, true>;
+        auto k = three ? k_assemble<3, double, true> : k_assemble<2, double, true>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
                                              ctx->J, ctx->d_errmax, ctx->d_flags);

@@ -43,7 +43,8 @@ struct BiState {
     int restartOnBreakdown;
     int restartPending;
     int stagnates;
-    int pad;
+    int replacements;
+    int verifyTrue;
 };
 
 template <typename T> struct V2T;
@@ -312,6 +313,30 @@ __device__ __forceinline__ void spmv_row(const Phys& P, const TM* __restrict__ A
     const CellIdx ci = cell_of(P, col, h);
     const int nOff = 2 * P.dim;
     a0 = 0.0; a1 = 0.0;
+    const bool interior = ci.i > 0 && ci.i < P.nx - 1 && ci.j > 0 && ci.j < P.ny - 1 &&
+                          (P.dim == 2 || (ci.k > 0 && ci.k < P.nz - 1));
+    if (P.dim == 3 && interior) {
+        // all seven blocks exist: issue every load before the arithmetic
+        const int64_t base = (int64_t)(col ^ 1) * P.Nh;
+        const int64_t nb[7] = {base + h - P.planeh, base + h - P.nxh, base + h - 1 + ci.b, s,
+                               base + h + ci.b, base + h + P.nxh, base + h + P.planeh};
+        const int bands[7] = {5, 3, 1, 0, 2, 4, 6};
+        double B[7][4];
+        double xv[7][2];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            load_block(A, P.N, bands[q], s, B[q]);
+            auto xk = x[nb[q]];
+            xv[q][0] = (double)xk.x;
+            xv[q][1] = (double)xk.y;
+        }
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            a0 += B[q][0] * xv[q][0]; a0 += B[q][1] * xv[q][1];
+            a1 += B[q][2] * xv[q][0]; a1 += B[q][3] * xv[q][1];
+        }
+        return;
+    }
     // ascending columns: lower bands, diagonal, upper bands
     for (int q = 0; q <= nOff; ++q) {
         int band;
@@ -577,6 +602,50 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_xr(const __grid_constant__ P
     }
 }
 
+// Residual replacement after convergence: r = r0hat = b - A x with max-norm and r . r. If the
+// true residual misses the criterion by more than 10x the iteration resumes from x.
+template <typename TM, typename TV>
+__global__ void __launch_bounds__(kSolBlock) k_bicg_true_residual(const __grid_constant__ Phys P, const TM* __restrict__ A,
+                                                                   const typename V2T<TV>::type* __restrict__ b,
+                                                                   const typename V2T<TV>::type* __restrict__ x,
+                                                                   typename V2T<TV>::type* __restrict__ r,
+                                                                   typename V2T<TV>::type* __restrict__ r0,
+                                                                   typename V2T<TV>::type* __restrict__ v,
+                                                                   typename V2T<TV>::type* __restrict__ p,
+                                                                   BiState* st, double* partials, unsigned* counter) {
+    if (st->status != ST_CONVERGED) return;
+    double red[2] = {0.0, 0.0};  // sum r.r, max |r|
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1;
+        spmv_row<TM, TV>(P, A, x, s, a0, a1);
+        auto bs = b[s];
+        typename V2T<TV>::type o, z;
+        o.x = (TV)((double)bs.x - a0);
+        o.y = (TV)((double)bs.y - a1);
+        z.x = (TV)0; z.y = (TV)0;
+        r[s] = o; r0[s] = o; v[s] = z; p[s] = z;
+        red[0] += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+        red[1] = fmax(red[1], fmax(absn((double)o.x), absn((double)o.y)));
+    }
+    double out[2];
+    if (grid_reduce<1, 1>(red, partials, counter, out) && threadIdx.x == 0) {
+        const double err = out[1];
+        if (err / fmax(1e-20, st->initResErr) <= 10 * st->relTol || err <= 10 * st->absTol) return;
+        st->replacements += 1;
+        st->restarts += 1;
+        st->status = ST_RUNNING;
+        st->lastResErr = st->resErr;
+        st->resErr = err;
+        st->stagnates = 0;
+        st->restartPending = 0;
+        st->rho = 1.0; st->alpha = 1.0; st->omega = 1.0;
+        st->r0r0 = out[0];
+        st->iter += 1;
+        iteration_top(st, out[0], out[0]);
+    }
+}
+
 // ---- mixed precision: defect correction ----------------------------------------------------
 
 __global__ void k_to_float(const __grid_constant__ Phys P, const double2* __restrict__ a, float2* __restrict__ b) {
@@ -689,7 +758,7 @@ static ewg_status ensure_ws(ewg_ctx* ctx, bool needFloat) {
         w->gridRed = ctx->numSMs * 4;
         if ((e = cudaMalloc(&w->partials, sizeof(double) * kMaxRed * w->gridRed * 2)) != cudaSuccess) return cuda_fail(ctx, e, "alloc partials");
         if ((e = cudaMalloc(&w->counter, sizeof(unsigned) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc counter");
-        if ((e = cudaMemset(w->counter, 0, sizeof(unsigned) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "memset counter");
+        if ((e = cudaMemsetAsync(w->counter, 0, sizeof(unsigned) * 4, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "memset counter");
         if ((e = cudaMalloc(&w->st, sizeof(BiState))) != cudaSuccess) return cuda_fail(ctx, e, "alloc state");
         if ((e = cudaMalloc(&w->flags, sizeof(int) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc flags");
         if ((e = cudaMalloc(&w->dmax, sizeof(double) * 2)) != cudaSuccess) return cuda_fail(ctx, e, "alloc dmax");
@@ -790,6 +859,7 @@ static ewg_status bicgstab(ewg_ctx* ctx, KrylovWs<T>& w, const ewg_solve_opts* o
     init.maxRes = o->linear_solver_max_error;
     init.maxIter = maxIter;
     init.restartOnBreakdown = o->restart_on_breakdown;
+    init.verifyTrue = o->verify_true_residual;
     init.w = o->preconditioner_relaxation;
     if ((e = cudaMemcpyAsync(sw->st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "upload state");
@@ -821,8 +891,15 @@ static ewg_status bicgstab(ewg_ctx* ctx, KrylovWs<T>& w, const ewg_solve_opts* o
         if ((e = cudaMemcpyAsync(sw->h_st, sw->st, sizeof(BiState), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
             return cuda_fail(ctx, e, "read state");
         if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync bicgstab");
+        if (sw->h_st->status == ST_CONVERGED && o->verify_true_residual && sw->h_st->replacements < 3) {
+            auto kfn = k_bicg_true_residual<T, T>;
+            EWG_LAUNCH(ctx, K_BICG_TRUE_RESIDUAL, kfn, G, kSolBlock, P, A, w.b, w.x, w.r, w.r0, w.v, w.p, sw->st, part, cnt);
+            if ((e = cudaMemcpyAsync(sw->h_st, sw->st, sizeof(BiState), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+                return cuda_fail(ctx, e, "read state");
+            if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sync true residual");
+        }
         if (sw->h_st->status != ST_RUNNING) break;
-        if (++guard > maxIter + 2) { ctx->err = "bicgstab: status never left RUNNING"; return EWG_ERR_TIMEOUT; }
+        if (++guard > maxIter + 8) { ctx->err = "bicgstab: status never left RUNNING"; return EWG_ERR_TIMEOUT; }
     }
     const BiState& hs = *sw->h_st;
     *itersOut = hs.iter;

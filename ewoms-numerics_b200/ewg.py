@@ -73,7 +73,7 @@ class SolveOpts(C.Structure):
                 ("preconditioner_relaxation", C.c_double),
                 ("defect_tolerance", C.c_double), ("inner_tolerance", C.c_double),
                 ("max_defect_iterations", C.c_int32), ("check_interval", C.c_int32),
-                ("restart_on_breakdown", C.c_int32)]
+                ("restart_on_breakdown", C.c_int32), ("verify_true_residual", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -106,7 +106,8 @@ def default_solve_opts(**kw) -> SolveOpts:
                   linear_solver_tolerance=1e-10, linear_solver_abs_tolerance=1e-10,
                   linear_solver_max_error=1e7, linear_solver_max_iterations=1000,
                   preconditioner_relaxation=1.0, defect_tolerance=0.0, inner_tolerance=1e-4,
-                  max_defect_iterations=50, check_interval=0, restart_on_breakdown=1)
+                  max_defect_iterations=50, check_interval=0, restart_on_breakdown=1,
+                  verify_true_residual=1)
     for k, v in kw.items():
         setattr(o, k, v)
     return o
@@ -468,8 +469,9 @@ class Context:
         """The cudaStream_t (as an integer handle) all work of this context runs on."""
         return self.lib.ewg_get_stream(self.h)
 
-    def profile_enable(self, on=True):
-        self._check(self.lib.ewg_profile_enable(self.h, int(on)), "profile_enable")
+    def profile_enable(self, on=True, period=1):
+        """Time kernel launches with CUDA events: every `period`-th launch of each class."""
+        self._check(self.lib.ewg_profile_enable(self.h, int(period) if on else 0), "profile_enable")
 
     def profile_reset(self):
         self._check(self.lib.ewg_profile_reset(self.h), "profile_reset")

@@ -121,11 +121,14 @@ typedef struct ewg_solve_opts {
     int32_t restart_on_breakdown;     /* 1: when |r0hat . r| <= 1e-12 |r0hat| |r| at the top of an
                                          iteration, restart with r0hat = r (x kept). 0: exactly the
                                          reference, which then breaks down (EWG_ERR_BREAKDOWN) */
+    int32_t verify_true_residual;     /* 1: on convergence recompute b - A x; if it misses the
+                                         criterion by more than 10x, continue from x with the true
+                                         residual (at most 3 replacements). 0: exactly the reference */
 } ewg_solve_opts;
 
 typedef struct ewg_solve_report {
     int32_t converged;
-    int32_t restarts;                 /* shadow-residual restarts taken */
+    int32_t restarts;                 /* shadow-residual restarts and residual replacements */
     int32_t iterations;               /* BiCGStab iterations (sum over defect-correction passes) */
     int32_t outer_iterations;         /* defect-correction passes (1 for FP64) */
     int32_t status;                   /* ewg_status of the solve */
@@ -242,8 +245,9 @@ void* ewg_get_stream(ewg_ctx* ctx);
 /* Kernel classes: count and names. */
 int32_t ewg_profile_num_kernels(void);
 const char* ewg_profile_kernel_name(int32_t id);
-/* Per-kernel-class device time: with profiling on, every launch is bracketed by a CUDA event pair
- * on the context stream. Launches are always counted. */
+/* Per-kernel-class device time: with profiling on, launches are bracketed by a CUDA event pair
+ * on the context stream: every launch for on == 1, every on-th launch of each class for on > 1
+ * (the reported time is then scaled to all launches). Launches are always counted. */
 ewg_status ewg_profile_enable(ewg_ctx* ctx, int32_t on);
 ewg_status ewg_profile_reset(ewg_ctx* ctx);
 ewg_status ewg_profile_get(ewg_ctx* ctx, int32_t id, double* ms_total, int64_t* launches);

@@ -777,9 +777,12 @@ static double dot(const std::vector<double>& a, const std::vector<double>& b) {
 // t == y) and the criterion update order.
 // Extension (off = exactly the reference): when the shadow residual has become orthogonal to
 // the residual (|r0hat . r| <= 1e-12 |r0hat| |r|), restart with r0hat = r, keeping x.
+// Second extension (off = exactly the reference): on convergence the true residual b - A x is
+// recomputed; if it misses the criterion by more than a factor 10 (the recursively updated
+// residual has drifted), the iteration continues from x with r = r0hat = b - A x (at most 3 times).
 static bool bicgstab(const Bcrs& A, Precond& M, const std::vector<double>& b, std::vector<double>& x,
-                     Criterion& crit, int maxIter, bool restartOnBreakdown, int* iters,
-                     int* restarts) {
+                     Criterion& crit, int maxIter, bool restartOnBreakdown, bool verifyTrue,
+                     int* iters, int* restarts) {
     const double breakdownEps = std::numeric_limits<double>::min() * 1e10;
     const int64_t n2 = (int64_t)b.size();
     x.assign(n2, 0.0);
@@ -793,6 +796,23 @@ static bool bicgstab(const Bcrs& A, Precond& M, const std::vector<double>& b, st
     double rho = 1.0, alpha = 1.0, omega = 1.0;
     std::vector<double> v(n2, 0.0), p(n2, 0.0), y(n2, 0.0), z(n2, 0.0);
     std::vector<double>& h = x; std::vector<double>& s = r; std::vector<double>& t = y;
+    int replacements = 0;
+    // true-residual check; returns true when the iteration must go on from the replaced residual
+    auto replaceResidual = [&]() -> bool {
+        if (!verifyTrue || replacements >= 3) return false;
+        std::vector<double> ax(n2);
+        A.mv(x.data(), ax.data());
+        double err = 0.0;
+        for (int64_t i = 0; i < n2; ++i) { r[i] = b[i] - ax[i]; err = std::max(err, std::abs(r[i])); }
+        if (err / std::max(1e-20, crit.initResErr) <= 10 * crit.relTol || err <= 10 * crit.absTol) return false;
+        ++replacements;
+        ++*restarts;
+        r0hat = r; r0r0 = dot(r, r);
+        rho = 1.0; alpha = 1.0; omega = 1.0;
+        std::fill(v.begin(), v.end(), 0.0); std::fill(p.begin(), p.end(), 0.0);
+        crit.lastResErr = crit.resErr; crit.resErr = err; crit.stagnates = false;
+        return true;
+    };
     int it = 0;
     for (; it < maxIter; ++it) {
         double rho_i = dot(r0hat, r);
@@ -825,7 +845,10 @@ static bool bicgstab(const Bcrs& A, Precond& M, const std::vector<double>& b, st
             tmp = v[i]; tmp *= alpha; s[i] -= tmp;
         }
         crit.updateErrors(y.data(), s.data(), n2);
-        if (crit.converged()) { *iters = it; return true; }
+        if (crit.converged()) {
+            if (!replaceResidual()) { *iters = it; return true; }
+            continue;
+        }
         if (crit.failed()) { *iters = it; return false; }
         z = s;
         M.apply(s.data(), z.data());
@@ -836,7 +859,10 @@ static bool bicgstab(const Bcrs& A, Precond& M, const std::vector<double>& b, st
         if (std::abs(omega) <= breakdownEps) throw BreakdownError("Breakdown of the BiCGStab solver (stagnation detected)");
         for (int64_t i = 0; i < n2; ++i) x[i] += omega * z[i];
         crit.updateErrors(z.data(), r.data(), n2);
-        if (crit.converged()) { *iters = it; return true; }
+        if (crit.converged()) {
+            if (!replaceResidual()) { *iters = it; return true; }
+            continue;
+        }
         if (crit.failed()) { *iters = it; return false; }
         for (int64_t i = 0; i < n2; ++i) r[i] += -omega * t[i];
     }
@@ -967,7 +993,7 @@ int orc_solve(orc_ctx* o, const ewg_solve_opts* so, int ordering, double* dx, in
         std::vector<double> x;
         int it = 0, restarts = 0;
         bool ok = bicgstab(A, M, C.resid, x, crit, so->linear_solver_max_iterations,
-                           so->restart_on_breakdown != 0, &it, &restarts);
+                           so->restart_on_breakdown != 0, so->verify_true_residual != 0, &it, &restarts);
         if (dx) std::memcpy(dx, x.data(), sizeof(double) * x.size());
         if (iterations) *iterations = it;
         if (finalRes) *finalRes = crit.resErr;

@@ -41,8 +41,11 @@ def test_missing_parameter_file_rejected(driver, tmp_path):
 def test_driver_ten_steps_match_oracle(driver, tmp_path, preset):
     gold = np.load(os.path.join(ROOT, "tests", "golden", "lens2d_golden.npz"))
     outf = tmp_path / "x.bin"
+    # the golden run uses a fixed dt = 250 s; with NewtonTargetIterations = 18 the reference's
+    # suggestTimeStepSize never shrinks the step below MaxTimeStepSize (newtonmethod.hh:527-544)
     out = subprocess.run([driver, f"--preset={preset}", "--end-time=2500", "--initial-time-step-size=250",
-                          "--max-time-step-size=250", f"--output={outf}"], capture_output=True, text=True)
+                          "--max-time-step-size=250", "--newton-target-iterations=18", f"--output={outf}"],
+                         capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     steps = [ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]
     assert len(steps) == 10

@@ -259,3 +259,20 @@ def test_mixed_precision_newton(ewg_mod):
     a, b = c64.get_solution(0), c32.get_solution(0)
     assert rel_close(b[:, 0], a[:, 0], 1e-8)[0]
     assert np.max(np.abs(b[:, 1] - a[:, 1])) <= 1e-6
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+def test_repeated_import_and_solve_is_bitwise_reproducible(ewg_mod, oracle_mod, precond):
+    """Fresh contexts on recycled device memory: the imported matrix and the whole BiCGStab run
+    are stream-ordered and deterministic, so repeated runs agree bit for bit."""
+    case = _cases(ewg_mod)["lens3d_16x12x10"]()
+    outs = []
+    for _ in range(4):
+        ctx, o = _system(ewg_mod, oracle_mod, case, 21)
+        rep = ctx.solve(ewg_mod.default_solve_opts(precond=precond, linear_solver_max_iterations=2000))
+        outs.append((rep.iterations, ctx.update()))
+        ctx.close()
+    for it, dx in outs[1:]:
+        assert it == outs[0][0] and np.array_equal(dx, outs[0][1])
+    res = o.apply_jacobian(outs[0][1]) - o.residual()
+    assert np.max(np.abs(res)) <= 1e-8 * np.max(np.abs(o.residual())) + 1e-9
