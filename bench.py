@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
     return ap.parse_args()
 
 
@@ -157,6 +158,14 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------------------------
 # algorithmic bytes per kernel launch (FP64 s = 8, FP32 s = 4); see DESIGN.md
+
+
+def mixed_opts(ewg):
+    """The mixed-precision form: FP32 Jacobian, ILU(0) and BiCGStab solve each Newton correction
+    to a relative 1e-3 (the reference's default LinearSolverTolerance) inside the FP64 defect
+    check; residual, update and the Newton test (1e-8) stay FP64."""
+    return ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-3,
+                                  inner_tolerance=1e-3, max_defect_iterations=3)
 
 
 def geometry(n):
@@ -300,7 +309,7 @@ def run_ours(args, rank, world, local, pg):
     ctx = ewg.Context(case)
     ctx.apply_initial_solution()
 
-    def one_step(dt=250.0):
+    def one_step(dt=250.0, sopts=sopts):
         h = dt
         for _ in range(10):
             st, rep = ctx.newton_apply(h, nopts, sopts)
@@ -336,9 +345,42 @@ def run_ours(args, rank, world, local, pg):
     ms_local = ev0.elapsed_time(ev1)
     prof = ctx.profile()
     ctx.profile_enable(False)
+    x_plain = ctx.get_solution(0)
     ms = max_over_ranks(pg, ms_local)
     total_cells = sum_over_ranks(pg, float(N))
     value = total_cells * args.steps / (ms * 1e-3) / 1e6
+
+    # ---- the other forms on the same K steps (replayed from the snapshot) ----
+    forms = {}
+    if not args.no_forms:
+        variants = {
+            # the reference's own default linear tolerance (LinearSolverTolerance 1e-3,
+            # fvbasediscretization.hh:249) with the FP64 solver
+            "fp64_reference_linear_tol": ewg.default_solve_opts(linear_solver_tolerance=1e-3),
+            # FP32 Jacobian / ILU / BiCGStab, FP64 residual, update and Newton test
+            "mixed": mixed_opts(ewg),
+        }
+        for fname, fo in variants.items():
+            ctx.set_solution(1, snap1)
+            ctx.set_solution(0, snap0)
+            torch.cuda.synchronize()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            freps = [one_step(sopts=fo) for _ in range(args.steps)]
+            f1.record(stream)
+            torch.cuda.synchronize()
+            f_ms = max_over_ranks(pg, f0.elapsed_time(f1))
+            xf = ctx.get_solution(0)
+            forms[fname] = {"s_per_step": f_ms / args.steps / 1e3,
+                            "mcells_per_s": total_cells * args.steps / (f_ms * 1e-3) / 1e6,
+                            "newton_its": [r.iterations for r in freps],
+                            "linear_its": [r.linear_iterations for r in freps],
+                            "max_rel_dpw_vs_plain": float(np.max(np.abs(xf[:, 0] - x_plain[:, 0])) / np.max(np.abs(x_plain[:, 0]))),
+                            "max_abs_dSn_vs_plain": float(np.max(np.abs(xf[:, 1] - x_plain[:, 1]))),
+                            "speedup_vs_plain": ms / f_ms}
+        ctx.set_solution(1, x_plain)
+        ctx.set_solution(0, x_plain)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
@@ -427,7 +469,7 @@ def run_ours(args, rank, world, local, pg):
                     "update": sum(r.t_update for r in reps) / len(reps)},
         "roofline": roofline, "linearization": lin, "bicgstab": bicg,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "gpu_launches": launches, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+        "gpu_launches": launches, "e2e": e2e, "forms": forms, "cpu_baseline": cpu, "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     ctx.close()

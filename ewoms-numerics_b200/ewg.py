@@ -323,6 +323,21 @@ def load(path: str = LIB_PATH):
         "ewg_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
         "ewg_profile_reset": (C.c_int, [C.c_void_p]),
         "ewg_profile_get": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(C.c_int64)]),
+        "ewg_net_num_params": (C.c_int64, []),
+        "ewg_net_create": (C.c_int, [C.c_uint64, P(C.c_void_p)]),
+        "ewg_net_destroy": (None, [C.c_void_p]),
+        "ewg_net_last_error": (C.c_char_p, [C.c_void_p]),
+        "ewg_net_get_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int64]),
+        "ewg_net_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int64]),
+        "ewg_net_set_scales": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_net_get_scales": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_net_eval_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                        P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float)]),
+        "ewg_net_record_sample": (C.c_int, [C.c_void_p, C.c_void_p, d]),
+        "ewg_net_num_samples": (C.c_int64, [C.c_void_p]),
+        "ewg_net_train": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int32, C.c_float, P(C.c_float)]),
+        "ewg_net_eval_samples": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int32, P(C.c_float)]),
+        "ewg_predict_guess": (C.c_int, [C.c_void_p, C.c_void_p, d, P(C.c_int32), P(d), P(d)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -504,3 +519,119 @@ class Context:
             self.advance_time_level()
             reports.append(rep)
         return reports
+
+
+# ------------------------------------------------------------------------------------------
+# learned Newton initial guess
+
+NET_CIN = (16, 32, 32, 32)
+NET_COUT = (32, 32, 32, 8)
+NET_CIN_REAL = (5, 32, 32, 32)
+NET_COUT_REAL = (32, 32, 32, 2)
+
+
+def net_layout():
+    """[(w_offset, b_offset, cin_pad, cout_pad)] of the flat FP32 parameter vector."""
+    out, off = [], 0
+    for ci, co in zip(NET_CIN, NET_COUT):
+        w = off
+        off += 27 * co * ci
+        out.append((w, off, ci, co))
+        off += co
+    return out
+
+
+class GuessNet:
+    """The learned initial-guess network (ewg_net): device training and inference."""
+
+    def __init__(self, seed: int = 0):
+        lib = load()
+        self.lib = lib
+        h = C.c_void_p()
+        st = lib.ewg_net_create(seed, C.byref(h))
+        if st != EWG_OK:
+            raise EwgError(st, "ewg_net_create")
+        self.h = h
+        self.n_params = lib.ewg_net_num_params()
+
+    def _check(self, st, what):
+        if st != EWG_OK:
+            raise EwgError(st, f"{what}: {self.lib.ewg_net_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ewg_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        self._check(self.lib.ewg_net_get_params(self.h, _ptr(p, C.c_float), self.n_params), "get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self.lib.ewg_net_set_params(self.h, _ptr(p, C.c_float), self.n_params), "set_params")
+
+    def scales(self) -> np.ndarray:
+        s = np.zeros(8)
+        self._check(self.lib.ewg_net_get_scales(self.h, _ptr(s)), "get_scales")
+        return s
+
+    def set_scales(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        self._check(self.lib.ewg_net_set_scales(self.h, _ptr(s)), "set_scales")
+
+    def eval_host(self, feats, targets=None, grads=False):
+        """feats [B, D, H, W, 5] float32 -> (outputs [B, D, H, W, 2], loss, grads or None)."""
+        feats = np.ascontiguousarray(feats, dtype=np.float32)
+        B, D, H, W, _ = feats.shape
+        out = np.zeros((B, D, H, W, 2), dtype=np.float32)
+        loss = C.c_float()
+        g = np.zeros(self.n_params, dtype=np.float32) if grads else None
+        t = None if targets is None else np.ascontiguousarray(targets, dtype=np.float32)
+        st = self.lib.ewg_net_eval_host(self.h, B, D, H, W, _ptr(feats, C.c_float),
+                                        None if t is None else _ptr(t, C.c_float), _ptr(out, C.c_float),
+                                        C.byref(loss), None if g is None else _ptr(g, C.c_float))
+        self._check(st, "eval_host")
+        return out, loss.value, g
+
+    def record(self, ctx: "Context", dt: float):
+        self._check(self.lib.ewg_net_record_sample(self.h, ctx.h, dt), "record_sample")
+
+    @property
+    def n_samples(self) -> int:
+        return self.lib.ewg_net_num_samples(self.h)
+
+    def train(self, idx, lr=1e-3) -> float:
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        loss = C.c_float()
+        self._check(self.lib.ewg_net_train(self.h, _ptr(idx, C.c_int64), len(idx), lr, C.byref(loss)), "train")
+        return loss.value
+
+    def eval_samples(self, idx) -> float:
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        loss = C.c_float()
+        self._check(self.lib.ewg_net_eval_samples(self.h, _ptr(idx, C.c_int64), len(idx), C.byref(loss)), "eval")
+        return loss.value
+
+    def save(self, path):
+        np.savez_compressed(path, params=self.params(), scales=self.scales())
+
+    def load_file(self, path):
+        z = np.load(path)
+        self.set_scales(z["scales"])
+        self.set_params(z["params"])
+
+    def predict_guess(self, ctx: "Context", dt: float):
+        """Writes solution(0) of ctx; returns (used_guess, residual of guess, residual of previous)."""
+        used = C.c_int32()
+        rg, rp = C.c_double(), C.c_double()
+        st = self.lib.ewg_predict_guess(ctx.h, self.h, dt, C.byref(used), C.byref(rg), C.byref(rp))
+        ctx._check(st, "predict_guess")
+        return bool(used.value), rg.value, rp.value

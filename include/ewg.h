@@ -237,6 +237,40 @@ ewg_status ewg_newton_update(ewg_ctx* ctx);
 ewg_status ewg_newton_apply(ewg_ctx* ctx, double dt, const ewg_newton_opts* nopts,
                             const ewg_solve_opts* sopts, ewg_newton_report* report);
 
+/* ---- learned Newton initial guess (no reference counterpart; the hook is where the reference
+ * copies solution(1) into solution(0), fvbasediscretization.hh:1396-1407 / updateBegin :1311) ---
+ *
+ * A 4-layer 3x3x3 convolutional network (channels 5 -> 32 -> 32 -> 32 -> 2, ReLU between layers),
+ * BF16 weights and activations with FP32 accumulation, trained on the device by its own forward
+ * and backward kernels on samples recorded from converged simulator steps. */
+typedef struct ewg_net ewg_net;
+int64_t ewg_net_num_params(void);
+ewg_status ewg_net_create(uint64_t seed, ewg_net** out);
+void ewg_net_destroy(ewg_net* net);
+const char* ewg_net_last_error(const ewg_net* net);
+/* FP32 master parameters: per layer W[27][Cout_pad][Cin_pad] then b[Cout_pad], with Cin_pad
+ * 16/32/32/32 and Cout_pad 32/32/32/8 (padded entries are zero). */
+ewg_status ewg_net_get_params(ewg_net* net, float* params, int64_t count);
+ewg_status ewg_net_set_params(ewg_net* net, const float* params, int64_t count);
+/* Input / output normalisation: {p scale, lnK mean, lnK scale, porosity mean, porosity scale,
+ * dt scale, dp_w scale, dS_n scale}. */
+ewg_status ewg_net_set_scales(ewg_net* net, const double* scales8);
+ewg_status ewg_net_get_scales(ewg_net* net, double* scales8);
+/* Forward (and with grads != NULL backward) on host data: features [B][D][H][W][5], targets
+ * [..][2] (nullable), outputs [..][2]; loss = mean squared error. For tests and tooling. */
+ewg_status ewg_net_eval_host(ewg_net* net, int32_t B, int32_t D, int32_t H, int32_t W, const float* features,
+                             const float* targets, float* outputs, float* loss, float* grads);
+/* Record the converged step held by ctx (solution(1) -> solution(0), step size dt) as a sample. */
+ewg_status ewg_net_record_sample(ewg_net* net, ewg_ctx* ctx, double dt);
+int64_t ewg_net_num_samples(const ewg_net* net);
+/* Adam steps over the given recorded samples (one sample per step); mean loss out. */
+ewg_status ewg_net_train(ewg_net* net, const int64_t* sample_idx, int32_t steps, float lr, float* mean_loss);
+ewg_status ewg_net_eval_samples(ewg_net* net, const int64_t* sample_idx, int32_t count, float* mean_loss);
+/* Predict solution(0) for the step of size dt from solution(1); keep the prediction only if its
+ * residual max-norm does not exceed that of solution(1), else solution(0) = solution(1). */
+ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* net, double dt, int32_t* used_guess, double* res_guess,
+                             double* res_prev);
+
 /* ---- instrumentation (no reference counterpart; the analogue of the reference's phase timers,
  * newtonmethod.hh:488-500) --------------------------------------------------------------- */
 

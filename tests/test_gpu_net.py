@@ -1,0 +1,97 @@
+"""GPU tests of the learned initial-guess network: the device forward pass and gradients against
+the FP64 NumPy oracle (BF16 weights / activations / gradients, FP32 accumulation: outputs within
+3e-2 relative to the output scale, gradient direction cosine > 0.995 and norm within 5 %), the
+training loop, and the fallback semantics of ewg_predict_guess."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_params(ewg, rng, scale=0.3):
+    p = np.zeros(ewg.GuessNet().n_params, dtype=np.float32)
+    for (w, b, ci, co), cir, cor in zip(ewg.net_layout(), ewg.NET_CIN_REAL, ewg.NET_COUT_REAL):
+        W = np.zeros((27, co, ci), dtype=np.float32)
+        W[:, :cor, :cir] = rng.normal(0, scale / np.sqrt(27 * cir) * 3, size=(27, cor, cir))
+        p[w:b] = W.ravel()
+        p[b:b + cor] = rng.normal(0, 0.05, size=cor)
+    return p
+
+
+def _bf16(a):
+    """Round to bfloat16 (nearest even) and back."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("shape", [(1, 4, 5, 6), (2, 5, 6, 7)])
+def test_forward_and_gradients_match_oracle(ewg_mod, shape):
+    import net_oracle
+    rng = np.random.default_rng(1)
+    net = ewg_mod.GuessNet(seed=3)
+    p = _random_params(ewg_mod, rng)
+    net.set_params(p)
+    B, D, H, W = shape
+    f = rng.normal(size=(B, D, H, W, 5)).astype(np.float32)
+    t = rng.normal(size=(B, D, H, W, 2)).astype(np.float32)
+    y, loss, g = net.eval_host(f, t, grads=True)
+    # the oracle sees the BF16-rounded weights and inputs the device uses
+    pb = _bf16(p).astype(np.float64)
+    for (w, b, ci, co) in ewg_mod.net_layout():
+        pb[b:b + co] = p[b:b + co]  # biases stay FP32 on the device
+    lo, yo, go = net_oracle.loss_and_grads(pb, _bf16(f).astype(np.float64), t.astype(np.float64))
+    scale = np.max(np.abs(yo))
+    assert np.max(np.abs(y - yo)) <= 3e-2 * scale, (np.max(np.abs(y - yo)), scale)
+    assert loss == pytest.approx(lo, rel=3e-2)
+    cos = float(g @ go / (np.linalg.norm(g) * np.linalg.norm(go)))
+    assert cos > 0.995, cos
+    assert abs(np.linalg.norm(g) / np.linalg.norm(go) - 1) < 0.05
+    # per layer too: every layer's gradient points the same way
+    for (w, b, ci, co) in ewg_mod.net_layout():
+        gl, gol = g[w:b], go[w:b]
+        assert float(gl @ gol / (np.linalg.norm(gl) * np.linalg.norm(gol) + 1e-30)) > 0.99
+
+
+def test_training_reduces_loss(ewg_mod):
+    """Fit a smooth local map of the inputs: the loss must drop by an order of magnitude."""
+    case = ewg_mod.lens3d_case(16, 16, 16, seed=4)
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    net = ewg_mod.GuessNet(seed=0)
+    # record a few real simulator steps (solution(1) -> solution(0))
+    for k in range(4):
+        st, rep = ctx.newton_apply(100.0)
+        assert st == 0
+        net.record(ctx, 100.0)
+        ctx.advance_time_level()
+    idx = np.arange(net.n_samples)
+    l0 = net.eval_samples(idx)
+    for _ in range(60):
+        net.train(idx, lr=2e-3)
+    l1 = net.eval_samples(idx)
+    assert l1 < 0.5 * l0, (l0, l1)
+
+
+def test_guess_fallback_keeps_previous_solution(ewg_mod):
+    """An untrained network predicts garbage: the guess is rejected and solution(0) stays the
+    previous solution; with a zero network the guess equals the previous solution and is kept."""
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=6)
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    st, rep = ctx.newton_apply(100.0)
+    assert st == 0
+    ctx.advance_time_level()
+    x1 = ctx.get_solution(1)
+    net = ewg_mod.GuessNet(seed=1)
+    p = net.params()
+    rng = np.random.default_rng(0)
+    net.set_params(p + rng.normal(0, 1.0, size=p.shape).astype(np.float32) * (p != 0))
+    used, rg, rp = net.predict_guess(ctx, 100.0)
+    assert not used and rg > rp
+    assert np.array_equal(ctx.get_solution(0), x1)
+    net.set_params(np.zeros_like(p))
+    used, rg, rp = net.predict_guess(ctx, 100.0)
+    assert used and rg == rp
+    assert np.array_equal(ctx.get_solution(0), x1)
