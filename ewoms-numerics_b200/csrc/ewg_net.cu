@@ -209,27 +209,38 @@ __global__ void k_targets(const __grid_constant__ Phys P, const double2* __restr
     }
 }
 
-// x_guess = x_prev + de-normalised prediction; S_n of the guess kept in [0, 1]
+// x_guess = x_prev + de-normalised prediction. The saturation increment is applied where it
+// exceeds snThreshold (S_n kept in [0, 1]); the pressure increment only with applyPressure: a
+// local network's pressure error raises the residual of the stiff pressure equation, while the
+// saturation near the front is what costs Newton iterations.
 __global__ void k_apply_guess(const __grid_constant__ Phys P, const double2* __restrict__ xprev, const float* __restrict__ pred,
-                              double tp, double ts, double2* __restrict__ xguess) {
+                              double tp, double ts, int applyPressure, double snThreshold, double2* __restrict__ xguess) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < P.N; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = split_of(P, c);
         const double2 a = xprev[s];
-        const double sn = fmin(fmax((1.0 - a.y) + (double)pred[2 * c + 1] * ts, 0.0), 1.0);
-        xguess[s] = make_double2(a.x + (double)pred[2 * c] * tp, 1.0 - sn);
+        double dsn = (double)pred[2 * c + 1] * ts;
+        if (fabs(dsn) < snThreshold) dsn = 0.0;
+        const double sn = fmin(fmax((1.0 - a.y) + dsn, 0.0), 1.0);
+        const double dp = applyPressure ? (double)pred[2 * c] * tp : 0.0;
+        xguess[s] = make_double2(a.x + dp, 1.0 - sn);
     }
 }
 
-// MSE over the two outputs; gradient 2 (y - t) / count into channels 0..1 of dY (16 wide, BF16)
+// Weighted MSE over the two outputs, sum_v (w0 e0^2 + w1 e1^2) / (2 V); gradient into channels
+// 0..1 of dY (16 wide, BF16)
+// Cells of the plume and its front (S_n of the input above 1e-3, or a saturation target above
+// 0.05 in normalised units) weigh wFront times more: elsewhere the saturation increment is zero.
 __global__ void k_mse(int64_t V, const float* __restrict__ y, const float* __restrict__ t, __nv_bfloat16* __restrict__ dY,
-                      float* __restrict__ loss) {
+                      float* __restrict__ loss, float w0, float w1, const __nv_bfloat16* __restrict__ feat, float wFront) {
     float l = 0.f;
     const float inv = 1.f / (float)(2 * V);
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
         const float e0 = y[2 * v] - t[2 * v], e1 = y[2 * v + 1] - t[2 * v + 1];
-        l += e0 * e0 + e1 * e1;
+        const bool front = __bfloat162float(feat[v * 16 + 1]) > 1e-3f || fabsf(t[2 * v + 1]) > 0.05f;
+        const float wf = front ? wFront : 1.f;
+        l += wf * (w0 * e0 * e0 + w1 * e1 * e1);
         __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(dY + v * 16);
-        o[0] = __floats2bfloat162_rn(2.f * e0 * inv, 2.f * e1 * inv);
+        o[0] = __floats2bfloat162_rn(2.f * wf * w0 * e0 * inv, 2.f * wf * w1 * e1 * inv);
         for (int k = 1; k < 8; ++k) o[k] = __floats2bfloat162_rn(0.f, 0.f);
     }
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
@@ -292,6 +303,10 @@ struct ewg_net {
     int64_t capV = 0;
     FeatureScales fs{1e4, std::log(9.05e-12), 2.0, 0.4, 0.1, 250.0};
     double tp = 100.0, ts = 0.01;         // output scales (Pa, saturation)
+    float lossW[2] = {1.f, 1.f};          // loss weights of the two outputs
+    float wFront = 1.f;                   // extra loss weight of plume / front cells
+    int applyPressure = 0;                // guess mode: apply the predicted pressure increment
+    double snThreshold = 0.0;             // guess mode: ignore |dS_n| below this
     // recorded training samples (features BF16 [V][16], targets FP32 [V][2]) per volume
     struct Sample { __nv_bfloat16* f; float* t; int D, H, W; };
     std::vector<Sample> samples;
@@ -481,6 +496,17 @@ ewg_status ewg_net_set_scales(ewg_net* n, const double* s /* pScale, lnKMean, ln
     return EWG_OK;
 }
 
+ewg_status ewg_net_set_options(ewg_net* n, float lossWeightP, float lossWeightS, int32_t applyPressure,
+                               double snThreshold) {
+    if (!n || lossWeightP < 0 || lossWeightS < 0 || snThreshold < 0) return EWG_ERR_INVALID;
+    n->wFront = lossWeightS > 1.f ? lossWeightS : 1.f;
+    n->lossW[0] = lossWeightP;
+    n->lossW[1] = lossWeightS;
+    n->applyPressure = applyPressure != 0;
+    n->snThreshold = snThreshold;
+    return EWG_OK;
+}
+
 ewg_status ewg_net_get_scales(ewg_net* n, double* s) {
     if (!n || !s) return EWG_ERR_INVALID;
     const double v[8] = {n->fs.pScale, n->fs.lnKMean, n->fs.lnKScale, n->fs.phiMean, n->fs.phiScale, n->fs.dtScale, n->tp, n->ts};
@@ -507,7 +533,7 @@ ewg_status ewg_net_eval_host(ewg_net* n, int32_t B, int32_t D, int32_t H, int32_
         e = cudaMemcpyAsync(n->target, target, sizeof(float) * V * 2, cudaMemcpyHostToDevice, n->stream);
         if (!e) e = cudaMemsetAsync(n->dLoss, 0, sizeof(float), n->stream);
         if (e) return net_fail(n, e, "upload targets");
-        k_mse<<<256, 256, 0, n->stream>>>(V, n->out, n->target, n->grad16, n->dLoss);
+        k_mse<<<256, 256, 0, n->stream>>>(V, n->out, n->target, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
         if (grads) {
             if ((e = cudaMemsetAsync(n->grads, 0, sizeof(float) * n->nParams, n->stream))) return net_fail(n, e, "zero grads");
             backward(n, d);
@@ -561,7 +587,7 @@ ewg_status ewg_net_train(ewg_net* n, const int64_t* sampleIdx, int32_t steps, fl
         if (!e) e = cudaMemsetAsync(n->grads, 0, sizeof(float) * n->nParams, n->stream);
         if (e) return net_fail(n, e, "train setup");
         forward(n, d);
-        k_mse<<<256, 256, 0, n->stream>>>(V, n->out, s.t, n->grad16, n->dLoss);
+        k_mse<<<256, 256, 0, n->stream>>>(V, n->out, s.t, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
         backward(n, d);
         n->adamStep += 1;
         const float b1 = 0.9f, b2 = 0.999f;
@@ -590,7 +616,7 @@ ewg_status ewg_net_eval_samples(ewg_net* n, const int64_t* sampleIdx, int32_t co
         cudaMemcpyAsync(n->act[0], s.f, sizeof(__nv_bfloat16) * d.V() * 16, cudaMemcpyDeviceToDevice, n->stream);
         cudaMemsetAsync(n->dLoss, 0, sizeof(float), n->stream);
         forward(n, d);
-        k_mse<<<256, 256, 0, n->stream>>>(d.V(), n->out, s.t, n->grad16, n->dLoss);
+        k_mse<<<256, 256, 0, n->stream>>>(d.V(), n->out, s.t, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
         float l = 0.f;
         cudaMemcpyAsync(&l, n->dLoss, sizeof(float), cudaMemcpyDeviceToHost, n->stream);
         cudaError_t e = cudaStreamSynchronize(n->stream);
@@ -616,7 +642,7 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* n, double dt, int32_t* usedG
     if ((e = cudaStreamSynchronize(ctx->stream))) return cuda_fail(ctx, e, "sync ctx");
     k_features<<<512, 256, 0, n->stream>>>(P, ctx->x1, ctx->perm, dt, n->fs, n->act[0]);
     forward(n, d);
-    k_apply_guess<<<512, 256, 0, n->stream>>>(P, ctx->x1, n->out, n->tp, n->ts, ctx->x0);
+    k_apply_guess<<<512, 256, 0, n->stream>>>(P, ctx->x1, n->out, n->tp, n->ts, n->applyPressure, n->snThreshold, ctx->x0);
     if ((e = cudaGetLastError())) return cuda_fail(ctx, e, "guess kernels");
     if ((e = cudaStreamSynchronize(n->stream))) return cuda_fail(ctx, e, "sync guess");
     double rg = 0.0, rp = 0.0;

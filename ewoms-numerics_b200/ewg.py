@@ -331,6 +331,7 @@ def load(path: str = LIB_PATH):
         "ewg_net_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int64]),
         "ewg_net_set_scales": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_net_get_scales": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_net_set_options": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_int32, d]),
         "ewg_net_eval_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                         P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float)]),
         "ewg_net_record_sample": (C.c_int, [C.c_void_p, C.c_void_p, d]),
@@ -587,6 +588,10 @@ class GuessNet:
         s = np.ascontiguousarray(s, dtype=np.float64)
         self._check(self.lib.ewg_net_set_scales(self.h, _ptr(s)), "set_scales")
 
+    def set_options(self, loss_weight_p=1.0, loss_weight_s=1.0, apply_pressure=False, sn_threshold=0.0):
+        self._check(self.lib.ewg_net_set_options(self.h, loss_weight_p, loss_weight_s, int(apply_pressure),
+                                                 sn_threshold), "set_options")
+
     def eval_host(self, feats, targets=None, grads=False):
         """feats [B, D, H, W, 5] float32 -> (outputs [B, D, H, W, 2], loss, grads or None)."""
         feats = np.ascontiguousarray(feats, dtype=np.float32)
@@ -620,13 +625,17 @@ class GuessNet:
         self._check(self.lib.ewg_net_eval_samples(self.h, _ptr(idx, C.c_int64), len(idx), C.byref(loss)), "eval")
         return loss.value
 
-    def save(self, path):
-        np.savez_compressed(path, params=self.params(), scales=self.scales())
+    def save(self, path, options=None):
+        np.savez_compressed(path, params=self.params(), scales=self.scales(),
+                            options=np.array(options if options is not None else [0.1, 1.0, 0.0, 0.0]))
 
     def load_file(self, path):
         z = np.load(path)
         self.set_scales(z["scales"])
         self.set_params(z["params"])
+        if "options" in z:
+            o = z["options"]
+            self.set_options(float(o[0]), float(o[1]), bool(o[2]), float(o[3]))
 
     def predict_guess(self, ctx: "Context", dt: float):
         """Writes solution(0) of ctx; returns (used_guess, residual of guess, residual of previous)."""

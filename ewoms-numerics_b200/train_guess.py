@@ -119,6 +119,9 @@ def main():
     ap.add_argument("--eval-members", type=int, default=3)
     ap.add_argument("--out", default=os.path.join(HERE, "data", "guess_net_lens3d.npz"))
     ap.add_argument("--report", default=None)
+    ap.add_argument("--loss-weight-p", type=float, default=0.05)
+    ap.add_argument("--sn-threshold", type=float, default=0.002)
+    ap.add_argument("--front-weight", type=float, default=20.0)
     args = ap.parse_args()
     t0 = time.perf_counter()
 
@@ -127,6 +130,8 @@ def main():
 
     sopts = mixed_opts()
     net = ewg.GuessNet(seed=0)
+    options = [args.loss_weight_p, args.front_weight, 0.0, args.sn_threshold]
+    net.set_options(options[0], options[1], False, options[3])
     tp, ts = estimate_scales(args.n, sopts)
     sc = net.scales()
     sc[6], sc[7] = tp, ts
@@ -152,7 +157,7 @@ def main():
         hist.append((it + len(idx), ltr, lho))
         log(f"iter {it + len(idx)}: train {ltr:.4g} held-out {lho:.4g}")
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
-    net.save(args.out)
+    net.save(args.out, options)
     log(f"saved {args.out}")
     ev = evaluate(net, hold_seeds[:args.eval_members], args.n, args.steps, sopts)
     for e in ev:

@@ -256,6 +256,11 @@ ewg_status ewg_net_set_params(ewg_net* net, const float* params, int64_t count);
  * dt scale, dp_w scale, dS_n scale}. */
 ewg_status ewg_net_set_scales(ewg_net* net, const double* scales8);
 ewg_status ewg_net_get_scales(ewg_net* net, double* scales8);
+/* Training loss weights of (dp_w, dS_n) (a saturation weight above 1 also weighs the cells of the
+ * plume and its front by that factor), and the guess mode: apply_pressure 0 keeps p_w of the
+ * previous solution and applies only the saturation increment, dropping |dS_n| < sn_threshold. */
+ewg_status ewg_net_set_options(ewg_net* net, float loss_weight_p, float loss_weight_s, int32_t apply_pressure,
+                               double sn_threshold);
 /* Forward (and with grads != NULL backward) on host data: features [B][D][H][W][5], targets
  * [..][2] (nullable), outputs [..][2]; loss = mean squared error. For tests and tooling. */
 ewg_status ewg_net_eval_host(ewg_net* net, int32_t B, int32_t D, int32_t H, int32_t W, const float* features,
