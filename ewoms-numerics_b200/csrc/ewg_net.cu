@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -665,3 +666,130 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* n, double dt, int32_t* usedG
 }
 
 }  // extern "C"
+
+// ---- forward pass that allocates nothing ----------------------------------------------------
+//
+// ewg_net_forward_noalloc runs the same four k_conv3d launches as the forward pass of
+// ewg_net_eval_host, for callers that must not allocate device memory: a host simulator that
+// hands all of the device's memory to its own arena up front, code that runs while another
+// thread captures a CUDA graph in global capture mode (cudaMalloc is illegal then), and time-step
+// loops that cannot afford the device-wide synchronisation of cudaMalloc / cudaFree. The caller
+// passes the FP32 parameters, the features and the output on the device; the BF16 weights, the
+// 16-channel BF16 features and two 32-channel activation buffers live in one file-scope device
+// array of fixed size, which every GPU that loads this library holds until the process exits.
+namespace ewg {
+namespace {
+
+constexpr int64_t kNoAllocMaxVoxels = EWG_NET_NOALLOC_MAX_VOXELS;
+constexpr int64_t kNoAllocWeights = (int64_t)kTaps * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 8);
+constexpr size_t kNoAllocOffFeat = (sizeof(__nv_bfloat16) * kNoAllocWeights + 255) / 256 * 256;
+constexpr size_t kNoAllocOffActA = kNoAllocOffFeat + sizeof(__nv_bfloat16) * kNoAllocMaxVoxels * 16;
+constexpr size_t kNoAllocOffActB = kNoAllocOffActA + sizeof(__nv_bfloat16) * kNoAllocMaxVoxels * 32;
+constexpr size_t kNoAllocBytes = kNoAllocOffActB + sizeof(__nv_bfloat16) * kNoAllocMaxVoxels * 32;
+constexpr int kNoAllocMaxDevices = 64;
+
+// The scratch. Its name in host code is only a handle for cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_netScratch[kNoAllocBytes];
+
+std::mutex g_netScratchMutex;
+unsigned char* g_netScratchPtr[kNoAllocMaxDevices] = {};
+
+// features [V][5] FP32 -> [V][16] BF16, channels 5..15 zero (every word of the buffer the
+// convolution reads for these V voxels is written here)
+__global__ void k_pack_features(int64_t V, const float* __restrict__ f5, __nv_bfloat16* __restrict__ f16) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V * 16; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = i >> 4;
+        const int k = (int)(i & 15);
+        f16[i] = __float2bfloat16(k < 5 ? f5[v * 5 + k] : 0.f);
+    }
+}
+
+template <int CIN, int COUT, int EPI>
+cudaError_t noalloc_conv_attr() {
+    return cudaFuncSetAttribute(k_conv3d<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(__nv_bfloat16) * kTaps * COUT * CIN));
+}
+
+template <int CIN, int COUT, int EPI>
+void noalloc_conv(cudaStream_t st, const VolDims& d, const __nv_bfloat16* in, const __nv_bfloat16* W,
+                  const float* bias, void* out, int outC) {
+    const size_t smem = sizeof(__nv_bfloat16) * kTaps * COUT * CIN;
+    const int64_t tiles = (d.V() + 15) / 16;
+    int64_t blocks = (tiles + 3) / 4;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_conv3d<CIN, COUT, EPI><<<(int)blocks, 128, smem, st>>>(d, in, W, bias, nullptr, 0, out, outC);
+}
+
+ewg_status noalloc_fail(char* msg, int32_t len, ewg_status st, const char* text) {
+    if (msg && len > 0) std::snprintf(msg, (size_t)len, "%s", text);
+    return st;
+}
+
+// Once per device, with that device current: the scratch's device address and the kernels'
+// shared-memory limits.
+ewg_status noalloc_setup(int dev, unsigned char** out, char* msg, int32_t len) {
+    std::lock_guard<std::mutex> lock(g_netScratchMutex);
+    if (!g_netScratchPtr[dev]) {
+        unsigned char* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_netScratch);
+        if (e == cudaSuccess) e = noalloc_conv_attr<16, 32, EPI_BIAS_RELU>();
+        if (e == cudaSuccess) e = noalloc_conv_attr<32, 32, EPI_BIAS_RELU>();
+        if (e == cudaSuccess) e = noalloc_conv_attr<32, 8, EPI_BIAS>();
+        if (e != cudaSuccess) {
+            char text[256];
+            std::snprintf(text, sizeof(text), "no-allocation scratch set-up: %s", cudaGetErrorString(e));
+            return noalloc_fail(msg, len, EWG_ERR_CUDA, text);
+        }
+        g_netScratchPtr[dev] = ptr;
+    }
+    *out = g_netScratchPtr[dev];
+    return EWG_OK;
+}
+
+}  // namespace
+}  // namespace ewg
+
+extern "C" ewg_status ewg_net_forward_noalloc(const float* params, int32_t B, int32_t D, int32_t H, int32_t W,
+                                              const float* features, float* outputs, void* stream, char* message,
+                                              int32_t message_len) {
+    if (message && message_len > 0) message[0] = '\0';
+    if (!params || !features || !outputs || B < 1 || D < 1 || H < 1 || W < 1)
+        return noalloc_fail(message, message_len, EWG_ERR_INVALID, "null pointer or non-positive extent");
+    VolDims d{D, H, W, B};
+    const int64_t V = d.V();
+    if (V > kNoAllocMaxVoxels) {
+        char text[256];
+        std::snprintf(text, sizeof(text),
+                      "batch of %lld voxels exceeds the no-allocation limit of %lld voxels (B*D*H*W)",
+                      (long long)V, (long long)kNoAllocMaxVoxels);
+        return noalloc_fail(message, message_len, EWG_ERR_INVALID, text);
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(message, message_len, EWG_ERR_NO_DEVICE, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return noalloc_fail(message, message_len, EWG_ERR_INVALID, "device ordinal above 63");
+    unsigned char* base = nullptr;
+    ewg_status st = noalloc_setup(dev, &base, message, message_len);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    __nv_bfloat16* wf[kNetLayers];
+    int64_t woff = 0, poff = 0, boff[kNetLayers];
+    for (int l = 0; l < kNetLayers; ++l) {
+        wf[l] = reinterpret_cast<__nv_bfloat16*>(base) + woff;
+        k_cast_weights<<<64, 256, 0, s>>>(kCin[l], kCout[l], kCout[l], params + poff, wf[l], nullptr);
+        woff += layer_w(l);
+        boff[l] = poff + layer_w(l);
+        poff = boff[l] + kCout[l];
+    }
+    __nv_bfloat16* feat = reinterpret_cast<__nv_bfloat16*>(base + kNoAllocOffFeat);
+    __nv_bfloat16* actA = reinterpret_cast<__nv_bfloat16*>(base + kNoAllocOffActA);
+    __nv_bfloat16* actB = reinterpret_cast<__nv_bfloat16*>(base + kNoAllocOffActB);
+    k_pack_features<<<256, 256, 0, s>>>(V, features, feat);
+    noalloc_conv<16, 32, EPI_BIAS_RELU>(s, d, feat, wf[0], params + boff[0], actA, 32);
+    noalloc_conv<32, 32, EPI_BIAS_RELU>(s, d, actA, wf[1], params + boff[1], actB, 32);
+    noalloc_conv<32, 32, EPI_BIAS_RELU>(s, d, actB, wf[2], params + boff[2], actA, 32);
+    noalloc_conv<32, 8, EPI_BIAS>(s, d, actA, wf[3], params + boff[3], outputs, 2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(message, message_len, EWG_ERR_CUDA, cudaGetErrorString(e));
+    return EWG_OK;
+}

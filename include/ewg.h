@@ -276,6 +276,27 @@ ewg_status ewg_net_eval_samples(ewg_net* net, const int64_t* sample_idx, int32_t
 ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* net, double dt, int32_t* used_guess, double* res_guess,
                              double* res_prev);
 
+/* Forward pass of the guess network that allocates no memory (no reference counterpart). For
+ * callers that cannot call cudaMalloc: a host simulator whose own arena owns the device's memory,
+ * code running while a CUDA graph is captured in global mode (cudaMalloc is illegal then), and
+ * step loops that cannot take the device-wide synchronisation of cudaMalloc / cudaFree.
+ *   params    device, FP32, the layout of ewg_net_get_params (ewg_net_num_params() floats)
+ *   features  device, FP32 [B][D][H][W][5];  outputs  device, FP32 [B][D][H][W][2]
+ *   stream    cudaStream_t the work is enqueued on (NULL: the legacy default stream); the call
+ *             returns after enqueueing, the outputs are ready once the stream has reached it.
+ *   message   optional buffer of message_len bytes for the reason of a failure.
+ * The intermediate activations and BF16 weights live in one fixed device array of about 10 MB
+ * that every GPU loading this library holds until exit; B*D*H*W above
+ * EWG_NET_NOALLOC_MAX_VOXELS is rejected with EWG_ERR_INVALID. The first call on a device looks
+ * the array up (cudaGetSymbolAddress) and sets kernel attributes: make that first call before
+ * any stream capture. All calls on a device share the array, so calls whose work overlaps on the
+ * GPU (different streams, or different host threads) race and corrupt each other's results:
+ * order them on one stream. Outputs equal those of ewg_net_eval_host for the same parameters. */
+#define EWG_NET_NOALLOC_MAX_VOXELS 65536
+ewg_status ewg_net_forward_noalloc(const float* params, int32_t B, int32_t D, int32_t H, int32_t W,
+                                   const float* features, float* outputs, void* stream, char* message,
+                                   int32_t message_len);
+
 /* ---- instrumentation (no reference counterpart; the analogue of the reference's phase timers,
  * newtonmethod.hh:488-500) --------------------------------------------------------------- */
 
