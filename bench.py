@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--ensemble-members", type=int, default=64)
+    ap.add_argument("--ensemble-steps", type=int, default=3)
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -294,6 +297,69 @@ def run_reference(args, rank, world, pg):
     print(json.dumps(line), flush=True)
 
 
+def ensemble_cases(ewg, members, seed=3):
+    """Batched-ensemble workload: seeded lens realizations with cube grids drawn from
+    {32, 48, 64, 96, 128}^3, sigma in [0.5, 1.5], correlation length in [4, 12] cells and
+    dt in {100, 250, 500} s."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([32, 48, 64, 96, 128], size=members)
+    cases, dts = [], []
+    for m in range(members):
+        n = int(sizes[m])
+        cases.append(ewg.lens3d_case(n, n, n, seed=seed * 1000 + m, sigma=float(rng.uniform(0.5, 1.5)),
+                                     corr_cells=float(rng.uniform(4.0, 12.0))))
+        dts.append(float(rng.choice([100.0, 250.0, 500.0])))
+    return cases, dts
+
+
+def run_ensemble(args, rank, pg, torch, ewg):
+    """The batched ensemble form: every member advances one implicit step per timed step (its own
+    dt, FP64 residual / update / Newton test, FP32 Jacobian, ILU(0) and BiCGStab), all members in
+    the same launches with the BiCGStab iteration replayed from a CUDA graph."""
+    cases, dts = ensemble_cases(ewg, args.ensemble_members, seed=3 + rank)
+    so = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-3,
+                                verify_true_residual=0)
+    ens = ewg.Ensemble(cases, precision=ewg.PRECISION_MIXED)
+    ens.apply_initial_solution()
+    t0 = time.perf_counter()
+    shapes = ens.autotune(dts, so)
+    tune_s = time.perf_counter() - t0
+    ens.apply_initial_solution()
+    ens.advance(1, dts, sopts=so)  # warm-up step
+    stream = torch.cuda.ExternalStream(ens.stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    # every member advances ensemble_steps steps at its own pace
+    st, reps, sts = ens.advance(args.ensemble_steps, dts, sopts=so)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    stats = [(reps, sts)]
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    cells = ens.total_cells
+    total = sum_over_ranks(pg, float(cells))
+    newton = [r.newton_iterations / args.ensemble_steps for reps, _ in stats for r in reps]
+    out = {
+        "workload": f"{len(cases)} lens realizations, cube grids from {{32,48,64,96,128}}^3, {cells} cells, "
+                    f"dt from {{100,250,500}} s, mixed precision (FP32 inner BiCGStab to rel 1e-3, Newton tol 1e-8)",
+        "members": len(cases), "cells": cells, "steps": args.ensemble_steps,
+        "s_per_step": ms / args.ensemble_steps / 1e3,
+        "mcells_steps_per_s": total * args.ensemble_steps / (ms * 1e-3) / 1e6,
+        "newton_iterations_per_step_mean": float(np.mean(newton)),
+        "newton_iterations_per_step_max": float(np.max(newton)),
+        "halvings": int(sum(r.halvings for reps, _ in stats for r in reps)),
+        "rounds": [s.rounds for _, s in stats], "linear_iterations": [s.linear_iterations for _, s in stats],
+        "phase_s": {"linearize": sum(s.t_linearize for _, s in stats) / len(stats),
+                    "solve": sum(s.t_solve for _, s in stats) / len(stats),
+                    "update": sum(s.t_update for _, s in stats) / len(stats)},
+        "launch_shapes": shapes, "autotune_s": tune_s,
+    }
+    ens.close()
+    return out
+
+
 def run_ours(args, rank, world, local, pg):
     import torch
 
@@ -309,9 +375,15 @@ def run_ours(args, rank, world, local, pg):
     ctx = ewg.Context(case)
     ctx.apply_initial_solution()
 
-    def one_step(dt=250.0, sopts=sopts):
+    guess_log = []
+
+    def one_step(dt=250.0, sopts=sopts, net=None):
         h = dt
         for _ in range(10):
+            if net is not None:
+                # the learned initial guess replaces solution(0) only if its residual is smaller
+                used, rg, rp = net.predict_guess(ctx, h)
+                guess_log.append((used, rg, rp))
             st, rep = ctx.newton_apply(h, nopts, sopts)
             if st == ewg.EWG_OK:
                 ctx.advance_time_level()
@@ -353,21 +425,26 @@ def run_ours(args, rank, world, local, pg):
     # ---- the other forms on the same K steps (replayed from the snapshot) ----
     forms = {}
     if not args.no_forms:
+        net = ewg.GuessNet(seed=0)
+        net.load_file(os.path.join(ROOT, "ewoms-numerics_b200", "data", "guess_net_lens3d.npz"))
         variants = {
             # the reference's own default linear tolerance (LinearSolverTolerance 1e-3,
             # fvbasediscretization.hh:249) with the FP64 solver
-            "fp64_reference_linear_tol": ewg.default_solve_opts(linear_solver_tolerance=1e-3),
+            "fp64_reference_linear_tol": (ewg.default_solve_opts(linear_solver_tolerance=1e-3), None),
             # FP32 Jacobian / ILU / BiCGStab, FP64 residual, update and Newton test
-            "mixed": mixed_opts(ewg),
+            "mixed": (mixed_opts(ewg), None),
+            # the same with the learned Newton initial guess (kept only where it lowers the residual)
+            "learned_mixed": (mixed_opts(ewg), net),
         }
-        for fname, fo in variants.items():
+        for fname, (fo, fnet) in variants.items():
             ctx.set_solution(1, snap1)
             ctx.set_solution(0, snap0)
+            guess_log.clear()
             torch.cuda.synchronize()
             f0 = torch.cuda.Event(enable_timing=True)
             f1 = torch.cuda.Event(enable_timing=True)
             f0.record(stream)
-            freps = [one_step(sopts=fo) for _ in range(args.steps)]
+            freps = [one_step(sopts=fo, net=fnet) for _ in range(args.steps)]
             f1.record(stream)
             torch.cuda.synchronize()
             f_ms = max_over_ranks(pg, f0.elapsed_time(f1))
@@ -379,6 +456,10 @@ def run_ours(args, rank, world, local, pg):
                             "max_rel_dpw_vs_plain": float(np.max(np.abs(xf[:, 0] - x_plain[:, 0])) / np.max(np.abs(x_plain[:, 0]))),
                             "max_abs_dSn_vs_plain": float(np.max(np.abs(xf[:, 1] - x_plain[:, 1]))),
                             "speedup_vs_plain": ms / f_ms}
+            if fnet is not None:
+                forms[fname]["guess_used"] = [bool(u) for u, _, _ in guess_log]
+                forms[fname]["guess_residual_ratio"] = [rg / rp if rp > 0 else None for _, rg, rp in guess_log]
+        net.close()
         ctx.set_solution(1, x_plain)
         ctx.set_solution(0, x_plain)
 
@@ -412,6 +493,10 @@ def run_ours(args, rank, world, local, pg):
         e2e = {"value": total_cells * args.steps / (e_ms * 1e-3) / 1e6, "unit": "Mcells/s",
                "h2d_bytes_per_step": 2 * N * 16, "d2h_bytes_per_step": N * 16,
                "ms_per_step": e_ms / args.steps}
+
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = run_ensemble(args, rank, pg, torch, ewg)
 
     if rank != 0:
         ctx.close()
@@ -469,7 +554,8 @@ def run_ours(args, rank, world, local, pg):
                     "update": sum(r.t_update for r in reps) / len(reps)},
         "roofline": roofline, "linearization": lin, "bicgstab": bicg,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "gpu_launches": launches, "e2e": e2e, "forms": forms, "cpu_baseline": cpu, "clocks": clk.summary(),
+        "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "cpu_baseline": cpu,
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     ctx.close()

@@ -136,11 +136,7 @@ void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p) {
     P.nx = g->nx;
     P.ny = g->ny;
     P.nz = g->dim == 3 ? g->nz : 1;
-    P.N = (int64_t)P.nx * P.ny * P.nz;
-    P.Nh = P.N / 2;
-    P.nxh = P.nx / 2;
-    P.planeh = (int64_t)P.nx * P.ny / 2;
-    P.nb = 1 + 2 * P.dim;
+    set_index_constants(P);
     P.L[0] = g->lx;
     P.L[1] = g->ly;
     P.L[2] = g->dim == 3 ? g->lz : 1.0;
@@ -205,6 +201,28 @@ __global__ void k_lens_flags(const __grid_constant__ Phys P, uint8_t* __restrict
         }
         lens[s] = in ? 1 : 0;
     }
+}
+
+// launchers of the layout kernels for a problem that has no context (ensemble members)
+static int layout_grid(const Phys& P) {
+    int64_t g = (P.N + kApiBlock - 1) / kApiBlock;
+    return (int)(g < 4096 ? (g > 0 ? g : 1) : 4096);
+}
+cudaError_t layout_natural_to_split(const Phys& P, cudaStream_t st, const double2* nat, double2* spl) {
+    k_natural_to_split<<<layout_grid(P), kApiBlock, 0, st>>>(P, nat, spl);
+    return cudaGetLastError();
+}
+cudaError_t layout_split_to_natural(const Phys& P, cudaStream_t st, const double2* spl, double2* nat) {
+    k_split_to_natural<<<layout_grid(P), kApiBlock, 0, st>>>(P, spl, nat);
+    return cudaGetLastError();
+}
+cudaError_t layout_scalar_to_split(const Phys& P, cudaStream_t st, const double* nat, double* spl) {
+    k_scalar_to_split<<<layout_grid(P), kApiBlock, 0, st>>>(P, nat, spl);
+    return cudaGetLastError();
+}
+cudaError_t layout_lens_flags(const Phys& P, cudaStream_t st, uint8_t* lens) {
+    k_lens_flags<<<layout_grid(P), kApiBlock, 0, st>>>(P, lens);
+    return cudaGetLastError();
 }
 
 // natural row c of the reference BCRS, columns ascending: the band of each entry
@@ -443,6 +461,7 @@ ewg_status ewg_create(const ewg_grid* grid, const ewg_problem* problem, const do
     if (e != cudaSuccess) return fail("upload permeability");
     {
         ewg_status bst = compute_boundary_constants(ctx);
+        if (bst == EWG_OK) bst = build_interior_tables(ctx);
         if (bst != EWG_OK) { g_createError = ctx->err; ewg_destroy(ctx); return bst; }
     }
     // reference BCRS pattern
@@ -463,7 +482,7 @@ void ewg_destroy(ewg_ctx* ctx) {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     solver_free(ctx);
-    void* ps[] = {ctx->x0, ctx->x1, ctx->sold, ctx->r, ctx->dx, ctx->d_stage, ctx->perm, ctx->lens, ctx->iq, ctx->J, ctx->J32,
+    void* ps[] = {ctx->x0, ctx->x1, ctx->sold, ctx->r, ctx->dx, ctx->d_stage, ctx->perm, ctx->lens, ctx->iq, ctx->J, ctx->J32, ctx->geo,
                   ctx->d_errmax, ctx->d_flags, ctx->d_rowPtr, ctx->d_colIdx};
     for (void* p : ps) if (p) cudaFree(p);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);

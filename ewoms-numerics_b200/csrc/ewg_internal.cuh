@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/ewg.h"
 
@@ -39,6 +40,36 @@ struct LawDev {
     double pe, negInvLambda, krwExp, krnExp, bcLowSw, bcPcLow, bcSlopeLow, bcSlopeOne;
 };
 
+// Division by a run-time invariant divisor d >= 1 for 0 <= n < 2^32 with one multiply-high
+// (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI 1994):
+// q = (t + ((n - t) >> s1)) >> s2 with t = mulhi(m, n), m = floor(2^32 (2^l - d) / d) + 1,
+// l = ceil(log2 d), (s1, s2) = (1, l - 1); d = 1 uses m = 0, s1 = s2 = 0.
+struct FastDiv {
+    uint32_t d, m, s1, s2;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    if (d <= 1) {
+        f.d = 1; f.m = 0; f.s1 = 0; f.s2 = 0;
+        return f;
+    }
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    f.s1 = 1;
+    f.s2 = l - 1;
+    return f;
+}
+__host__ __device__ inline uint32_t fastdiv(const FastDiv& f, uint32_t n) {
+#ifdef __CUDA_ARCH__
+    const uint32_t t = __umulhi(f.m, n);
+#else
+    const uint32_t t = (uint32_t)(((uint64_t)f.m * n) >> 32);
+#endif
+    return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 // Everything a kernel needs about the problem, passed by value.
 struct Phys {
     int dim, nx, ny, nz;
@@ -57,7 +88,35 @@ struct Phys {
     // p_cnw and the phase mobilities k_r / mu
     double bndPc[2];
     double bndLam[2][2];
+    FastDiv fdNxh, fdNy;     // divisions by nx / 2 and ny in cell_of (N < 2^31)
 };
+
+// Geometry of one interior face seen from a cell, per (axis, cell index along the axis, side):
+// the two-point gradient coefficient dA / |dA|^2 with dA = x_j - x_i along the axis
+// (fvbasegradientcalculator.hh:194-240) and, for faces normal to gravity (y), the hydrostatic
+// correction (pStat_j - pStat_i) / |dA|^2 of each phase (darcyfluxmodule.hh:216-290). The values
+// are computed on the host with the same IEEE operations the kernels would use, so reading them
+// from the table gives the same bits as recomputing them per cell.
+struct FaceGeo {
+    double coef, dA, gt[2];
+};
+// Index of (axis, idx, side) in the face-geometry table.
+__host__ __device__ inline int face_geo_index(const int n[3], int axis, int idx, int side) {
+    int off = axis == 0 ? 0 : (axis == 1 ? 2 * n[0] : 2 * (n[0] + n[1]));
+    return off + 2 * idx + side;
+}
+
+// Derived index constants of the split storage order from dim, nx, ny, nz.
+inline void set_index_constants(Phys& P) {
+    if (P.dim == 2) P.nz = 1;
+    P.N = (int64_t)P.nx * P.ny * P.nz;
+    P.Nh = P.N / 2;
+    P.nxh = P.nx / 2;
+    P.planeh = (int64_t)P.nx * P.ny / 2;
+    P.nb = 1 + 2 * P.dim;
+    P.fdNxh = make_fastdiv((uint32_t)P.nxh);
+    P.fdNy = make_fastdiv((uint32_t)P.ny);
+}
 
 struct CellIdx {
     int64_t c;               // natural index
@@ -67,13 +126,15 @@ struct CellIdx {
 
 __host__ __device__ inline CellIdx cell_of(const Phys& P, int col, int64_t h) {
     CellIdx r;
-    int64_t row = h / P.nxh;              // x-row index j + ny*k
-    int64_t hx = h - row * P.nxh;
-    r.j = (int)(row % P.ny);
-    r.k = (int)(row / P.ny);
+    const uint32_t hh = (uint32_t)h;
+    const uint32_t row = fastdiv(P.fdNxh, hh);   // x-row index j + ny*k
+    const uint32_t hx = hh - row * (uint32_t)P.nxh;
+    const uint32_t k = fastdiv(P.fdNy, row);
+    r.j = (int)(row - k * (uint32_t)P.ny);
+    r.k = (int)k;
     r.b = col ^ ((r.j + r.k) & 1);
     r.i = (int)(2 * hx + r.b);
-    r.c = row * P.nx + r.i;
+    r.c = (int64_t)row * P.nx + r.i;
     return r;
 }
 
@@ -158,6 +219,7 @@ struct ewg_ctx {
     double* perm = nullptr;
     uint8_t* lens = nullptr;
     double* iq = nullptr;       // 6 planes: pc, dpc, lw, dlw, ln, dln
+    ewg::FaceGeo* geo = nullptr;     // face-geometry table (3D fast path)
     double2* r = nullptr;       // residual
     double* J = nullptr;        // nb*4 planes, FP64
     float* J32 = nullptr;       // nb*4 planes, FP32 (mixed precision)
@@ -188,6 +250,12 @@ void prof_flush(ewg_ctx* ctx);  // call after the stream is synchronised
         kernel<<<(grid), (block), 0, (ctx)->stream>>>(__VA_ARGS__);      \
         ::ewg::prof_end((ctx), (id));                                    \
     } while (0)
+#define EWG_LAUNCH_SMEM(ctx, id, kernel, grid, block, smem, ...)           \
+    do {                                                                 \
+        ::ewg::prof_begin((ctx), (id));                                  \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__); \
+        ::ewg::prof_end((ctx), (id));                                    \
+    } while (0)
 
 void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p);
 ewg_status cuda_fail(ewg_ctx* ctx, cudaError_t e, const char* what);
@@ -199,6 +267,17 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
                             double2* r, double* maxOut, int* nonfinite);
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x);
 ewg_status compute_boundary_constants(ewg_ctx* ctx);
+// face-geometry table of a 3D grid (allocated on the device)
+ewg_status build_interior_tables(ewg_ctx* ctx);
+// host side of the same: 2 (nx + ny + nz) entries in face_geo_index order
+void build_face_geo(const Phys& P, std::vector<FaceGeo>& geo);
+// the S_w = 1 free-flow boundary constants of P (bndPc, bndLam), computed on the device
+cudaError_t boundary_constants(Phys& P, cudaStream_t stream);
+// layout kernels for problems without a context (ensemble members)
+cudaError_t layout_natural_to_split(const Phys& P, cudaStream_t st, const double2* nat, double2* spl);
+cudaError_t layout_split_to_natural(const Phys& P, cudaStream_t st, const double2* spl, double2* nat);
+cudaError_t layout_scalar_to_split(const Phys& P, cudaStream_t st, const double* nat, double* spl);
+cudaError_t layout_lens_flags(const Phys& P, cudaStream_t st, uint8_t* lens);
 
 // solver (ewg_solver.cu)
 ewg_status solver_solve(ewg_ctx* ctx, const ewg_solve_opts* o, ewg_solve_report* rep);

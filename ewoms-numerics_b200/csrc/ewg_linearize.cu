@@ -18,8 +18,9 @@
 //                (lensproblem.hh:464-533, immiscibleboundaryratevector.hh:91-153), division by
 //                the cell volume, and the residual max-norm of NewtonMethod::preSolve_.
 #include <cstdio>
+#include <vector>
 
-#include "ewg_physics.cuh"
+#include "ewg_assemble.cuh"
 
 namespace ewg {
 
@@ -29,36 +30,9 @@ __global__ void __launch_bounds__(kLinBlock) k_intensive(const __grid_constant__
                                                          const double2* __restrict__ x,
                                                          const uint8_t* __restrict__ lens,
                                                          double* __restrict__ iq) {
-    const int64_t N = P.N;
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < N;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        const double Sw = x[s].y;
-        const LawDev& L = P.law[lens[s]];
-        MatOut m = material(L, Sw);
-        // mobility = kr / mu as an AD quotient with a constant denominator
-        double muw = P.mu[0], mun = P.mu[1];
-        iq[s] = m.pc.v;
-        iq[N + s] = m.pc.d;
-        iq[2 * N + s] = m.krw.v / muw;
-        iq[3 * N + s] = (muw * m.krw.d) / (muw * muw);
-        iq[4 * N + s] = m.krn.v / mun;
-        iq[5 * N + s] = (mun * m.krn.d) / (mun * mun);
-    }
-}
-
-__device__ __forceinline__ void store_block(double* J, int64_t N, int band, int64_t s, const double b[4]) {
-    double* base = J + (int64_t)band * 4 * N + s;
-    base[0] = b[0];
-    base[N] = b[1];
-    base[2 * N] = b[2];
-    base[3 * N] = b[3];
-}
-__device__ __forceinline__ void store_block(float* J, int64_t N, int band, int64_t s, const double b[4]) {
-    float* base = J + (int64_t)band * 4 * N + s;
-    base[0] = (float)b[0];
-    base[N] = (float)b[1];
-    base[2 * N] = (float)b[2];
-    base[3 * N] = (float)b[3];
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x)
+        intensive_cell(P, x, lens, iq, s);
 }
 
 // Non-negative doubles compare like their bit patterns as unsigned integers.
@@ -75,114 +49,7 @@ __device__ __forceinline__ void block_max_publish(double v, unsigned long long* 
     }
 }
 
-// One interior face seen from the focus cell i (darcyfluxmodule.hh:185-324, 461-527;
-// immisciblelocalresidual.hh:123-149): adds the mass fluxes to R_i and dR_i/dx_i and returns the
-// block dR_j/dx_i of the neighbour's local residual (already divided by the neighbour's volume).
-template <int AXIS>
-__device__ __forceinline__ void interior_face(const Phys& P, int side, int idxA, double Ki, const double pI[2],
-                                              double dpcI, const double lam[2], const double dlam[2],
-                                              double2 xj, double Kj, double pcj, const double lamj[2],
-                                              double R[2], double D[2][2], double Dj[4]) {
-    const double h = P.h[AXIS];
-    const double xc = (idxA + 0.5) * h;
-    const double xcj = (idxA + (side ? 1 : -1) + 0.5) * h;
-    const double dA = xcj - xc;
-    const double distSq = dA * dA;
-    const double coef = dA / distSq;
-    const double nA = side ? 1.0 : -1.0;
-    const double Kf = harmonic_mean(Ki, Kj);
-    const double area = P.area[AXIS];
-#pragma unroll
-    for (int a = 0; a < 2; ++a) {
-        const double pJ = a == 0 ? xj.x : xj.x + (pcj - 0.0);
-        const double deltay = pJ - pI[a];
-        double grad = deltay * coef;
-        const double dgP = -coef;
-        const double dgS = a == 0 ? 0.0 : -dpcI * coef;
-        if (AXIS == 1) {
-            // gravity correction; for the other axes the hydrostatic terms are exactly zero
-            const double xf = (idxA + side) * h;
-            const double gIn = -P.g * (xc - xf), gEx = -P.g * (xcj - xf);
-            const double rho = P.rho[a];
-            const double pStatIn = -rho * gIn;
-            const double pStatEx = -(rho * gEx);
-            grad = grad + dA * ((pStatEx - pStatIn) / distSq);
-        }
-        const bool upExt = grad * nA > 0;
-        const double lamU = upExt ? lamj[a] : lam[a];
-        const double dlamU = upExt ? 0.0 : dlam[a];
-        const double sK = Kf * grad;
-        const double vel = sK * (-lamU);
-        const double dvelP = (Kf * dgP) * (-lamU);
-        const double dvelS = (Kf * dgS) * (-lamU) + (-dlamU) * sK;
-        const double rho = P.rho[a];
-        const double F = vel * nA * rho * area;
-        const double dFP = dvelP * nA * rho * area;
-        const double dFS = dvelS * nA * rho * area;
-        R[a] += F;
-        D[a][0] += dFP;
-        D[a][1] += dFS;
-        Dj[2 * a] = -dFP / P.vol;
-        Dj[2 * a + 1] = -dFS / P.vol;
-    }
-}
-
-// One boundary face of the lens problem (lensproblem.hh:464-533): free flow with the hydrostatic
-// S_w = 1 state on the left / right faces (immiscibleboundaryratevector.hh:91-153, boundary
-// gradient fvbasegradientcalculator.hh:277-312, darcyfluxmodule.hh:333-453), the DNAPL inlet on
-// the top face, no flow elsewhere.
-template <int DIM, int AXIS>
-__device__ __forceinline__ void boundary_face(const Phys& P, int side, const int idx[3], int lensI, double Ki,
-                                              const double pI[2], double dpcI, const double lam[2],
-                                              const double dlam[2], double R[2], double D[2][2]) {
-    double xc[3], xf[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xc[d] = d < DIM ? (idx[d] + 0.5) * P.h[d] : 0.0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xf[d] = xc[d];
-    xf[AXIS] = (idx[AXIS] + side) * P.h[AXIS];
-    const double area = P.area[AXIS];
-    const bool left = xf[0] < 0.0 + P.eps, right = xf[0] > P.L[0] - P.eps;
-    if (left || right) {
-        const double g1 = -P.g;
-        const double depth = P.L[1] - xf[1];
-        const double pw = left ? P.pRef - P.leftScale * P.rho[0] * g1 * depth : P.pRef - P.rho[0] * g1 * depth;
-        const double pB[2] = {pw, pw + P.bndPc[in_lens(P, xf) ? 1 : 0] - 0.0};
-        const double dA = xf[AXIS] - xc[AXIS];
-        const double distSq = dA * dA;
-        const double distIn = xc[AXIS] - xf[AXIS];
-        const double absDistSq = distIn * distIn;
-        const double gTimesDist = AXIS == 1 ? g1 * distIn : 0.0;
-        const double coef = dA / distSq;
-        const double nA = side ? 1.0 : -1.0;
-#pragma unroll
-        for (int a = 0; a < 2; ++a) {
-            const double deltay = pB[a] - pI[a];
-            double grad = deltay * coef;
-            const double dgP = -coef;
-            const double dgS = a == 0 ? 0.0 : -dpcI * coef;
-            const double rho = P.rho[a];
-            const double pStatIn = -gTimesDist * rho;
-            grad = grad + distIn * (pStatIn / absDistSq);
-            const bool upB = grad * nA > 0;
-            const double lamU = upB ? P.bndLam[lensI][a] : lam[a];
-            const double dlamU = upB ? 0.0 : dlam[a];
-            const double sK = Ki * grad;
-            const double vel = sK * (-lamU);
-            const double dvelP = (Ki * dgP) * (-lamU);
-            const double dvelS = (Ki * dgS) * (-lamU) + (-dlamU) * sK;
-            R[a] += vel * nA * rho * area;
-            D[a][0] += dvelP * nA * rho * area;
-            D[a][1] += dvelS * nA * rho * area;
-        }
-        return;
-    }
-    const bool upper = xf[1] > P.L[1] - P.eps;
-    bool inlet = upper && xf[0] > P.inletXlo && xf[0] < P.inletXhi;
-    if (DIM == 3) inlet = inlet && xf[2] > P.inletZlo && xf[2] < P.inletZhi;
-    if (inlet) R[1] += P.inletRate * area;
-}
-
+// General per-cell kernel (2D grids): runtime face loops, geometry from cell positions.
 template <int DIM, typename JT, bool WITH_J>
 __global__ void __launch_bounds__(kLinBlock) k_assemble(
     const __grid_constant__ Phys P, const double2* __restrict__ x, const double2* __restrict__ sold,
@@ -321,6 +188,76 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
     block_max_publish(localMax, errmax);
 }
 
+
+// 3D grids: every cell through assemble_cell3 (face geometry from the table)
+template <typename JT, bool WITH_J, int MINB>
+__global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3(
+    const __grid_constant__ Phys P, const FaceGeo* __restrict__ geo, const double2* __restrict__ x,
+    const double2* __restrict__ sold, const double* __restrict__ perm, const uint8_t* __restrict__ lens,
+    const double* __restrict__ iq, double dt, double2* __restrict__ rOut, JT* __restrict__ J,
+    unsigned long long* errmax, int* flags) {
+    double localMax = 0.0;
+    int bad = 0;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x)
+        localMax = fmax(localMax, assemble_cell3<JT, WITH_J>(P, geo, x, sold, perm, lens, iq, dt, rOut, J, s, bad,
+                                                             NbrGlobal{reinterpret_cast<const double*>(x), perm, iq, P.N}));
+    if (bad) atomicOr(flags, 1);
+    block_max_publish(localMax, errmax);
+}
+
+// 3D grids, x and y neighbours staged in shared memory: a block takes kLinBlock consecutive half
+// indices [h0, h0 + kLinBlock) of one colour; their x and y neighbours are the other colour's half
+// indices [h0 - nx/2, h0 + kLinBlock + nx/2), which the block first copies (p_w, K, p_c, lambda_w,
+// lambda_n) with coalesced loads. z neighbours are read from the global arrays.
+constexpr int kMaxStagedNxh = 384;
+constexpr int kStageCap = kLinBlock + 2 * kMaxStagedNxh;
+
+template <typename JT, bool WITH_J, int MINB>
+__global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3s(
+    const __grid_constant__ Phys P, const FaceGeo* __restrict__ geo, const double2* __restrict__ x,
+    const double2* __restrict__ sold, const double* __restrict__ perm, const uint8_t* __restrict__ lens,
+    const double* __restrict__ iq, double dt, double2* __restrict__ rOut, JT* __restrict__ J,
+    unsigned long long* errmax, int* flags) {
+    extern __shared__ __align__(16) double stage[];
+    const int64_t tilesPerColour = (P.Nh + kLinBlock - 1) / kLinBlock;
+    const int cap = kLinBlock + 2 * P.nxh;
+    double* sPw = stage;
+    double* sK = stage + cap;
+    double* sPc = stage + 2 * cap;
+    double* sLw = stage + 3 * cap;
+    double* sLn = stage + 4 * cap;
+    const double* xs = reinterpret_cast<const double*>(x);
+    double localMax = 0.0;
+    int bad = 0;
+    for (int64_t tile = blockIdx.x; tile < 2 * tilesPerColour; tile += gridDim.x) {
+        const int col = tile >= tilesPerColour ? 1 : 0;
+        const int64_t h0 = (tile - col * tilesPerColour) * kLinBlock;
+        const int64_t other = (int64_t)(col ^ 1) * P.Nh;
+        int64_t lo = h0 - P.nxh, hi = h0 + kLinBlock + P.nxh;
+        if (lo < 0) lo = 0;
+        if (hi > P.Nh) hi = P.Nh;
+        __syncthreads();  // the previous tile is done with the stage
+        for (int64_t t = threadIdx.x; t < hi - lo; t += blockDim.x) {
+            const int64_t sj = other + lo + t;
+            sPw[t] = xs[2 * sj];
+            sK[t] = perm[sj];
+            sPc[t] = iq[sj];
+            sLw[t] = iq[2 * P.N + sj];
+            sLn[t] = iq[4 * P.N + sj];
+        }
+        __syncthreads();
+        const int64_t h = h0 + threadIdx.x;
+        if (h < P.Nh) {
+            const NbrStaged nbr{NbrGlobal{xs, perm, iq, P.N}, sPw, sK, sPc, sLw, sLn, other + lo};
+            localMax = fmax(localMax, assemble_cell3<JT, WITH_J>(P, geo, x, sold, perm, lens, iq, dt, rOut, J,
+                                                                 (int64_t)col * P.Nh + h, bad, nbr));
+        }
+    }
+    if (bad) atomicOr(flags, 1);
+    block_max_publish(localMax, errmax);
+}
+
 // S_w = 1 state of the free-flow boundary per region: p_cnw and k_r / mu of both phases
 __global__ void k_boundary_constants(const __grid_constant__ Phys P, double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -360,29 +297,98 @@ ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold) {
     return cuda_fail(ctx, cudaGetLastError(), "k_storage");
 }
 
-ewg_status compute_boundary_constants(ewg_ctx* ctx) {
+cudaError_t boundary_constants(Phys& P, cudaStream_t stream) {
     double* d = nullptr;
     cudaError_t e = cudaMalloc(&d, sizeof(double) * 6);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "alloc boundary constants");
-    k_boundary_constants<<<1, 32, 0, ctx->stream>>>(ctx->P, d);
+    if (e != cudaSuccess) return e;
+    k_boundary_constants<<<1, 32, 0, stream>>>(P, d);
     double h[6] = {0, 0, 0, 0, 0, 0};
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(d);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "boundary constants");
+    if (e != cudaSuccess) return e;
     for (int r = 0; r < 2; ++r) {
-        ctx->P.bndPc[r] = h[3 * r];
-        ctx->P.bndLam[r][0] = h[3 * r + 1];
-        ctx->P.bndLam[r][1] = h[3 * r + 2];
+        P.bndPc[r] = h[3 * r];
+        P.bndLam[r][0] = h[3 * r + 1];
+        P.bndLam[r][1] = h[3 * r + 2];
     }
-    return EWG_OK;
+    return cudaSuccess;
+}
+
+ewg_status compute_boundary_constants(ewg_ctx* ctx) {
+    return cuda_fail(ctx, boundary_constants(ctx->P, ctx->stream), "boundary constants");
 }
 
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x) {
     int grid = grid_size_for(ctx, (const void*)k_initial, kLinBlock);
     EWG_LAUNCH(ctx, K_INITIAL, k_initial, grid, kLinBlock, ctx->P, x);
     return cuda_fail(ctx, cudaGetLastError(), "k_initial");
+}
+
+void build_face_geo(const Phys& P, std::vector<FaceGeo>& geo) {
+    const int n3[3] = {P.nx, P.ny, P.nz};
+    geo.assign(2 * (n3[0] + n3[1] + n3[2]), FaceGeo{});
+    for (int axis = 0; axis < 3; ++axis)
+        for (int idx = 0; idx < n3[axis]; ++idx)
+            for (int side = 0; side < 2; ++side) {
+                // the operations of interior_face, in the same order
+                const double h = P.h[axis];
+                const double xc = (idx + 0.5) * h;
+                const double xcj = (idx + (side ? 1 : -1) + 0.5) * h;
+                const double dA = xcj - xc;
+                const double distSq = dA * dA;
+                FaceGeo G;
+                G.coef = dA / distSq;
+                G.dA = dA;
+                G.gt[0] = G.gt[1] = 0.0;
+                if (axis == 1) {
+                    const double xf = (idx + side) * h;
+                    const double gIn = -P.g * (xc - xf), gEx = -P.g * (xcj - xf);
+                    for (int a = 0; a < 2; ++a) {
+                        const double rho = P.rho[a];
+                        const double pStatIn = -rho * gIn;
+                        const double pStatEx = -(rho * gEx);
+                        G.gt[a] = (pStatEx - pStatIn) / distSq;
+                    }
+                }
+                geo[face_geo_index(n3, axis, idx, side)] = G;
+            }
+}
+
+ewg_status build_interior_tables(ewg_ctx* ctx) {
+    const Phys& P = ctx->P;
+    if (P.dim != 3) return EWG_OK;
+    std::vector<FaceGeo> geo;
+    build_face_geo(P, geo);
+    cudaError_t e;
+    if ((e = cudaMalloc(&ctx->geo, sizeof(FaceGeo) * geo.size())) != cudaSuccess) return cuda_fail(ctx, e, "alloc face geometry");
+    if ((e = cudaMemcpyAsync(ctx->geo, geo.data(), sizeof(FaceGeo) * geo.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return cuda_fail(ctx, e, "upload face geometry");
+    // the host vector goes out of scope: finish the copy first
+    return cuda_fail(ctx, cudaStreamSynchronize(ctx->stream), "sync tables");
+}
+
+// resident blocks per SM the interior kernel is compiled for (register budget 65536 / (256 x it))
+#ifndef EWG_INTERIOR_MIN_BLOCKS
+#define EWG_INTERIOR_MIN_BLOCKS 3
+#endif
+constexpr int kInteriorMinBlocks = EWG_INTERIOR_MIN_BLOCKS;
+
+template <typename JT, bool WITH_J>
+static void launch_assemble3(ewg_ctx* ctx, double dt, const double2* x, double2* r, JT* J) {
+    if (ctx->P.nxh <= kMaxStagedNxh) {
+        auto k = k_assemble3s<JT, WITH_J, kInteriorMinBlocks>;
+        const size_t smem = sizeof(double) * 5 * (kLinBlock + 2 * (size_t)ctx->P.nxh);
+        int g = grid_size_for(ctx, (const void*)k, kLinBlock, smem);
+        EWG_LAUNCH_SMEM(ctx, K_ASSEMBLE, k, g, kLinBlock, smem, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens,
+                        ctx->iq, dt, r, J, ctx->d_errmax, ctx->d_flags);
+        return;
+    }
+    auto k = k_assemble3<JT, WITH_J, kInteriorMinBlocks>;
+    int g = grid_size_for(ctx, (const void*)k, kLinBlock);
+    EWG_LAUNCH(ctx, K_ASSEMBLE, k, g, kLinBlock, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
+               r, J, ctx->d_errmax, ctx->d_flags);
 }
 
 ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const double2* x,
@@ -396,21 +402,28 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
     EWG_LAUNCH(ctx, K_INTENSIVE, k_intensive, g1, kLinBlock, ctx->P, x, ctx->lens, ctx->iq);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_intensive");
     const bool three = ctx->P.dim == 3;
-    if (!withJacobian) {
-        auto k = three ? k_assemble<3, double, false> : k_assemble<2, double, false>;
+    if (three) {
+        if (!withJacobian)
+            launch_assemble3<double, false>(ctx, dt, x, r, nullptr);
+        else if (ctx->jacPrecision == EWG_PRECISION_MIXED)
+            launch_assemble3<float, true>(ctx, dt, x, r, ctx->J32);
+        else
+            launch_assemble3<double, true>(ctx, dt, x, r, ctx->J);
+    } else if (!withJacobian) {
+        auto k = k_assemble<2, double, false>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
-                                             nullptr, ctx->d_errmax, ctx->d_flags);
+                   nullptr, ctx->d_errmax, ctx->d_flags);
     } else if (ctx->jacPrecision == EWG_PRECISION_MIXED) {
-        auto k = three ? k_assemble<3, float, true> : k_assemble<2, float, true>;
+        auto k = k_assemble<2, float, true>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
-                                             ctx->J32, ctx->d_errmax, ctx->d_flags);
+                   ctx->J32, ctx->d_errmax, ctx->d_flags);
     } else {
-        auto k = three ? k_assemble<3, double, true> : k_assemble<2, double, true>;
+        auto k = k_assemble<2, double, true>;
         int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
         EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt, r,
-                                             ctx->J, ctx->d_errmax, ctx->d_flags);
+                   ctx->J, ctx->d_errmax, ctx->d_flags);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_assemble");
     if (maxOut || nonfinite) {

@@ -99,6 +99,26 @@ class NewtonReport(C.Structure):
                 ("t_linearize", C.c_double), ("t_solve", C.c_double), ("t_update", C.c_double)]
 
 
+class EnsembleOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("use_graph", C.c_int32), ("check_interval", C.c_int32),
+                ("max_divisions", C.c_int32)]
+
+
+class EnsembleReport(C.Structure):
+    _fields_ = [("status", C.c_int32), ("newton_iterations", C.c_int32),
+                ("linear_iterations", C.c_int32), ("halvings", C.c_int32), ("dt", C.c_double),
+                ("error", C.c_double)]
+
+
+class EnsembleStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("linear_iterations", C.c_int32), ("t_linearize", C.c_double),
+                ("t_solve", C.c_double), ("t_update", C.c_double)]
+
+
+ENSEMBLE_KERNEL_CLASSES = ("intensive", "assemble", "factor", "cell", "ilu_black", "ilu_red",
+                           "spmv_alpha", "spmv_omega", "bicg_p", "bicg_hs", "bicg_xr")
+
+
 def default_solve_opts(**kw) -> SolveOpts:
     """Reference defaults (fvbasediscretization.hh:249-252, parallelbicgstabbackend.hh:48,
     parallelbasebackend.hh:514) with the graded linear tolerance 1e-10 unless overridden."""
@@ -339,6 +359,26 @@ def load(path: str = LIB_PATH):
         "ewg_net_train": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int32, C.c_float, P(C.c_float)]),
         "ewg_net_eval_samples": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int32, P(C.c_float)]),
         "ewg_predict_guess": (C.c_int, [C.c_void_p, C.c_void_p, d, P(C.c_int32), P(d), P(d)]),
+        "ewg_default_ensemble_opts": (None, [P(EnsembleOpts)]),
+        "ewg_ensemble_create": (C.c_int, [C.c_int32, P(Grid), P(Problem), P(P(d)), P(EnsembleOpts),
+                                          P(C.c_void_p)]),
+        "ewg_ensemble_destroy": (None, [C.c_void_p]),
+        "ewg_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+        "ewg_ensemble_create_error": (C.c_char_p, []),
+        "ewg_ensemble_num_members": (C.c_int32, [C.c_void_p]),
+        "ewg_ensemble_num_cells": (C.c_int64, [C.c_void_p, C.c_int32]),
+        "ewg_ensemble_get_stream": (C.c_void_p, [C.c_void_p]),
+        "ewg_ensemble_apply_initial_solution": (C.c_int, [C.c_void_p]),
+        "ewg_ensemble_set_solution": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(d)]),
+        "ewg_ensemble_get_solution": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(d)]),
+        "ewg_ensemble_linearize": (C.c_int, [C.c_void_p, P(d), P(d)]),
+        "ewg_ensemble_get_residual": (C.c_int, [C.c_void_p, C.c_int32, P(d)]),
+        "ewg_ensemble_autotune": (C.c_int, [C.c_void_p, P(d), P(SolveOpts)]),
+        "ewg_ensemble_get_launch_shapes": (C.c_int, [C.c_void_p, P(C.c_int32), C.c_int32, P(C.c_int32)]),
+        "ewg_ensemble_step": (C.c_int, [C.c_void_p, P(d), P(NewtonOpts), P(SolveOpts), P(EnsembleReport),
+                                        P(EnsembleStats)]),
+        "ewg_ensemble_advance": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(NewtonOpts), P(SolveOpts),
+                                           P(EnsembleReport), P(EnsembleStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -644,3 +684,119 @@ class GuessNet:
         st = self.lib.ewg_predict_guess(ctx.h, self.h, dt, C.byref(used), C.byref(rg), C.byref(rp))
         ctx._check(st, "predict_guess")
         return bool(used.value), rg.value, rp.value
+
+
+# ------------------------------------------------------------------------------------------
+# batched ensemble
+
+
+class Ensemble:
+    """Many lens problems (3D, even nx) in one device context, advanced together
+    (ewg_ensemble_* in include/ewg.h). Host arrays are natural order, N_m x 2 float64."""
+
+    def __init__(self, cases, precision=PRECISION_MIXED, use_graph=True, check_interval=8,
+                 max_divisions=10):
+        lib = load()
+        self.lib = lib
+        self.cases = list(cases)
+        M = len(self.cases)
+        grids = (Grid * M)(*[c.grid for c in self.cases])
+        probs = (Problem * M)(*[c.problem for c in self.cases])
+        self._perms = [np.ascontiguousarray(c.perm, dtype=np.float64) for c in self.cases]
+        parr = (C.POINTER(C.c_double) * M)(*[_ptr(p) for p in self._perms])
+        o = EnsembleOpts()
+        lib.ewg_default_ensemble_opts(C.byref(o))
+        o.precision, o.use_graph, o.check_interval = precision, int(use_graph), check_interval
+        o.max_divisions = max_divisions
+        h = C.c_void_p()
+        st = lib.ewg_ensemble_create(M, grids, probs, parr, C.byref(o), C.byref(h))
+        if st != EWG_OK:
+            raise EwgError(st, lib.ewg_ensemble_create_error().decode())
+        self.h = h
+        self.M = M
+        self.n = [c.grid.n_cells for c in self.cases]
+
+    def _check(self, st, what=""):
+        if st != EWG_OK:
+            raise EwgError(st, f"{what}: {self.lib.ewg_ensemble_last_error(self.h).decode()}")
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ewg_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def total_cells(self) -> int:
+        return int(self.lib.ewg_ensemble_num_cells(self.h, -1))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.ewg_ensemble_get_stream(self.h)
+
+    def _dt(self, dt):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (self.M,)))
+        return a
+
+    def apply_initial_solution(self):
+        self._check(self.lib.ewg_ensemble_apply_initial_solution(self.h), "apply_initial_solution")
+
+    def set_solution(self, member, time_idx, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n[member], 2)
+        self._check(self.lib.ewg_ensemble_set_solution(self.h, member, time_idx, _ptr(x)), "set_solution")
+
+    def get_solution(self, member, time_idx=0, out=None):
+        x = np.zeros((self.n[member], 2)) if out is None else out
+        self._check(self.lib.ewg_ensemble_get_solution(self.h, member, time_idx, _ptr(x)), "get_solution")
+        return x
+
+    def linearize(self, dt):
+        d = self._dt(dt)
+        norms = np.zeros(self.M)
+        self._check(self.lib.ewg_ensemble_linearize(self.h, _ptr(d), _ptr(norms)), "linearize")
+        return norms
+
+    def residual(self, member):
+        r = np.zeros((self.n[member], 2))
+        self._check(self.lib.ewg_ensemble_get_residual(self.h, member, _ptr(r)), "get_residual")
+        return r
+
+    def autotune(self, dt, sopts=None):
+        d = self._dt(dt)
+        sopts = sopts or default_solve_opts()
+        self._check(self.lib.ewg_ensemble_autotune(self.h, _ptr(d), C.byref(sopts)), "autotune")
+        return self.launch_shapes()
+
+    def launch_shapes(self):
+        g = np.zeros(len(ENSEMBLE_KERNEL_CLASSES), dtype=np.int32)
+        v = C.c_int32()
+        self._check(self.lib.ewg_ensemble_get_launch_shapes(self.h, _ptr(g, C.c_int32), len(g), C.byref(v)),
+                    "launch_shapes")
+        out = dict(zip(ENSEMBLE_KERNEL_CLASSES, (int(x) for x in g)))
+        out["assemble_variant"] = v.value
+        return out
+
+    def step(self, dt, nopts=None, sopts=None, check=True):
+        """One implicit step of every member (own dt each). Returns (status, reports, stats)."""
+        return self.advance(1, dt, nopts, sopts, check)
+
+    def advance(self, steps, dt, nopts=None, sopts=None, check=True):
+        """`steps` implicit steps of every member, each at its own pace. Returns (status, reports,
+        stats); reports sum the iterations over each member's accepted steps."""
+        d = self._dt(dt)
+        nopts = nopts or default_newton_opts()
+        sopts = sopts or default_solve_opts()
+        reps = (EnsembleReport * self.M)()
+        stats = EnsembleStats()
+        st = self.lib.ewg_ensemble_advance(self.h, int(steps), _ptr(d), C.byref(nopts), C.byref(sopts), reps,
+                                           C.byref(stats))
+        if check:
+            self._check(st, "advance")
+        return st, list(reps), stats
+

@@ -297,6 +297,82 @@ ewg_status ewg_net_forward_noalloc(const float* params, int32_t B, int32_t D, in
                                    const float* features, float* outputs, void* stream, char* message,
                                    int32_t message_len);
 
+/* ---- batched ensemble (no reference counterpart: the reference runs one lens problem per
+ * Simulator; an ensemble of permeability realizations is many such runs of
+ * NewtonMethod::apply, newtonmethod.hh:308-517, with FvBaseProblem::timeIntegration's step
+ * halving, fvbaseproblem.hh:507-550) ------------------------------------------------------------
+ *
+ * All members live in one context and share every launch: each kernel covers the tiles of the
+ * members in its phase, BiCGStab keeps one state per member and its iterations are replayed from a
+ * CUDA graph; each member runs its own Newton iterations and time steps. 3D grids only (even nx),
+ * ILU(0) only. */
+typedef struct ewg_ensemble ewg_ensemble;
+
+typedef struct ewg_ensemble_opts {
+    int32_t precision;       /* EWG_PRECISION_MIXED (default): Jacobian, ILU(0) and BiCGStab of the
+                                Newton correction in FP32, residual, update and Newton test in FP64.
+                                EWG_PRECISION_FP64: everything in FP64 */
+    int32_t use_graph;       /* 1: replay the BiCGStab iterations from a CUDA graph */
+    int32_t check_interval;  /* BiCGStab iterations per graph replay / host status read */
+    int32_t max_divisions;   /* time-step halvings before a member's step fails (10) */
+} ewg_ensemble_opts;
+
+typedef struct ewg_ensemble_report {
+    int32_t status;             /* EWG_OK, or the failure of the member's last attempt */
+    int32_t newton_iterations;  /* of the accepted attempt */
+    int32_t linear_iterations;  /* BiCGStab iterations over all attempts of this step */
+    int32_t halvings;           /* step-size halvings before the accepted attempt */
+    double dt;                  /* step size of the accepted attempt */
+    double error;               /* last Newton error */
+} ewg_ensemble_report;
+
+typedef struct ewg_ensemble_stats {
+    int32_t rounds;             /* supersteps that linearized at least one member */
+    int32_t linear_iterations;  /* BiCGStab iterations summed over members */
+    double t_linearize, t_solve, t_update;  /* device seconds per phase */
+} ewg_ensemble_stats;
+
+void ewg_default_ensemble_opts(ewg_ensemble_opts* opts);
+/* members problems: grids[m], problems[m] and a natural-order permeability field perms[m]
+ * (N_m doubles, borrowed for the call). opts may be NULL (defaults). */
+ewg_status ewg_ensemble_create(int32_t members, const ewg_grid* grids, const ewg_problem* problems,
+                               const double* const* perms, const ewg_ensemble_opts* opts, ewg_ensemble** out);
+void ewg_ensemble_destroy(ewg_ensemble* ens);
+const char* ewg_ensemble_last_error(const ewg_ensemble* ens);
+const char* ewg_ensemble_create_error(void);
+int32_t ewg_ensemble_num_members(const ewg_ensemble* ens);
+/* cells of one member; member < 0: all members */
+int64_t ewg_ensemble_num_cells(const ewg_ensemble* ens, int32_t member);
+void* ewg_ensemble_get_stream(ewg_ensemble* ens);
+/* LensProblem::initial into both time levels of every member */
+ewg_status ewg_ensemble_apply_initial_solution(ewg_ensemble* ens);
+/* solution(time_idx) of one member, natural order N_m x {p_w, S_w} (as ewg_set_solution) */
+ewg_status ewg_ensemble_set_solution(ewg_ensemble* ens, int32_t member, int32_t time_idx, const double* x);
+ewg_status ewg_ensemble_get_solution(ewg_ensemble* ens, int32_t member, int32_t time_idx, double* x);
+/* linearizeDomain() of every member at solution(0) with its own step size dt[m]; the residual
+ * max-norm of each member into max_norms[m] (nullable) */
+ewg_status ewg_ensemble_linearize(ewg_ensemble* ens, const double* dt, double* max_norms);
+/* residual of one member from the last linearization (natural order, N_m x 2) */
+ewg_status ewg_ensemble_get_residual(ewg_ensemble* ens, int32_t member, double* r);
+/* Launch-shape autotuner: times each kernel class at 1..8 resident blocks per SM (and the
+ * assembly's register-budget variants) on the current state with step sizes dt, keeps the fastest.
+ * Results do not depend on the choice. */
+ewg_status ewg_ensemble_autotune(ewg_ensemble* ens, const double* dt, const ewg_solve_opts* sopts);
+/* the chosen blocks per kernel class (count >= 11 entries) and assembly variant */
+ewg_status ewg_ensemble_get_launch_shapes(const ewg_ensemble* ens, int32_t* grids, int32_t count,
+                                          int32_t* assemble_variant);
+/* One implicit-Euler step of every member with its own step size dt[m]: Newton as ewg_newton_apply
+ * per member (the same tolerances and iteration rules), a failed attempt restores solution(0) and
+ * retries with half the step size, accepted members advance their time level. reports (nullable)
+ * receives one entry per member. Returns EWG_OK if every member's step was accepted. */
+ewg_status ewg_ensemble_step(ewg_ensemble* ens, const double* dt, const ewg_newton_opts* nopts,
+                             const ewg_solve_opts* sopts, ewg_ensemble_report* reports, ewg_ensemble_stats* stats);
+/* `steps` implicit steps of every member, each member at its own pace: a member that finishes a
+ * Newton iteration or a step goes on at once instead of waiting for the others (the report sums
+ * Newton / BiCGStab iterations and halvings over the member's accepted steps). */
+ewg_status ewg_ensemble_advance(ewg_ensemble* ens, int32_t steps, const double* dt, const ewg_newton_opts* nopts,
+                                const ewg_solve_opts* sopts, ewg_ensemble_report* reports, ewg_ensemble_stats* stats);
+
 /* ---- instrumentation (no reference counterpart; the analogue of the reference's phase timers,
  * newtonmethod.hh:488-500) --------------------------------------------------------------- */
 

@@ -48,13 +48,17 @@ def test_struct_layout_matches_c(tmp_path):
                    'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
                    'sizeof(ewg_grid),sizeof(ewg_material),sizeof(ewg_problem),sizeof(ewg_solve_opts),'
                    'sizeof(ewg_solve_report),sizeof(ewg_lin_report),sizeof(ewg_newton_opts),'
-                   'sizeof(ewg_newton_report),offsetof(ewg_problem,lens),offsetof(ewg_solve_opts,restart_on_breakdown));}\n')
+                   'sizeof(ewg_newton_report),offsetof(ewg_problem,lens),offsetof(ewg_solve_opts,restart_on_breakdown));'
+                   'printf("%zu %zu %zu %zu\\n",sizeof(ewg_ensemble_opts),sizeof(ewg_ensemble_report),'
+                   'sizeof(ewg_ensemble_stats),offsetof(ewg_ensemble_stats,t_linearize));}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
     got = [int(v) for v in subprocess.check_output([str(exe)]).split()]
     want = [C.sizeof(ewg.Grid), C.sizeof(ewg.Material), C.sizeof(ewg.Problem), C.sizeof(ewg.SolveOpts),
             C.sizeof(ewg.SolveReport), C.sizeof(ewg.LinReport), C.sizeof(ewg.NewtonOpts),
-            C.sizeof(ewg.NewtonReport), ewg.Problem.lens.offset, ewg.SolveOpts.restart_on_breakdown.offset]
+            C.sizeof(ewg.NewtonReport), ewg.Problem.lens.offset, ewg.SolveOpts.restart_on_breakdown.offset,
+            C.sizeof(ewg.EnsembleOpts), C.sizeof(ewg.EnsembleReport), C.sizeof(ewg.EnsembleStats),
+            ewg.EnsembleStats.t_linearize.offset]
     assert got == want
 
 
@@ -77,3 +81,17 @@ def test_invalid_grid_rejected(lib):
     with pytest.raises(ewg.EwgError) as ei:
         ewg.Context(case)
     assert ei.value.status in (1, 7)
+
+
+def test_ensemble_without_device_or_bad_grid_fails_loudly(lib):
+    """Ensembles take 3D grids with even nx and a device; anything else is an error status."""
+    import ewg
+    import torch
+    bad = ewg.lens3d_case(7, 4, 4, seed=0)
+    with pytest.raises(ewg.EwgError) as ei:
+        ewg.Ensemble([bad])
+    assert ei.value.status == 1
+    if not torch.cuda.is_available():
+        with pytest.raises(ewg.EwgError) as ei:
+            ewg.Ensemble([ewg.lens3d_case(8, 4, 4, seed=0)])
+        assert ei.value.status == 7

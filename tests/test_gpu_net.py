@@ -68,8 +68,10 @@ def test_training_reduces_loss(ewg_mod):
         ctx.advance_time_level()
     idx = np.arange(net.n_samples)
     l0 = net.eval_samples(idx)
-    for _ in range(60):
-        net.train(idx, lr=2e-3)
+    # Adam at lr 1e-3: the loss drops to below 0.1 of its start within 80 steps in repeated runs
+    # (the gradient sums use atomics, so runs differ at float rounding; lr 2e-3 oscillates)
+    for _ in range(80):
+        net.train(idx, lr=1e-3)
     l1 = net.eval_samples(idx)
     assert l1 < 0.5 * l0, (l0, l1)
 

@@ -15,7 +15,7 @@ SRC = r'''
 using namespace ewg;
 int check(int dim, int nx, int ny, int nz) {
     Phys P{}; P.dim = dim; P.nx = nx; P.ny = ny; P.nz = dim == 3 ? nz : 1;
-    P.N = (int64_t)nx * ny * P.nz; P.Nh = P.N / 2; P.nxh = nx / 2; P.planeh = (int64_t)nx * ny / 2;
+    set_index_constants(P);
     std::vector<int> seen(P.N, 0);
     int bad = 0;
     for (int col = 0; col < 2; ++col)
@@ -46,6 +46,13 @@ int main() {
     int bad = 0;
     bad += check(2, 48, 32, 1); bad += check(2, 2, 1, 1); bad += check(2, 6, 5, 1);
     bad += check(3, 4, 3, 3); bad += check(3, 8, 6, 4); bad += check(3, 2, 1, 5); bad += check(3, 16, 7, 9);
+    bad += check(3, 34, 18, 6); bad += check(3, 256, 12, 3); bad += check(3, 98, 97, 5);
+    // the division by invariant integers used by cell_of, against plain division
+    for (uint32_t d = 1; d < 3000; ++d) {
+        FastDiv f = make_fastdiv(d);
+        for (uint32_t n = 0; n < 20000; n += 7) if (fastdiv(f, n) != n / d) ++bad;
+        for (uint32_t n = 0x7fffffffu; n > 0x7fff0000u; n -= 977) if (fastdiv(f, n) != n / d) ++bad;
+    }
     printf("%d\n", bad);
     return bad != 0;
 }
