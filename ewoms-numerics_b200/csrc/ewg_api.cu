@@ -171,6 +171,9 @@ void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p) {
         P.lensHi[a] = p->lens_hi[a];
     }
     P.eps = p->eps;
+    for (int a = 0; a < 3; ++a)
+        for (int ph = 0; ph < 2; ++ph) P.rhoArea[a][ph] = P.rho[ph] * P.area[a];
+    P.invVol = 1.0 / P.vol;
     P.law[0] = make_law(p->outer);
     P.law[1] = make_law(p->lens);
 }

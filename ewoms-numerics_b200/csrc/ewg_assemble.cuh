@@ -166,11 +166,10 @@ template <int AXIS>
 __device__ __forceinline__ void interior_face_tab(const Phys& P, const FaceGeo& G, int side, double Ki,
                                                   const double pI[2], double dpcI, const double lam[2],
                                                   const double dlam[2], double pwj, double Kj, double pcj,
-                                                  double lwj, double lnj, double negInvV, double R[2],
-                                                  double D[2][2], double Dj[4]) {
+                                                  double lwj, double lnj, double R[2], double D[2][2],
+                                                  double Dj[4]) {
     const double coef = G.coef;
     const double Kf = harmonic_mean(Ki, Kj);
-    const double area = P.area[AXIS];
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         const double pJ = a == 0 ? pwj : pwj + (pcj - 0.0);
@@ -187,15 +186,16 @@ __device__ __forceinline__ void interior_face_tab(const Phys& P, const FaceGeo& 
         const double vel = sK * (-lamU);
         const double dvelP = (Kf * dgP) * (-lamU);
         const double dvelS = (Kf * dgS) * (-lamU) + (-dlamU) * sK;
-        const double rho = P.rho[a];
-        const double F = ((side ? vel : -vel) * rho) * area;
-        const double dFP = ((side ? dvelP : -dvelP) * rho) * area;
-        const double dFS = ((side ? dvelS : -dvelS) * rho) * area;
+        // mass flux (v . n) rho A; the neighbour's block is divided by its volume
+        const double ra = side ? P.rhoArea[AXIS][a] : -P.rhoArea[AXIS][a];
+        const double F = vel * ra;
+        const double dFP = dvelP * ra;
+        const double dFS = dvelS * ra;
         R[a] += F;
         D[a][0] += dFP;
         D[a][1] += dFS;
-        Dj[2 * a] = dFP * negInvV;
-        Dj[2 * a + 1] = dFS * negInvV;
+        Dj[2 * a] = dFP * -P.invVol;
+        Dj[2 * a + 1] = dFS * -P.invVol;
     }
 }
 
@@ -205,36 +205,21 @@ struct NbrVals {
     double pw, K, pc, lw, ln;
 };
 
-// Neighbour values read from the global arrays.
+// Neighbour values read from the global arrays (32-bit cell indices: N < 2^31).
 struct NbrGlobal {
-    const double* xs;   // x as doubles {p_w, S_w} per cell
+    const double2* x;
     const double* perm;
-    const double* iq;
-    int64_t N;
-    __device__ __forceinline__ NbrVals operator()(int q, int64_t sj) const {
+    const double* pc;   // intensive-quantity planes 0, 2, 4
+    const double* lw;
+    const double* ln;
+    __device__ __forceinline__ NbrVals operator()(int q, int sj) const {
         (void)q;
-        return {xs[2 * sj], perm[sj], iq[sj], iq[2 * N + sj], iq[4 * N + sj]};
+        return {x[sj].x, perm[sj], pc[sj], lw[sj], ln[sj]};
     }
 };
-
-// Neighbours across x and y faces from a block's shared-memory copy of the other colour's half
-// indices [r0, r0 + count); z neighbours from the global arrays.
-struct NbrStaged {
-    NbrGlobal g;
-    const double* sPw;
-    const double* sK;
-    const double* sPc;
-    const double* sLw;
-    const double* sLn;
-    int64_t r0;  // split position of the first staged entry
-    __device__ __forceinline__ NbrVals operator()(int q, int64_t sj) const {
-        if (q < 4) {
-            const int64_t t = sj - r0;
-            return {sPw[t], sK[t], sPc[t], sLw[t], sLn[t]};
-        }
-        return g(q, sj);
-    }
-};
+__device__ __forceinline__ NbrGlobal nbr_global(const double2* x, const double* perm, const double* iq, int64_t N) {
+    return NbrGlobal{x, perm, iq, iq + 2 * N, iq + 4 * N};
+}
 
 // One cell of a 3D grid: fluxes over its interior faces in intersection order (-x, +x, -y, +y,
 // -z, +z), the implicit-Euler storage term (fvbaselocalresidual.hh:494-629), its boundary faces,
@@ -248,44 +233,51 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
                                                  JT* __restrict__ J, int64_t s, int& bad, const NB& nbr) {
     const int64_t N = P.N;
     const double V = P.vol;
-    const double invV = 1.0 / V, negInvV = -invV;
     const int n3[3] = {P.nx, P.ny, P.nz};
-    const int col = s >= P.Nh ? 1 : 0;
-    const int64_t h = s - col * P.Nh;
+    const int s32 = (int)s;  // N < 2^31: 32-bit cell indices
+    const int Nh32 = (int)P.Nh;
+    const int col = s32 >= Nh32 ? 1 : 0;
+    const int h = s32 - col * Nh32;
     const CellIdx ci = cell_of(P, col, h);
     const int idx[3] = {ci.i, ci.j, ci.k};
     const bool has[6] = {ci.i > 0, ci.i < P.nx - 1, ci.j > 0, ci.j < P.ny - 1, ci.k > 0, ci.k < P.nz - 1};
-    const double2 xi = x[s];
-    const double Ki = perm[s];
-    const double pci = iq[s], dpci = iq[N + s];
-    const double lam[2] = {iq[2 * N + s], iq[4 * N + s]};
-    const double dlam[2] = {iq[3 * N + s], iq[5 * N + s]};
+    const double2 xi = x[s32];
+    const double Ki = perm[s32];
+    const double* iq1 = iq + N;
+    const double* iq2 = iq + 2 * N;
+    const double* iq3 = iq + 3 * N;
+    const double* iq4 = iq + 4 * N;
+    const double* iq5 = iq + 5 * N;
+    const double pci = iq[s32], dpci = iq1[s32];
+    const double lam[2] = {iq2[s32], iq4[s32]};
+    const double dlam[2] = {iq3[s32], iq5[s32]};
     const double pI[2] = {xi.x, xi.x + (pci - 0.0)};
-    const int64_t base = (int64_t)(col ^ 1) * P.Nh;
-    const int64_t nb[6] = {base + h - 1 + ci.b, base + h + ci.b, base + h - P.nxh,
-                           base + h + P.nxh, base + h - P.planeh, base + h + P.planeh};
+    const int base = (col ^ 1) * Nh32;
+    const int nxh = P.nxh, planeh = (int)P.planeh;
+    const int nb[6] = {base + h - 1 + ci.b, base + h + ci.b, base + h - nxh, base + h + nxh, base + h - planeh,
+                       base + h + planeh};
     double R[2] = {0.0, 0.0};
     double D[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         if (!has[q]) continue;
         const int axis = q >> 1, side = q & 1;
-        const int64_t sj = nb[q];
+        const int sj = nb[q];
         const FaceGeo G = geo[face_geo_index(n3, axis, idx[axis], side)];
         const NbrVals nv = nbr(q, sj);
         const double pwj = nv.pw, Kj = nv.K, pcj = nv.pc, lwj = nv.lw, lnj = nv.ln;
         double Dj[4];
         if (axis == 0)
-            interior_face_tab<0>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, negInvV, R, D, Dj);
+            interior_face_tab<0>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         else if (axis == 1)
-            interior_face_tab<1>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, negInvV, R, D, Dj);
+            interior_face_tab<1>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         else
-            interior_face_tab<2>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, negInvV, R, D, Dj);
+            interior_face_tab<2>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         if (WITH_J) store_block(J, N, opposite_band(band_of(axis, side)), sj, Dj);
     }
     // storage: (phi S rho - storage(x_old)) V / dt
     {
-        const double2 so = sold[s];
+        const double2 so = sold[s32];
         const double Sw = xi.y;
         const double fac = V / dt;
         const double sw0 = P.porosity * Sw * P.rho[0];
@@ -300,7 +292,7 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
     for (int q = 0; q < 6; ++q) {
         if (has[q]) continue;
         const int axis = q >> 1, side = q & 1;
-        const int li = lens[s];
+        const int li = lens[s32];
         if (axis == 0)
             boundary_face<3, 0>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
         else if (axis == 1)
@@ -308,12 +300,13 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
         else
             boundary_face<3, 2>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
     }
+    const double invV = P.invVol;
     R[0] *= invV;
     R[1] *= invV;
-    rOut[s] = make_double2(R[0], R[1]);
+    rOut[s32] = make_double2(R[0], R[1]);
     if (WITH_J) {
         const double blk[4] = {D[0][0] * invV, D[0][1] * invV, D[1][0] * invV, D[1][1] * invV};
-        store_block(J, N, 0, s, blk);
+        store_block(J, N, 0, s32, blk);
     }
     if (!(fabs(R[0]) <= 1.7976931348623157e308) || !(fabs(R[1]) <= 1.7976931348623157e308)) bad = 1;
     return fmax(fabs(R[0]), fabs(R[1]));

@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(kEnsTile, MINB) ke_assemble(
                 mx = fmax(mx, assemble_cell3<JT, WITH_J>(
                                   P, geo + sm.geoOff, x + off, sold + off, perm + off, lens + off, iq + 6 * off, dt,
                                   r + off, WITH_J ? J + kEnsBands * 4 * off : J, col * P.Nh + h, bad,
-                                  NbrGlobal{reinterpret_cast<const double*>(x + off), perm + off, iq + 6 * off, P.N}));
+                                  nbr_global(x + off, perm + off, iq + 6 * off, P.N)));
         }
         if (bad) atomicOr(&flags[m], 1);
         block_max_atomic(mx, &errmax[m]);

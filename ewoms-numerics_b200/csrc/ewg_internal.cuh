@@ -89,6 +89,8 @@ struct Phys {
     double bndPc[2];
     double bndLam[2][2];
     FastDiv fdNxh, fdNy;     // divisions by nx / 2 and ny in cell_of (N < 2^31)
+    double rhoArea[3][2];    // rho_alpha * face area per axis (mass flux per unit velocity)
+    double invVol;           // 1 / cell volume
 };
 
 // Geometry of one interior face seen from a cell, per (axis, cell index along the axis, side):
@@ -248,12 +250,6 @@ void prof_flush(ewg_ctx* ctx);  // call after the stream is synchronised
     do {                                                                 \
         ::ewg::prof_begin((ctx), (id));                                  \
         kernel<<<(grid), (block), 0, (ctx)->stream>>>(__VA_ARGS__);      \
-        ::ewg::prof_end((ctx), (id));                                    \
-    } while (0)
-#define EWG_LAUNCH_SMEM(ctx, id, kernel, grid, block, smem, ...)           \
-    do {                                                                 \
-        ::ewg::prof_begin((ctx), (id));                                  \
-        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__); \
         ::ewg::prof_end((ctx), (id));                                    \
     } while (0)
 

@@ -201,59 +201,7 @@ __global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3(
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
          s += (int64_t)gridDim.x * blockDim.x)
         localMax = fmax(localMax, assemble_cell3<JT, WITH_J>(P, geo, x, sold, perm, lens, iq, dt, rOut, J, s, bad,
-                                                             NbrGlobal{reinterpret_cast<const double*>(x), perm, iq, P.N}));
-    if (bad) atomicOr(flags, 1);
-    block_max_publish(localMax, errmax);
-}
-
-// 3D grids, x and y neighbours staged in shared memory: a block takes kLinBlock consecutive half
-// indices [h0, h0 + kLinBlock) of one colour; their x and y neighbours are the other colour's half
-// indices [h0 - nx/2, h0 + kLinBlock + nx/2), which the block first copies (p_w, K, p_c, lambda_w,
-// lambda_n) with coalesced loads. z neighbours are read from the global arrays.
-constexpr int kMaxStagedNxh = 384;
-constexpr int kStageCap = kLinBlock + 2 * kMaxStagedNxh;
-
-template <typename JT, bool WITH_J, int MINB>
-__global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3s(
-    const __grid_constant__ Phys P, const FaceGeo* __restrict__ geo, const double2* __restrict__ x,
-    const double2* __restrict__ sold, const double* __restrict__ perm, const uint8_t* __restrict__ lens,
-    const double* __restrict__ iq, double dt, double2* __restrict__ rOut, JT* __restrict__ J,
-    unsigned long long* errmax, int* flags) {
-    extern __shared__ __align__(16) double stage[];
-    const int64_t tilesPerColour = (P.Nh + kLinBlock - 1) / kLinBlock;
-    const int cap = kLinBlock + 2 * P.nxh;
-    double* sPw = stage;
-    double* sK = stage + cap;
-    double* sPc = stage + 2 * cap;
-    double* sLw = stage + 3 * cap;
-    double* sLn = stage + 4 * cap;
-    const double* xs = reinterpret_cast<const double*>(x);
-    double localMax = 0.0;
-    int bad = 0;
-    for (int64_t tile = blockIdx.x; tile < 2 * tilesPerColour; tile += gridDim.x) {
-        const int col = tile >= tilesPerColour ? 1 : 0;
-        const int64_t h0 = (tile - col * tilesPerColour) * kLinBlock;
-        const int64_t other = (int64_t)(col ^ 1) * P.Nh;
-        int64_t lo = h0 - P.nxh, hi = h0 + kLinBlock + P.nxh;
-        if (lo < 0) lo = 0;
-        if (hi > P.Nh) hi = P.Nh;
-        __syncthreads();  // the previous tile is done with the stage
-        for (int64_t t = threadIdx.x; t < hi - lo; t += blockDim.x) {
-            const int64_t sj = other + lo + t;
-            sPw[t] = xs[2 * sj];
-            sK[t] = perm[sj];
-            sPc[t] = iq[sj];
-            sLw[t] = iq[2 * P.N + sj];
-            sLn[t] = iq[4 * P.N + sj];
-        }
-        __syncthreads();
-        const int64_t h = h0 + threadIdx.x;
-        if (h < P.Nh) {
-            const NbrStaged nbr{NbrGlobal{xs, perm, iq, P.N}, sPw, sK, sPc, sLw, sLn, other + lo};
-            localMax = fmax(localMax, assemble_cell3<JT, WITH_J>(P, geo, x, sold, perm, lens, iq, dt, rOut, J,
-                                                                 (int64_t)col * P.Nh + h, bad, nbr));
-        }
-    }
+                                                             nbr_global(x, perm, iq, P.N)));
     if (bad) atomicOr(flags, 1);
     block_max_publish(localMax, errmax);
 }
@@ -377,14 +325,6 @@ constexpr int kInteriorMinBlocks = EWG_INTERIOR_MIN_BLOCKS;
 
 template <typename JT, bool WITH_J>
 static void launch_assemble3(ewg_ctx* ctx, double dt, const double2* x, double2* r, JT* J) {
-    if (ctx->P.nxh <= kMaxStagedNxh) {
-        auto k = k_assemble3s<JT, WITH_J, kInteriorMinBlocks>;
-        const size_t smem = sizeof(double) * 5 * (kLinBlock + 2 * (size_t)ctx->P.nxh);
-        int g = grid_size_for(ctx, (const void*)k, kLinBlock, smem);
-        EWG_LAUNCH_SMEM(ctx, K_ASSEMBLE, k, g, kLinBlock, smem, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens,
-                        ctx->iq, dt, r, J, ctx->d_errmax, ctx->d_flags);
-        return;
-    }
     auto k = k_assemble3<JT, WITH_J, kInteriorMinBlocks>;
     int g = grid_size_for(ctx, (const void*)k, kLinBlock);
     EWG_LAUNCH(ctx, K_ASSEMBLE, k, g, kLinBlock, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
