@@ -224,9 +224,15 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-# ncu dram bytes (read + write) per launch at the full 256x256x128 workload, from the captures
-# summarised in profiles/ (scaled from the captured case by cell count where noted there).
-NCU_TRAFFIC = {}
+# ncu DRAM bytes (read + write) per launch of the FP64 kernels at the full 256x256x128 workload:
+# the --set full capture of the 128x128x64 case (profiles/kernels_lens3d_128x128x64_fp64_ncu.md)
+# scaled by the cell count (x 8); the traffic of these streaming kernels grows in proportion.
+NCU_TRAFFIC = {
+    "bicg_spmv_omega": (281.86e6 + 17.78e6) * 8,
+    "ilu_black_apply": (133.48e6 + 4.35e6) * 8,
+    "ilu_red_apply": (133.50e6 + 4.21e6) * 8,
+    "bicg_xr": (83.93e6 + 3.81e6) * 8,
+}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -351,6 +357,9 @@ def run_ensemble(args, rank, pg, torch, ewg):
         "newton_iterations_per_step_max": float(np.max(newton)),
         "halvings": int(sum(r.halvings for reps, _ in stats for r in reps)),
         "rounds": [s.rounds for _, s in stats], "linear_iterations": [s.linear_iterations for _, s in stats],
+        # BiCGStab work actually done: cells x iterations summed over members, and the HBM rate it
+        # implies at the FP32 per-iteration bytes of the single-problem kernels (s = 4)
+        "bicgstab_cell_iterations_per_s": sum(s.cell_iterations for _, s in stats) / sum(s.t_solve for _, s in stats),
         "phase_s": {"linearize": sum(s.t_linearize for _, s in stats) / len(stats),
                     "solve": sum(s.t_solve for _, s in stats) / len(stats),
                     "update": sum(s.t_update for _, s in stats) / len(stats)},
@@ -509,7 +518,7 @@ def run_ours(args, rank, world, local, pg):
     db = kernel_bytes(dname, N, F, s_mat=s, s_vec=s)
     avg_ms = dms / dn
     achieved = db / (avg_ms * 1e-3) / 1e9 if db else None
-    traffic = NCU_TRAFFIC.get(dname)
+    traffic = NCU_TRAFFIC.get(dname) if not mixed else None
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic,
                 "algorithmic_bytes_per_launch": db, "avg_launch_ms": avg_ms, "launches": dn,

@@ -46,7 +46,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     # the C++ host driver over the C ABI
     drv_src = os.path.join(HERE, "host", "lens_gpu.cc")
     drv = os.path.join(HERE, "lens_gpu")
-    if force or _stale(drv, [drv_src, os.path.join(HERE, "host", "ewg.hh"), OUT]):
+    if force or _stale(drv, [drv_src, os.path.join(HERE, "host", "ewg.hh"), os.path.join(HERE, "host", "vtkwriter.hh"),
+                             OUT]):
         cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-o", drv, drv_src, "-L", HERE, "-lewg",
                "-Wl,-rpath,$ORIGIN"]
         if verbose:

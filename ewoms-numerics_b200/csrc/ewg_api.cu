@@ -228,6 +228,16 @@ cudaError_t layout_lens_flags(const Phys& P, cudaStream_t st, uint8_t* lens) {
     return cudaGetLastError();
 }
 
+// p_c, lambda_w, lambda_n of every cell (split-order cache planes 0, 2, 4) in natural order
+__global__ void k_iq_natural(const __grid_constant__ Phys P, const double* __restrict__ iq, double* __restrict__ out) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < P.N; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = split_of(P, c);
+        out[3 * c] = iq[s];
+        out[3 * c + 1] = iq[2 * P.N + s];
+        out[3 * c + 2] = iq[4 * P.N + s];
+    }
+}
+
 // natural row c of the reference BCRS, columns ascending: the band of each entry
 __device__ __forceinline__ int band_for_column(const Phys& P, int64_t c, int64_t col) {
     if (col < 0 || col >= P.N) return -1;
@@ -549,6 +559,22 @@ static ewg_status ensure_j32(ewg_ctx* ctx) {
     return cuda_fail(ctx, e, "zero J32");
 }
 
+// ImmiscibleModel::updateBegin (immisciblemodel.hh:278-293): p_w of the first DOF of solution(0)
+// (natural cell 0 is split position 0). Only the finite-difference linearizer uses it.
+static ewg_status update_reference_pressure(ewg_ctx* ctx, bool force) {
+    if (!force && (ctx->localLinearizer != EWG_LOCAL_LINEARIZER_FD || ctx->refPressure > 0)) return EWG_OK;
+    double p = 0.0;
+    cudaError_t e = cudaMemcpyAsync(&p, &ctx->x0[0].x, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "read reference pressure");
+    if (!(p > 0) || !std::isfinite(p)) {
+        ctx->err = "finite-difference linearizer: the reference pressure (p_w of cell 0) must be positive";
+        return EWG_ERR_NONFINITE;
+    }
+    ctx->refPressure = p;
+    return EWG_OK;
+}
+
 static ewg_status linearize_impl(ewg_ctx* ctx, double dt, ewg_lin_report* rep) {
     if (!(dt > 0)) { ctx->err = "dt must be positive"; return EWG_ERR_INVALID; }
     if (ctx->jacPrecision == EWG_PRECISION_MIXED) {
@@ -577,7 +603,48 @@ static ewg_status linearize_impl(ewg_ctx* ctx, double dt, ewg_lin_report* rep) {
 
 ewg_status ewg_linearize(ewg_ctx* ctx, double dt, ewg_lin_report* rep) {
     if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    // a context that never ran updateBegin takes the reference pressure of the current iterate
+    ewg_status st = update_reference_pressure(ctx, false);
+    if (st) return st;
     return linearize_impl(ctx, dt, rep);
+}
+
+ewg_status ewg_update_begin(ewg_ctx* ctx) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    return update_reference_pressure(ctx, true);
+}
+
+ewg_status ewg_get_intensive_quantities(ewg_ctx* ctx, double* out) {
+    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+    ewg_status st = launch_intensive(ctx, ctx->x0);
+    if (st) return st;
+    double* d = nullptr;
+    const size_t bytes = sizeof(double) * 3 * ctx->P.N;
+    cudaError_t e = cudaMalloc(&d, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "alloc intensive output");
+    k_iq_natural<<<lgrid(ctx, (const void*)k_iq_natural), kApiBlock, 0, ctx->stream>>>(ctx->P, ctx->iq, d);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    return cuda_fail(ctx, e, "intensive quantities");
+}
+
+ewg_status ewg_set_local_linearizer(ewg_ctx* ctx, int32_t kind, int32_t method) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    if (kind != EWG_LOCAL_LINEARIZER_AD && kind != EWG_LOCAL_LINEARIZER_FD) {
+        ctx->err = "unknown local linearizer";
+        return EWG_ERR_INVALID;
+    }
+    if (method < -1 || method > 1) {
+        ctx->err = "NumericDifferenceMethod must be -1, 0 or +1";
+        return EWG_ERR_INVALID;
+    }
+    ctx->localLinearizer = kind;
+    ctx->fdMethod = method;
+    ctx->jacFromLinearizer = false;
+    ctx->iluValid = false;
+    return EWG_OK;
 }
 
 ewg_status ewg_get_residual(ewg_ctx* ctx, double* r) {
@@ -717,8 +784,9 @@ ewg_status ewg_newton_apply(ewg_ctx* ctx, double dt, const ewg_newton_opts* no, 
         if (numIterations >= no->newton_max_iterations) return error * 4.0 < lastError;
         return true;
     };
-    ewg_status status = EWG_OK;
-    while (proceed()) {
+    // model.update() calls updateBegin() right before NewtonMethod::apply (fvbasediscretization.hh:1242)
+    ewg_status status = update_reference_pressure(ctx, true);
+    while (status == EWG_OK && proceed()) {
         lastError = error;
         ewg_lin_report lr = {};
         ewg_status st = linearize_impl(ctx, dt, &lr);

@@ -1156,6 +1156,7 @@ ewg_status ensemble_advance(ewg_ensemble* e, int steps, const double* dt, const 
                 }
                 mr[m].linear += b.iter;
                 S.linear_iterations += b.iter;
+                S.cell_iterations += (double)e->hm[m].P.N * b.iter;
                 if (b.status == ST_CONVERGED) upd.push_back(m);
                 else fail(m, b.status == ST_BREAKDOWN ? EWG_ERR_BREAKDOWN : EWG_ERR_NOT_CONVERGED);
                 mr[m].phase = PH_LIN;  // provisional; settle() or the checks below decide

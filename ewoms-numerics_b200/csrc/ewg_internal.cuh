@@ -207,6 +207,9 @@ struct ewg_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
     int jacPrecision = EWG_PRECISION_FP64;   // what ewg_linearize writes
+    int localLinearizer = EWG_LOCAL_LINEARIZER_AD;  // LocalLinearizerSplice
+    int fdMethod = 1;                        // NumericDifferenceMethod of the FD linearizer
+    double refPressure = -1.0;               // ImmiscibleModel::updateBegin's reference pressure (unset)
     bool jacFromLinearizer = false;          // J/r valid
     bool iluValid = false;
     int iluKind = -1, iluPrecision = -1;
@@ -262,6 +265,8 @@ ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold);
 ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const double2* x,
                             double2* r, double* maxOut, int* nonfinite);
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x);
+// intensive quantities (p_c, lambda_w, lambda_n with d/dS_w) of state x into ctx->iq
+ewg_status launch_intensive(ewg_ctx* ctx, const double2* x);
 ewg_status compute_boundary_constants(ewg_ctx* ctx);
 // face-geometry table of a 3D grid (allocated on the device)
 ewg_status build_interior_tables(ewg_ctx* ctx);

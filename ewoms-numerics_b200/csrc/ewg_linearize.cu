@@ -206,6 +206,169 @@ __global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3(
     block_max_publish(localMax, errmax);
 }
 
+// ---- finite-difference local linearizer ---------------------------------------------------------
+//
+// FvBaseFdLocalLinearizer (fvbasefdlocallinearizer.hh:221-237, 393-453): the local residual of
+// the element of cell i (its own row and the face-flux contributions to its neighbours' rows) is
+// evaluated at the primary variables and at the own primary variable deflected by
+// eps = BaseEpsilon / primaryVarWeight (0.9123e-10; weight 10 / p_ref for the pressure, 1 for the
+// saturation, immisciblemodel.hh:298-310), and the Jacobian column i is the difference quotient
+// (NumericDifferenceMethod +1 forward, 0 central, -1 backward). Values only: the deflected own
+// intensive quantities are re-evaluated, the neighbours' come from the cache.
+
+struct FdState {
+    double pw, Sw, pc, lw, ln;
+};
+
+// local residual of element s at own state st: own row R (volumetric) and the neighbour rows Fn
+// per face slot (band order -x, +x, -y, +y[, -z, +z]; zero where no neighbour)
+template <int DIM>
+__device__ __forceinline__ void fd_local_residual(const Phys& P, int col, int64_t h, const CellIdx& ci,
+                                                  const FdState& st, double Ki, int lensI, double2 so, double dt,
+                                                  const double2* __restrict__ x, const double* __restrict__ perm,
+                                                  const double* __restrict__ iq, double R[2], double Fn[6][2]) {
+    const int64_t N = P.N;
+    const int idx[3] = {ci.i, ci.j, ci.k};
+    const double pI[2] = {st.pw, st.pw + (st.pc - 0.0)};
+    const double lam[2] = {st.lw, st.ln};
+    const double zero2[2] = {0.0, 0.0};
+    double Ddummy[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    R[0] = R[1] = 0.0;
+#pragma unroll
+    for (int axis = 0; axis < DIM; ++axis) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int q = 2 * axis + side;
+            Fn[q][0] = Fn[q][1] = 0.0;
+            const int64_t sj = neighbour_split(P, col, h, ci, axis, side);
+            if (sj < 0) continue;
+            const double2 xj = x[sj];
+            const double lamj[2] = {iq[2 * N + sj], iq[4 * N + sj]};
+            double F[2] = {0.0, 0.0};
+            double Dj[4];
+            if (axis == 0)
+                interior_face<0>(P, side, idx[0], Ki, pI, 0.0, lam, zero2, xj, perm[sj], iq[sj], lamj, F, Ddummy, Dj);
+            else if (axis == 1)
+                interior_face<1>(P, side, idx[1], Ki, pI, 0.0, lam, zero2, xj, perm[sj], iq[sj], lamj, F, Ddummy, Dj);
+            else
+                interior_face<2>(P, side, idx[2], Ki, pI, 0.0, lam, zero2, xj, perm[sj], iq[sj], lamj, F, Ddummy, Dj);
+            R[0] += F[0];
+            R[1] += F[1];
+            Fn[q][0] = (0.0 - F[0]) / P.vol;
+            Fn[q][1] = (0.0 - F[1]) / P.vol;
+        }
+    }
+    {
+        const double fac = P.vol / dt;
+        const double sw0 = P.porosity * st.Sw * P.rho[0];
+        const double sn0 = P.porosity * (1.0 - (0.0 + st.Sw)) * P.rho[1];
+        R[0] += (sw0 - so.x) * fac;
+        R[1] += (sn0 - so.y) * fac;
+    }
+    const int nAx[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+    for (int axis = 0; axis < DIM; ++axis) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const bool has = side == 0 ? idx[axis] > 0 : idx[axis] < nAx[axis] - 1;
+            if (has) continue;
+            if (axis == 0)
+                boundary_face<DIM, 0>(P, side, idx, lensI, Ki, pI, 0.0, lam, zero2, R, Ddummy);
+            else if (axis == 1)
+                boundary_face<DIM, 1>(P, side, idx, lensI, Ki, pI, 0.0, lam, zero2, R, Ddummy);
+            else
+                boundary_face<DIM, 2>(P, side, idx, lensI, Ki, pI, 0.0, lam, zero2, R, Ddummy);
+        }
+    }
+    R[0] /= P.vol;
+    R[1] /= P.vol;
+}
+
+template <int DIM>
+__device__ __forceinline__ FdState fd_state(const Phys& P, const LawDev& L, double pw, double Sw) {
+    const MatOut m = material(L, Sw);
+    return FdState{pw, Sw, m.pc.v, m.krw.v / P.mu[0], m.krn.v / P.mu[1]};
+}
+
+template <int DIM, typename JT>
+__global__ void __launch_bounds__(kLinBlock) k_assemble_fd(
+    const __grid_constant__ Phys P, const double2* __restrict__ x, const double2* __restrict__ sold,
+    const double* __restrict__ perm, const uint8_t* __restrict__ lens, const double* __restrict__ iq, double dt,
+    double refPressure, int method, double2* __restrict__ rOut, JT* __restrict__ J, unsigned long long* errmax,
+    int* flags) {
+    const int64_t N = P.N;
+    const double baseEps = fmax(0.9123e-10, 2.220446049250313e-16 * 1.23e3);
+    double localMax = 0.0;
+    int bad = 0;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int col = s >= P.Nh ? 1 : 0;
+        const int64_t h = s - col * P.Nh;
+        const CellIdx ci = cell_of(P, col, h);
+        const double2 xi = x[s];
+        const double Ki = perm[s];
+        const int li = lens[s];
+        const double2 so = sold[s];
+        const FdState base{xi.x, xi.y, iq[s], iq[2 * N + s], iq[4 * N + s]};
+        double R0[2], F0[6][2];
+        fd_local_residual<DIM>(P, col, h, ci, base, Ki, li, so, dt, x, perm, iq, R0, F0);
+        rOut[s] = make_double2(R0[0], R0[1]);
+        const double e = fmax(fabs(R0[0]), fabs(R0[1]));
+        if (!(fabs(R0[0]) <= 1.7976931348623157e308) || !(fabs(R0[1]) <= 1.7976931348623157e308)) bad = 1;
+        localMax = fmax(localMax, e);
+        double Jd[4];
+        double Jn[6][4];
+#pragma unroll
+        for (int pv = 0; pv < 2; ++pv) {
+            const double pvWeight = pv == 0 ? 10 / refPressure : 1.0;
+            const double eps = baseEps / pvWeight;
+            double pri[2] = {xi.x, xi.y};
+            double delta = 0.0;
+            double dR[2], dF[6][2];
+            double Rp[2], Fp[6][2];
+            if (method >= 0) {
+                pri[pv] += eps;
+                delta += eps;
+                fd_local_residual<DIM>(P, col, h, ci, fd_state<DIM>(P, P.law[li], pri[0], pri[1]), Ki, li, so, dt, x,
+                                       perm, iq, Rp, Fp);
+                dR[0] = Rp[0]; dR[1] = Rp[1];
+                for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] = Fp[q][0]; dF[q][1] = Fp[q][1]; }
+            } else {
+                dR[0] = R0[0]; dR[1] = R0[1];
+                for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] = F0[q][0]; dF[q][1] = F0[q][1]; }
+            }
+            if (method <= 0) {
+                pri[pv] -= delta + eps;
+                delta += eps;
+                fd_local_residual<DIM>(P, col, h, ci, fd_state<DIM>(P, P.law[li], pri[0], pri[1]), Ki, li, so, dt, x,
+                                       perm, iq, Rp, Fp);
+                dR[0] -= Rp[0]; dR[1] -= Rp[1];
+                for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] -= Fp[q][0]; dF[q][1] -= Fp[q][1]; }
+            } else {
+                dR[0] -= R0[0]; dR[1] -= R0[1];
+                for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] -= F0[q][0]; dF[q][1] -= F0[q][1]; }
+            }
+            // block entry [eq][pv]
+            Jd[pv] = dR[0] / delta;
+            Jd[2 + pv] = dR[1] / delta;
+            for (int q = 0; q < 2 * DIM; ++q) {
+                Jn[q][pv] = dF[q][0] / delta;
+                Jn[q][2 + pv] = dF[q][1] / delta;
+            }
+        }
+        store_block(J, N, 0, s, Jd);
+#pragma unroll
+        for (int axis = 0; axis < DIM; ++axis)
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int64_t sj = neighbour_split(P, col, h, ci, axis, side);
+                if (sj >= 0) store_block(J, N, opposite_band(band_of(axis, side)), sj, Jn[2 * axis + side]);
+            }
+    }
+    if (bad) atomicOr(flags, 1);
+    block_max_publish(localMax, errmax);
+}
+
 // S_w = 1 state of the free-flow boundary per region: p_cnw and k_r / mu of both phases
 __global__ void k_boundary_constants(const __grid_constant__ Phys P, double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -266,6 +429,12 @@ cudaError_t boundary_constants(Phys& P, cudaStream_t stream) {
 
 ewg_status compute_boundary_constants(ewg_ctx* ctx) {
     return cuda_fail(ctx, boundary_constants(ctx->P, ctx->stream), "boundary constants");
+}
+
+ewg_status launch_intensive(ewg_ctx* ctx, const double2* x) {
+    int g1 = grid_size_for(ctx, (const void*)k_intensive, kLinBlock);
+    EWG_LAUNCH(ctx, K_INTENSIVE, k_intensive, g1, kLinBlock, ctx->P, x, ctx->lens, ctx->iq);
+    return cuda_fail(ctx, cudaGetLastError(), "k_intensive");
 }
 
 ewg_status launch_initial_solution(ewg_ctx* ctx, double2* x) {
@@ -342,7 +511,20 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
     EWG_LAUNCH(ctx, K_INTENSIVE, k_intensive, g1, kLinBlock, ctx->P, x, ctx->lens, ctx->iq);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_intensive");
     const bool three = ctx->P.dim == 3;
-    if (three) {
+    if (withJacobian && ctx->localLinearizer == EWG_LOCAL_LINEARIZER_FD) {
+        const int m = ctx->fdMethod;
+        if (ctx->jacPrecision == EWG_PRECISION_MIXED) {
+            auto k = three ? k_assemble_fd<3, float> : k_assemble_fd<2, float>;
+            int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
+            EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
+                       ctx->refPressure, m, r, ctx->J32, ctx->d_errmax, ctx->d_flags);
+        } else {
+            auto k = three ? k_assemble_fd<3, double> : k_assemble_fd<2, double>;
+            int g2 = grid_size_for(ctx, (const void*)k, kLinBlock);
+            EWG_LAUNCH(ctx, K_ASSEMBLE, k, g2, kLinBlock, ctx->P, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
+                       ctx->refPressure, m, r, ctx->J, ctx->d_errmax, ctx->d_flags);
+        }
+    } else if (three) {
         if (!withJacobian)
             launch_assemble3<double, false>(ctx, dt, x, r, nullptr);
         else if (ctx->jacPrecision == EWG_PRECISION_MIXED)

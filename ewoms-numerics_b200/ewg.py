@@ -31,6 +31,7 @@ STATUS_NAMES = {0: "EWG_OK", 1: "EWG_ERR_INVALID", 2: "EWG_ERR_CUDA", 3: "EWG_ER
 LAW_VG, LAW_BC = 0, 1
 PRECOND_ILU0, PRECOND_JACOBI = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+LOCAL_LINEARIZER_AD, LOCAL_LINEARIZER_FD = 0, 1
 
 
 class Grid(C.Structure):
@@ -112,7 +113,7 @@ class EnsembleReport(C.Structure):
 
 class EnsembleStats(C.Structure):
     _fields_ = [("rounds", C.c_int32), ("linear_iterations", C.c_int32), ("t_linearize", C.c_double),
-                ("t_solve", C.c_double), ("t_update", C.c_double)]
+                ("t_solve", C.c_double), ("t_update", C.c_double), ("cell_iterations", C.c_double)]
 
 
 ENSEMBLE_KERNEL_CLASSES = ("intensive", "assemble", "factor", "cell", "ilu_black", "ilu_red",
@@ -324,6 +325,9 @@ def load(path: str = LIB_PATH):
         "ewg_advance_time_level": (C.c_int, [C.c_void_p]),
         "ewg_restore_time_level": (C.c_int, [C.c_void_p]),
         "ewg_linearize": (C.c_int, [C.c_void_p, d, P(LinReport)]),
+        "ewg_set_local_linearizer": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "ewg_update_begin": (C.c_int, [C.c_void_p]),
+        "ewg_get_intensive_quantities": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_get_residual": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(d)]),
         "ewg_residual_norm": (C.c_int, [C.c_void_p, P(d), d, P(d)]),
@@ -447,6 +451,21 @@ class Context:
 
     def restore_time_level(self):
         self._check(self.lib.ewg_restore_time_level(self.h), "restore_time_level")
+
+    def set_local_linearizer(self, kind: int, method: int = 1):
+        """LOCAL_LINEARIZER_AD (default) or LOCAL_LINEARIZER_FD with NumericDifferenceMethod
+        `method` (-1 backward, 0 central, +1 forward)."""
+        self._check(self.lib.ewg_set_local_linearizer(self.h, kind, method), "set_local_linearizer")
+
+    def update_begin(self):
+        """ImmiscibleModel::updateBegin: records the FD linearizer's reference pressure."""
+        self._check(self.lib.ewg_update_begin(self.h), "update_begin")
+
+    def intensive_quantities(self):
+        """N x {p_cnw, lambda_w, lambda_n} of solution(0), natural order."""
+        out = np.zeros((self.n, 3))
+        self._check(self.lib.ewg_get_intensive_quantities(self.h, _ptr(out)), "intensive_quantities")
+        return out
 
     def linearize(self, dt) -> LinReport:
         rep = LinReport()

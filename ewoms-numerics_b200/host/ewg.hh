@@ -48,6 +48,15 @@ public:
     void advanceTimeLevel() { check(ewg_advance_time_level(ctx_), "ewg_advance_time_level"); }
     void restoreTimeLevel() { check(ewg_restore_time_level(ctx_), "ewg_restore_time_level"); }
 
+    void setLocalLinearizer(int kind, int numericDifferenceMethod) {
+        check(ewg_set_local_linearizer(ctx_, kind, numericDifferenceMethod), "ewg_set_local_linearizer");
+    }
+    void updateBegin() { check(ewg_update_begin(ctx_), "ewg_update_begin"); }
+    // N x {p_cnw, lambda_w, lambda_n} of solution(0)
+    void getIntensiveQuantities(double* out) {
+        check(ewg_get_intensive_quantities(ctx_, out), "ewg_get_intensive_quantities");
+    }
+
     ewg_lin_report linearize(double dt) {
         ewg_lin_report rep{};
         check(ewg_linearize(ctx_, dt, &rep), "ewg_linearize");

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "ewg.hh"
+#include "vtkwriter.hh"
 
 namespace {
 
@@ -38,6 +39,8 @@ struct Params {
         {"PreconditionerRelaxation", "1"}, {"Preconditioner", "ilu0"},
         {"LinearSolverPrecision", "fp64"}, {"RestartOnBreakdown", "1"},
         {"PermFile", ""},              {"Output", ""},
+        {"EnableVtkOutput", "1"},      {"OutputDir", "."},
+        {"LocalLinearizer", "ad"},     {"NumericDifferenceMethod", "1"},
     };
     std::string get(const std::string& k) const {
         auto it = values.find(k);
@@ -223,6 +226,32 @@ NewtonResult newtonApply(ewg::Context& ctx, double dt, const Params& p, const ew
     return res;
 }
 
+// the fields of VtkMultiPhaseModule for solution(0): pressures, densities, saturations,
+// mobilities, relative permeabilities, viscosities, porosity, intrinsic permeability
+std::vector<ewg::VtkMultiWriter::Field> vtkFields(ewg::Context& ctx, const ewg_grid& g, const ewg_problem& pr,
+                                                  const std::vector<double>& perm) {
+    const int64_t N = ctx.numCells();
+    std::vector<double> x(2 * N), iq(3 * N);
+    ctx.getSolution(0, x.data());
+    ctx.getIntensiveQuantities(iq.data());
+    using F = ewg::VtkMultiWriter::Field;
+    std::vector<F> f = {{"pressure_w", 1, {}}, {"pressure_n", 1, {}}, {"density_w", 1, {}}, {"density_n", 1, {}},
+                        {"saturation_w", 1, {}}, {"saturation_n", 1, {}}, {"mobility_w", 1, {}},
+                        {"mobility_n", 1, {}}, {"relativePerm_w", 1, {}}, {"relativePerm_n", 1, {}},
+                        {"viscosity_w", 1, {}}, {"viscosity_n", 1, {}}, {"porosity", 1, {}},
+                        {"intrinsicPerm", g.dim * g.dim, {}}};
+    for (auto& fi : f) fi.values.reserve(N * fi.components);
+    for (int64_t c = 0; c < N; ++c) {
+        const double pw = x[2 * c], sw = x[2 * c + 1], pc = iq[3 * c], lw = iq[3 * c + 1], ln = iq[3 * c + 2];
+        const double v[13] = {pw, pw + pc, pr.rho_w, pr.rho_n, sw, 1.0 - sw, lw, ln,
+                              lw * pr.mu_w, ln * pr.mu_n, pr.mu_w, pr.mu_n, pr.porosity};
+        for (int k = 0; k < 13; ++k) f[k].values.push_back(v[k]);
+        for (int r = 0; r < g.dim; ++r)
+            for (int q = 0; q < g.dim; ++q) f[13].values.push_back(r == q ? perm[c] : 0.0);
+    }
+    return f;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -253,7 +282,15 @@ int main(int argc, char** argv) {
         so.precond = p.get("Preconditioner") == "jacobi" ? EWG_PRECOND_JACOBI : EWG_PRECOND_ILU0;
         so.precision = p.get("LinearSolverPrecision") == "mixed" ? EWG_PRECISION_MIXED : EWG_PRECISION_FP64;
         so.restart_on_breakdown = p.i("RestartOnBreakdown");
+        const std::string ll = p.get("LocalLinearizer");
+        if (ll != "ad" && ll != "fd") throw std::runtime_error("LocalLinearizer must be 'ad' or 'fd'");
+        ctx.setLocalLinearizer(ll == "fd" ? EWG_LOCAL_LINEARIZER_FD : EWG_LOCAL_LINEARIZER_AD,
+                               p.i("NumericDifferenceMethod"));
         ctx.applyInitialSolution();
+        // LensProblem::name(): lens_<model>_<discretization>[_ad]
+        ewg::VtkMultiWriter vtk(p.get("OutputDir"), ll == "ad" ? "lens_immiscible_ecfv_ad" : "lens_immiscible_ecfv");
+        const bool vtkOut = p.i("EnableVtkOutput") != 0;
+        if (vtkOut) vtk.write(0.0, g, vtkFields(ctx, g, pr, perm));
         const double endTime = p.d("EndTime");
         const double maxDt = p.d("MaxTimeStepSize");
         const int maxDivisions = p.i("MaxTimeStepDivisions");
@@ -267,6 +304,7 @@ int main(int argc, char** argv) {
             NewtonResult nr;
             bool ok = false;
             for (int attempt = 0; attempt < maxDivisions; ++attempt) {
+                ctx.updateBegin();  // model.update() -> updateBegin() before NewtonMethod::apply
                 if (so.precision == EWG_PRECISION_MIXED) {
                     // ewg_newton_apply selects the Jacobian precision; the low-level path uses
                     // the FP64 Jacobian, so mixed precision runs through the high-level call
@@ -297,6 +335,7 @@ int main(int argc, char** argv) {
             ++step;
             std::printf("Time step %d done. t=%g s, dt=%g s, Newton iterations %d, linear iterations %d\n",
                         step, t, dt, nr.iterations, nr.linearIterations);
+            if (vtkOut) vtk.write(t, g, vtkFields(ctx, g, pr, perm));
             // nextTimeStepSize: min(MaxTimeStepSize, suggestTimeStepSize(dt))
             int n = nr.iterations;
             double next = n > target ? dt / (1.0 + double(n - target) / target)

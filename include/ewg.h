@@ -93,6 +93,12 @@ typedef struct ewg_problem {
     ewg_material lens;              /* material inside the lens */
 } ewg_problem;
 
+/* LocalLinearizerSplice: how the local Jacobian of an element is formed. */
+typedef enum ewg_local_linearizer {
+    EWG_LOCAL_LINEARIZER_AD = 0,  /* AutoDiffLocalLinearizer (fvbaseadlocallinearizer.hh:178-297), default */
+    EWG_LOCAL_LINEARIZER_FD = 1   /* FiniteDifferenceLocalLinearizer (fvbasefdlocallinearizer.hh:221-453) */
+} ewg_local_linearizer;
+
 typedef enum ewg_precond_kind {
     EWG_PRECOND_ILU0 = 0,       /* block ILU(0), red-black (2-colour) ordering on the device */
     EWG_PRECOND_JACOBI = 1      /* block Jacobi, one sweep with relaxation */
@@ -195,6 +201,17 @@ ewg_status ewg_restore_time_level(ewg_ctx* ctx);
 
 /* ---- FvBaseLinearizer ---------------------------------------------------------------- */
 
+/* Select the local linearizer (SET_TAG_PROP(..., LocalLinearizerSplice, ...)). For
+ * EWG_LOCAL_LINEARIZER_FD, numeric_difference_method is NumericDifferenceMethod: -1 backward,
+ * 0 central, +1 forward differences (the reference's default); the deflection is
+ * BaseEpsilon / primaryVarWeight with the pressure weight 10 / p_ref (immisciblemodel.hh:298-310). */
+ewg_status ewg_set_local_linearizer(ewg_ctx* ctx, int32_t kind, int32_t numeric_difference_method);
+/* FvBaseDiscretization::updateBegin (ImmiscibleModel::updateBegin, immisciblemodel.hh:278-293):
+ * records p_ref = p_w of cell 0 of solution(0). model.update() calls it before every Newton solve
+ * (fvbasediscretization.hh:1242); ewg_newton_apply does so itself, and a context that never ran it
+ * takes p_ref from solution(0) at its first finite-difference linearization. */
+ewg_status ewg_update_begin(ewg_ctx* ctx);
+
 /* linearizeDomain() at the current iterate with time-step size dt: residual r(x) and Jacobian
  * dr/dx into device buffers (fvbaselinearizer.hh:166-197, 401-512). */
 ewg_status ewg_linearize(ewg_ctx* ctx, double dt, ewg_lin_report* report);
@@ -203,6 +220,10 @@ ewg_status ewg_get_residual(ewg_ctx* ctx, double* r);
 /* jacobian() as the reference's BCRS: row_ptr[N+1], col_idx[nnzb] (sorted per row), blocks
  * [nnzb][2][2]. Any pointer may be NULL to skip it. */
 ewg_status ewg_get_jacobian_bcrs(ewg_ctx* ctx, int32_t* row_ptr, int32_t* col_idx, double* blocks);
+/* Intensive quantities of solution(0) per cell, natural order, N x {p_cnw, lambda_w, lambda_n}
+ * (ImmiscibleIntensiveQuantities, immiscibleintensivequantities.hh:87-145; lambda = k_r / mu):
+ * what VtkMultiPhaseModule writes (io/vtkmultiphasemodule.hh:318-337). */
+ewg_status ewg_get_intensive_quantities(ewg_ctx* ctx, double* out);
 /* Residual-only evaluation at x (natural order, N x 2) without touching the Jacobian or the
  * stored iterate: max-norm of r(x). Used by the Newton initial-guess fallback. */
 ewg_status ewg_residual_norm(ewg_ctx* ctx, const double* x, double dt, double* max_norm);
@@ -330,6 +351,7 @@ typedef struct ewg_ensemble_stats {
     int32_t rounds;             /* supersteps that linearized at least one member */
     int32_t linear_iterations;  /* BiCGStab iterations summed over members */
     double t_linearize, t_solve, t_update;  /* device seconds per phase */
+    double cell_iterations;     /* sum over members of cells x BiCGStab iterations */
 } ewg_ensemble_stats;
 
 void ewg_default_ensemble_opts(ewg_ensemble_opts* opts);

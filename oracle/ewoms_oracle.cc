@@ -249,6 +249,12 @@ struct Ctx {
     std::vector<double> blocks;      // nnzb x 4
     std::vector<IQ> iqCache;
     bool recycleStorage = true;
+    // LocalLinearizerSplice: false = AutoDiffLocalLinearizer, true = FiniteDifferenceLocalLinearizer
+    // with NumericDifferenceMethod fdMethod (-1 backward, 0 central, +1 forward) and the reference
+    // pressure of ImmiscibleModel::updateBegin for the pressure weight (immisciblemodel.hh:278-310)
+    bool fd = false;
+    int fdMethod = 1;
+    double refPressure = -1.0;  // unset until updateBegin
     int nthreads = 1;
     std::string err;
 
@@ -289,16 +295,16 @@ struct Ctx {
     double gravity(int a) const { return a == 1 ? -prob.gravity : 0.0; }
 };
 
-static IQ computeIQ(const Ctx& C, int64_t c, const double* x, bool variable) {
+static IQ computeIQAt(const Ctx& C, int64_t c, double pw, double sw, bool variable) {
     IQ q;
     const Law& L = C.law[C.inLens[c]];
-    Eval Sw = variable ? Eval::variable(x[2 * c + 1], 1) : Eval(x[2 * c + 1]);
+    Eval Sw = variable ? Eval::variable(sw, 1) : Eval(sw);
     q.S[0] = Sw;
     q.S[1] = 1.0 - (Eval(0.0) + Sw);
     Eval pC[2];
     capillaryPressures(pC, L, q.S[0]);
     relativePermeabilities(q.kr, L, q.S[0]);
-    Eval p0 = variable ? Eval::variable(x[2 * c + 0], 0) : Eval(x[2 * c + 0]);
+    Eval p0 = variable ? Eval::variable(pw, 0) : Eval(pw);
     for (int a = 0; a < 2; ++a) q.p[a] = p0 + (pC[a] - pC[0]);
     q.mu[0] = Eval(C.prob.mu_w); q.mu[1] = Eval(C.prob.mu_n);
     q.rho[0] = Eval(C.prob.rho_w); q.rho[1] = Eval(C.prob.rho_n);
@@ -306,6 +312,9 @@ static IQ computeIQ(const Ctx& C, int64_t c, const double* x, bool variable) {
     q.porosity = C.prob.porosity;
     q.K = C.perm[c];
     return q;
+}
+static IQ computeIQ(const Ctx& C, int64_t c, const double* x, bool variable) {
+    return computeIQAt(C, c, x[2 * c + 0], x[2 * c + 1], variable);
 }
 
 // ImmiscibleLocalResidual::computeStorage: phi * S_a * rho_a
@@ -456,19 +465,12 @@ static void boundaryRate(const Ctx& C, int64_t ci, const Face& f, const IQ& qi, 
 
 // FvBaseAdLocalLinearizer::linearize + FvBaseLocalResidual::eval for one element, then the
 // column scatter of FvBaseLinearizer::linearizeElement_.
-static void linearizeElement(Ctx& C, int64_t e, double dt, int newtonIteration,
-                             const std::vector<int32_t>& diagPos, double* errOut) {
-    Face f[6];
-    C.faces(e, f);
-    const int nf = C.numFaces();
-    // stencil DOFs: the element, then one DOF per neighbouring element (intersection order)
-    int64_t dofs[7]; int ndof = 0;
-    dofs[ndof++] = e;
-    int faceDof[6];
-    for (int k = 0; k < nf; ++k) { faceDof[k] = -1; if (f[k].nbr >= 0) { faceDof[k] = ndof; dofs[ndof++] = f[k].nbr; } }
-    const IQ& qi = C.iqCache[e];
-    // local residual: one 2-vector of AD values per stencil DOF (eq index == phase index)
-    Eval R[7][2];
+// FvBaseLocalResidual::eval for one element whose own DOF has the intensive quantities qi:
+// fluxes, volume terms, boundary, volumetric division. `stashed` marks a finite-difference
+// evaluation at deflected primary variables, which reads the storage cache and never writes it
+// (fvbaselocalresidual.hh:541-567, haveStashedIntensiveQuantities()).
+static void evalLocal(Ctx& C, int64_t e, const IQ& qi, double dt, int newtonIteration, bool stashed,
+                      const Face f[6], int nf, const int faceDof[6], int ndof, Eval R[7][2]) {
     for (int d = 0; d < ndof; ++d) { R[d][0] = Eval(0.0); R[d][1] = Eval(0.0); }
     // evalFluxes: residual[i] += flux, residual[j] -= flux
     for (int k = 0; k < nf; ++k) {
@@ -487,7 +489,7 @@ static void linearizeElement(Ctx& C, int64_t e, double dt, int newtonIteration,
         Eval tmp[2];
         storageOf<Eval>(qi, tmp);
         double tmp2[2];
-        if (newtonIteration == 0) {
+        if (newtonIteration == 0 && !stashed) {
             if (!C.recycleStorage) {
                 IQ qold = computeIQ(C, e, C.sol[1].data(), false);
                 storageOf<double>(qold, tmp2);
@@ -517,6 +519,53 @@ static void linearizeElement(Ctx& C, int64_t e, double dt, int newtonIteration,
     for (int d = 0; d < ndof; ++d) {
         double V = C.vol();
         for (int a = 0; a < 2; ++a) R[d][a] /= V;
+    }
+}
+
+// FvBaseAdLocalLinearizer::linearize (AD) or FvBaseFdLocalLinearizer::linearize (finite
+// differences, fvbasefdlocallinearizer.hh:221-237, 393-453) for one element, then the column
+// scatter of FvBaseLinearizer::linearizeElement_.
+static void linearizeElement(Ctx& C, int64_t e, double dt, int newtonIteration,
+                             const std::vector<int32_t>& diagPos, double* errOut) {
+    Face f[6];
+    C.faces(e, f);
+    const int nf = C.numFaces();
+    // stencil DOFs: the element, then one DOF per neighbouring element (intersection order)
+    int64_t dofs[7]; int ndof = 0;
+    dofs[ndof++] = e;
+    int faceDof[6];
+    for (int k = 0; k < nf; ++k) { faceDof[k] = -1; if (f[k].nbr >= 0) { faceDof[k] = ndof; dofs[ndof++] = f[k].nbr; } }
+    // local residual: one 2-vector of AD values per stencil DOF (eq index == phase index)
+    Eval R[7][2];
+    evalLocal(C, e, C.iqCache[e], dt, newtonIteration, false, f, nf, faceDof, ndof, R);
+    if (C.fd) {
+        // BaseEpsilon / primaryVarWeight; the weight is 10 / p_ref for the pressure, 1 otherwise
+        const double baseEps = std::max(0.9123e-10, std::numeric_limits<double>::epsilon() * 1.23e3);
+        for (int pv = 0; pv < 2; ++pv) {
+            const double pvWeight = pv == 0 ? 10 / C.refPressure : 1.0;
+            const double eps = baseEps / pvWeight;
+            double priVars[2] = {C.sol[0][2 * e], C.sol[0][2 * e + 1]};
+            double delta = 0.0;
+            double deriv[7][2];
+            Eval Rp[7][2];
+            if (C.fdMethod >= 0) {
+                priVars[pv] += eps;
+                delta += eps;
+                evalLocal(C, e, computeIQAt(C, e, priVars[0], priVars[1], false), dt, newtonIteration, true, f, nf, faceDof, ndof, Rp);
+                for (int d = 0; d < ndof; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] = Rp[d][a].v;
+            } else {
+                for (int d = 0; d < ndof; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] = R[d][a].v;
+            }
+            if (C.fdMethod <= 0) {
+                priVars[pv] -= delta + eps;
+                delta += eps;
+                evalLocal(C, e, computeIQAt(C, e, priVars[0], priVars[1], false), dt, newtonIteration, true, f, nf, faceDof, ndof, Rp);
+                for (int d = 0; d < ndof; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] -= Rp[d][a].v;
+            } else {
+                for (int d = 0; d < ndof; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] -= R[d][a].v;
+            }
+            for (int d = 0; d < ndof; ++d) for (int a = 0; a < 2; ++a) R[d][a].d[pv] = deriv[d][a] / delta;
+        }
     }
     // scatter: residual row of the focus DOF and the Jacobian column of the focus DOF
     C.resid[2 * e] = R[0][0].v; C.resid[2 * e + 1] = R[0][1].v;
@@ -909,6 +958,8 @@ const char* orc_last_error(const orc_ctx* c) { return c->C.err.c_str(); }
 int64_t orc_num_cells(const orc_ctx* c) { return c->C.N; }
 int64_t orc_num_blocks(const orc_ctx* c) { return (int64_t)c->C.colIdx.size(); }
 void orc_set_recycle_first_iteration_storage(orc_ctx* c, int on) { c->C.recycleStorage = on != 0; }
+// kind 0: AD, 1: finite differences with NumericDifferenceMethod `method`
+void orc_set_local_linearizer(orc_ctx* c, int kind, int method) { c->C.fd = kind == 1; c->C.fdMethod = method; }
 
 void orc_set_solution(orc_ctx* c, int t, const double* x) { c->C.sol[t].assign(x, x + 2 * c->C.N); }
 void orc_get_solution(const orc_ctx* c, int t, double* x) { std::memcpy(x, c->C.sol[t].data(), sizeof(double) * 2 * c->C.N); }
@@ -928,7 +979,10 @@ void orc_apply_initial_solution(orc_ctx* o) {
 }
 void orc_advance_time_level(orc_ctx* o) { o->C.sol[1] = o->C.sol[0]; }
 
+void orc_update_begin(orc_ctx* o) { o->C.refPressure = o->C.sol[0][0]; }
 int orc_linearize(orc_ctx* o, double dt, int it, double* error) {
+    // a context that never ran updateBegin takes the reference pressure of the current iterate
+    if (o->C.fd && !(o->C.refPressure > 0)) o->C.refPressure = o->C.sol[0][0];
     try {
         double e = linearize(o->C, dt, it);
         if (error) *error = e;
@@ -1032,6 +1086,8 @@ int orc_newton_apply(orc_ctx* o, double dt, const ewg_newton_opts* no, const ewg
         return true;
     };
     int status = 0;
+    // ImmiscibleModel::updateBegin, called before every Newton solve: p_w of the first DOF
+    C.refPressure = C.sol[0][0];
     try {
         while (proceed()) {
             lastError = error;

@@ -52,6 +52,8 @@ def load():
         "orc_num_cells": (C.c_int64, [C.c_void_p]),
         "orc_num_blocks": (C.c_int64, [C.c_void_p]),
         "orc_set_recycle_first_iteration_storage": (None, [C.c_void_p, C.c_int]),
+        "orc_set_local_linearizer": (None, [C.c_void_p, C.c_int, C.c_int]),
+        "orc_update_begin": (None, [C.c_void_p]),
         "orc_set_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_get_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_apply_initial_solution": (None, [C.c_void_p]),
@@ -114,6 +116,15 @@ class Oracle:
 
     def set_recycle_first_iteration_storage(self, on: bool):
         self.lib.orc_set_recycle_first_iteration_storage(self.h, int(on))
+
+    def set_local_linearizer(self, kind: int, method: int = 1):
+        """kind 0: AutoDiffLocalLinearizer; 1: FiniteDifferenceLocalLinearizer with
+        NumericDifferenceMethod `method` (-1 backward, 0 central, +1 forward)."""
+        self.lib.orc_set_local_linearizer(self.h, int(kind), int(method))
+
+    def update_begin(self):
+        """ImmiscibleModel::updateBegin: the reference pressure for the FD pressure weight."""
+        self.lib.orc_update_begin(self.h)
 
     def set_solution(self, t, x):
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)

@@ -44,7 +44,8 @@ def test_driver_ten_steps_match_oracle(driver, tmp_path, preset):
     # the golden run uses a fixed dt = 250 s; with NewtonTargetIterations = 18 the reference's
     # suggestTimeStepSize never shrinks the step below MaxTimeStepSize (newtonmethod.hh:527-544)
     out = subprocess.run([driver, f"--preset={preset}", "--end-time=2500", "--initial-time-step-size=250",
-                          "--max-time-step-size=250", "--newton-target-iterations=18", f"--output={outf}"],
+                          "--max-time-step-size=250", "--newton-target-iterations=18", f"--output={outf}",
+                          f"--output-dir={tmp_path}"],
                          capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     steps = [ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]
@@ -55,3 +56,78 @@ def test_driver_ten_steps_match_oracle(driver, tmp_path, preset):
     xo = gold[f"{preset}_run10_x"]
     assert rel_close(x[:, 0], xo[:, 0], 1e-8)[0]
     assert np.max(np.abs(x[:, 1] - xo[:, 1])) <= 1e-8
+
+
+def _vtu_fields(path):
+    import xml.etree.ElementTree as ET
+    root = ET.parse(path).getroot()
+    piece = root.find("UnstructuredGrid/Piece")
+    fields = {a.get("Name"): np.array(a.text.split(), dtype=np.float64)
+              for a in piece.find("CellData").findall("DataArray")}
+    return piece, fields
+
+
+def test_vtk_writer_layout(tmp_path):
+    """The VTK writer on its own (host code, no device): point / cell counts, connectivity of a
+    hexahedron, field lengths, and the collection file listing every step."""
+    src = tmp_path / "vtk.cc"
+    src.write_text(r'''
+#include "vtkwriter.hh"
+int main(int argc, char** argv) {
+    ewg_grid g{}; g.dim = 3; g.nx = 3; g.ny = 2; g.nz = 2; g.lx = 3.0; g.ly = 1.0; g.lz = 2.0;
+    ewg::VtkMultiWriter w(argv[1], "probe");
+    for (int s = 0; s < 2; ++s) {
+        std::vector<ewg::VtkMultiWriter::Field> f = {{"saturation_w", 1, {}}, {"intrinsicPerm", 9, {}}};
+        for (int c = 0; c < 12; ++c) {
+            f[0].values.push_back(c + 0.5 * s);
+            for (int k = 0; k < 9; ++k) f[1].values.push_back(k % 4 == 0 ? 1e-12 * (c + 1) : 0.0);
+        }
+        w.write(250.0 * s, g, f);
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "vtk"
+    subprocess.check_call(["g++", "-std=c++17", "-I", os.path.join(ROOT, "ewoms-numerics_b200", "host"),
+                           str(src), "-o", str(exe)])
+    subprocess.check_call([str(exe), str(tmp_path)])
+    piece, f = _vtu_fields(tmp_path / "probe-00001.vtu")
+    assert piece.get("NumberOfPoints") == str(4 * 3 * 3) and piece.get("NumberOfCells") == "12"
+    assert np.array_equal(f["saturation_w"], np.arange(12) + 0.5)
+    assert f["intrinsicPerm"].shape == (108,) and f["intrinsicPerm"][9] == 2e-12
+    conn = np.array(piece.find("Cells/DataArray[@Name='connectivity']").text.split(), dtype=np.int64)
+    # first hexahedron: points (0,0,0) (1,0,0) (1,1,0) (0,1,0) and the same one layer up
+    assert list(conn[:8]) == [0, 1, 5, 4, 12, 13, 17, 16]
+    pvd = (tmp_path / "probe.pvd").read_text()
+    assert 'timestep="0"' in pvd and 'timestep="250"' in pvd and "probe-00001.vtu" in pvd
+
+
+@pytest.mark.gpu
+def test_driver_vtk_output(driver, tmp_path):
+    """VtkMultiWriter output of the driver: one .vtu per step plus the initial state, listed in the
+    .pvd, with the final fields equal to the solution the driver writes."""
+    outf = tmp_path / "x.bin"
+    out = subprocess.run([driver, "--preset=baseline", "--end-time=500", "--initial-time-step-size=250",
+                          "--max-time-step-size=250", f"--output={outf}", f"--output-dir={tmp_path}"],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    names = sorted(p.name for p in tmp_path.glob("lens_immiscible_ecfv_ad-*.vtu"))
+    assert names == ["lens_immiscible_ecfv_ad-00000.vtu", "lens_immiscible_ecfv_ad-00001.vtu",
+                     "lens_immiscible_ecfv_ad-00002.vtu"]
+    piece, f = _vtu_fields(tmp_path / names[-1])
+    x = np.fromfile(outf, dtype=np.float64).reshape(-1, 2)
+    assert np.array_equal(f["pressure_w"], x[:, 0]) and np.array_equal(f["saturation_w"], x[:, 1])
+    assert np.allclose(f["saturation_n"], 1.0 - x[:, 1])
+    assert np.all(f["pressure_n"] >= f["pressure_w"])
+    assert np.all((f["relativePerm_w"] >= 0) & (f["relativePerm_w"] <= 1))
+    assert "lens_immiscible_ecfv_ad-00002.vtu" in (tmp_path / "lens_immiscible_ecfv_ad.pvd").read_text()
+
+
+@pytest.mark.gpu
+def test_driver_fd_linearizer_runs(driver, tmp_path):
+    """LocalLinearizerSplice = FiniteDifferenceLocalLinearizer through the driver's parameters."""
+    out = subprocess.run([driver, "--preset=baseline", "--end-time=500", "--initial-time-step-size=250",
+                          "--max-time-step-size=250", "--local-linearizer=fd", "--numeric-difference-method=0",
+                          "--enable-vtk-output=0"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert len([ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]) == 2

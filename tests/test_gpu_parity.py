@@ -276,3 +276,84 @@ def test_repeated_import_and_solve_is_bitwise_reproducible(ewg_mod, oracle_mod, 
         assert it == outs[0][0] and np.array_equal(dx, outs[0][1])
     res = o.apply_jacobian(outs[0][1]) - o.residual()
     assert np.max(np.abs(res)) <= 1e-8 * np.max(np.abs(o.residual())) + 1e-9
+
+
+# ---- finite-difference local linearizer (FvBaseFdLocalLinearizer) ----------------------------
+# A difference quotient divides residual differences by the deflection (0.9123e-11 p_ref for the
+# pressure, 0.9123e-10 for the saturation). The two-point gradient is a sum of terms of size
+# rho g ~ 1e4 Pa/m while the pressure deflection moves it by ~1e-5 Pa/m, so one rounding
+# difference between two evaluation orders (the GPU fuses multiply-adds, the oracle does not)
+# moves a pressure derivative by ~1e-7 of its size; the GPU and oracle FD Jacobians are compared
+# at FD_RTOL of each component's magnitude. The residual is not differenced and keeps LIN_RTOL.
+FD_RTOL = 1e-4
+
+
+@pytest.mark.parametrize("name", ["baseline", "reference", "brooks_corey", "lens3d_8x6x4", "lens3d_16x12x10"])
+@pytest.mark.parametrize("method", [1, 0, -1])
+def test_fd_linearizer_matches_oracle(ewg_mod, oracle_mod, name, method):
+    case = _cases(ewg_mod)[name]()
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x = _perturb(ewg_mod, case, o.get_solution(0), 21)
+    ctx = ewg_mod.Context(case)
+    ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+    o.set_local_linearizer(1, method)
+    for c in (ctx, o):
+        c.set_solution(1, x)
+        c.set_solution(0, x)
+    o.set_recycle_first_iteration_storage(False)
+    ctx.linearize(250.0)
+    o.linearize(250.0, 0)
+    r_g, r_o = ctx.residual(), o.residual()
+    _, _, b_g = ctx.jacobian_bcrs()
+    _, _, b_o = o.jacobian_bcrs()
+    assert rel_close(r_g, r_o, LIN_RTOL, scale=max(np.max(np.abs(r_o)), 1e-3))[0]
+    for eq in range(2):
+        for pv in range(2):
+            ok, e, s = rel_close(b_g[:, eq, pv], b_o[:, eq, pv], FD_RTOL)
+            assert ok, ("fd vs oracle fd", eq, pv, e, s)
+
+
+@pytest.mark.parametrize("name", ["baseline", "lens3d_8x6x4"])
+@pytest.mark.parametrize("method", [1, 0])
+def test_fd_linearizer_close_to_ad(ewg_mod, name, method):
+    """Away from the laws' kinks and from upwind ties (saturations in (0.3, 1), pressures off
+    hydrostatic), the FD Jacobian is the AD Jacobian to the quotient's truncation error."""
+    case = _cases(ewg_mod)[name]()
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x = ctx.get_solution(0)
+    rng = np.random.Generator(np.random.PCG64(0))
+    x[:, 1] = rng.uniform(0.3, 1.0, size=len(x))
+    x[:, 0] += rng.normal(0, 50.0, size=len(x))
+    ctx.set_solution(1, x)
+    ctx.set_solution(0, x)
+    ctx.linearize(250.0)
+    _, _, b_ad = ctx.jacobian_bcrs()
+    ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+    ctx.linearize(250.0)
+    _, _, b_fd = ctx.jacobian_bcrs()
+    for eq in range(2):
+        for pv in range(2):
+            ok, e, s = rel_close(b_fd[:, eq, pv], b_ad[:, eq, pv], 1e-4 if method else 1e-5)
+            assert ok, ("fd vs ad", eq, pv, e, s)
+
+
+@pytest.mark.parametrize("name", ["baseline", "lens3d_8x6x4"])
+def test_fd_newton_steps_match_oracle(ewg_mod, oracle_mod, name):
+    """Five implicit steps with the FD local linearizer on both sides: identical Newton
+    iteration counts and fields within 1e-8 of the oracle."""
+    case = _cases(ewg_mod)[name]()
+    ctx = ewg_mod.Context(case)
+    ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, 1)
+    o = oracle_mod.Oracle(case)
+    o.set_local_linearizer(1, 1)
+    ctx.apply_initial_solution()
+    o.apply_initial_solution()
+    so = ewg_mod.default_solve_opts(verify_true_residual=0)
+    reps = ctx.run(5, 250.0, sopts=so)
+    oreps = o.run(5, 250.0, sopts=so)
+    assert [r.iterations for r in reps] == [a for a, _ in oreps]
+    xg, xo = ctx.get_solution(0), o.get_solution(0)
+    assert rel_close(xg[:, 0], xo[:, 0], 1e-8)[0]
+    assert np.max(np.abs(xg[:, 1] - xo[:, 1])) <= 1e-8

@@ -120,6 +120,33 @@ def test_ad_jacobian_matches_finite_differences(oracle_mod, ewg_mod):
         assert np.max(np.abs(a - b)) <= 2e-5 * scale, (pv, np.max(np.abs(a - b)), scale)
 
 
+@pytest.mark.parametrize("method", [1, 0, -1])
+def test_fd_local_linearizer_matches_ad(oracle_mod, ewg_mod, method):
+    """FvBaseFdLocalLinearizer restated: same residual as the AD linearizer, Jacobian within the
+    difference quotient's error (forward / backward first order, central second order)."""
+    case = ewg_mod.baseline_case()
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x = o.get_solution(0)
+    rng = np.random.Generator(np.random.PCG64(0))
+    x[:, 1] = rng.uniform(0.3, 1.0, size=len(x))
+    x[:, 0] += rng.normal(0, 50.0, size=len(x))
+    o.set_solution(1, x)
+    o.set_solution(0, x)
+    o.linearize(250.0)
+    r_ad = o.residual()
+    _, _, J_ad = o.jacobian_bcrs()
+    o.set_local_linearizer(1, method)
+    o.linearize(250.0)
+    assert np.array_equal(o.residual(), r_ad)
+    _, _, J_fd = o.jacobian_bcrs()
+    tol = 5e-5 if method else 5e-6
+    for eq in range(2):
+        for pv in range(2):
+            a, b = J_fd[:, eq, pv], J_ad[:, eq, pv]
+            assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (eq, pv)
+
+
 def test_mass_conservation(oracle_mod, ewg_mod):
     """sum_i R_i V_i = storage change / dt + boundary outflow: interior face fluxes cancel."""
     case = ewg_mod.baseline_case()
