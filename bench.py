@@ -165,10 +165,11 @@ class ClockSampler:
 
 def mixed_opts(ewg):
     """The mixed-precision form: FP32 Jacobian, ILU(0) and BiCGStab solve each Newton correction
-    to a relative 1e-3 (the reference's default LinearSolverTolerance) inside the FP64 defect
-    check; residual, update and the Newton test (1e-8) stay FP64."""
-    return ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-3,
-                                  inner_tolerance=1e-3, max_defect_iterations=3)
+    to a relative 1e-3 (the reference's default LinearSolverTolerance); the FP64 defect check
+    accepts the correction once the FP64 defect is reduced by 1e-2 (at most 3 FP32 passes).
+    Residual, update and the Newton test (1e-8) stay FP64: Newton is the defect correction."""
+    return ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-2,
+                                  inner_tolerance=1e-3, max_defect_iterations=3, linear_solver_max_iterations=5000)
 
 
 def geometry(n):
@@ -379,16 +380,25 @@ def run_ours(args, rank, world, local, pg):
     case = ewg.lens3d_case(nx, ny, nz, seed=rank)
     N, F = geometry((nx, ny, nz))
     mixed = args.precision == "mixed"
-    sopts = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED if mixed else ewg.PRECISION_FP64)
+    # the graded linear tolerance (rel. 1e-10) needs more than the reference's default 1000
+    # BiCGStab iterations on this grid in some Newton iterations; a linear-solver failure would
+    # halve the time step and change the workload, so the limit is raised for every form
+    max_its = 5000
+    sopts = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED if mixed else ewg.PRECISION_FP64,
+                                   linear_solver_max_iterations=max_its)
     nopts = ewg.default_newton_opts()
     ctx = ewg.Context(case)
     ctx.apply_initial_solution()
 
     guess_log = []
 
+    halvings = []
+
     def one_step(dt=250.0, sopts=sopts, net=None):
         h = dt
-        for _ in range(10):
+        for attempt in range(10):
+            if attempt:
+                halvings.append(h)
             if net is not None:
                 # the learned initial guess replaces solution(0) only if its residual is smaller
                 used, rg, rp = net.predict_guess(ctx, h)
@@ -439,7 +449,8 @@ def run_ours(args, rank, world, local, pg):
         variants = {
             # the reference's own default linear tolerance (LinearSolverTolerance 1e-3,
             # fvbasediscretization.hh:249) with the FP64 solver
-            "fp64_reference_linear_tol": (ewg.default_solve_opts(linear_solver_tolerance=1e-3), None),
+            "fp64_reference_linear_tol": (ewg.default_solve_opts(linear_solver_tolerance=1e-3,
+                                                                 linear_solver_max_iterations=max_its), None),
             # FP32 Jacobian / ILU / BiCGStab, FP64 residual, update and Newton test
             "mixed": (mixed_opts(ewg), None),
             # the same with the learned Newton initial guess (kept only where it lowers the residual)
@@ -558,6 +569,7 @@ def run_ours(args, rank, world, local, pg):
                    "cells": N, "interior_faces": F, "precision": args.precision,
                    "l2": "working set (> 4 GB) larger than L2 (126 MB); no flush needed"},
         "newton_its": [r.iterations for r in reps], "linear_its": [r.linear_iterations for r in reps],
+        "time_step_halvings": len(halvings),
         "phase_s": {"linearize": sum(r.t_linearize for r in reps) / len(reps),
                     "solve": sum(r.t_solve for r in reps) / len(reps),
                     "update": sum(r.t_update for r in reps) / len(reps)},

@@ -10,9 +10,9 @@
 //     per-cell vector (red-black split order inside the member, as for a single context) and the
 //     plane blocks 6 off_m (intensive-quantity cache, stride N_m), 28 off_m (7 Jacobian bands),
 //     4 off_m (inverted diagonal blocks) and 12 off_m (L factors of the black rows, stride N_m/2).
-//   * Work is cut into tiles of kEnsTile consecutive half indices of one member; a block works on
-//     one tile at a time (both colours of a half index per thread for cell kernels, one colour
-//     for the ILU sweeps). Every kernel is a persistent loop of resident blocks over the tile
+//   * Work is cut into tiles of kEnsTileH consecutive half indices of one member; a block of
+//     kEnsTile threads works on one tile at a time (each thread a strided set of half indices:
+//     both colours for cell kernels, one colour for the ILU sweeps). Every kernel is a persistent loop of resident blocks over the tile
 //     table; tiles of members outside the current round (Newton finished, or BiCGStab stopped)
 //     are skipped, so members of uneven size stop independently inside shared launches.
 //   * BiCGStab state (bicgstabsolver.hh:116-326 with CombinedCriterion) is one BiState per
@@ -21,7 +21,7 @@
 //     scalars.
 //   * The nine kernels of a BiCGStab iteration are captured check_interval times over in one CUDA
 //     graph that is replayed until no member is running.
-//   * Launch shapes: the block is the tile (kEnsTile threads); an autotuner times, per kernel
+//   * Launch shapes: the block is fixed (kEnsTile threads); an autotuner times, per kernel
 //     class, the number of resident blocks (multiples of the SM count) and, for the assembly,
 //     the register budget variant, and keeps the fastest. Sum reductions do not depend on the
 //     launch shape, so results do not depend on the tuning.
@@ -43,8 +43,12 @@ thread_local std::string g_ensCreateError;
 
 namespace ewg {
 
-constexpr int kEnsTile = 256;  // half indices per tile = threads per block
+constexpr int kEnsTile = 256;    // threads per block
+constexpr int kEnsTileH = 1024;  // half indices per tile (4 per thread: the tile prologue is amortized)
 constexpr int kEnsBands = 7;   // 3D: diagonal + 6 faces
+// resident blocks per SM the BiCGStab kernels are compiled for (register budgets 64 and 48)
+constexpr int kEnsBlocksSpmv = 4;
+constexpr int kEnsBlocksVec = 5;
 
 struct EnsMember {
     Phys P;
@@ -86,6 +90,10 @@ __device__ __forceinline__ int begin_tile(const EnsMember* __restrict__ mem, con
     for (int i = threadIdx.x; i < (int)(sizeof(EnsMember) / 8); i += blockDim.x) dst[i] = src[i];
     __syncthreads();
     return m;
+}
+
+__device__ __forceinline__ int64_t tile_end(const Phys& P, int64_t h0) {
+    return h0 + kEnsTileH < P.Nh ? h0 + kEnsTileH : P.Nh;
 }
 
 // Block-wide max of non-negative doubles published with an integer atomicMax on the bit pattern.
@@ -182,25 +190,26 @@ __global__ void __launch_bounds__(kEnsTile) ke_levels(ENS_ARGS, const int* __res
     ENS_TILE_LOOP {
         if (begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh) < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        for (int col = 0; col < 2; ++col) {
-            const int64_t s = sm.off + col * P.Nh + h;
-            if (mode == 0) {
-                const CellIdx ci = cell_of(P, col, h);
-                const double y = (ci.j + 0.5) * P.h[1];
-                const double depth = P.L[1] - y;
-                const double densityW = P.rho[0];
-                const double2 v = make_double2(P.pRef - densityW * (-P.g) * depth, 1.0);
-                x0[s] = v;
-                x1[s] = v;
-            } else if (mode == 1) {
-                x1[s] = x0[s];
-            } else if (mode == 2) {
-                x0[s] = x1[s];
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            for (int col = 0; col < 2; ++col) {
+                const int64_t s = sm.off + col * P.Nh + h;
+                if (mode == 0) {
+                    const CellIdx ci = cell_of(P, col, h);
+                    const double y = (ci.j + 0.5) * P.h[1];
+                    const double depth = P.L[1] - y;
+                    const double densityW = P.rho[0];
+                    const double2 v = make_double2(P.pRef - densityW * (-P.g) * depth, 1.0);
+                    x0[s] = v;
+                    x1[s] = v;
+                } else if (mode == 1) {
+                    x1[s] = x0[s];
+                } else if (mode == 2) {
+                    x0[s] = x1[s];
+                }
+                const double Sw = x1[s].y;
+                sold[s] = make_double2(P.porosity * Sw * P.rho[0], P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1]);
             }
-            const double Sw = x1[s].y;
-            sold[s] = make_double2(P.porosity * Sw * P.rho[0], P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1]);
         }
     }
 }
@@ -214,10 +223,11 @@ __global__ void __launch_bounds__(kEnsTile) ke_intensive(ENS_ARGS, const int* __
         if (begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh) < 0) continue;
         const Phys& P = sm.P;
         const int64_t off = sm.off;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        intensive_cell(P, x + off, lens + off, iq + 6 * off, h);
-        intensive_cell(P, x + off, lens + off, iq + 6 * off, P.Nh + h);
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            intensive_cell(P, x + off, lens + off, iq + 6 * off, h);
+            intensive_cell(P, x + off, lens + off, iq + 6 * off, P.Nh + h);
+        }
     }
 }
 
@@ -234,10 +244,10 @@ __global__ void __launch_bounds__(kEnsTile, MINB) ke_assemble(
         if (m < 0) continue;
         const Phys& P = sm.P;
         const int64_t off = sm.off;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         double mx = 0.0;
         int bad = 0;
-        if (h < P.Nh) {
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
             const double dt = dtArr[m];
             for (int col = 0; col < 2; ++col)
                 mx = fmax(mx, assemble_cell3<JT, WITH_J>(
@@ -261,20 +271,21 @@ __global__ void __launch_bounds__(kEnsTile) ke_update(ENS_ARGS, const int* __res
         const int m = begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        int bad = 0;
-        for (int col = 0; col < 2; ++col) {
-            const int64_t s = sm.off + col * P.Nh + h;
-            const auto d = dx[s];
-            const double d0 = (double)d.x, d1 = (double)d.y;
-            if (!isfinite(d0) || !isfinite(d1)) bad = 1;
-            double2 v = x0[s];
-            v.x -= d0;
-            v.y -= d1;
-            x0[s] = v;
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            int bad = 0;
+            for (int col = 0; col < 2; ++col) {
+                const int64_t s = sm.off + col * P.Nh + h;
+                const auto d = dx[s];
+                const double d0 = (double)d.x, d1 = (double)d.y;
+                if (!isfinite(d0) || !isfinite(d1)) bad = 1;
+                double2 v = x0[s];
+                v.x -= d0;
+                v.y -= d1;
+                x0[s] = v;
+            }
+            if (bad) atomicOr(&flags[m], 2);
         }
-        if (bad) atomicOr(&flags[m], 2);
     }
 }
 
@@ -291,9 +302,10 @@ __global__ void __launch_bounds__(kEnsTile) ke_diag_inverse_red(ENS_ARGS, const 
         const int m = begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        if (!diag_inverse_row(P.N, J + kEnsBands * 4 * sm.off, Dinv + 4 * sm.off, h)) atomicOr(&flags[m], 4);
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            if (!diag_inverse_row(P.N, J + kEnsBands * 4 * sm.off, Dinv + 4 * sm.off, h)) atomicOr(&flags[m], 4);
+        }
     }
 }
 
@@ -307,10 +319,11 @@ __global__ void __launch_bounds__(kEnsTile) ke_ilu_black_factor(ENS_ARGS, const 
         const int m = begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        if (!ilu_black_factor_row(P, J + kEnsBands * 4 * sm.off, Dinv + 4 * sm.off, L + 12 * sm.off, h))
-            atomicOr(&flags[m], 4);
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            if (!ilu_black_factor_row(P, J + kEnsBands * 4 * sm.off, Dinv + 4 * sm.off, L + 12 * sm.off, h))
+                atomicOr(&flags[m], 4);
+        }
     }
 }
 
@@ -323,15 +336,16 @@ __global__ void __launch_bounds__(kEnsTile) ke_rhs(ENS_ARGS, const int* __restri
     ENS_TILE_LOOP {
         if (begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh) < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        for (int col = 0; col < 2; ++col) {
-            const int64_t s = sm.off + col * P.Nh + h;
-            const double2 v = r[s];
-            typename V2T<T>::type o;
-            o.x = (T)v.x;
-            o.y = (T)v.y;
-            b[s] = o;
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            for (int col = 0; col < 2; ++col) {
+                const int64_t s = sm.off + col * P.Nh + h;
+                const double2 v = r[s];
+                typename V2T<T>::type o;
+                o.x = (T)v.x;
+                o.y = (T)v.y;
+                b[s] = o;
+            }
         }
     }
 }
@@ -348,7 +362,7 @@ __global__ void ke_bicg_arm(const int* __restrict__ mask, int M, BiState tmpl, B
 #define ENS_BICG_ARGS BiState *__restrict__ st, double *__restrict__ partials, unsigned *__restrict__ counters
 
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_bicg_init(ENS_ARGS, const typename V2T<T>::type* __restrict__ b,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_bicg_init(ENS_ARGS, const typename V2T<T>::type* __restrict__ b,
                                                          typename V2T<T>::type* __restrict__ x,
                                                          typename V2T<T>::type* __restrict__ r,
                                                          typename V2T<T>::type* __restrict__ r0,
@@ -360,9 +374,9 @@ __global__ void __launch_bounds__(kEnsTile) ke_bicg_init(ENS_ARGS, const typenam
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_PENDING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         double red[2] = {0.0, 0.0};  // sum b.b, max |b|
-        if (h < P.Nh)
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = sm.off + col * P.Nh + h;
                 const auto bs = b[s];
@@ -376,7 +390,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_bicg_init(ENS_ARGS, const typenam
                 red[1] = fmax(red[1], fmax(absn(b0), absn(b1)));
             }
         double out[2];
-        if (member_reduce<1, 1>(red, sm.tile0 + sh[1] / kEnsTile, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
+        if (member_reduce<1, 1>(red, sm.tile0 + sh[1] / kEnsTileH, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
             BiState* s = st + m;
             s->resErr = fmax(out[1], DBL_MIN * 1e10);
             s->initResErr = s->resErr;
@@ -396,7 +410,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_bicg_init(ENS_ARGS, const typenam
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_bicg_p(ENS_ARGS, const typename V2T<T>::type* __restrict__ r,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_bicg_p(ENS_ARGS, const typename V2T<T>::type* __restrict__ r,
                                                       typename V2T<T>::type* __restrict__ r0,
                                                       typename V2T<T>::type* __restrict__ v,
                                                       typename V2T<T>::type* __restrict__ p,
@@ -407,33 +421,34 @@ __global__ void __launch_bounds__(kEnsTile) ke_bicg_p(ENS_ARGS, const typename V
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        const bool restart = st[m].restartPending != 0;
-        const double beta = st[m].beta, omega = st[m].omega;
-        for (int col = 0; col < 2; ++col) {
-            const int64_t s = sm.off + col * P.Nh + h;
-            const auto rs = r[s];
-            typename V2T<T>::type vs = v[s], ps = p[s];
-            if (restart) {
-                r0[s] = rs;
-                vs.x = (T)0; vs.y = (T)0;
-                ps = vs;
-                v[s] = vs;
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            const bool restart = st[m].restartPending != 0;
+            const double beta = st[m].beta, omega = st[m].omega;
+            for (int col = 0; col < 2; ++col) {
+                const int64_t s = sm.off + col * P.Nh + h;
+                const auto rs = r[s];
+                typename V2T<T>::type vs = v[s], ps = p[s];
+                if (restart) {
+                    r0[s] = rs;
+                    vs.x = (T)0; vs.y = (T)0;
+                    ps = vs;
+                    v[s] = vs;
+                }
+                double t0 = (double)vs.x * omega, t1 = (double)vs.y * omega;
+                t0 -= (double)ps.x; t1 -= (double)ps.y;
+                t0 *= -beta; t1 *= -beta;
+                typename V2T<T>::type o;
+                o.x = (T)((double)rs.x + t0);
+                o.y = (T)((double)rs.y + t1);
+                p[s] = o;
             }
-            double t0 = (double)vs.x * omega, t1 = (double)vs.y * omega;
-            t0 -= (double)ps.x; t1 -= (double)ps.y;
-            t0 *= -beta; t1 *= -beta;
-            typename V2T<T>::type o;
-            o.x = (T)((double)rs.x + t0);
-            o.y = (T)((double)rs.y + t1);
-            p[s] = o;
         }
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_ilu_black_apply(ENS_ARGS, const T* __restrict__ Dinv, const T* __restrict__ L,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_ilu_black_apply(ENS_ARGS, const T* __restrict__ Dinv, const T* __restrict__ L,
                                                                const typename V2T<T>::type* __restrict__ d,
                                                                typename V2T<T>::type* __restrict__ y,
                                                                const BiState* __restrict__ st) {
@@ -443,15 +458,16 @@ __global__ void __launch_bounds__(kEnsTile) ke_ilu_black_apply(ENS_ARGS, const T
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        const int64_t off = sm.off;
-        ilu_black_apply_row<T, T>(P, Dinv + 4 * off, L + 12 * off, d + off, y + off, st[m].w, h);
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            const int64_t off = sm.off;
+            ilu_black_apply_row<T, T>(P, Dinv + 4 * off, L + 12 * off, d + off, y + off, st[m].w, h);
+        }
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_ilu_red_apply(ENS_ARGS, const T* __restrict__ J, const T* __restrict__ Dinv,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_ilu_red_apply(ENS_ARGS, const T* __restrict__ J, const T* __restrict__ Dinv,
                                                              const typename V2T<T>::type* __restrict__ d,
                                                              typename V2T<T>::type* __restrict__ y,
                                                              const BiState* __restrict__ st) {
@@ -461,17 +477,18 @@ __global__ void __launch_bounds__(kEnsTile) ke_ilu_red_apply(ENS_ARGS, const T* 
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
-        if (h >= P.Nh) continue;
-        const int64_t off = sm.off;
-        const double w = st[m].w;
-        ilu_red_apply_row<T, T>(P, J + kEnsBands * 4 * off, Dinv + 4 * off, d + off, y + off, w, 1.0 / w, h);
+        const int64_t hEnd = tile_end(P, sh[1]);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            const int64_t off = sm.off;
+            const double w = st[m].w;
+            ilu_red_apply_row<T, T>(P, J + kEnsBands * 4 * off, Dinv + 4 * off, d + off, y + off, w, 1.0 / w, h);
+        }
     }
 }
 
 // v = A y; alpha = rho_i / (r0hat . v)
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_spmv_alpha(ENS_ARGS, const T* __restrict__ J,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_alpha(ENS_ARGS, const T* __restrict__ J,
                                                           const typename V2T<T>::type* __restrict__ y,
                                                           const typename V2T<T>::type* __restrict__ r0,
                                                           typename V2T<T>::type* __restrict__ v, ENS_BICG_ARGS) {
@@ -481,10 +498,10 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_alpha(ENS_ARGS, const T* __r
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         const int64_t off = sm.off;
         double red[1] = {0.0};
-        if (h < P.Nh)
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = col * P.Nh + h;
                 double a0, a1;
@@ -496,7 +513,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_alpha(ENS_ARGS, const T* __r
                 red[0] += (double)rh.x * (double)o.x + (double)rh.y * (double)o.y;
             }
         double out[1];
-        if (member_reduce<1, 0>(red, sm.tile0 + sh[1] / kEnsTile, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
+        if (member_reduce<1, 0>(red, sm.tile0 + sh[1] / kEnsTileH, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
             BiState* s = st + m;
             const double breakdownEps = DBL_MIN * 1e10;
             s->restartPending = 0;
@@ -510,7 +527,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_alpha(ENS_ARGS, const T* __r
 
 // h = x + alpha y (in x), s = r - alpha v (in r); criterion on s with y as change indicator
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_hs(ENS_ARGS, typename V2T<T>::type* __restrict__ x,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_hs(ENS_ARGS, typename V2T<T>::type* __restrict__ x,
                                                   const typename V2T<T>::type* __restrict__ y,
                                                   typename V2T<T>::type* __restrict__ r,
                                                   const typename V2T<T>::type* __restrict__ v, ENS_BICG_ARGS) {
@@ -520,10 +537,10 @@ __global__ void __launch_bounds__(kEnsTile) ke_hs(ENS_ARGS, typename V2T<T>::typ
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         const double alpha = st[m].alpha;
         double red[2] = {0.0, 0.0};  // max |s|, any y != 0
-        if (h < P.Nh)
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = sm.off + col * P.Nh + h;
                 const auto ys = y[s], xs = x[s], rs = r[s], vs = v[s];
@@ -538,7 +555,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_hs(ENS_ARGS, typename V2T<T>::typ
                 if (ys.x != (T)0 || ys.y != (T)0) red[1] = 1.0;
             }
         double out[2];
-        if (member_reduce<0, 2>(red, sm.tile0 + sh[1] / kEnsTile, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
+        if (member_reduce<0, 2>(red, sm.tile0 + sh[1] / kEnsTileH, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
             BiState* s = st + m;
             s->lastResErr = s->resErr;
             s->resErr = out[0];
@@ -550,7 +567,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_hs(ENS_ARGS, typename V2T<T>::typ
 
 // t = A z; omega = (t . s) / (t . t)
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_spmv_omega(ENS_ARGS, const T* __restrict__ J,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_omega(ENS_ARGS, const T* __restrict__ J,
                                                           const typename V2T<T>::type* __restrict__ z,
                                                           const typename V2T<T>::type* __restrict__ sres,
                                                           typename V2T<T>::type* __restrict__ tv, ENS_BICG_ARGS) {
@@ -560,10 +577,10 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_omega(ENS_ARGS, const T* __r
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         const int64_t off = sm.off;
         double red[2] = {0.0, 0.0};
-        if (h < P.Nh)
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = col * P.Nh + h;
                 double a0, a1;
@@ -577,7 +594,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_omega(ENS_ARGS, const T* __r
                 red[1] += t0 * (double)ss.x + t1 * (double)ss.y;
             }
         double out[2];
-        if (member_reduce<2, 0>(red, sm.tile0 + sh[1] / kEnsTile, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
+        if (member_reduce<2, 0>(red, sm.tile0 + sh[1] / kEnsTileH, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
             BiState* s = st + m;
             const double breakdownEps = DBL_MIN * 1e10;
             if (fabs(out[0]) <= breakdownEps) { s->status = ST_BREAKDOWN; continue; }
@@ -590,7 +607,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_spmv_omega(ENS_ARGS, const T* __r
 // x += omega z; criterion on r (still s) with z as change indicator; r += -omega t; then the next
 // iteration's r0hat . r and r . r
 template <typename T>
-__global__ void __launch_bounds__(kEnsTile) ke_xr(ENS_ARGS, typename V2T<T>::type* __restrict__ x,
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_xr(ENS_ARGS, typename V2T<T>::type* __restrict__ x,
                                                   const typename V2T<T>::type* __restrict__ z,
                                                   typename V2T<T>::type* __restrict__ r,
                                                   const typename V2T<T>::type* __restrict__ tv,
@@ -601,10 +618,10 @@ __global__ void __launch_bounds__(kEnsTile) ke_xr(ENS_ARGS, typename V2T<T>::typ
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
         const Phys& P = sm.P;
-        const int64_t h = sh[1] + threadIdx.x;
+        const int64_t hEnd = tile_end(P, sh[1]);
         const double omega = st[m].omega;
         double red[4] = {0.0, 0.0, 0.0, 0.0};  // sum r0.r', sum r'.r', max |s|, any z != 0
-        if (h < P.Nh)
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = sm.off + col * P.Nh + h;
                 const auto xs = x[s], zs = z[s], rs = r[s], ts = tv[s], rh = r0[s];
@@ -622,7 +639,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_xr(ENS_ARGS, typename V2T<T>::typ
                 red[1] += r0v * r0v + r1v * r1v;
             }
         double out[4];
-        if (member_reduce<2, 2>(red, sm.tile0 + sh[1] / kEnsTile, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
+        if (member_reduce<2, 2>(red, sm.tile0 + sh[1] / kEnsTileH, sm.tile0, sm.ntiles, partials, &counters[m], out) && threadIdx.x == 0) {
             BiState* s = st + m;
             s->lastResErr = s->resErr;
             s->resErr = out[2];
@@ -1369,7 +1386,7 @@ ewg_status ewg_ensemble_create(int32_t members, const ewg_grid* grids, const ewg
         }
         const int64_t n = (int64_t)g.nx * g.ny * g.nz;
         total += n;
-        tiles += (n / 2 + kEnsTile - 1) / kEnsTile;
+        tiles += (n / 2 + kEnsTileH - 1) / kEnsTileH;
     }
     if (total >= ((int64_t)1 << 31) || tiles >= ((int64_t)1 << 31)) {
         g_ensCreateError = "ensemble too large (2^31 cells)";
@@ -1422,9 +1439,9 @@ ewg_status ewg_ensemble_create(int32_t members, const ewg_grid* grids, const ewg
         build_face_geo(em.P, g);
         geoAll.insert(geoAll.end(), g.begin(), g.end());
         em.tile0 = (int32_t)e->hTiles.size();
-        const int64_t nt = (em.P.Nh + kEnsTile - 1) / kEnsTile;
+        const int64_t nt = (em.P.Nh + kEnsTileH - 1) / kEnsTileH;
         em.ntiles = (int32_t)nt;
-        for (int64_t t = 0; t < nt; ++t) e->hTiles.push_back(make_int2(m, (int)(t * kEnsTile)));
+        for (int64_t t = 0; t < nt; ++t) e->hTiles.push_back(make_int2(m, (int)(t * kEnsTileH)));
         off += em.P.N;
     }
     e->nTiles = (int)e->hTiles.size();

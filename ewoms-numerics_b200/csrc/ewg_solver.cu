@@ -22,6 +22,11 @@
 
 namespace ewg {
 
+// The BiCGStab kernels with grid reductions run on a fixed grid of kRedBlocksPerSM blocks per SM
+// (deterministic partial sums); they are compiled to fit that many resident blocks, so the grid
+// runs in one wave.
+constexpr int kRedBlocksPerSM = 4;
+
 
 // ---- deterministic grid reduction -----------------------------------------------------------
 
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(kSolBlock) k_spmv(const __grid_constant__ Phys
 // ---- BiCGStab kernels ------------------------------------------------------------------------
 
 template <typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_init(const __grid_constant__ Phys P,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_init(const __grid_constant__ Phys P,
                                                           const typename V2T<TV>::type* __restrict__ b,
                                                           typename V2T<TV>::type* __restrict__ x,
                                                           typename V2T<TV>::type* __restrict__ r,
@@ -212,7 +217,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_init(const __grid_constant__
 
 // p = r + (-beta) (omega v - p); on a restart r0hat = r, v = p = 0 first
 template <typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_p(const __grid_constant__ Phys P,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_p(const __grid_constant__ Phys P,
                                                        const typename V2T<TV>::type* __restrict__ r,
                                                        typename V2T<TV>::type* __restrict__ r0,
                                                        typename V2T<TV>::type* __restrict__ v,
@@ -243,7 +248,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_p(const __grid_constant__ Ph
 
 // v = A y; alpha = rho_i / (r0hat . v)
 template <typename TM, typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_alpha(const __grid_constant__ Phys P, const TM* __restrict__ A,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_spmv_alpha(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                                 const typename V2T<TV>::type* __restrict__ y,
                                                                 const typename V2T<TV>::type* __restrict__ r0,
                                                                 typename V2T<TV>::type* __restrict__ v,
@@ -273,7 +278,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_alpha(const __grid_cons
 
 // h = x + alpha y (in x), s = r - alpha v (in r); criterion on s with y as change indicator
 template <typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_hs(const __grid_constant__ Phys P,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_hs(const __grid_constant__ Phys P,
                                                         typename V2T<TV>::type* __restrict__ x,
                                                         const typename V2T<TV>::type* __restrict__ y,
                                                         typename V2T<TV>::type* __restrict__ r,
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_hs(const __grid_constant__ P
 
 // t = A z; omega = (t . s) / (t . t)
 template <typename TM, typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_omega(const __grid_constant__ Phys P, const TM* __restrict__ A,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_spmv_omega(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                                 const typename V2T<TV>::type* __restrict__ z,
                                                                 const typename V2T<TV>::type* __restrict__ sres,
                                                                 typename V2T<TV>::type* __restrict__ t,
@@ -337,7 +342,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_spmv_omega(const __grid_cons
 // x += omega z; criterion on r (still s) with z as change indicator; r += -omega t;
 // then the next iteration's r0hat . r and r . r
 template <typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_xr(const __grid_constant__ Phys P,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_xr(const __grid_constant__ Phys P,
                                                         typename V2T<TV>::type* __restrict__ x,
                                                         const typename V2T<TV>::type* __restrict__ z,
                                                         typename V2T<TV>::type* __restrict__ r,
@@ -378,7 +383,7 @@ __global__ void __launch_bounds__(kSolBlock) k_bicg_xr(const __grid_constant__ P
 // Residual replacement after convergence: r = r0hat = b - A x with max-norm and r . r. If the
 // true residual misses the criterion by more than 10x the iteration resumes from x.
 template <typename TM, typename TV>
-__global__ void __launch_bounds__(kSolBlock) k_bicg_true_residual(const __grid_constant__ Phys P, const TM* __restrict__ A,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_true_residual(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                                    const typename V2T<TV>::type* __restrict__ b,
                                                                    const typename V2T<TV>::type* __restrict__ x,
                                                                    typename V2T<TV>::type* __restrict__ r,
@@ -441,7 +446,7 @@ __global__ void k_defect_accumulate(const __grid_constant__ Phys P, double2* __r
     }
 }
 
-__global__ void __launch_bounds__(kSolBlock) k_defect_residual(const __grid_constant__ Phys P, const float* __restrict__ A,
+__global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_defect_residual(const __grid_constant__ Phys P, const float* __restrict__ A,
                                                                 const double2* __restrict__ b,
                                                                 const double2* __restrict__ x64,
                                                                 double2* __restrict__ r64, double* partials,
@@ -528,7 +533,7 @@ static ewg_status ensure_ws(ewg_ctx* ctx, bool needFloat) {
         SolverWs* w = new SolverWs();
         ctx->sv = w;
         if ((e = alloc_ws(w->d, ctx->P)) != cudaSuccess) return cuda_fail(ctx, e, "alloc solver vectors");
-        w->gridRed = ctx->numSMs * 4;
+        w->gridRed = ctx->numSMs * kRedBlocksPerSM;
         if ((e = cudaMalloc(&w->partials, sizeof(double) * kMaxRed * w->gridRed * 2)) != cudaSuccess) return cuda_fail(ctx, e, "alloc partials");
         if ((e = cudaMalloc(&w->counter, sizeof(unsigned) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc counter");
         if ((e = cudaMemsetAsync(w->counter, 0, sizeof(unsigned) * 4, ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "memset counter");

@@ -31,7 +31,13 @@ def mixed_opts():
                                   inner_tolerance=1e-3, max_defect_iterations=3)
 
 
+SHAPE = None  # (nx, ny, nz): train on the 3D lens problem at this size (sigma 1, length 8, dt 250)
+
+
 def member(seed: int, n: int):
+    if SHAPE is not None:
+        # the benchmark's problem family: same grid, field statistics and step size, other seeds
+        return ewg.lens3d_case(*SHAPE, seed=seed), 250.0
     rng = np.random.default_rng(seed)
     sigma = float(rng.uniform(0.5, 1.5))
     corr = float(rng.uniform(4.0, 12.0))
@@ -122,7 +128,14 @@ def main():
     ap.add_argument("--loss-weight-p", type=float, default=0.05)
     ap.add_argument("--sn-threshold", type=float, default=0.002)
     ap.add_argument("--front-weight", type=float, default=20.0)
+    ap.add_argument("--shape", default=None, help="nx,ny,nz of the lens problem to train on instead of cubes")
+    ap.add_argument("--train-seeds", default=None, help="first,count of the training realizations")
+    ap.add_argument("--hold-seeds", default=None, help="first,count of the held-out realizations")
+    ap.add_argument("--apply-pressure", type=int, default=0)
     args = ap.parse_args()
+    global SHAPE
+    if args.shape:
+        SHAPE = tuple(int(v) for v in args.shape.split(","))
     t0 = time.perf_counter()
 
     def log(msg):
@@ -130,8 +143,8 @@ def main():
 
     sopts = mixed_opts()
     net = ewg.GuessNet(seed=0)
-    options = [args.loss_weight_p, args.front_weight, 0.0, args.sn_threshold]
-    net.set_options(options[0], options[1], False, options[3])
+    options = [args.loss_weight_p, args.front_weight, float(args.apply_pressure), args.sn_threshold]
+    net.set_options(options[0], options[1], bool(args.apply_pressure), options[3])
     tp, ts = estimate_scales(args.n, sopts)
     sc = net.scales()
     sc[6], sc[7] = tp, ts
@@ -139,6 +152,12 @@ def main():
     log(f"output scales dp {tp:.3g} Pa, dSn {ts:.3g}")
     train_seeds = list(range(1000, 1000 + args.members))
     hold_seeds = list(range(2000, 2000 + max(2, args.members // 6)))
+    if args.train_seeds:
+        a, b = (int(v) for v in args.train_seeds.split(","))
+        train_seeds = list(range(a, a + b))
+    if args.hold_seeds:
+        a, b = (int(v) for v in args.hold_seeds.split(","))
+        hold_seeds = list(range(a, a + b))
     generate(net, train_seeds, args.n, args.steps, sopts, log)
     n_train = net.n_samples
     generate(net, hold_seeds, args.n, args.steps, sopts, log)
