@@ -230,6 +230,7 @@ def measured_peak():
 # scaled by the cell count (x 8); the traffic of these streaming kernels grows in proportion.
 NCU_TRAFFIC = {
     "bicg_spmv_omega": (281.86e6 + 17.78e6) * 8,
+    "bicg_spmv_alpha": (281.20e6 + 14.63e6) * 8,
     "ilu_black_apply": (133.48e6 + 4.35e6) * 8,
     "ilu_red_apply": (133.50e6 + 4.21e6) * 8,
     "bicg_xr": (83.93e6 + 3.81e6) * 8,

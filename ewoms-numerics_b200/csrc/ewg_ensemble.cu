@@ -44,7 +44,12 @@ thread_local std::string g_ensCreateError;
 namespace ewg {
 
 constexpr int kEnsTile = 256;    // threads per block
-constexpr int kEnsTileH = 1024;  // half indices per tile (4 per thread: the tile prologue is amortized)
+// half indices per tile (8 per thread with 2048: the tile prologue is amortized; 1024 and 4096
+// measured 4 % slower on the 64-member benchmark ensemble)
+#ifndef EWG_ENS_TILE_H
+#define EWG_ENS_TILE_H 2048
+#endif
+constexpr int kEnsTileH = EWG_ENS_TILE_H;
 constexpr int kEnsBands = 7;   // 3D: diagonal + 6 faces
 // resident blocks per SM the BiCGStab kernels are compiled for (register budgets 64 and 48)
 constexpr int kEnsBlocksSpmv = 4;
