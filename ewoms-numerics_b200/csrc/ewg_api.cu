@@ -3,6 +3,7 @@
 // (nonlinear/newtonmethod.hh:308-517) on device-resident data.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 

@@ -12,22 +12,37 @@
 namespace ewg {
 
 // intensive quantities of one cell that its neighbours need (immiscibleintensivequantities.hh
-// :87-145): p_c, lambda_w = k_rw / mu_w, lambda_n = k_rn / mu_n, each with d/dS_w, in 6 planes
+// :87-145): p_c, lambda_w = k_rw / mu_w, lambda_n = k_rn / mu_n, each with d/dS_w
+struct IqVals {
+    double pc, dpc, lw, dlw, ln, dln;
+};
+__device__ __forceinline__ IqVals intensive_values(const Phys& P, double Sw, int lensFlag) {
+    const LawDev& L = P.law[lensFlag];
+    MatOut m = material(L, Sw);
+    // mobility = kr / mu as an AD quotient with a constant denominator
+    const double muw = P.mu[0], mun = P.mu[1];
+    IqVals o;
+    o.pc = m.pc.v;
+    o.dpc = m.pc.d;
+    o.lw = m.krw.v / muw;
+    o.dlw = (muw * m.krw.d) / (muw * muw);
+    o.ln = m.krn.v / mun;
+    o.dln = (mun * m.krn.d) / (mun * mun);
+    return o;
+}
+
+// the same, written to the cache in 6 planes (pc, dpc, lw, dlw, ln, dln)
 __device__ __forceinline__ void intensive_cell(const Phys& P, const double2* __restrict__ x,
                                                const uint8_t* __restrict__ lens, double* __restrict__ iq,
                                                int64_t s) {
     const int64_t N = P.N;
-    const double Sw = x[s].y;
-    const LawDev& L = P.law[lens[s]];
-    MatOut m = material(L, Sw);
-    // mobility = kr / mu as an AD quotient with a constant denominator
-    double muw = P.mu[0], mun = P.mu[1];
-    iq[s] = m.pc.v;
-    iq[N + s] = m.pc.d;
-    iq[2 * N + s] = m.krw.v / muw;
-    iq[3 * N + s] = (muw * m.krw.d) / (muw * muw);
-    iq[4 * N + s] = m.krn.v / mun;
-    iq[5 * N + s] = (mun * m.krn.d) / (mun * mun);
+    const IqVals o = intensive_values(P, x[s].y, lens[s]);
+    iq[s] = o.pc;
+    iq[N + s] = o.dpc;
+    iq[2 * N + s] = o.lw;
+    iq[3 * N + s] = o.dlw;
+    iq[4 * N + s] = o.ln;
+    iq[5 * N + s] = o.dln;
 }
 
 __device__ __forceinline__ void store_block(double* J, int64_t N, int band, int64_t s, const double b[4]) {
@@ -221,41 +236,26 @@ __device__ __forceinline__ NbrGlobal nbr_global(const double2* x, const double* 
     return NbrGlobal{x, perm, iq, iq + 2 * N, iq + 4 * N};
 }
 
+// What the element of a cell needs of the cell itself.
+struct OwnVals {
+    double pw, Sw, K, pc, dpc, lam[2], dlam[2];
+};
+
 // One cell of a 3D grid: fluxes over its interior faces in intersection order (-x, +x, -y, +y,
 // -z, +z), the implicit-Euler storage term (fvbaselocalresidual.hh:494-629), its boundary faces,
 // division by the cell volume. Writes r_s and the Jacobian column of s; returns max |r_s|
-// (NaN / Inf set *bad). `nbr` supplies the neighbour values.
+// (NaN / Inf set *bad). `idx` is the cell's (i, j, k), `has` says which faces have a neighbour,
+// `nb` holds the neighbours' split-order positions and `nbr` supplies their values.
 template <typename JT, bool WITH_J, class NB>
-__device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* __restrict__ geo,
-                                                 const double2* __restrict__ x, const double2* __restrict__ sold,
-                                                 const double* __restrict__ perm, const uint8_t* __restrict__ lens,
-                                                 const double* __restrict__ iq, double dt, double2* __restrict__ rOut,
-                                                 JT* __restrict__ J, int64_t s, int& bad, const NB& nbr) {
+__device__ __forceinline__ double assemble_core3(const Phys& P, const FaceGeo* __restrict__ geo, const int idx[3],
+                                                 const bool has[6], const int nb[6], int s32, const OwnVals& o,
+                                                 double2 so, const uint8_t* __restrict__ lens, double dt,
+                                                 double2* __restrict__ rOut, JT* __restrict__ J, int& bad,
+                                                 const NB& nbr) {
     const int64_t N = P.N;
     const double V = P.vol;
     const int n3[3] = {P.nx, P.ny, P.nz};
-    const int s32 = (int)s;  // N < 2^31: 32-bit cell indices
-    const int Nh32 = (int)P.Nh;
-    const int col = s32 >= Nh32 ? 1 : 0;
-    const int h = s32 - col * Nh32;
-    const CellIdx ci = cell_of(P, col, h);
-    const int idx[3] = {ci.i, ci.j, ci.k};
-    const bool has[6] = {ci.i > 0, ci.i < P.nx - 1, ci.j > 0, ci.j < P.ny - 1, ci.k > 0, ci.k < P.nz - 1};
-    const double2 xi = x[s32];
-    const double Ki = perm[s32];
-    const double* iq1 = iq + N;
-    const double* iq2 = iq + 2 * N;
-    const double* iq3 = iq + 3 * N;
-    const double* iq4 = iq + 4 * N;
-    const double* iq5 = iq + 5 * N;
-    const double pci = iq[s32], dpci = iq1[s32];
-    const double lam[2] = {iq2[s32], iq4[s32]};
-    const double dlam[2] = {iq3[s32], iq5[s32]};
-    const double pI[2] = {xi.x, xi.x + (pci - 0.0)};
-    const int base = (col ^ 1) * Nh32;
-    const int nxh = P.nxh, planeh = (int)P.planeh;
-    const int nb[6] = {base + h - 1 + ci.b, base + h + ci.b, base + h - nxh, base + h + nxh, base + h - planeh,
-                       base + h + planeh};
+    const double pI[2] = {o.pw, o.pw + (o.pc - 0.0)};
     double R[2] = {0.0, 0.0};
     double D[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
@@ -268,17 +268,16 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
         const double pwj = nv.pw, Kj = nv.K, pcj = nv.pc, lwj = nv.lw, lnj = nv.ln;
         double Dj[4];
         if (axis == 0)
-            interior_face_tab<0>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
+            interior_face_tab<0>(P, G, side, o.K, pI, o.dpc, o.lam, o.dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         else if (axis == 1)
-            interior_face_tab<1>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
+            interior_face_tab<1>(P, G, side, o.K, pI, o.dpc, o.lam, o.dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         else
-            interior_face_tab<2>(P, G, side, Ki, pI, dpci, lam, dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
+            interior_face_tab<2>(P, G, side, o.K, pI, o.dpc, o.lam, o.dlam, pwj, Kj, pcj, lwj, lnj, R, D, Dj);
         if (WITH_J) store_block(J, N, opposite_band(band_of(axis, side)), sj, Dj);
     }
     // storage: (phi S rho - storage(x_old)) V / dt
     {
-        const double2 so = sold[s32];
-        const double Sw = xi.y;
+        const double Sw = o.Sw;
         const double fac = V / dt;
         const double sw0 = P.porosity * Sw * P.rho[0];
         const double sn0 = P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1];
@@ -294,11 +293,11 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
         const int axis = q >> 1, side = q & 1;
         const int li = lens[s32];
         if (axis == 0)
-            boundary_face<3, 0>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
+            boundary_face<3, 0>(P, side, idx, li, o.K, pI, o.dpc, o.lam, o.dlam, R, D);
         else if (axis == 1)
-            boundary_face<3, 1>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
+            boundary_face<3, 1>(P, side, idx, li, o.K, pI, o.dpc, o.lam, o.dlam, R, D);
         else
-            boundary_face<3, 2>(P, side, idx, li, Ki, pI, dpci, lam, dlam, R, D);
+            boundary_face<3, 2>(P, side, idx, li, o.K, pI, o.dpc, o.lam, o.dlam, R, D);
     }
     const double invV = P.invVol;
     R[0] *= invV;
@@ -310,6 +309,40 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
     }
     if (!(fabs(R[0]) <= 1.7976931348623157e308) || !(fabs(R[1]) <= 1.7976931348623157e308)) bad = 1;
     return fmax(fabs(R[0]), fabs(R[1]));
+}
+
+// One cell of a 3D grid at split-order position s with its own and its neighbours' values read
+// from the global arrays and the intensive-quantity cache.
+template <typename JT, bool WITH_J, class NB>
+__device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* __restrict__ geo,
+                                                 const double2* __restrict__ x, const double2* __restrict__ sold,
+                                                 const double* __restrict__ perm, const uint8_t* __restrict__ lens,
+                                                 const double* __restrict__ iq, double dt, double2* __restrict__ rOut,
+                                                 JT* __restrict__ J, int64_t s, int& bad, const NB& nbr) {
+    const int64_t N = P.N;
+    const int s32 = (int)s;  // N < 2^31: 32-bit cell indices
+    const int Nh32 = (int)P.Nh;
+    const int col = s32 >= Nh32 ? 1 : 0;
+    const int h = s32 - col * Nh32;
+    const CellIdx ci = cell_of(P, col, h);
+    const int idx[3] = {ci.i, ci.j, ci.k};
+    const bool has[6] = {ci.i > 0, ci.i < P.nx - 1, ci.j > 0, ci.j < P.ny - 1, ci.k > 0, ci.k < P.nz - 1};
+    const double2 xi = x[s32];
+    OwnVals o;
+    o.pw = xi.x;
+    o.Sw = xi.y;
+    o.K = perm[s32];
+    o.pc = iq[s32];
+    o.dpc = iq[N + s32];
+    o.lam[0] = iq[2 * N + s32];
+    o.lam[1] = iq[4 * N + s32];
+    o.dlam[0] = iq[3 * N + s32];
+    o.dlam[1] = iq[5 * N + s32];
+    const int base = (col ^ 1) * Nh32;
+    const int nxh = P.nxh, planeh = (int)P.planeh;
+    const int nb[6] = {base + h - 1 + ci.b, base + h + ci.b, base + h - nxh, base + h + nxh, base + h - planeh,
+                       base + h + planeh};
+    return assemble_core3<JT, WITH_J>(P, geo, idx, has, nb, s32, o, sold[s32], lens, dt, rOut, J, bad, nbr);
 }
 
 }  // namespace ewg

@@ -500,6 +500,8 @@ static void launch_assemble3(ewg_ctx* ctx, double dt, const double2* x, double2*
                r, J, ctx->d_errmax, ctx->d_flags);
 }
 
+static ewg_status read_linearize_result(ewg_ctx* ctx, double* maxOut, int* nonfinite);
+
 ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const double2* x,
                             double2* r, double* maxOut, int* nonfinite) {
     cudaError_t e;
@@ -507,11 +509,12 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
         return cuda_fail(ctx, e, "memset errmax");
     if ((e = cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "memset flags");
+    const bool three = ctx->P.dim == 3;
+    const bool fd = withJacobian && ctx->localLinearizer == EWG_LOCAL_LINEARIZER_FD;
     int g1 = grid_size_for(ctx, (const void*)k_intensive, kLinBlock);
     EWG_LAUNCH(ctx, K_INTENSIVE, k_intensive, g1, kLinBlock, ctx->P, x, ctx->lens, ctx->iq);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_intensive");
-    const bool three = ctx->P.dim == 3;
-    if (withJacobian && ctx->localLinearizer == EWG_LOCAL_LINEARIZER_FD) {
+    if (fd) {
         const int m = ctx->fdMethod;
         if (ctx->jacPrecision == EWG_PRECISION_MIXED) {
             auto k = three ? k_assemble_fd<3, float> : k_assemble_fd<2, float>;
@@ -548,6 +551,12 @@ ewg_status launch_linearize(ewg_ctx* ctx, double dt, bool withJacobian, const do
                    ctx->J, ctx->d_errmax, ctx->d_flags);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "k_assemble");
+    return read_linearize_result(ctx, maxOut, nonfinite);
+}
+
+// the residual max-norm and the non-finite flag of the last linearization, read back when asked
+static ewg_status read_linearize_result(ewg_ctx* ctx, double* maxOut, int* nonfinite) {
+    cudaError_t e;
     if (maxOut || nonfinite) {
         // small synchronous read-back: the Newton loop needs the error on the host
         unsigned long long bits = 0;
