@@ -484,6 +484,34 @@ def run_ours(args, rank, world, local, pg):
         ctx.set_solution(1, x_plain)
         ctx.set_solution(0, x_plain)
 
+    # ---- the local linearizers on the final state: AD (the timed path) and finite differences ----
+    linearizers = {}
+    if not args.no_forms:
+        peak_l, _ = measured_peak()
+        lb_l = lin_bytes(N, F, 8)
+        # one short FP64 Newton pass selects the FP64 Jacobian (the forms above end in FP32)
+        ctx.newton_apply(250.0, ewg.default_newton_opts(newton_max_iterations=1),
+                         ewg.default_solve_opts(linear_solver_tolerance=1e-3))
+        ctx.restore_time_level()
+        ctx.set_solution(1, x_plain)
+        ctx.set_solution(0, x_plain)
+        for lname, kind, method in (("ad", ewg.LOCAL_LINEARIZER_AD, 1), ("fd_forward", ewg.LOCAL_LINEARIZER_FD, 1),
+                                    ("fd_central", ewg.LOCAL_LINEARIZER_FD, 0)):
+            ctx.set_local_linearizer(kind, method)
+            ctx.linearize(250.0)
+            torch.cuda.synchronize()
+            l0 = torch.cuda.Event(enable_timing=True)
+            l1 = torch.cuda.Event(enable_timing=True)
+            l0.record(stream)
+            for _ in range(10):
+                ctx.linearize(250.0)
+            l1.record(stream)
+            torch.cuda.synchronize()
+            l_ms = max_over_ranks(pg, l0.elapsed_time(l1)) / 10
+            linearizers[lname] = {"ms_per_linearization": l_ms, "mcells_per_s": N / (l_ms * 1e-3) / 1e6,
+                                  "frac_of_lin_bytes": lb_l / (l_ms * 1e-3) / 1e9 / peak_l}
+        ctx.set_local_linearizer(ewg.LOCAL_LINEARIZER_AD, 1)
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -574,7 +602,7 @@ def run_ours(args, rank, world, local, pg):
         "phase_s": {"linearize": sum(r.t_linearize for r in reps) / len(reps),
                     "solve": sum(r.t_solve for r in reps) / len(reps),
                     "update": sum(r.t_update for r in reps) / len(reps)},
-        "roofline": roofline, "linearization": lin, "bicgstab": bicg,
+        "roofline": roofline, "linearization": lin, "linearizers": linearizers, "bicgstab": bicg,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "cpu_baseline": cpu,
         "clocks": clk.summary(),

@@ -292,6 +292,50 @@ def lens3d_case(nx=256, ny=256, nz=128, seed=0, sigma=1.0, corr_cells=8.0,
 
 
 # ------------------------------------------------------------------------------------------
+# vertex-centred (VCFV) cases: the same problems with one DOF and one permeability per grid vertex
+
+
+def vertex_positions(grid: Grid):
+    """Vertex coordinates (x, y, z) as flat arrays, x fastest: index * h per axis."""
+    nz = grid.nz if grid.dim == 3 else 0
+    hx, hy = grid.lx / grid.nx, grid.ly / grid.ny
+    hz = grid.lz / grid.nz if grid.dim == 3 else 0.0
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(grid.ny + 1), np.arange(grid.nx + 1), indexing="ij")
+    return (i * hx).ravel(), (j * hy).ravel(), (k * hz).ravel()
+
+
+def n_vertices(grid: Grid) -> int:
+    return (grid.nx + 1) * (grid.ny + 1) * ((grid.nz + 1) if grid.dim == 3 else 1)
+
+
+def in_lens_vertices(grid: Grid, problem: Problem) -> np.ndarray:
+    """isInLens_ (lensproblem.hh:596-604) at the vertex positions."""
+    pos = vertex_positions(grid)
+    m = np.ones(n_vertices(grid), dtype=bool)
+    for a in range(grid.dim):
+        m &= (pos[a] >= problem.lens_lo[a] - problem.eps) & (pos[a] <= problem.lens_hi[a] + problem.eps)
+    return m
+
+
+def vcfv_case(case: LensCase, seed: int | None = None, sigma: float = 1.0, corr_cells: float = 8.0) -> LensCase:
+    """The vertex-centred version of a lens case: permeability per vertex. The 2D presets take
+    their lens / outer values by vertex position; lens3d draws its log-normal field on the vertex
+    grid (seed defaults to 0)."""
+    g, p = case.grid, case.problem
+    lens = in_lens_vertices(g, p)
+    if case.name == "lens3d":
+        shape = (g.nz + 1, g.ny + 1, g.nx + 1)
+        f = gaussian_log_field(shape, sigma=sigma, corr_cells=corr_cells, seed=0 if seed is None else seed).ravel()
+        lnk = np.log(9.05e-12) + f
+        perm = np.exp(np.where(lens, lnk + np.log(0.1), lnk))
+    else:
+        k_lens = float(case.perm[in_lens(g, p)][0])
+        k_out = float(case.perm[~in_lens(g, p)][0])
+        perm = np.where(lens, k_lens, k_out)
+    return LensCase("vcfv_" + case.name, g, p, np.ascontiguousarray(perm, dtype=np.float64), case.dt, case.n_steps)
+
+
+# ------------------------------------------------------------------------------------------
 # library loading
 
 _lib = None

@@ -924,6 +924,485 @@ static Bcrs systemMatrix(const Ctx& C) {
     return A;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Vertex-centred finite volumes (VcfvDiscretization, discretizations/vcfv/) for the same model and
+// problem with P1 finite-element gradients (UseP1FiniteElementGradients, as lens_immiscible_vcfv_ad
+// sets): DOFs at the grid vertices, control volumes from the sub-control volumes (SCVs) that each
+// element gives its corners, fluxes over the sub-control-volume faces (SCVFs) that join the element
+// centre to its edges (vcfvstencil.hh:866-1016). Structured grids of axis-aligned boxes: every
+// element has the same local geometry, built once from the reference element in DUNE's numbering
+// (vertex v has local coordinates given by its bits; edges and faces as in the tables of
+// vcfvstencil.hh:595-716), with global vectors taken relative to the element's lower corner.
+
+struct VGeom {
+    int dim = 2, nv = 4, ne = 4, nf = 4, nfv = 2;
+    double h[3] = {1, 1, 1};
+    int vb[8][3] = {};
+    int ei[12] = {}, ej[12] = {};        // SCVF interior / exterior vertex
+    double ip[12][3] = {};               // SCVF integration point (local)
+    double nrm[12][3] = {}, area[12] = {};
+    double G[12][8][3] = {};             // global P1 shape-function gradients at ip
+    double scvVol = 0.0;
+    double scvCenter[8][3] = {};         // local
+    int fv[6][4] = {};                   // vertices of each element face
+    double bip[6][4][3] = {}, barea[6][4] = {};
+    double fnrm[6][3] = {};              // outer unit normal of each element face
+    int faxis[6] = {}, fside[6] = {};
+};
+
+static void cross3(const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// normalOfQuadrilateral3D (vcfvstencil.hh:568-583): 0.5 (p2 - p0) x (p3 - p1)
+static void quadNormal(const double p0[3], const double p1[3], const double p2[3], const double p3[3], double n[3]) {
+    double a[3], b[3];
+    for (int d = 0; d < 3; ++d) { a[d] = p2[d] - p0[d]; b[d] = p3[d] - p1[d]; }
+    cross3(a, b, n);
+    for (int d = 0; d < 3; ++d) n[d] *= 0.5;
+}
+static double norm3(const double n[3], int dim) {
+    double s = 0.0;
+    for (int d = 0; d < dim; ++d) s += n[d] * n[d];
+    return std::sqrt(s);
+}
+
+static VGeom makeVGeom(int dim, const double h[3]) {
+    VGeom g;
+    g.dim = dim;
+    g.nv = 1 << dim;
+    g.ne = dim == 2 ? 4 : 12;
+    g.nf = 2 * dim;
+    g.nfv = dim == 2 ? 2 : 4;
+    for (int d = 0; d < 3; ++d) g.h[d] = d < dim ? h[d] : 1.0;
+    for (int v = 0; v < g.nv; ++v)
+        for (int d = 0; d < 3; ++d) g.vb[v][d] = d < dim ? (v >> d) & 1 : 0;
+    auto glob = [&](const double l[3], double o[3]) { for (int d = 0; d < 3; ++d) o[d] = d < dim ? l[d] * g.h[d] : 0.0; };
+    double elemL[3] = {0.5, 0.5, dim == 3 ? 0.5 : 0.0}, elemG[3];
+    glob(elemL, elemG);
+    // element faces: 2a + s is the face with x_a = s (YaspGrid intersection order)
+    double faceL[6][3];
+    for (int f = 0; f < g.nf; ++f) {
+        int a = f >> 1, sd = f & 1;
+        g.faxis[f] = a; g.fside[f] = sd;
+        for (int d = 0; d < 3; ++d) faceL[f][d] = d < dim ? 0.5 : 0.0;
+        faceL[f][a] = sd;
+        for (int d = 0; d < 3; ++d) g.fnrm[f][d] = 0.0;
+        g.fnrm[f][a] = sd ? 1.0 : -1.0;
+        int m = 0;
+        for (int v = 0; v < g.nv; ++v) if (g.vb[v][a] == sd) g.fv[f][m++] = v;
+    }
+    // edges (reference-element numbering)
+    static const int e2[4][2] = {{0, 2}, {1, 3}, {0, 1}, {2, 3}};
+    static const int e3[12][2] = {{0, 4}, {1, 5}, {2, 6}, {3, 7}, {0, 2}, {1, 3},
+                                  {0, 1}, {2, 3}, {4, 6}, {5, 7}, {4, 5}, {6, 7}};
+    static const unsigned edgeToFaceHex[2][12] = {{0, 2, 3, 1, 4, 1, 2, 4, 0, 5, 5, 3},
+                                                  {2, 1, 0, 3, 0, 4, 4, 3, 5, 1, 2, 5}};
+    double edgeL[12][3], edgeG[12][3], faceG[6][3];
+    for (int f = 0; f < g.nf; ++f) glob(faceL[f], faceG[f]);
+    for (int k = 0; k < g.ne; ++k) {
+        int a = dim == 2 ? e2[k][0] : e3[k][0], b = dim == 2 ? e2[k][1] : e3[k][1];
+        for (int d = 0; d < 3; ++d) edgeL[k][d] = d < dim ? 0.5 * (g.vb[a][d] + g.vb[b][d]) : 0.0;
+        glob(edgeL[k], edgeG[k]);
+        int i = a, j = b;
+        if (g.ne == 4 && (i == 2 || j == 2)) std::swap(i, j);
+        g.ei[k] = i; g.ej[k] = j;
+        double n[3] = {0, 0, 0};
+        if (dim == 2) {
+            for (int d = 0; d < 3; ++d) g.ip[k][d] = (edgeL[k][d] + elemL[d]) * 0.5;
+            double diff[3];
+            for (int d = 0; d < 2; ++d) diff[d] = elemG[d] - edgeG[k][d];
+            n[0] = diff[1]; n[1] = -diff[0];
+            double xi[3], xj[3], li[3], lj[3];
+            for (int d = 0; d < 3; ++d) { li[d] = g.vb[i][d]; lj[d] = g.vb[j][d]; }
+            glob(li, xi); glob(lj, xj);
+            double dot = 0.0;
+            for (int d = 0; d < 2; ++d) dot += n[d] * (xj[d] - xi[d]);
+            if (dot < 0) for (int d = 0; d < 2; ++d) n[d] *= -1;
+        } else {
+            unsigned lf = edgeToFaceHex[0][k], rf = edgeToFaceHex[1][k];
+            for (int d = 0; d < 3; ++d) g.ip[k][d] = (((edgeL[k][d] + elemL[d]) + faceL[lf][d]) + faceL[rf][d]) * 0.25;
+            quadNormal(edgeG[k], faceG[rf], elemG, faceG[lf], n);
+        }
+        g.area[k] = norm3(n, dim);
+        for (int d = 0; d < 3; ++d) g.nrm[k][d] = d < dim ? n[d] / g.area[k] : 0.0;
+        // P1 (Q1) shape-function gradients at the integration point, mapped by the inverse
+        // transposed Jacobian diag(1/h)
+        for (int v = 0; v < g.nv; ++v)
+            for (int d = 0; d < dim; ++d) {
+                double q = g.vb[v][d] ? 1.0 : -1.0;
+                for (int e = 0; e < dim; ++e)
+                    if (e != d) q *= g.vb[v][e] ? g.ip[k][e] : 1.0 - g.ip[k][e];
+                g.G[k][v][d] = (1.0 / g.h[d]) * q;
+            }
+    }
+    // sub-control volumes: the box between the vertex and the element centre
+    double vol = 1.0;
+    for (int d = 0; d < dim; ++d) vol *= g.h[d];
+    g.scvVol = vol / g.nv;
+    for (int v = 0; v < g.nv; ++v)
+        for (int d = 0; d < 3; ++d) g.scvCenter[v][d] = d < dim ? (g.vb[v][d] + elemL[d]) * 0.5 : 0.0;
+    // boundary sub-faces: one per (element face, vertex of the face)
+    static const int leftEdgeHex[6][8] = {{0, -1, 4, -1, 8, -1, 2, -1}, {-1, 5, -1, 3, -1, 1, -1, 9},
+                                          {6, 1, -1, -1, 0, 10, -1, -1}, {-1, -1, 2, 7, -1, -1, 11, 3},
+                                          {4, 6, 7, 5, -1, -1, -1, -1}, {-1, -1, -1, -1, 10, 9, 8, 11}};
+    static const int rightEdgeHex[6][8] = {{4, -1, 2, -1, 0, -1, 8, -1}, {-1, 1, -1, 5, -1, 9, -1, 3},
+                                           {0, 6, -1, -1, 10, 1, -1, -1}, {-1, -1, 7, 3, -1, -1, 2, 11},
+                                           {6, 5, 4, 7, -1, -1, -1, -1}, {-1, -1, -1, -1, 8, 10, 11, 9}};
+    for (int f = 0; f < g.nf; ++f)
+        for (int m = 0; m < g.nfv; ++m) {
+            int v = g.fv[f][m];
+            double vl[3] = {(double)g.vb[v][0], (double)g.vb[v][1], (double)g.vb[v][2]};
+            if (dim == 2) {
+                for (int d = 0; d < 3; ++d) g.bip[f][m][d] = (vl[d] + faceL[f][d]) * 0.5;
+                int a = g.faxis[f];
+                g.barea[f][m] = 0.5 * g.h[1 - a];  // half of the face length
+            } else {
+                int le = leftEdgeHex[f][v], re = rightEdgeHex[f][v];
+                for (int d = 0; d < 3; ++d)
+                    g.bip[f][m][d] = (((vl[d] + faceL[f][d]) + edgeL[le][d]) + edgeL[re][d]) * 0.25;
+                double vg[3], n[3];
+                glob(vl, vg);
+                quadNormal(vg, edgeG[re], faceG[f], edgeG[le], n);
+                g.barea[f][m] = norm3(n, 3);
+            }
+        }
+    return g;
+}
+
+struct VCtx {
+    int dim = 2, n[3] = {1, 1, 1};   // elements per axis
+    int nvx[3] = {1, 1, 1};          // vertices per axis
+    double L[3] = {1, 1, 1}, h[3] = {1, 1, 1};
+    int64_t NE = 0, NV = 0;
+    ewg_problem prob{};
+    Law law[2];
+    VGeom geo;
+    std::vector<double> perm;               // per vertex
+    std::vector<unsigned char> inLens;      // per vertex
+    std::vector<double> totVol;             // dofTotalVolume per vertex
+    std::vector<double> sol[2], storageOld, resid;
+    std::vector<int32_t> rowPtr, colIdx;
+    std::vector<double> blocks;
+    std::vector<IQ> iqCache;
+    bool recycleStorage = true;
+    int nthreads = 1;
+    std::string err;
+
+    double gravity(int a) const { return a == 1 ? -prob.gravity : 0.0; }
+    void vijk(int64_t v, int64_t id[3]) const {
+        id[0] = v % nvx[0]; id[1] = (v / nvx[0]) % nvx[1]; id[2] = v / ((int64_t)nvx[0] * nvx[1]);
+    }
+    int64_t vindex(int64_t i, int64_t j, int64_t k) const { return i + nvx[0] * (j + (int64_t)nvx[1] * k); }
+    void vpos(int64_t v, double x[3]) const {
+        int64_t id[3]; vijk(v, id);
+        for (int d = 0; d < 3; ++d) x[d] = d < dim ? id[d] * h[d] : 0.0;
+    }
+    void eijk(int64_t e, int64_t id[3]) const {
+        id[0] = e % n[0]; id[1] = (e / n[0]) % n[1]; id[2] = e / ((int64_t)n[0] * n[1]);
+    }
+    // global vertex of local vertex lv of element e
+    int64_t evert(const int64_t eid[3], int lv) const {
+        return vindex(eid[0] + geo.vb[lv][0], eid[1] + geo.vb[lv][1], eid[2] + (dim == 3 ? geo.vb[lv][2] : 0));
+    }
+    bool isInLens(const double x[3]) const {
+        for (int a = 0; a < dim; ++a)
+            if (x[a] < prob.lens_lo[a] - prob.eps || x[a] > prob.lens_hi[a] + prob.eps) return false;
+        return true;
+    }
+};
+
+static IQ computeVIQ(const VCtx& C, int64_t v, const double* x) {
+    IQ q;
+    const Law& L = C.law[C.inLens[v]];
+    Eval Sw = Eval::variable(x[2 * v + 1], 1);
+    q.S[0] = Sw;
+    q.S[1] = 1.0 - (Eval(0.0) + Sw);
+    Eval pC[2];
+    capillaryPressures(pC, L, q.S[0]);
+    relativePermeabilities(q.kr, L, q.S[0]);
+    Eval p0 = Eval::variable(x[2 * v], 0);
+    for (int a = 0; a < 2; ++a) q.p[a] = p0 + (pC[a] - pC[0]);
+    q.mu[0] = Eval(C.prob.mu_w); q.mu[1] = Eval(C.prob.mu_n);
+    q.rho[0] = Eval(C.prob.rho_w); q.rho[1] = Eval(C.prob.rho_n);
+    for (int a = 0; a < 2; ++a) q.mob[a] = q.kr[a] / q.mu[a];
+    q.porosity = C.prob.porosity;
+    q.K = C.perm[v];
+    return q;
+}
+
+static inline Eval focusOr(const Eval& e, bool focus) { return focus ? e : Eval(e.v); }
+
+// Flux over SCVF k of an element whose local vertices have the intensive quantities q[],
+// derivatives with respect to local vertex `focus` (darcyfluxmodule.hh:185-324 with
+// P1FeGradientCalculator::calculateGradient, p1fegradientcalculator.hh:255-290; :461-527;
+// immisciblelocalresidual.hh:123-149), mass per area.
+static void vcfvFlux(const VCtx& C, const IQ* q[8], int k, int focus, Eval flux[2]) {
+    const VGeom& g = C.geo;
+    const int dim = C.dim;
+    const int i = g.ei[k], j = g.ej[k];
+    Eval grad[2][3];
+    for (int a = 0; a < 2; ++a) {
+        for (int d = 0; d < 3; ++d) grad[a][d] = Eval(0.0);
+        for (int v = 0; v < g.nv; ++v) {
+            Eval pv = focusOr(q[v]->p[a], v == focus);
+            for (int d = 0; d < dim; ++d) grad[a][d] += pv * g.G[k][v][d];
+        }
+    }
+    // gravity correction between the two vertices, estimated at the integration point
+    double posIn[3], posEx[3], posF[3];
+    for (int d = 0; d < 3; ++d) {
+        posIn[d] = g.vb[i][d] * g.h[d];
+        posEx[d] = g.vb[j][d] * g.h[d];
+        posF[d] = g.ip[k][d] * g.h[d];
+    }
+    double distIn[3], distEx[3], distTot[3];
+    for (int d = 0; d < 3; ++d) { distIn[d] = posIn[d] - posF[d]; distEx[d] = posEx[d] - posF[d]; distTot[d] = posEx[d] - posIn[d]; }
+    double absDistTotSq = 0.0;
+    for (int d = 0; d < dim; ++d) absDistTotSq += distTot[d] * distTot[d];
+    double gIn = 0.0, gEx = 0.0;
+    for (int d = 0; d < dim; ++d) { gIn += C.gravity(d) * distIn[d]; gEx += C.gravity(d) * distEx[d]; }
+    for (int a = 0; a < 2; ++a) {
+        Eval pStatIn = -(focusOr(q[i]->rho[a], i == focus) * gIn);
+        Eval pStatEx = -(focusOr(q[j]->rho[a], j == focus) * gEx);
+        Eval qq = (pStatEx - pStatIn) / absDistTotSq;
+        for (int d = 0; d < dim; ++d) grad[a][d] += Eval(distTot[d]) * qq;
+        for (int d = 0; d < dim; ++d)
+            if (!std::isfinite(grad[a][d].v)) throw std::runtime_error("Non-finite potential gradient");
+    }
+    // intersectionIntrinsicPermeability: entry-wise harmonic mean of the two vertices' tensors
+    double Kf[3][3];
+    for (int r = 0; r < dim; ++r)
+        for (int s2 = 0; s2 < dim; ++s2)
+            Kf[r][s2] = harmonicMean(r == s2 ? q[i]->K : 0.0, r == s2 ? q[j]->K : 0.0);
+    for (int a = 0; a < 2; ++a) {
+        Eval tmp(0.0);
+        for (int d = 0; d < dim; ++d) tmp += grad[a][d] * g.nrm[k][d];
+        const int up = tmp.v > 0 ? j : i;
+        Eval mob = focusOr(q[up]->mob[a], up == focus);
+        Eval vel[3];
+        for (int r = 0; r < dim; ++r) {
+            Eval s(0.0);
+            for (int c2 = 0; c2 < dim; ++c2) s += Kf[r][c2] * grad[a][c2];
+            vel[r] = s * (-mob);
+        }
+        Eval volFlux(0.0);
+        for (int d = 0; d < dim; ++d) volFlux += vel[d] * g.nrm[k][d];
+        Eval rho = focusOr(q[up]->rho[a], up == focus);
+        flux[a] = volFlux * rho;
+    }
+}
+
+// LensProblem::boundary at boundary sub-face (f, m) of element eid, interior vertex lv: the free-flow
+// state on the left / right faces with the two-point boundary gradient from the SCV centre
+// (fvbasegradientcalculator.hh:277-312, darcyfluxmodule.hh:333-453), the inlet mass rate, no flow
+// elsewhere; derivatives only when the vertex is the focus. Mass rate per area.
+static void vcfvBoundaryRate(const VCtx& C, const int64_t eid[3], int f, int m, const IQ& qv, int lv, int64_t gv,
+                             bool focus, Eval rate[2]) {
+    const VGeom& g = C.geo;
+    const ewg_problem& P = C.prob;
+    const int dim = C.dim;
+    double pos[3];  // absolute position of the integration point
+    for (int d = 0; d < 3; ++d) pos[d] = d < dim ? (eid[d] + g.bip[f][m][d]) * C.h[d] : 0.0;
+    double xmin = 0.0, xmax = C.L[0], ymax = C.L[1];
+    bool left = pos[0] < xmin + P.eps, right = pos[0] > xmax - P.eps;
+    rate[0] = Eval(0.0); rate[1] = Eval(0.0);
+    if (left || right) {
+        double pw, Sw = 1.0;
+        double depth = ymax - pos[1];
+        if (left) pw = P.p_ref - P.left_pressure_scale * P.rho_w * C.gravity(1) * depth;
+        else pw = P.p_ref - P.rho_w * C.gravity(1) * depth;
+        const Law& Lf = C.law[C.isInLens(pos) ? 1 : 0];
+        double pC[2];
+        capillaryPressures(pC, Lf, Sw);
+        double pB[2] = {pw, pw + pC[1] - pC[0]};
+        double rhoB[2] = {P.rho_w, P.rho_n}, muB[2] = {P.mu_w, P.mu_n};
+        // relative positions: integration point, SCV centre and vertex
+        double ipG[3], scvC[3], vG[3];
+        for (int d = 0; d < 3; ++d) {
+            ipG[d] = g.bip[f][m][d] * g.h[d];
+            scvC[d] = g.scvCenter[lv][d] * g.h[d];
+            vG[d] = g.vb[lv][d] * g.h[d];
+        }
+        double distSq = 0.0;
+        for (int d = 0; d < dim; ++d) { double t = ipG[d] - scvC[d]; distSq += t * t; }
+        Eval grad[2][3];
+        for (int a = 0; a < 2; ++a) {
+            Eval deltay = focus ? Eval(pB[a]) - qv.p[a] : Eval(pB[a] - qv.p[a].v);
+            for (int d = 0; d < dim; ++d) { double t = ipG[d] - scvC[d]; grad[a][d] = deltay * (t / distSq); }
+        }
+        double distIn[3];
+        for (int d = 0; d < 3; ++d) distIn[d] = vG[d] - ipG[d];
+        double absDistSq = 0.0, gTimesDist = 0.0;
+        for (int d = 0; d < dim; ++d) { absDistSq += distIn[d] * distIn[d]; gTimesDist += C.gravity(d) * distIn[d]; }
+        for (int a = 0; a < 2; ++a) {
+            Eval pStatIn = -gTimesDist * qv.rho[a];
+            Eval qq = pStatIn / absDistSq;
+            for (int d = 0; d < dim; ++d) grad[a][d] += distIn[d] * qq;
+            for (int d = 0; d < dim; ++d)
+                if (!std::isfinite(grad[a][d].v)) throw std::runtime_error("Non finite potential gradient");
+        }
+        // kr of the boundary state with the interior vertex's parameters
+        const Law& Li = C.law[C.inLens[gv]];
+        double krB[2];
+        relativePermeabilities(krB, Li, Sw);
+        for (int a = 0; a < 2; ++a) {
+            Eval tmp(0.0);
+            for (int d = 0; d < dim; ++d) tmp += grad[a][d] * g.fnrm[f][d];
+            Eval mob = (tmp.v > 0) ? Eval(krB[a] / muB[a]) : focusOr(qv.mob[a], focus);
+            Eval volFlux(0.0);
+            for (int d = 0; d < dim; ++d) {
+                Eval s2(0.0);
+                for (int c2 = 0; c2 < dim; ++c2) s2 += (d == c2 ? qv.K : 0.0) * grad[a][c2];
+                Eval vv = s2 * (-mob);
+                volFlux += vv * g.fnrm[f][d];
+            }
+            Eval density = (pB[a] > qv.p[a].v) ? Eval(rhoB[a]) : focusOr(qv.rho[a], focus);
+            rate[a] = rate[a] + volFlux * density;
+        }
+        return;
+    }
+    bool upper = pos[1] > ymax - P.eps;
+    bool inlet = upper && pos[0] > P.inlet_x_lo && pos[0] < P.inlet_x_hi;
+    if (inlet && dim == 3) inlet = pos[2] > P.inlet_z_lo && pos[2] < P.inlet_z_hi;
+    if (inlet) rate[1] = Eval(P.inlet_rate);
+}
+
+
+// FvBaseLocalResidual::eval for element eid with derivatives with respect to local vertex `focus`
+// (fvbaselocalresidual.hh:154-187): SCVF fluxes in edge order, the storage term of every vertex
+// with its SCV volume, the boundary sub-faces, then division by each vertex's total control
+// volume (UseVolumetricResidual).
+static void vcfvEvalLocal(VCtx& C, const int64_t eid[3], const int64_t gv[8], const IQ* q[8], int focus, double dt,
+                          int newtonIteration, Eval R[8][2]) {
+    const VGeom& g = C.geo;
+    for (int v = 0; v < g.nv; ++v) { R[v][0] = Eval(0.0); R[v][1] = Eval(0.0); }
+    for (int k = 0; k < g.ne; ++k) {
+        Eval flux[2];
+        vcfvFlux(C, q, k, focus, flux);
+        double alpha = 1.0;  // extrusion factor
+        alpha *= g.area[k];
+        for (int a = 0; a < 2; ++a) flux[a] = flux[a] * alpha;
+        for (int a = 0; a < 2; ++a) { R[g.ei[k]][a] += flux[a]; R[g.ej[k]][a] -= flux[a]; }
+    }
+    for (int v = 0; v < g.nv; ++v) {
+        double scvVolume = g.scvVol * 1.0;
+        Eval tmp[2];
+        if (v == focus) storageOf<Eval>(*q[v], tmp);
+        else { double t2[2]; storageOf<double>(*q[v], t2); tmp[0] = Eval(t2[0]); tmp[1] = Eval(t2[1]); }
+        double tmp2[2];
+        const int64_t G = gv[v];
+        if (newtonIteration == 0) {
+            if (!C.recycleStorage) {
+                IQ qold = computeVIQ(C, G, C.sol[1].data());
+                storageOf<double>(qold, tmp2);
+            } else {
+                tmp2[0] = tmp[0].v; tmp2[1] = tmp[1].v;
+            }
+            C.storageOld[2 * G] = tmp2[0]; C.storageOld[2 * G + 1] = tmp2[1];
+        } else {
+            tmp2[0] = C.storageOld[2 * G]; tmp2[1] = C.storageOld[2 * G + 1];
+        }
+        for (int a = 0; a < 2; ++a) {
+            tmp[a] -= Eval(tmp2[a]);
+            tmp[a] *= Eval(scvVolume / dt);
+            R[v][a] += tmp[a];
+        }
+    }
+    // boundary sub-faces (intersection order, then the face's vertices)
+    for (int f = 0; f < g.nf; ++f) {
+        const int a = g.faxis[f];
+        const bool onB = g.fside[f] == 0 ? eid[a] == 0 : eid[a] == C.n[a] - 1;
+        if (!onB) continue;
+        for (int m = 0; m < g.nfv; ++m) {
+            const int v = g.fv[f][m];
+            Eval rate[2];
+            vcfvBoundaryRate(C, eid, f, m, *q[v], v, gv[v], v == focus, rate);
+            for (int e = 0; e < 2; ++e) { rate[e] = rate[e] * (g.barea[f][m] * 1.0); R[v][e] += rate[e]; }
+        }
+    }
+    for (int v = 0; v < g.nv; ++v)
+        for (int a = 0; a < 2; ++a) R[v][a] /= C.totVol[gv[v]];
+}
+
+static void vcfvBuildPattern(VCtx& C) {
+    // createMatrix_: vertex rows couple to every vertex of the elements they belong to
+    C.rowPtr.assign(C.NV + 1, 0);
+    std::vector<int32_t> cols;
+    for (int64_t v = 0; v < C.NV; ++v) {
+        int64_t id[3]; C.vijk(v, id);
+        for (int64_t dk = (C.dim == 3 ? -1 : 0); dk <= (C.dim == 3 ? 1 : 0); ++dk)
+            for (int64_t dj = -1; dj <= 1; ++dj)
+                for (int64_t di = -1; di <= 1; ++di) {
+                    int64_t i = id[0] + di, j = id[1] + dj, k = id[2] + dk;
+                    if (i < 0 || j < 0 || k < 0 || i >= C.nvx[0] || j >= C.nvx[1] || k >= C.nvx[2]) continue;
+                    cols.push_back((int32_t)C.vindex(i, j, k));
+                }
+        C.rowPtr[v + 1] = (int32_t)cols.size();
+    }
+    C.colIdx = std::move(cols);
+    C.blocks.assign(C.colIdx.size() * 4, 0.0);
+}
+
+static int32_t vcfvBlockPos(const VCtx& C, int64_t row, int64_t col) {
+    for (int32_t q = C.rowPtr[row]; q < C.rowPtr[row + 1]; ++q) if (C.colIdx[q] == col) return q;
+    return -1;
+}
+
+// FvBaseLinearizer::linearize_ with FvBaseAdLocalLinearizer (fvbaseadlocallinearizer.hh:178-204):
+// per element, the intensive quantities of its vertices, then one evaluation of the local residual
+// per focus vertex, and the scatter residual_[globI] += r_i, J[globJ][globI] += dR_j / dx_i of
+// linearizeElement_ (fvbaselinearizer.hh:483-512), elements in index order.
+static double vcfvLinearize(VCtx& C, double dt, int newtonIteration) {
+    std::fill(C.resid.begin(), C.resid.end(), 0.0);
+    std::fill(C.blocks.begin(), C.blocks.end(), 0.0);
+    C.iqCache.resize(C.NV);
+    const double* x = C.sol[0].data();
+    parallelFor(C.nthreads, C.NV, [&](int64_t b, int64_t e, int) {
+        for (int64_t v = b; v < e; ++v) C.iqCache[v] = computeVIQ(C, v, x);
+    });
+    const VGeom& g = C.geo;
+    for (int64_t e = 0; e < C.NE; ++e) {
+        int64_t eid[3]; C.eijk(e, eid);
+        int64_t gv[8];
+        const IQ* q[8];
+        for (int v = 0; v < g.nv; ++v) { gv[v] = C.evert(eid, v); q[v] = &C.iqCache[gv[v]]; }
+        double res[8][2];
+        double jac[8][8][4];  // [dof][focus][eq*2+pv]
+        for (int f = 0; f < g.nv; ++f) {
+            Eval R[8][2];
+            vcfvEvalLocal(C, eid, gv, q, f, dt, newtonIteration, R);
+            for (int a = 0; a < 2; ++a) res[f][a] = R[f][a].v;
+            for (int d = 0; d < g.nv; ++d)
+                for (int eq = 0; eq < 2; ++eq)
+                    for (int pv = 0; pv < 2; ++pv) jac[d][f][2 * eq + pv] = R[d][eq].d[pv];
+        }
+        for (int i = 0; i < g.nv; ++i) {
+            const int64_t gi = gv[i];
+            for (int a = 0; a < 2; ++a) C.resid[2 * gi + a] += res[i][a];
+            for (int d = 0; d < g.nv; ++d) {
+                int32_t pos = vcfvBlockPos(C, gv[d], gi);
+                double* B = &C.blocks[4 * (size_t)pos];
+                for (int t = 0; t < 4; ++t) B[t] += jac[d][i][t];
+            }
+        }
+    }
+    double err = 0.0;
+    for (int64_t v = 0; v < C.NV; ++v) {
+        double a = std::abs(C.resid[2 * v]), b = std::abs(C.resid[2 * v + 1]);
+        if (!std::isfinite(a) || !std::isfinite(b)) return std::numeric_limits<double>::infinity();
+        err = std::max(err, std::max(a, b));
+    }
+    return err;
+}
+
+static Bcrs vcfvMatrix(const VCtx& C) {
+    Bcrs A; A.n = C.NV; A.rp = C.rowPtr; A.ci = C.colIdx; A.v = C.blocks; A.findDiag();
+    return A;
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -1164,6 +1643,183 @@ void orc_boundary_rates(orc_ctx* o, double* out) {
             out[1] += rate[1].v * C.area(f[k].axis);
         }
     }
+}
+
+}  // extern "C"
+
+// ---- vertex-centred discretization -------------------------------------------------------------
+
+struct orc_vcfv { VCtx C; };
+
+extern "C" {
+
+// perm: one permeability per vertex, vertices numbered x fastest ((nx+1) x (ny+1) [x (nz+1)])
+orc_vcfv* orc_vcfv_create(const ewg_grid* g, const ewg_problem* p, const double* perm, int nthreads) {
+    orc_vcfv* o = new orc_vcfv();
+    VCtx& C = o->C;
+    C.dim = g->dim;
+    C.n[0] = g->nx; C.n[1] = g->ny; C.n[2] = g->dim == 3 ? g->nz : 1;
+    C.L[0] = g->lx; C.L[1] = g->ly; C.L[2] = g->dim == 3 ? g->lz : 1.0;
+    for (int a = 0; a < 3; ++a) C.h[a] = C.L[a] / C.n[a];
+    for (int a = 0; a < 3; ++a) C.nvx[a] = a < C.dim ? C.n[a] + 1 : 1;
+    C.NE = (int64_t)C.n[0] * C.n[1] * C.n[2];
+    C.NV = (int64_t)C.nvx[0] * C.nvx[1] * C.nvx[2];
+    C.prob = *p;
+    C.law[0] = makeLaw(p->outer);
+    C.law[1] = makeLaw(p->lens);
+    C.geo = makeVGeom(C.dim, C.h);
+    C.perm.assign(perm, perm + C.NV);
+    C.inLens.resize(C.NV);
+    for (int64_t v = 0; v < C.NV; ++v) { double x[3]; C.vpos(v, x); C.inLens[v] = C.isInLens(x) ? 1 : 0; }
+    // dofTotalVolume: the SCV volumes summed over the elements in index order
+    C.totVol.assign(C.NV, 0.0);
+    for (int64_t e = 0; e < C.NE; ++e) {
+        int64_t eid[3]; C.eijk(e, eid);
+        for (int v = 0; v < C.geo.nv; ++v) C.totVol[C.evert(eid, v)] += C.geo.scvVol * 1.0;
+    }
+    C.sol[0].assign(2 * C.NV, 0.0); C.sol[1].assign(2 * C.NV, 0.0);
+    C.storageOld.assign(2 * C.NV, 0.0);
+    C.resid.assign(2 * C.NV, 0.0);
+    C.nthreads = std::max(1, nthreads);
+    vcfvBuildPattern(C);
+    return o;
+}
+void orc_vcfv_destroy(orc_vcfv* o) { delete o; }
+const char* orc_vcfv_last_error(const orc_vcfv* o) { return o->C.err.c_str(); }
+int64_t orc_vcfv_num_dofs(const orc_vcfv* o) { return o->C.NV; }
+int64_t orc_vcfv_num_blocks(const orc_vcfv* o) { return (int64_t)o->C.colIdx.size(); }
+void orc_vcfv_set_solution(orc_vcfv* o, int t, const double* x) { o->C.sol[t].assign(x, x + 2 * o->C.NV); }
+void orc_vcfv_get_solution(const orc_vcfv* o, int t, double* x) {
+    std::memcpy(x, o->C.sol[t].data(), sizeof(double) * 2 * o->C.NV);
+}
+// LensProblem::initial at the vertex positions
+void orc_vcfv_apply_initial_solution(orc_vcfv* o) {
+    VCtx& C = o->C;
+    for (int64_t v = 0; v < C.NV; ++v) {
+        double x[3]; C.vpos(v, x);
+        double depth = C.L[1] - x[1];
+        C.sol[0][2 * v] = C.prob.p_ref - C.prob.rho_w * C.gravity(1) * depth;
+        C.sol[0][2 * v + 1] = 1.0;
+    }
+    C.sol[1] = C.sol[0];
+}
+void orc_vcfv_advance_time_level(orc_vcfv* o) { o->C.sol[1] = o->C.sol[0]; }
+void orc_vcfv_total_volumes(const orc_vcfv* o, double* out) {
+    std::memcpy(out, o->C.totVol.data(), sizeof(double) * o->C.NV);
+}
+int orc_vcfv_linearize(orc_vcfv* o, double dt, int it, double* error) {
+    try {
+        double e = vcfvLinearize(o->C, dt, it);
+        if (error) *error = e;
+        return 0;
+    } catch (const std::exception& ex) { o->C.err = ex.what(); return 1; }
+}
+void orc_vcfv_get_residual(const orc_vcfv* o, double* r) {
+    std::memcpy(r, o->C.resid.data(), sizeof(double) * 2 * o->C.NV);
+}
+void orc_vcfv_get_jacobian_bcrs(const orc_vcfv* o, int32_t* rp, int32_t* ci, double* b) {
+    const VCtx& C = o->C;
+    if (rp) std::memcpy(rp, C.rowPtr.data(), sizeof(int32_t) * C.rowPtr.size());
+    if (ci) std::memcpy(ci, C.colIdx.data(), sizeof(int32_t) * C.colIdx.size());
+    if (b) std::memcpy(b, C.blocks.data(), sizeof(double) * C.blocks.size());
+}
+
+// NewtonMethod::apply at a fixed time-step size with BiCGStab and the block ILU(0) (natural order)
+// or block Jacobi preconditioner of so->precond
+int orc_vcfv_newton_apply(orc_vcfv* o, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
+                          int* newtonIts, int* linIts, double* errorOut) {
+    VCtx& C = o->C;
+    static const Ctx kNoGrid{};
+    int numIterations = 0, linTotal = 0;
+    double error = 1e100, lastError = 1e100;
+    auto converged = [&]() { return error <= no->newton_tolerance; };
+    auto proceed = [&]() {
+        if (numIterations < 1) return true;
+        if (converged()) return false;
+        if (numIterations >= no->newton_max_iterations) return error * 4.0 < lastError;
+        return true;
+    };
+    int status = 0;
+    try {
+        while (proceed()) {
+            double e = vcfvLinearize(C, dt, numIterations);
+            lastError = error;
+            error = e;
+            if (error > no->newton_max_error) throw std::runtime_error("Newton: error above NewtonMaxError");
+            if (!proceed()) { ++numIterations; break; }
+            Bcrs A = vcfvMatrix(C);
+            Precond M; M.kind = so->precond; M.ordering = ORC_ORDER_NATURAL; M.w = so->preconditioner_relaxation;
+            M.setup(kNoGrid, A);
+            Criterion crit{so->linear_solver_tolerance, so->linear_solver_abs_tolerance, so->linear_solver_max_error};
+            std::vector<double> dx;
+            int it = 0, restarts = 0;
+            bool ok = bicgstab(A, M, C.resid, dx, crit, so->linear_solver_max_iterations,
+                               so->restart_on_breakdown != 0, so->verify_true_residual != 0, &it, &restarts);
+            linTotal += it;
+            if (!ok) { status = EWG_ERR_NOT_CONVERGED; break; }
+            double one = 0.0;
+            for (double v : dx) one += std::abs(v);
+            if (!std::isfinite(one)) throw std::runtime_error("Non-finite update!");
+            for (int64_t i = 0; i < 2 * C.NV; ++i) C.sol[0][i] -= dx[i];
+            ++numIterations;
+        }
+    } catch (const BreakdownError& ex) { C.err = ex.what(); status = EWG_ERR_BREAKDOWN; }
+    catch (const std::exception& ex) { C.err = ex.what(); status = EWG_ERR_NONFINITE; }
+    if (newtonIts) *newtonIts = numIterations;
+    if (linIts) *linIts = linTotal;
+    if (errorOut) *errorOut = error;
+    if (status) return status;
+    return converged() ? 0 : EWG_ERR_NOT_CONVERGED;
+}
+
+// total mass of each phase (storage x total control volume) at time level t
+void orc_vcfv_global_storage(const orc_vcfv* o, int t, double* out) {
+    const VCtx& C = o->C;
+    out[0] = out[1] = 0.0;
+    for (int64_t v = 0; v < C.NV; ++v) {
+        IQ q = computeVIQ(C, v, C.sol[t].data());
+        double s[2]; storageOf<double>(q, s);
+        out[0] += s[0] * C.totVol[v]; out[1] += s[1] * C.totVol[v];
+    }
+}
+
+// sum of boundary mass rates x area over all boundary sub-faces at the current solution
+void orc_vcfv_boundary_rates(orc_vcfv* o, double* out) {
+    VCtx& C = o->C;
+    out[0] = out[1] = 0.0;
+    const VGeom& g = C.geo;
+    for (int64_t e = 0; e < C.NE; ++e) {
+        int64_t eid[3]; C.eijk(e, eid);
+        for (int f = 0; f < g.nf; ++f) {
+            const int a = g.faxis[f];
+            const bool onB = g.fside[f] == 0 ? eid[a] == 0 : eid[a] == C.n[a] - 1;
+            if (!onB) continue;
+            for (int m = 0; m < g.nfv; ++m) {
+                const int v = g.fv[f][m];
+                int64_t gv = C.evert(eid, v);
+                IQ q = computeVIQ(C, gv, C.sol[0].data());
+                Eval rate[2];
+                vcfvBoundaryRate(C, eid, f, m, q, v, gv, false, rate);
+                out[0] += rate[0].v * g.barea[f][m];
+                out[1] += rate[1].v * g.barea[f][m];
+            }
+        }
+    }
+}
+
+// the local geometry of the structured element: for each SCVF k (i, j, ip[3], nrm[3], area) and the
+// P1 gradients G[k][v][3]; scv volume
+void orc_vcfv_geometry(const orc_vcfv* o, int32_t* ij, double* ip, double* nrm, double* area, double* G,
+                       double* scvVol) {
+    const VGeom& g = o->C.geo;
+    for (int k = 0; k < g.ne; ++k) {
+        ij[2 * k] = g.ei[k]; ij[2 * k + 1] = g.ej[k];
+        for (int d = 0; d < 3; ++d) { ip[3 * k + d] = g.ip[k][d]; nrm[3 * k + d] = g.nrm[k][d]; }
+        area[k] = g.area[k];
+        for (int v = 0; v < g.nv; ++v)
+            for (int d = 0; d < 3; ++d) G[(k * 8 + v) * 3 + d] = g.G[k][v][d];
+    }
+    *scvVol = g.scvVol;
 }
 
 }  // extern "C"

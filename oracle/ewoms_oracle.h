@@ -76,6 +76,29 @@ void orc_global_storage(const orc_ctx* c, int time_idx, double* out2);
 /* Sum of boundary mass rates [kg/s] (positive = out of the domain) at solution(0), per phase. */
 void orc_boundary_rates(orc_ctx* c, double* out2);
 
+/* ---- vertex-centred finite volumes (VcfvDiscretization with P1 gradients) ----
+ * DOFs at the (nx+1) x (ny+1) [x (nz+1)] vertices, numbered x fastest; perm per vertex. */
+typedef struct orc_vcfv orc_vcfv;
+orc_vcfv* orc_vcfv_create(const ewg_grid* g, const ewg_problem* p, const double* perm, int nthreads);
+void orc_vcfv_destroy(orc_vcfv* c);
+const char* orc_vcfv_last_error(const orc_vcfv* c);
+int64_t orc_vcfv_num_dofs(const orc_vcfv* c);
+int64_t orc_vcfv_num_blocks(const orc_vcfv* c);
+void orc_vcfv_set_solution(orc_vcfv* c, int time_idx, const double* x);
+void orc_vcfv_get_solution(const orc_vcfv* c, int time_idx, double* x);
+void orc_vcfv_apply_initial_solution(orc_vcfv* c);
+void orc_vcfv_advance_time_level(orc_vcfv* c);
+void orc_vcfv_total_volumes(const orc_vcfv* c, double* out);
+int orc_vcfv_linearize(orc_vcfv* c, double dt, int newton_iteration, double* error);
+void orc_vcfv_get_residual(const orc_vcfv* c, double* r);
+void orc_vcfv_get_jacobian_bcrs(const orc_vcfv* c, int32_t* row_ptr, int32_t* col_idx, double* blocks);
+int orc_vcfv_newton_apply(orc_vcfv* c, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
+                          int* newton_iterations, int* linear_iterations, double* error);
+void orc_vcfv_global_storage(const orc_vcfv* c, int time_idx, double* out2);
+void orc_vcfv_boundary_rates(orc_vcfv* c, double* out2);
+void orc_vcfv_geometry(const orc_vcfv* c, int32_t* ij, double* ip, double* nrm, double* area, double* G,
+                       double* scv_volume);
+
 #ifdef __cplusplus
 }
 #endif

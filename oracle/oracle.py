@@ -73,6 +73,24 @@ def load():
         "orc_material_eval": (None, [P(ewg.Material), d, P(d)]),
         "orc_global_storage": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_boundary_rates": (None, [C.c_void_p, P(d)]),
+        "orc_vcfv_create": (C.c_void_p, [P(ewg.Grid), P(ewg.Problem), P(d), C.c_int]),
+        "orc_vcfv_destroy": (None, [C.c_void_p]),
+        "orc_vcfv_last_error": (C.c_char_p, [C.c_void_p]),
+        "orc_vcfv_num_dofs": (C.c_int64, [C.c_void_p]),
+        "orc_vcfv_num_blocks": (C.c_int64, [C.c_void_p]),
+        "orc_vcfv_set_solution": (None, [C.c_void_p, C.c_int, P(d)]),
+        "orc_vcfv_get_solution": (None, [C.c_void_p, C.c_int, P(d)]),
+        "orc_vcfv_apply_initial_solution": (None, [C.c_void_p]),
+        "orc_vcfv_advance_time_level": (None, [C.c_void_p]),
+        "orc_vcfv_total_volumes": (None, [C.c_void_p, P(d)]),
+        "orc_vcfv_linearize": (C.c_int, [C.c_void_p, d, C.c_int, P(d)]),
+        "orc_vcfv_get_residual": (None, [C.c_void_p, P(d)]),
+        "orc_vcfv_get_jacobian_bcrs": (None, [C.c_void_p, P(i32), P(i32), P(d)]),
+        "orc_vcfv_newton_apply": (C.c_int, [C.c_void_p, d, P(ewg.NewtonOpts), P(ewg.SolveOpts),
+                                            P(C.c_int), P(C.c_int), P(d)]),
+        "orc_vcfv_global_storage": (None, [C.c_void_p, C.c_int, P(d)]),
+        "orc_vcfv_boundary_rates": (None, [C.c_void_p, P(d)]),
+        "orc_vcfv_geometry": (None, [C.c_void_p, P(i32), P(d), P(d), P(d), P(d), P(d)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -235,3 +253,97 @@ def material_eval(mat: "ewg.Material", sw: float) -> np.ndarray:
     out = np.zeros(6)
     load().orc_material_eval(C.byref(mat), sw, _p(out))
     return out
+
+
+class VcfvOracle:
+    """CPU restatement of the vertex-centred (VCFV, P1 gradients) linearizer and Newton on one lens
+    case whose permeability is given per vertex (VcfvCase)."""
+
+    def __init__(self, case, nthreads: int = 1):
+        self.lib = load()
+        self.case = case
+        perm = np.ascontiguousarray(case.perm, dtype=np.float64)
+        self.h = self.lib.orc_vcfv_create(C.byref(case.grid), C.byref(case.problem), _p(perm), nthreads)
+        self.n = self.lib.orc_vcfv_num_dofs(self.h)
+        self.nnzb = self.lib.orc_vcfv_num_blocks(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.orc_vcfv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def err(self):
+        return self.lib.orc_vcfv_last_error(self.h).decode()
+
+    def vec(self):
+        return np.zeros((self.n, 2), dtype=np.float64)
+
+    def set_solution(self, t, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)
+        self.lib.orc_vcfv_set_solution(self.h, t, _p(x))
+
+    def get_solution(self, t=0):
+        x = self.vec()
+        self.lib.orc_vcfv_get_solution(self.h, t, _p(x))
+        return x
+
+    def apply_initial_solution(self):
+        self.lib.orc_vcfv_apply_initial_solution(self.h)
+
+    def advance_time_level(self):
+        self.lib.orc_vcfv_advance_time_level(self.h)
+
+    def total_volumes(self):
+        v = np.zeros(self.n, dtype=np.float64)
+        self.lib.orc_vcfv_total_volumes(self.h, _p(v))
+        return v
+
+    def linearize(self, dt, newton_iteration=0):
+        e = C.c_double()
+        if self.lib.orc_vcfv_linearize(self.h, dt, newton_iteration, C.byref(e)) != 0:
+            raise RuntimeError(self.err())
+        return e.value
+
+    def residual(self):
+        r = self.vec()
+        self.lib.orc_vcfv_get_residual(self.h, _p(r))
+        return r
+
+    def jacobian_bcrs(self):
+        rp = np.zeros(self.n + 1, dtype=np.int32)
+        ci = np.zeros(self.nnzb, dtype=np.int32)
+        b = np.zeros((self.nnzb, 2, 2), dtype=np.float64)
+        self.lib.orc_vcfv_get_jacobian_bcrs(self.h, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(b))
+        return rp, ci, b
+
+    def newton_apply(self, dt, nopts=None, sopts=None):
+        nopts = nopts or ewg.default_newton_opts()
+        sopts = sopts or ewg.default_solve_opts()
+        its, lin, err = C.c_int(), C.c_int(), C.c_double()
+        st = self.lib.orc_vcfv_newton_apply(self.h, dt, C.byref(nopts), C.byref(sopts), C.byref(its),
+                                            C.byref(lin), C.byref(err))
+        return st, its.value, lin.value, err.value
+
+    def global_storage(self, t=0):
+        out = np.zeros(2)
+        self.lib.orc_vcfv_global_storage(self.h, t, _p(out))
+        return out
+
+    def boundary_rates(self):
+        out = np.zeros(2)
+        self.lib.orc_vcfv_boundary_rates(self.h, _p(out))
+        return out
+
+    def geometry(self):
+        ne = 4 if self.case.grid.dim == 2 else 12
+        ij = np.zeros((ne, 2), dtype=np.int32)
+        ip = np.zeros((ne, 3)); nrm = np.zeros((ne, 3)); area = np.zeros(ne)
+        G = np.zeros((ne, 8, 3)); sv = C.c_double()
+        self.lib.orc_vcfv_geometry(self.h, _p(ij, C.c_int32), _p(ip), _p(nrm), _p(area), _p(G), C.byref(sv))
+        return {"ij": ij, "ip": ip, "nrm": nrm, "area": area, "G": G, "scv_volume": sv.value}

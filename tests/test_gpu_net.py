@@ -97,3 +97,50 @@ def test_guess_fallback_keeps_previous_solution(ewg_mod):
     used, rg, rp = net.predict_guess(ctx, 100.0)
     assert used and rg == rp
     assert np.array_equal(ctx.get_solution(0), x1)
+
+
+def test_trained_network_gain_on_held_out_member(ewg_mod):
+    """What the committed network gains on a held-out realization of its training family (48^3
+    cells, seed 2000: log-normal K with sigma and correlation length drawn like the training
+    members, mixed-precision Newton): the initial residual of every accepted guess is below that
+    of the previous solution, the guess is accepted in most steps, the converged states agree
+    with the runs from the previous solution to the Newton tolerance's effect, and Newton needs
+    no more iterations in total."""
+    import os
+    ewg = ewg_mod
+    here = os.path.dirname(os.path.abspath(__file__))
+    path = os.path.join(here, "..", "ewoms-numerics_b200", "data", "guess_net_lens3d.npz")
+    rng = np.random.default_rng(2000)
+    sigma = float(rng.uniform(0.5, 1.5))
+    corr = float(rng.uniform(4.0, 12.0))
+    dt = float(rng.choice((100.0, 250.0, 500.0)))
+    case = ewg.lens3d_case(48, 48, 48, seed=2000, sigma=sigma, corr_cells=corr)
+    so = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-3,
+                                inner_tolerance=1e-3, max_defect_iterations=3)
+    net = ewg.GuessNet(seed=0)
+    net.load_file(path)
+    runs = {}
+    for mode in ("previous", "learned"):
+        ctx = ewg.Context(case)
+        ctx.apply_initial_solution()
+        its, ratios = [], []
+        for _ in range(5):
+            if mode == "learned":
+                used, rg, rp = net.predict_guess(ctx, dt)
+                assert used == (rg <= rp)
+                ratios.append(rg / rp if used else None)
+            st, rep = ctx.newton_apply(dt, None, so)
+            assert st == ewg.EWG_OK
+            its.append(rep.iterations)
+            ctx.advance_time_level()
+        runs[mode] = (its, ratios, ctx.get_solution(0))
+        ctx.close()
+    net.close()
+    its_prev, _, x_prev = runs["previous"]
+    its_learn, ratios, x_learn = runs["learned"]
+    accepted = [r for r in ratios if r is not None]
+    print("newton previous", its_prev, "learned", its_learn, "residual ratios", ratios)
+    assert len(accepted) >= 3 and max(accepted) < 1.0
+    assert sum(its_learn) <= sum(its_prev)
+    assert np.max(np.abs(x_learn[:, 1] - x_prev[:, 1])) < 1e-6
+    assert np.max(np.abs(x_learn[:, 0] - x_prev[:, 0])) < 1e-6 * np.max(np.abs(x_prev[:, 0]))
