@@ -391,6 +391,21 @@ def load(path: str = LIB_PATH):
         "ewg_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
         "ewg_profile_reset": (C.c_int, [C.c_void_p]),
         "ewg_profile_get": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(C.c_int64)]),
+        "ewg_vcfv_create": (C.c_int, [P(Grid), P(Problem), P(d), P(C.c_void_p)]),
+        "ewg_vcfv_destroy": (None, [C.c_void_p]),
+        "ewg_vcfv_last_error": (C.c_char_p, [C.c_void_p]),
+        "ewg_vcfv_num_dofs": (C.c_int64, [C.c_void_p]),
+        "ewg_vcfv_launches": (C.c_int64, [C.c_void_p]),
+        "ewg_vcfv_set_solution": (C.c_int, [C.c_void_p, C.c_int32, P(d)]),
+        "ewg_vcfv_get_solution": (C.c_int, [C.c_void_p, C.c_int32, P(d)]),
+        "ewg_vcfv_apply_initial_solution": (C.c_int, [C.c_void_p]),
+        "ewg_vcfv_advance_time_level": (C.c_int, [C.c_void_p]),
+        "ewg_vcfv_restore_time_level": (C.c_int, [C.c_void_p]),
+        "ewg_vcfv_linearize": (C.c_int, [C.c_void_p, d, P(d)]),
+        "ewg_vcfv_get_residual": (C.c_int, [C.c_void_p, P(d)]),
+        "ewg_vcfv_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), C.c_int64, P(d)]),
+        "ewg_vcfv_newton_apply": (C.c_int, [C.c_void_p, d, P(NewtonOpts), P(SolveOpts), P(C.c_int32),
+                                            P(C.c_int32), P(d)]),
         "ewg_net_num_params": (C.c_int64, []),
         "ewg_net_create": (C.c_int, [C.c_uint64, P(C.c_void_p)]),
         "ewg_net_destroy": (None, [C.c_void_p]),
@@ -747,6 +762,111 @@ class GuessNet:
         st = self.lib.ewg_predict_guess(ctx.h, self.h, dt, C.byref(used), C.byref(rg), C.byref(rp))
         ctx._check(st, "predict_guess")
         return bool(used.value), rg.value, rp.value
+
+
+# ------------------------------------------------------------------------------------------
+# vertex-centred discretization
+
+
+def vcfv_pattern(grid: Grid):
+    """BCRS pattern of the vertex stencil: row v holds the vertices of its adjacent elements,
+    columns ascending (the order FvBaseLinearizer::createMatrix_ produces with std::set)."""
+    nvx, nvy = grid.nx + 1, grid.ny + 1
+    nvz = grid.nz + 1 if grid.dim == 3 else 1
+    rows, cols = [0], []
+    for k in range(nvz):
+        for j in range(nvy):
+            for i in range(nvx):
+                for dk in ((-1, 0, 1) if grid.dim == 3 else (0,)):
+                    for dj in (-1, 0, 1):
+                        for di in (-1, 0, 1):
+                            ii, jj, kk = i + di, j + dj, k + dk
+                            if 0 <= ii < nvx and 0 <= jj < nvy and 0 <= kk < nvz:
+                                cols.append(ii + nvx * (jj + nvy * kk))
+                rows.append(len(cols))
+    return np.array(rows, dtype=np.int32), np.array(cols, dtype=np.int32)
+
+
+class VcfvContext:
+    """One vertex-centred lens problem on the device (ewg_vcfv_* in include/ewg.h). Host arrays
+    are natural vertex order, NV x 2 float64."""
+
+    def __init__(self, case: LensCase):
+        self.lib = load()
+        self.case = case
+        self._perm = np.ascontiguousarray(case.perm, dtype=np.float64)
+        h = C.c_void_p()
+        st = self.lib.ewg_vcfv_create(C.byref(case.grid), C.byref(case.problem), _ptr(self._perm), C.byref(h))
+        if st != EWG_OK:
+            raise EwgError(st, "ewg_vcfv_create failed")
+        self.h = h
+        self.n = self.lib.ewg_vcfv_num_dofs(h)
+
+    def _check(self, st, what=""):
+        if st != EWG_OK:
+            raise EwgError(st, f"{what}: {self.lib.ewg_vcfv_last_error(self.h).decode()}")
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ewg_vcfv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.ewg_vcfv_launches(self.h))
+
+    def vec(self):
+        return np.zeros((self.n, 2), dtype=np.float64)
+
+    def set_solution(self, t, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)
+        self._check(self.lib.ewg_vcfv_set_solution(self.h, t, _ptr(x)), "set_solution")
+
+    def get_solution(self, t=0):
+        x = self.vec()
+        self._check(self.lib.ewg_vcfv_get_solution(self.h, t, _ptr(x)), "get_solution")
+        return x
+
+    def apply_initial_solution(self):
+        self._check(self.lib.ewg_vcfv_apply_initial_solution(self.h), "apply_initial_solution")
+
+    def advance_time_level(self):
+        self._check(self.lib.ewg_vcfv_advance_time_level(self.h), "advance_time_level")
+
+    def restore_time_level(self):
+        self._check(self.lib.ewg_vcfv_restore_time_level(self.h), "restore_time_level")
+
+    def linearize(self, dt) -> float:
+        e = C.c_double()
+        self._check(self.lib.ewg_vcfv_linearize(self.h, dt, C.byref(e)), "linearize")
+        return e.value
+
+    def residual(self):
+        r = self.vec()
+        self._check(self.lib.ewg_vcfv_get_residual(self.h, _ptr(r)), "get_residual")
+        return r
+
+    def jacobian_bcrs(self):
+        rp, ci = vcfv_pattern(self.case.grid)
+        b = np.zeros((len(ci), 2, 2), dtype=np.float64)
+        self._check(self.lib.ewg_vcfv_get_jacobian_bcrs(self.h, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32), len(ci),
+                                                        _ptr(b)), "get_jacobian_bcrs")
+        return rp, ci, b
+
+    def newton_apply(self, dt, nopts=None, sopts=None):
+        nopts = nopts or default_newton_opts()
+        sopts = sopts or default_solve_opts(precond=PRECOND_JACOBI)
+        its, lin, err = C.c_int32(), C.c_int32(), C.c_double()
+        st = self.lib.ewg_vcfv_newton_apply(self.h, dt, C.byref(nopts), C.byref(sopts), C.byref(its), C.byref(lin),
+                                            C.byref(err))
+        return st, its.value, lin.value, err.value
 
 
 # ------------------------------------------------------------------------------------------

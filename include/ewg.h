@@ -415,6 +415,43 @@ ewg_status ewg_profile_get(ewg_ctx* ctx, int32_t id, double* ms_total, int64_t* 
 void ewg_default_solve_opts(ewg_solve_opts* o);
 void ewg_default_newton_opts(ewg_newton_opts* o);
 
+/* ---- vertex-centred finite volumes (VcfvDiscretization with UseP1FiniteElementGradients, as
+ * tests/lens_immiscible_vcfv_ad.cc selects) ----------------------------------------------------
+ *
+ * The same model and lens problem with the DOFs at the grid vertices: (nx+1) x (ny+1) [x (nz+1)]
+ * vertices, natural order (x fastest), one {p_w, S_w} block per vertex; perm has one value per
+ * vertex and the lens region is taken at the vertex positions. Replaces, for the vertex-centred
+ * type tag, the Linearizer (fvbaselinearizer.hh:401-512, local residual of
+ * discretizations/vcfv/vcfvstencil.hh:866-1016 and p1fegradientcalculator.hh:255-290) and the
+ * Newton / BiCGStab path with block Jacobi (PreconditionerWrapperJacobi,
+ * istlpreconditionerwrappers.hh:145). No red-black constraint on nx. */
+typedef struct ewg_vcfv ewg_vcfv;
+
+ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, const double* perm, ewg_vcfv** out);
+void ewg_vcfv_destroy(ewg_vcfv* c);
+const char* ewg_vcfv_last_error(const ewg_vcfv* c);
+int64_t ewg_vcfv_num_dofs(const ewg_vcfv* c);
+/* kernels launched by the context so far */
+int64_t ewg_vcfv_launches(const ewg_vcfv* c);
+ewg_status ewg_vcfv_set_solution(ewg_vcfv* c, int32_t time_idx, const double* x);
+ewg_status ewg_vcfv_get_solution(ewg_vcfv* c, int32_t time_idx, double* x);
+/* LensProblem::initial at the vertex positions into solution(0) and solution(1) */
+ewg_status ewg_vcfv_apply_initial_solution(ewg_vcfv* c);
+ewg_status ewg_vcfv_advance_time_level(ewg_vcfv* c);   /* solution(1) = solution(0) */
+ewg_status ewg_vcfv_restore_time_level(ewg_vcfv* c);   /* solution(0) = solution(1) */
+/* Residual (per unit control volume) and Jacobian of solution(0) against the storage of
+ * solution(1); *error = max |r|. */
+ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error);
+ewg_status ewg_vcfv_get_residual(ewg_vcfv* c, double* r);
+/* The Jacobian's 2x2 blocks in the caller's BCRS pattern of the vertex stencil (row v holds the
+ * vertices of its adjacent elements, columns ascending). */
+ewg_status ewg_vcfv_get_jacobian_bcrs(ewg_vcfv* c, const int32_t* row_ptr, const int32_t* col_idx, int64_t nnzb,
+                                      double* blocks);
+/* NewtonMethod::apply at fixed dt with BiCGStab + block Jacobi (sopts->precond must be
+ * EWG_PRECOND_JACOBI). */
+ewg_status ewg_vcfv_newton_apply(ewg_vcfv* c, double dt, const ewg_newton_opts* nopts, const ewg_solve_opts* sopts,
+                                 int32_t* newton_iterations, int32_t* linear_iterations, double* error);
+
 #ifdef __cplusplus
 }
 #endif
