@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-vcfv", action="store_true")
     return ap.parse_args()
 
 
@@ -320,6 +321,64 @@ def ensemble_cases(ewg, members, seed=3):
     return cases, dts
 
 
+def vcfv_lin_bytes(nv, dim=3):
+    """Algorithmic bytes of one vertex-centred linearization: per vertex x (16), old storage (16),
+    K (8), lens flag (1), residual (16) and the 27 (9) Jacobian blocks of its row (32 each)."""
+    return nv * (16 + 16 + 8 + 1 + 16 + (27 if dim == 3 else 9) * 32)
+
+
+def run_vcfv(args, rank, pg, torch, ewg):
+    """The vertex-centred discretization: linearization of the bench grid (the same 3D lens with
+    the permeability field drawn on the vertex grid) at a state with a partly drained top fifth,
+    and one implicit step of a 64^3-element member (BiCGStab + block Jacobi at the reference's
+    linear tolerance 1e-3)."""
+    case = ewg.vcfv_case(ewg.lens3d_case(args.nx, args.ny, args.nz, seed=rank), seed=rank)
+    g = ewg.VcfvContext(case)
+    g.apply_initial_solution()
+    x = g.get_solution(0)
+    rng = np.random.default_rng(rank)
+    y = ewg.vertex_positions(case.grid)[1]
+    top = y > 0.8 * case.grid.ly
+    xp = x.copy()
+    xp[top, 1] = 1.0 - rng.uniform(0.0, 0.4, int(top.sum()))
+    g.set_solution(1, x)
+    g.set_solution(0, xp)
+    for _ in range(3):
+        g.linearize(250.0)
+    torch.cuda.synchronize()
+    barrier(pg)
+    reps = 10
+    l0 = g.launches
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        g.linearize(250.0)
+    t1 = time.perf_counter()
+    launches = g.launches - l0
+    ms = max_over_ranks(pg, (t1 - t0) / reps * 1e3)
+    nv = g.n
+    peak, _ = measured_peak()
+    lb = vcfv_lin_bytes(nv)
+    out = {"grid": f"{args.nx}x{args.ny}x{args.nz} elements, {nv} vertices",
+           "ms_per_linearization": ms, "mvertices_per_s": nv / (ms * 1e-3) / 1e6,
+           "algorithmic_bytes": lb, "achieved_gbs": lb / (ms * 1e-3) / 1e9, "frac": lb / (ms * 1e-3) / 1e9 / peak,
+           "launches_per_linearization": launches / reps,
+           "timing": "host clock around synchronous ewg_vcfv_linearize calls (two kernels and a 12-byte read-back each)"}
+    g.close()
+    small = ewg.vcfv_case(ewg.lens3d_case(64, 64, 64, seed=rank), seed=rank)
+    g = ewg.VcfvContext(small)
+    g.apply_initial_solution()
+    so = ewg.default_solve_opts(precond=ewg.PRECOND_JACOBI, linear_solver_tolerance=1e-3,
+                                linear_solver_max_iterations=2000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st, its, lin, err = g.newton_apply(250.0, None, so)
+    t1 = time.perf_counter()
+    out["step_64cubed"] = {"status": int(st), "newton_its": its, "linear_its": lin, "s_per_step": t1 - t0,
+                           "vertices": g.n}
+    g.close()
+    return out
+
+
 def run_ensemble(args, rank, pg, torch, ewg):
     """The batched ensemble form: every member advances one implicit step per timed step (its own
     dt, FP64 residual / update / Newton test, FP32 Jacobian, ILU(0) and BiCGStab), all members in
@@ -547,6 +606,10 @@ def run_ours(args, rank, world, local, pg):
     if not args.no_ensemble:
         ensemble = run_ensemble(args, rank, pg, torch, ewg)
 
+    vcfv = None
+    if not args.no_vcfv:
+        vcfv = run_vcfv(args, rank, pg, torch, ewg)
+
     if rank != 0:
         ctx.close()
         return
@@ -604,7 +667,7 @@ def run_ours(args, rank, world, local, pg):
                     "update": sum(r.t_update for r in reps) / len(reps)},
         "roofline": roofline, "linearization": lin, "linearizers": linearizers, "bicgstab": bicg,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "cpu_baseline": cpu,
+        "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "vcfv": vcfv, "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

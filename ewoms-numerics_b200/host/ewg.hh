@@ -91,6 +91,39 @@ private:
     ewg_ctx* ctx_ = nullptr;
 };
 
+// The vertex-centred discretization (ewg_vcfv_*): one DOF and one permeability per vertex.
+class VcfvContext {
+public:
+    VcfvContext(const ewg_grid& grid, const ewg_problem& problem, const std::vector<double>& permVertices) {
+        ewg_status st = ewg_vcfv_create(&grid, &problem, permVertices.data(), &c_);
+        if (st != EWG_OK) throw Error(st, "ewg_vcfv_create failed");
+    }
+    VcfvContext(const VcfvContext&) = delete;
+    VcfvContext& operator=(const VcfvContext&) = delete;
+    ~VcfvContext() { ewg_vcfv_destroy(c_); }
+
+    int64_t numDofs() const { return ewg_vcfv_num_dofs(c_); }
+    void applyInitialSolution() { check(ewg_vcfv_apply_initial_solution(c_), "ewg_vcfv_apply_initial_solution"); }
+    void advanceTimeLevel() { check(ewg_vcfv_advance_time_level(c_), "ewg_vcfv_advance_time_level"); }
+    void restoreTimeLevel() { check(ewg_vcfv_restore_time_level(c_), "ewg_vcfv_restore_time_level"); }
+    void getSolution(int timeIdx, double* x) { check(ewg_vcfv_get_solution(c_, timeIdx, x), "ewg_vcfv_get_solution"); }
+    // NewtonMethod::apply; returns the status (non-zero: the caller halves the step)
+    ewg_status newtonApply(double dt, const ewg_newton_opts& no, const ewg_solve_opts& so, int* its, int* linIts) {
+        int32_t a = 0, b = 0;
+        double err = 0;
+        ewg_status st = ewg_vcfv_newton_apply(c_, dt, &no, &so, &a, &b, &err);
+        if (its) *its = a;
+        if (linIts) *linIts = b;
+        return st;
+    }
+
+private:
+    void check(ewg_status st, const char* what) {
+        if (st != EWG_OK) throw Error(st, std::string(what) + ": " + ewg_vcfv_last_error(c_));
+    }
+    ewg_vcfv* c_ = nullptr;
+};
+
 }  // namespace ewg
 
 #endif

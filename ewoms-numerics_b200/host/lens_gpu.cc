@@ -41,6 +41,7 @@ struct Params {
         {"PermFile", ""},              {"Output", ""},
         {"EnableVtkOutput", "1"},      {"OutputDir", "."},
         {"LocalLinearizer", "ad"},     {"NumericDifferenceMethod", "1"},
+        {"Discretization", "ecfv"},
     };
     std::string get(const std::string& k) const {
         auto it = values.find(k);
@@ -254,6 +255,101 @@ std::vector<ewg::VtkMultiWriter::Field> vtkFields(ewg::Context& ctx, const ewg_g
 
 }  // namespace
 
+// lens_immiscible_vcfv_ad: the vertex-centred discretization with P1 gradients, block Jacobi.
+// K per vertex from the lens box at the vertex positions (or PermFile with one value per vertex);
+// VTK output as point data.
+void runVcfv(const Params& p, const ewg_grid& g, const ewg_problem& pr, const std::vector<double>& permCells,
+             const ewg_solve_opts& so) {
+    (void)permCells;
+    if (so.precond != EWG_PRECOND_JACOBI) throw std::runtime_error("Discretization=vcfv solves with Preconditioner=jacobi");
+    const int nz = g.dim == 3 ? g.nz : 1;
+    const int nvx = g.nx + 1, nvy = g.ny + 1, nvz = g.dim == 3 ? nz + 1 : 1;
+    const int64_t NV = (int64_t)nvx * nvy * nvz;
+    const double h[3] = {g.lx / g.nx, g.ly / g.ny, g.dim == 3 ? g.lz / nz : 1.0};
+    std::vector<double> perm(NV);
+    const std::string permFile = p.get("PermFile");
+    if (!permFile.empty()) {
+        std::ifstream f(permFile, std::ios::binary);
+        if (!f) throw std::runtime_error("cannot open permeability file " + permFile);
+        f.read(reinterpret_cast<char*>(perm.data()), sizeof(double) * NV);
+        if (f.gcount() != (std::streamsize)(sizeof(double) * NV))
+            throw std::runtime_error("permeability file holds fewer values than vertices");
+    } else {
+        const std::string preset = p.get("Preset");
+        const double kOuter = preset == "reference" ? 4.6e-10 : 9.05e-12;
+        const double kLens = preset == "reference" ? 9.05e-12 : 9.05e-13;
+        for (int64_t v = 0; v < NV; ++v) {
+            const int64_t idx[3] = {v % nvx, (v / nvx) % nvy, v / ((int64_t)nvx * nvy)};
+            bool in = true;
+            for (int a = 0; a < g.dim; ++a) {
+                const double x = idx[a] * h[a];
+                if (x < pr.lens_lo[a] - pr.eps || x > pr.lens_hi[a] + pr.eps) in = false;
+            }
+            perm[v] = in ? kLens : kOuter;
+        }
+    }
+    ewg::VcfvContext ctx(g, pr, perm);
+    ctx.applyInitialSolution();
+    ewg_newton_opts no;
+    ewg_default_newton_opts(&no);
+    no.newton_tolerance = p.d("NewtonTolerance");
+    no.newton_max_iterations = p.i("NewtonMaxIterations");
+    no.newton_max_error = p.d("NewtonMaxError");
+    ewg::VtkMultiWriter vtk(p.get("OutputDir"), "lens_immiscible_vcfv_ad");
+    const bool vtkOut = p.i("EnableVtkOutput") != 0;
+    std::vector<double> x(2 * NV);
+    auto fields = [&]() {
+        ctx.getSolution(0, x.data());
+        std::vector<ewg::VtkMultiWriter::Field> f = {{"pressure_w", 1, {}}, {"saturation_w", 1, {}},
+                                                     {"saturation_n", 1, {}}, {"intrinsicPerm", g.dim * g.dim, {}}};
+        for (int64_t v = 0; v < NV; ++v) {
+            f[0].values.push_back(x[2 * v]);
+            f[1].values.push_back(x[2 * v + 1]);
+            f[2].values.push_back(1.0 - x[2 * v + 1]);
+            for (int r = 0; r < g.dim; ++r)
+                for (int c = 0; c < g.dim; ++c) f[3].values.push_back(r == c ? perm[v] : 0.0);
+        }
+        return f;
+    };
+    if (vtkOut) vtk.write(0.0, g, fields(), true);
+    const double endTime = p.d("EndTime"), maxDt = p.d("MaxTimeStepSize");
+    const int maxDivisions = p.i("MaxTimeStepDivisions"), target = p.i("NewtonTargetIterations");
+    double t = 0.0, dt = std::min(p.d("InitialTimeStepSize"), maxDt);
+    int step = 0;
+    auto wall0 = std::chrono::steady_clock::now();
+    while (t < endTime * (1 - 1e-12)) {
+        dt = std::min(dt, endTime - t);
+        int its = 0, lin = 0;
+        bool ok = false;
+        for (int attempt = 0; attempt < maxDivisions; ++attempt) {
+            if (ctx.newtonApply(dt, no, so, &its, &lin) == EWG_OK) { ok = true; break; }
+            ctx.restoreTimeLevel();
+            std::printf("Newton solver did not converge with dt=%g seconds. Retrying with time step of %g seconds\n",
+                        dt, dt / 2.0);
+            dt /= 2.0;
+        }
+        if (!ok) throw std::runtime_error("Newton solver didn't converge after " + std::to_string(maxDivisions) +
+                                          " time-step divisions. dt=" + std::to_string(dt));
+        ctx.advanceTimeLevel();
+        t += dt;
+        ++step;
+        std::printf("Time step %d done. t=%g s, dt=%g s, Newton iterations %d, linear iterations %d\n", step, t, dt,
+                    its, lin);
+        if (vtkOut) vtk.write(t, g, fields(), true);
+        double next = its > target ? dt / (1.0 + double(its - target) / target)
+                                   : dt * (1.0 + double(target - its) / target / 1.2);
+        dt = std::min(maxDt, next);
+    }
+    double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+    std::printf("Simulation of %d time steps took %g seconds\n", step, wall);
+    const std::string out = p.get("Output");
+    if (!out.empty()) {
+        ctx.getSolution(0, x.data());
+        std::ofstream f(out, std::ios::binary);
+        f.write(reinterpret_cast<const char*>(x.data()), sizeof(double) * x.size());
+    }
+}
+
 int main(int argc, char** argv) {
     Params p;
     try {
@@ -270,7 +366,6 @@ int main(int argc, char** argv) {
         ewg_problem pr;
         std::vector<double> perm;
         makeProblem(p, g, pr, perm);
-        ewg::Context ctx(g, pr, perm);
         ewg_solve_opts so;
         ewg_default_solve_opts(&so);
         so.linear_solver_tolerance = p.d("LinearSolverTolerance");
@@ -282,6 +377,13 @@ int main(int argc, char** argv) {
         so.precond = p.get("Preconditioner") == "jacobi" ? EWG_PRECOND_JACOBI : EWG_PRECOND_ILU0;
         so.precision = p.get("LinearSolverPrecision") == "mixed" ? EWG_PRECISION_MIXED : EWG_PRECISION_FP64;
         so.restart_on_breakdown = p.i("RestartOnBreakdown");
+        const std::string disc = p.get("Discretization");
+        if (disc == "vcfv") {
+            runVcfv(p, g, pr, perm, so);
+            return 0;
+        }
+        if (disc != "ecfv") throw std::runtime_error("Discretization must be 'ecfv' or 'vcfv'");
+        ewg::Context ctx(g, pr, perm);
         const std::string ll = p.get("LocalLinearizer");
         if (ll != "ad" && ll != "fd") throw std::runtime_error("LocalLinearizer must be 'ad' or 'fd'");
         ctx.setLocalLinearizer(ll == "fd" ? EWG_LOCAL_LINEARIZER_FD : EWG_LOCAL_LINEARIZER_AD,

@@ -6,7 +6,9 @@
 // relativePerm_<phase>, viscosity_<phase>, porosity, intrinsicPerm; phases "w" and "n".
 //
 // Structured grids only: cells are axis-aligned quadrilaterals (2D) or hexahedra (3D) on the
-// uniform grid [0,lx] x [0,ly] (x [0,lz]); points are the grid vertices, x fastest. Data is ASCII.
+// uniform grid [0,lx] x [0,ly] (x [0,lz]); points are the grid vertices, x fastest. Data is ASCII,
+// per cell (cell-centred discretization) or per vertex (vertex-centred, written as PointData like
+// the reference's vertex-centred VTK output).
 #ifndef EWG_HOST_VTKWRITER_HH
 #define EWG_HOST_VTKWRITER_HH
 
@@ -38,25 +40,28 @@ public:
 
     // Writes <dir>/<simName>-<index>.vtu for the state at `time` and rewrites the collection.
     // Returns the file name written.
-    std::string write(double time, const ewg_grid& g, const std::vector<Field>& fields) {
+    // pointData: the fields hold one value (x components) per grid vertex instead of per cell
+    std::string write(double time, const ewg_grid& g, const std::vector<Field>& fields, bool pointData = false) {
         std::ostringstream fn;
         fn << name_ << "-" << std::setw(5) << std::setfill('0') << index_ << ".vtu";
         const std::string file = fn.str();
-        writeVtu(dir_ + "/" + file, g, fields);
+        writeVtu(dir_ + "/" + file, g, fields, pointData);
         steps_.emplace_back(time, file);
         writePvd();
         ++index_;
         return file;
     }
 
-    static void writeVtu(const std::string& path, const ewg_grid& g, const std::vector<Field>& fields) {
+    static void writeVtu(const std::string& path, const ewg_grid& g, const std::vector<Field>& fields,
+                         bool pointData = false) {
         const int dim = g.dim;
         const int nx = g.nx, ny = g.ny, nz = dim == 3 ? g.nz : 1;
         const int64_t nCells = (int64_t)nx * ny * nz;
         const int px = nx + 1, py = ny + 1, pz = dim == 3 ? nz + 1 : 1;
         const int64_t nPoints = (int64_t)px * py * pz;
+        const int64_t nValues = pointData ? (int64_t)(nx + 1) * (ny + 1) * (dim == 3 ? nz + 1 : 1) : nCells;
         for (const Field& f : fields)
-            if ((int64_t)f.values.size() != nCells * f.components)
+            if ((int64_t)f.values.size() != nValues * f.components)
                 throw std::runtime_error("vtk field '" + f.name + "' has the wrong length");
         std::ofstream o(path);
         if (!o) throw std::runtime_error("cannot open '" + path + "' for writing");
@@ -65,14 +70,14 @@ public:
           << "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
           << " <UnstructuredGrid>\n"
           << "  <Piece NumberOfPoints=\"" << nPoints << "\" NumberOfCells=\"" << nCells << "\">\n";
-        o << "   <CellData>\n";
+        o << (pointData ? "   <PointData>\n" : "   <CellData>\n");
         for (const Field& f : fields) {
             o << "    <DataArray type=\"Float64\" Name=\"" << f.name << "\" NumberOfComponents=\"" << f.components
               << "\" format=\"ascii\">\n";
             for (size_t k = 0; k < f.values.size(); ++k) o << f.values[k] << ((k + 1) % 8 ? " " : "\n");
             o << "\n    </DataArray>\n";
         }
-        o << "   </CellData>\n";
+        o << (pointData ? "   </PointData>\n" : "   </CellData>\n");
         o << "   <Points>\n    <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
         const double hx = g.lx / nx, hy = g.ly / ny, hz = dim == 3 ? g.lz / nz : 0.0;
         for (int k = 0; k < pz; ++k)

@@ -131,3 +131,35 @@ def test_driver_fd_linearizer_runs(driver, tmp_path):
                           "--enable-vtk-output=0"], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert len([ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]) == 2
+
+
+def test_driver_vcfv_needs_jacobi(driver):
+    out = subprocess.run([driver, "--discretization=vcfv", "--preconditioner=ilu0"], capture_output=True, text=True)
+    assert out.returncode == 2 and "jacobi" in out.stderr
+
+
+@pytest.mark.gpu
+def test_driver_vcfv_runs_and_matches_oracle(driver, tmp_path, oracle_mod, ewg_mod):
+    """lens_immiscible_vcfv_ad through the driver: two steps of the baseline preset on the vertex
+    grid with block Jacobi; the final state equals the oracle's VCFV Newton run to the solver
+    tolerance's effect, and the VTK output carries the vertex fields as point data."""
+    outf = tmp_path / "x.bin"
+    out = subprocess.run([driver, "--discretization=vcfv", "--preconditioner=jacobi", "--preset=baseline",
+                          "--cells-x=24", "--cells-y=16", "--end-time=500", "--initial-time-step-size=250",
+                          "--max-time-step-size=250", f"--output={outf}", f"--output-dir={tmp_path}"],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    x = np.fromfile(outf, dtype=np.float64).reshape(-1, 2)
+    case = ewg_mod.vcfv_case(ewg_mod.baseline_case(24, 16))
+    o = oracle_mod.VcfvOracle(case)
+    o.apply_initial_solution()
+    so = ewg_mod.default_solve_opts(precond=ewg_mod.PRECOND_JACOBI)
+    for _ in range(2):
+        st, its, lin, err = o.newton_apply(250.0, None, so)
+        assert st == 0
+        o.advance_time_level()
+    xo = o.get_solution(0)
+    assert np.max(np.abs(x[:, 0] - xo[:, 0])) <= 1e-8 * np.max(np.abs(xo[:, 0]))
+    assert np.max(np.abs(x[:, 1] - xo[:, 1])) <= 1e-8
+    vtu = (tmp_path / "lens_immiscible_vcfv_ad-00002.vtu").read_text()
+    assert "<PointData>" in vtu and 'Name="saturation_n"' in vtu
