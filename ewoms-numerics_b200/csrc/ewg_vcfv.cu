@@ -286,8 +286,18 @@ __global__ void kv_total_volume(VDims D, int dim, double scvVol, double* __restr
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 
+// SCVF endpoints (interior i, exterior j) of the structured element, as build_vgeom orders them
+__device__ constexpr int kEdge2[4][2] = {{2, 0}, {1, 3}, {0, 1}, {3, 2}};
+__device__ constexpr int kEdge3[12][2] = {{0, 4}, {1, 5}, {2, 6}, {3, 7}, {0, 2}, {1, 3},
+                                          {0, 1}, {2, 3}, {4, 6}, {5, 7}, {4, 5}, {6, 7}};
+
 // Element contribution to the row of local vertex A (compile time) of the element at offset
-// (ox, oy, oz) from the thread's vertex, added to r and to the shared-memory block accumulators.
+// (ox, oy, oz) from the thread's vertex, added to r and to the shared-memory block accumulators:
+// the SCVFs touching A (edge order, resolved at compile time), the storage of A's SCV and A's
+// boundary sub-faces, divided by A's control volume. The potential gradient, whose sign picks the
+// upstream vertex, is summed with explicitly rounded operations in the reference's order; the flux
+// factor K_f (-lambda) n rho |A| is formed once per face and phase, so every derivative is one or
+// two products (the same values to a few ulps).
 template <int DIM, int A>
 __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, const VGeomDev* __restrict__ geo,
                                              const double2* __restrict__ x, const double2* __restrict__ sold,
@@ -295,67 +305,62 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
                                              const double* __restrict__ iq, double dt, double V, int v,
                                              const int eidx[3], double r[2], double* acc, int& bad) {
     constexpr int NV = 1 << DIM;
-    const int NVt = D.NV;
+    constexpr int NE = DIM == 3 ? 12 : 4;
+    const int64_t NVt = D.NV;
     const int sy = D.nvx, sz = D.nvx * D.nvy;
-    // global index of element vertex w: vertex + (bits(w) - bits(A))
     auto gidx = [&](int w) {
         const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
         const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
         return v + dx + sy * dy + sz * dz;
     };
-    double pw[NV], pn[NV];
+    double pw[NV], pn[NV], dpc[NV];
 #pragma unroll
     for (int w = 0; w < NV; ++w) {
         const int g = gidx(w);
         pw[w] = x[g].x;
         pn[w] = pw[w] + (iq[g] - 0.0);
+        dpc[w] = iq[NVt + g];
     }
     double Rv[2] = {0.0, 0.0};
     double Rd[NV][2][2];
 #pragma unroll
     for (int w = 0; w < NV; ++w) Rd[w][0][0] = Rd[w][0][1] = Rd[w][1][0] = Rd[w][1][1] = 0.0;
-    const int ne = geo->ne;
-    for (int k = 0; k < ne; ++k) {
-        const int i = geo->ei[k], j = geo->ej[k];
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+        const int i = DIM == 3 ? kEdge3[k][0] : kEdge2[k][0];
+        const int j = DIM == 3 ? kEdge3[k][1] : kEdge2[k][1];
         if (i != A && j != A) continue;
-        const double sgn = i == A ? 1.0 : -1.0;
+        const bool plus = i == A;
         const double ns = geo->nsign[k];
         const double area = geo->area[k];
         const int gi = gidx(i), gj = gidx(j);
         const double Kf = harmonic_mean(perm[gi], perm[gj]);
+        double G[NV];
+#pragma unroll
+        for (int w = 0; w < NV; ++w) G[w] = geo->G[k][w];
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
             double g = 0.0;
 #pragma unroll
-            for (int w = 0; w < NV; ++w) g = dadd(g, dmul(a == 0 ? pw[w] : pn[w], geo->G[k][w]));
+            for (int w = 0; w < NV; ++w) g = dadd(g, dmul(a == 0 ? pw[w] : pn[w], G[w]));
             g = dadd(g, geo->gtab[k][a]);
-            const double t = dmul(g, ns);
-            const int up = t > 0.0 ? j : i;
-            const int gu = up == i ? gi : gj;
-            const double lam = iq[(a == 0 ? 2 : 4) * (int64_t)NVt + gu];
-            const double dlam = iq[(a == 0 ? 3 : 5) * (int64_t)NVt + gu];
-            const double rho = P.rho[a];
-            const double s = dmul(Kf, g);
-            const double vel = dmul(s, -lam);
-            const double F = dmul(dmul(dmul(vel, ns), rho), area);
-            Rv[a] = sgn > 0 ? dadd(Rv[a], F) : __dsub_rn(Rv[a], F);
+            const bool upJ = dmul(g, ns) > 0.0;
+            const int gu = upJ ? gj : gi;
+            const double lam = iq[(a == 0 ? 2 : 4) * NVt + gu];
+            const double dlam = iq[(a == 0 ? 3 : 5) * NVt + gu];
+            const double nra = ns * P.rho[a] * area;        // n rho |A|
+            double Cf = Kf * (-lam) * nra;                  // dF / dg
+            double Dl = (-dlam) * (Kf * g) * nra;           // dF / dS of the upstream vertex via lambda
+            if (!plus) { Cf = -Cf; Dl = -Dl; }
+            Rv[a] += g * Cf;
 #pragma unroll
             for (int w = 0; w < NV; ++w) {
-                const double G = geo->G[k][w];
-                const double gd1 = a == 0 ? 0.0 : dmul(iq[(int64_t)NVt + gidx(w)], G);
-                const double sd0 = dmul(Kf, G), sd1 = dmul(Kf, gd1);
-                const double vd0 = dmul(sd0, -lam);
-                const double vd1 = w == up ? dadd(dmul(sd1, -lam), dmul(-dlam, s)) : dmul(sd1, -lam);
-                const double Fd0 = dmul(dmul(dmul(vd0, ns), rho), area);
-                const double Fd1 = dmul(dmul(dmul(vd1, ns), rho), area);
-                if (sgn > 0) {
-                    Rd[w][a][0] = dadd(Rd[w][a][0], Fd0);
-                    Rd[w][a][1] = dadd(Rd[w][a][1], Fd1);
-                } else {
-                    Rd[w][a][0] = __dsub_rn(Rd[w][a][0], Fd0);
-                    Rd[w][a][1] = __dsub_rn(Rd[w][a][1], Fd1);
-                }
+                const double gc = G[w] * Cf;
+                Rd[w][a][0] += gc;
+                if (a == 1) Rd[w][1][1] += dpc[w] * gc;
             }
+            if (upJ) Rd[j][a][1] += Dl;
+            else Rd[i][a][1] += Dl;
         }
     }
     // storage of the SCV of A: (storage - storage_old) * V_scv / dt
@@ -365,10 +370,10 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
         const double c = geo->scvVol * 1.0 / dt;
         const double stw = P.porosity * Sw * P.rho[0];
         const double stn = P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1];
-        Rv[0] = dadd(Rv[0], dmul(stw - so.x, c));
-        Rv[1] = dadd(Rv[1], dmul(stn - so.y, c));
-        Rd[A][0][1] = dadd(Rd[A][0][1], dmul(dmul(P.porosity, P.rho[0]), c));
-        Rd[A][1][1] = dadd(Rd[A][1][1], dmul(dmul(-P.porosity, P.rho[1]), c));
+        Rv[0] += (stw - so.x) * c;
+        Rv[1] += (stn - so.y) * c;
+        Rd[A][0][1] += P.porosity * P.rho[0] * c;
+        Rd[A][1][1] += -P.porosity * P.rho[1] * c;
     }
     // boundary sub-faces of A in this element (intersection order)
 #pragma unroll
@@ -391,46 +396,37 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
             const double ns = sd ? 1.0 : -1.0;
             const double K = perm[v];
             const int li = lens[v];
-            const double dpc = iq[(int64_t)NVt + v];
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 const double pI = a == 0 ? pw[A] : pn[A];
-                const double deltay = pB[a] - pI;
-                const double g = dmul(deltay, coef);
-                // d(deltay)/dp = -1, d(deltay)/dS = -dpc (non-wetting phase)
-                const double gd0 = dmul(-1.0, coef), gd1 = a == 0 ? 0.0 : dmul(-dpc, coef);
-                const double t = dmul(g, ns);
-                const bool upB = t > 0.0;
-                const double lam = upB ? P.bndLam[li][a] : iq[(a == 0 ? 2 : 4) * (int64_t)NVt + v];
-                const double dlam = upB ? 0.0 : iq[(a == 0 ? 3 : 5) * (int64_t)NVt + v];
-                const double s = dmul(K, g);
-                const double rate = dmul(dmul(dmul(dmul(s, -lam), ns), P.rho[a]), barea);
-                const double vd0 = dmul(dmul(K, gd0), -lam);
-                const double vd1 = dadd(dmul(dmul(K, gd1), -lam), dmul(-dlam, s));
-                Rv[a] = dadd(Rv[a], rate);
-                Rd[A][a][0] = dadd(Rd[A][a][0], dmul(dmul(dmul(vd0, ns), P.rho[a]), barea));
-                Rd[A][a][1] = dadd(Rd[A][a][1], dmul(dmul(dmul(vd1, ns), P.rho[a]), barea));
+                const double g = dmul(pB[a] - pI, coef);
+                const bool upB = dmul(g, ns) > 0.0;
+                const double lam = upB ? P.bndLam[li][a] : iq[(a == 0 ? 2 : 4) * NVt + v];
+                const double dlam = upB ? 0.0 : iq[(a == 0 ? 3 : 5) * NVt + v];
+                const double nra = ns * P.rho[a] * barea;
+                const double Cf = K * (-lam) * nra;          // d rate / d g
+                Rv[a] += g * Cf;
+                // dg/dp = -coef, dg/dS = -dpc coef (non-wetting phase)
+                Rd[A][a][0] += -coef * Cf;
+                Rd[A][a][1] += (a == 1 ? -dpc[A] * coef * Cf : 0.0) + (-dlam) * (K * g) * nra;
             }
             continue;
         }
         const bool upper = pos[1] > P.L[1] - P.eps;
         bool inlet = upper && pos[0] > P.inletXlo && pos[0] < P.inletXhi;
         if (DIM == 3) inlet = inlet && pos[2] > P.inletZlo && pos[2] < P.inletZhi;
-        if (inlet) Rv[1] = dadd(Rv[1], dmul(P.inletRate, barea));
+        if (inlet) Rv[1] += P.inletRate * barea;
     }
     // volumetric residual, then the scatter into the row
-    r[0] = dadd(r[0], Rv[0] / V);
-    r[1] = dadd(r[1], Rv[1] / V);
+    r[0] += Rv[0] / V;
+    r[1] += Rv[1] / V;
 #pragma unroll
     for (int w = 0; w < NV; ++w) {
         const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
         const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
         const int band = (dx + 1) + 3 * (dy + 1) + (DIM == 3 ? 9 * (dz + 1) : 0);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            double* slot = acc + (band * 4 + e) * kVBlock;
-            *slot = dadd(*slot, Rd[w][e >> 1][e & 1] / V);
-        }
+        for (int e = 0; e < 4; ++e) acc[(band * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] / V;
     }
     if (!isfinite(Rv[0]) || !isfinite(Rv[1])) bad = 1;
 }
