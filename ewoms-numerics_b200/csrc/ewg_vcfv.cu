@@ -294,7 +294,7 @@ __device__ constexpr int kEdge3[12][2] = {{0, 4}, {1, 5}, {2, 6}, {3, 7}, {0, 2}
 // Element contribution to the row of local vertex A (compile time) of the element at offset
 // (ox, oy, oz) from the thread's vertex, added to r and to the shared-memory block accumulators:
 // the SCVFs touching A (edge order, resolved at compile time), the storage of A's SCV and A's
-// boundary sub-faces, divided by A's control volume. The potential gradient, whose sign picks the
+// boundary sub-faces, scaled by 1 / A's control volume. The potential gradient, whose sign picks the
 // upstream vertex, is summed with explicitly rounded operations in the reference's order; the flux
 // factor K_f (-lambda) n rho |A| is formed once per face and phase, so every derivative is one or
 // two products (the same values to a few ulps).
@@ -418,15 +418,16 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
         if (inlet) Rv[1] += P.inletRate * barea;
     }
     // volumetric residual, then the scatter into the row
-    r[0] += Rv[0] / V;
-    r[1] += Rv[1] / V;
+    const double invV = 1.0 / V;
+    r[0] += Rv[0] * invV;
+    r[1] += Rv[1] * invV;
 #pragma unroll
     for (int w = 0; w < NV; ++w) {
         const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
         const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
         const int band = (dx + 1) + 3 * (dy + 1) + (DIM == 3 ? 9 * (dz + 1) : 0);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[(band * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] / V;
+        for (int e = 0; e < 4; ++e) acc[(band * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] * invV;
     }
     if (!isfinite(Rv[0]) || !isfinite(Rv[1])) bad = 1;
 }
