@@ -69,6 +69,7 @@ struct ewg_vcfv {
     ewg::VGeomDev* geo = nullptr;
     double2 *x0 = nullptr, *x1 = nullptr, *sold = nullptr, *r = nullptr;
     double *perm = nullptr, *totVol = nullptr, *iq = nullptr, *J = nullptr;
+    double* kedge = nullptr;  // harmonic-mean permeability of each edge, plane per axis, at the lower vertex
     uint8_t* lens = nullptr;
     unsigned long long* d_errmax = nullptr;
     int* d_flags = nullptr;
@@ -283,6 +284,17 @@ __global__ void kv_total_volume(VDims D, int dim, double scvVol, double* __restr
     }
 }
 
+// the face permeability of every edge, harmonic mean of its two vertices (symmetric in its
+// arguments, so either end gets the same value), stored at the edge's lower vertex per axis
+__global__ void kv_edge_perm(VDims D, int dim, const double* __restrict__ perm, double* __restrict__ kedge) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < D.NV; v += gridDim.x * blockDim.x) {
+        const int i = v % D.nvx, j = (v / D.nvx) % D.nvy, k = v / (D.nvx * D.nvy);
+        const int id[3] = {i, j, k}, n[3] = {D.nvx, D.nvy, D.nvz}, st[3] = {1, D.nvx, D.nvx * D.nvy};
+        for (int ax = 0; ax < 3; ++ax)
+            kedge[(int64_t)ax * D.NV + v] = ax < dim && id[ax] + 1 < n[ax] ? harmonic_mean(perm[v], perm[v + st[ax]]) : 0.0;
+    }
+}
+
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 
@@ -302,7 +314,8 @@ template <int DIM, int A>
 __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, const VGeomDev* __restrict__ geo,
                                              const double2* __restrict__ x, const double2* __restrict__ sold,
                                              const double* __restrict__ perm, const uint8_t* __restrict__ lens,
-                                             const double* __restrict__ iq, double dt, double V, int v,
+                                             const double* __restrict__ iq, const double* __restrict__ kedge,
+                                             double cst, double V, int v,
                                              const int eidx[3], double r[2], double* acc, int& bad) {
     constexpr int NV = 1 << DIM;
     constexpr int NE = DIM == 3 ? 12 : 4;
@@ -334,7 +347,8 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
         const double ns = geo->nsign[k];
         const double area = geo->area[k];
         const int gi = gidx(i), gj = gidx(j);
-        const double Kf = harmonic_mean(perm[gi], perm[gj]);
+        const int ax = (i ^ j) == 1 ? 0 : ((i ^ j) == 2 ? 1 : 2);
+        const double Kf = kedge[ax * NVt + (gi < gj ? gi : gj)];
         double G[NV];
 #pragma unroll
         for (int w = 0; w < NV; ++w) G[w] = geo->G[k][w];
@@ -367,7 +381,7 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
     {
         const double Sw = x[v].y;
         const double2 so = sold[v];
-        const double c = geo->scvVol * 1.0 / dt;
+        const double c = cst;
         const double stw = P.porosity * Sw * P.rho[0];
         const double stn = P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1];
         Rv[0] += (stw - so.x) * c;
@@ -451,7 +465,8 @@ __global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ P
                                                        const VGeomDev* __restrict__ geo,
                                                        const double2* __restrict__ x, const double2* __restrict__ sold,
                                                        const double* __restrict__ perm, const uint8_t* __restrict__ lens,
-                                                       const double* __restrict__ iq, const double* __restrict__ totVol,
+                                                       const double* __restrict__ iq, const double* __restrict__ kedge,
+                                                       const double* __restrict__ totVol,
                                                        double dt, double2* __restrict__ rOut, double* __restrict__ J,
                                                        unsigned long long* errmax, int* flags) {
     constexpr int NB = DIM == 3 ? 27 : 9;
@@ -464,6 +479,7 @@ __global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ P
     if (v < D.NV) {
         const int i = v % D.nvx, j = (v / D.nvx) % D.nvy, k = v / (D.nvx * D.nvy);
         const double V = totVol[v];
+        const double cst = geo->scvVol * 1.0 / dt;  // V_scv / dt of the storage term
         double r[2] = {0.0, 0.0};
         // elements around the vertex in element order; the vertex is local vertex A = ~offset bits
 #define EWG_VCFV_ELEM(EO)                                                                                   \
@@ -473,7 +489,7 @@ __global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ P
                                  DIM == 3 ? k - (((EO) >> 2) & 1 ? 0 : 1) : 0};                             \
             if (eidx[0] >= 0 && eidx[1] >= 0 && eidx[2] >= 0 && eidx[0] < D.nex && eidx[1] < D.ney &&       \
                 eidx[2] < D.nez)                                                                            \
-                vcfv_element<DIM, A>(P, D, geo, x, sold, perm, lens, iq, dt, V, v, eidx, r, acc, bad);      \
+                vcfv_element<DIM, A>(P, D, geo, x, sold, perm, lens, iq, kedge, cst, V, v, eidx, r, acc, bad); \
         }
         EWG_VCFV_ELEM(0) EWG_VCFV_ELEM(1) EWG_VCFV_ELEM(2) EWG_VCFV_ELEM(3)
         if (DIM == 3) { EWG_VCFV_ELEM(4) EWG_VCFV_ELEM(5) EWG_VCFV_ELEM(6) EWG_VCFV_ELEM(7) }
@@ -731,7 +747,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
     const size_t v2 = sizeof(double2) * nv, v1 = sizeof(double) * nv;
     struct A { void** p; size_t n; } allocs[] = {
         {(void**)&c->x0, v2}, {(void**)&c->x1, v2}, {(void**)&c->sold, v2}, {(void**)&c->r, v2},
-        {(void**)&c->perm, v1}, {(void**)&c->totVol, v1}, {(void**)&c->iq, 6 * v1},
+        {(void**)&c->perm, v1}, {(void**)&c->totVol, v1}, {(void**)&c->iq, 6 * v1}, {(void**)&c->kedge, 3 * v1},
         {(void**)&c->J, (size_t)c->nb * 4 * v1}, {(void**)&c->lens, (size_t)nv}, {(void**)&c->geo, sizeof(VGeomDev)},
         {(void**)&c->d_errmax, sizeof(unsigned long long)}, {(void**)&c->d_flags, sizeof(int)},
         {(void**)&c->s_b, v2}, {(void**)&c->s_x, v2}, {(void**)&c->s_r, v2}, {(void**)&c->s_r0, v2},
@@ -758,6 +774,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
         ewg_status s = fail(e, "upload"); ewg_vcfv_destroy(c); return s;
     }
     kv_total_volume<<<vgrid(c, nv), kVApi, 0, c->stream>>>(c->D, grid->dim, c->hgeo.scvVol, c->totVol);
+    kv_edge_perm<<<vgrid(c, nv), kVApi, 0, c->stream>>>(c->D, grid->dim, c->perm, c->kedge);
     if ((e = cudaGetLastError()) != cudaSuccess) { ewg_status s = fail(e, "total volume"); ewg_vcfv_destroy(c); return s; }
     if ((e = boundary_constants(c->P, c->stream)) != cudaSuccess) { ewg_status s = fail(e, "boundary constants"); ewg_vcfv_destroy(c); return s; }
     const int smem = (int)(sizeof(double) * c->nb * 4 * kVBlock);
@@ -773,7 +790,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
 void ewg_vcfv_destroy(ewg_vcfv* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* ps[] = {c->x0, c->x1, c->sold, c->r, c->perm, c->totVol, c->iq, c->J, c->lens, c->geo, c->d_errmax,
+    void* ps[] = {c->x0, c->x1, c->sold, c->r, c->perm, c->totVol, c->kedge, c->iq, c->J, c->lens, c->geo, c->d_errmax,
                   c->d_flags, c->s_b, c->s_x, c->s_r, c->s_r0, c->s_v, c->s_p, c->s_y, c->s_z, c->s_t, c->s_dinv,
                   c->s_red};
     for (void* p : ps) if (p) cudaFree(p);
@@ -841,10 +858,10 @@ ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error) {
     const int blocks = (c->D.NV + kVBlock - 1) / kVBlock;
     const size_t smem = sizeof(double) * c->nb * 4 * kVBlock;
     if (c->P.dim == 3)
-        kv_assemble<3><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq,
+        kv_assemble<3><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
                                                               c->totVol, dt, c->r, c->J, c->d_errmax, c->d_flags);
     else
-        kv_assemble<2><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq,
+        kv_assemble<2><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
                                                               c->totVol, dt, c->r, c->J, c->d_errmax, c->d_flags);
     if ((st = vcheck(c, "kv_assemble"))) return st;
     unsigned long long bits = 0;
