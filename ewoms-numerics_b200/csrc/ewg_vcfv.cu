@@ -441,7 +441,10 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
         const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
         const int band = (dx + 1) + 3 * (dy + 1) + (DIM == 3 ? 9 * (dz + 1) : 0);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[(band * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] * invV;
+        // the dz = +1 plane reuses the dz = -1 plane's slots (flushed after the lower elements)
+        const int slot = DIM == 3 && band >= 18 ? band - 18 : band;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[(slot * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] * invV;
     }
     if (!isfinite(Rv[0]) || !isfinite(Rv[1])) bad = 1;
 }
@@ -460,8 +463,15 @@ __device__ __forceinline__ void vblock_max(double v, unsigned long long* out) {
     }
 }
 
+// Accumulator slots per thread: 3D rows have 27 blocks, but the 4 elements below the vertex (the
+// first in element order) are the only ones that reach the dz = -1 plane and the 4 above the only
+// ones that reach dz = +1, so after the lower four the dz = -1 blocks are complete, written out,
+// and their slots reused: 18 blocks live at a time.
 template <int DIM>
-__global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ Phys P, VDims D,
+__host__ __device__ constexpr int vcfv_slots() { return DIM == 3 ? 18 : 9; }
+
+template <int DIM>
+__global__ void __launch_bounds__(kVBlock, DIM == 3 ? 6 : 4) kv_assemble(const __grid_constant__ Phys P, VDims D,
                                                        const VGeomDev* __restrict__ geo,
                                                        const double2* __restrict__ x, const double2* __restrict__ sold,
                                                        const double* __restrict__ perm, const uint8_t* __restrict__ lens,
@@ -469,10 +479,10 @@ __global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ P
                                                        const double* __restrict__ totVol,
                                                        double dt, double2* __restrict__ rOut, double* __restrict__ J,
                                                        unsigned long long* errmax, int* flags) {
-    constexpr int NB = DIM == 3 ? 27 : 9;
+    constexpr int NS = vcfv_slots<DIM>();
     extern __shared__ double vacc[];
     double* acc = vacc + threadIdx.x;
-    for (int q = 0; q < NB * 4; ++q) acc[q * kVBlock] = 0.0;
+    for (int q = 0; q < NS * 4; ++q) acc[q * kVBlock] = 0.0;
     const int v = blockIdx.x * kVBlock + threadIdx.x;
     double err = 0.0;
     int bad = 0;
@@ -492,10 +502,23 @@ __global__ void __launch_bounds__(kVBlock) kv_assemble(const __grid_constant__ P
                 vcfv_element<DIM, A>(P, D, geo, x, sold, perm, lens, iq, kedge, cst, V, v, eidx, r, acc, bad); \
         }
         EWG_VCFV_ELEM(0) EWG_VCFV_ELEM(1) EWG_VCFV_ELEM(2) EWG_VCFV_ELEM(3)
-        if (DIM == 3) { EWG_VCFV_ELEM(4) EWG_VCFV_ELEM(5) EWG_VCFV_ELEM(6) EWG_VCFV_ELEM(7) }
+        if (DIM == 3) {
+            // the dz = -1 blocks (bands 0..8) are complete: write them and free their slots
+#pragma unroll 1
+            for (int q = 0; q < 36; ++q) {
+                J[(int64_t)q * D.NV + v] = acc[q * kVBlock];
+                acc[q * kVBlock] = 0.0;
+            }
+            EWG_VCFV_ELEM(4) EWG_VCFV_ELEM(5) EWG_VCFV_ELEM(6) EWG_VCFV_ELEM(7)
+        }
 #undef EWG_VCFV_ELEM
         rOut[v] = make_double2(r[0], r[1]);
-        for (int q = 0; q < NB * 4; ++q) J[(int64_t)q * D.NV + v] = acc[q * kVBlock];
+        if (DIM == 3) {
+            for (int q = 36; q < 72; ++q) J[(int64_t)q * D.NV + v] = acc[q * kVBlock];         // dz = 0
+            for (int q = 0; q < 36; ++q) J[(int64_t)(q + 72) * D.NV + v] = acc[q * kVBlock];  // dz = +1
+        } else {
+            for (int q = 0; q < 36; ++q) J[(int64_t)q * D.NV + v] = acc[q * kVBlock];
+        }
         err = fmax(fabs(r[0]), fabs(r[1]));
         if (!(err <= 1.7976931348623157e308)) bad = 1;
     }
@@ -777,7 +800,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
     kv_edge_perm<<<vgrid(c, nv), kVApi, 0, c->stream>>>(c->D, grid->dim, c->perm, c->kedge);
     if ((e = cudaGetLastError()) != cudaSuccess) { ewg_status s = fail(e, "total volume"); ewg_vcfv_destroy(c); return s; }
     if ((e = boundary_constants(c->P, c->stream)) != cudaSuccess) { ewg_status s = fail(e, "boundary constants"); ewg_vcfv_destroy(c); return s; }
-    const int smem = (int)(sizeof(double) * c->nb * 4 * kVBlock);
+    const int smem = (int)(sizeof(double) * (grid->dim == 3 ? vcfv_slots<3>() : vcfv_slots<2>()) * 4 * kVBlock);
     e = grid->dim == 3 ? cudaFuncSetAttribute(kv_assemble<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
                        : cudaFuncSetAttribute(kv_assemble<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess || (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
@@ -856,7 +879,7 @@ ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error) {
     ewg_status st = vcheck(c, "kv_intensive");
     if (st) return st;
     const int blocks = (c->D.NV + kVBlock - 1) / kVBlock;
-    const size_t smem = sizeof(double) * c->nb * 4 * kVBlock;
+    const size_t smem = sizeof(double) * (c->P.dim == 3 ? vcfv_slots<3>() : vcfv_slots<2>()) * 4 * kVBlock;
     if (c->P.dim == 3)
         kv_assemble<3><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
                                                               c->totVol, dt, c->r, c->J, c->d_errmax, c->d_flags);
