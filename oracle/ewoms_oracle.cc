@@ -1088,6 +1088,11 @@ struct VCtx {
     std::vector<double> blocks;
     std::vector<IQ> iqCache;
     bool recycleStorage = true;
+    // FiniteDifferenceLocalLinearizer with NumericDifferenceMethod fdMethod and the reference
+    // pressure of ImmiscibleModel::updateBegin (p_w of the first DOF) for the pressure weight
+    bool fd = false;
+    int fdMethod = 1;
+    double refPressure = -1.0;
     int nthreads = 1;
     std::string err;
 
@@ -1114,16 +1119,16 @@ struct VCtx {
     }
 };
 
-static IQ computeVIQ(const VCtx& C, int64_t v, const double* x) {
+static IQ computeVIQAt(const VCtx& C, int64_t v, double pw, double sw) {
     IQ q;
     const Law& L = C.law[C.inLens[v]];
-    Eval Sw = Eval::variable(x[2 * v + 1], 1);
+    Eval Sw = Eval::variable(sw, 1);
     q.S[0] = Sw;
     q.S[1] = 1.0 - (Eval(0.0) + Sw);
     Eval pC[2];
     capillaryPressures(pC, L, q.S[0]);
     relativePermeabilities(q.kr, L, q.S[0]);
-    Eval p0 = Eval::variable(x[2 * v], 0);
+    Eval p0 = Eval::variable(pw, 0);
     for (int a = 0; a < 2; ++a) q.p[a] = p0 + (pC[a] - pC[0]);
     q.mu[0] = Eval(C.prob.mu_w); q.mu[1] = Eval(C.prob.mu_n);
     q.rho[0] = Eval(C.prob.rho_w); q.rho[1] = Eval(C.prob.rho_n);
@@ -1132,6 +1137,7 @@ static IQ computeVIQ(const VCtx& C, int64_t v, const double* x) {
     q.K = C.perm[v];
     return q;
 }
+static IQ computeVIQ(const VCtx& C, int64_t v, const double* x) { return computeVIQAt(C, v, x[2 * v], x[2 * v + 1]); }
 
 static inline Eval focusOr(const Eval& e, bool focus) { return focus ? e : Eval(e.v); }
 
@@ -1276,7 +1282,7 @@ static void vcfvBoundaryRate(const VCtx& C, const int64_t eid[3], int f, int m, 
 // with its SCV volume, the boundary sub-faces, then division by each vertex's total control
 // volume (UseVolumetricResidual).
 static void vcfvEvalLocal(VCtx& C, const int64_t eid[3], const int64_t gv[8], const IQ* q[8], int focus, double dt,
-                          int newtonIteration, Eval R[8][2]) {
+                          int newtonIteration, Eval R[8][2], bool stashed = false) {
     const VGeom& g = C.geo;
     for (int v = 0; v < g.nv; ++v) { R[v][0] = Eval(0.0); R[v][1] = Eval(0.0); }
     for (int k = 0; k < g.ne; ++k) {
@@ -1294,7 +1300,7 @@ static void vcfvEvalLocal(VCtx& C, const int64_t eid[3], const int64_t gv[8], co
         else { double t2[2]; storageOf<double>(*q[v], t2); tmp[0] = Eval(t2[0]); tmp[1] = Eval(t2[1]); }
         double tmp2[2];
         const int64_t G = gv[v];
-        if (newtonIteration == 0) {
+        if (newtonIteration == 0 && !stashed) {
             if (!C.recycleStorage) {
                 IQ qold = computeVIQ(C, G, C.sol[1].data());
                 storageOf<double>(qold, tmp2);
@@ -1371,6 +1377,52 @@ static double vcfvLinearize(VCtx& C, double dt, int newtonIteration) {
         for (int v = 0; v < g.nv; ++v) { gv[v] = C.evert(eid, v); q[v] = &C.iqCache[gv[v]]; }
         double res[8][2];
         double jac[8][8][4];  // [dof][focus][eq*2+pv]
+        if (C.fd) {
+            // FvBaseFdLocalLinearizer (fvbasefdlocallinearizer.hh:221-237, 393-453): the local
+            // residual at the primary variables, then, per focus vertex and primary variable, at the
+            // deflected variable (only that vertex's intensive quantities re-evaluated, the storage
+            // cache read, not written), eps = BaseEpsilon / primaryVarWeight
+            Eval R0[8][2];
+            vcfvEvalLocal(C, eid, gv, q, -1, dt, newtonIteration, R0);
+            for (int f = 0; f < g.nv; ++f)
+                for (int a = 0; a < 2; ++a) res[f][a] = R0[f][a].v;
+            const double baseEps = std::max(0.9123e-10, std::numeric_limits<double>::epsilon() * 1.23e3);
+            for (int f = 0; f < g.nv; ++f) {
+                const IQ* qd[8];
+                for (int w = 0; w < g.nv; ++w) qd[w] = q[w];
+                for (int pv = 0; pv < 2; ++pv) {
+                    const double pvWeight = pv == 0 ? 10 / C.refPressure : 1.0;
+                    const double eps = baseEps / pvWeight;
+                    double priVars[2] = {C.sol[0][2 * gv[f]], C.sol[0][2 * gv[f] + 1]};
+                    double delta = 0.0;
+                    double deriv[8][2];
+                    Eval Rp[8][2];
+                    if (C.fdMethod >= 0) {
+                        priVars[pv] += eps;
+                        delta += eps;
+                        IQ qf = computeVIQAt(C, gv[f], priVars[0], priVars[1]);
+                        qd[f] = &qf;
+                        vcfvEvalLocal(C, eid, gv, qd, -1, dt, newtonIteration, Rp, true);
+                        for (int d = 0; d < g.nv; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] = Rp[d][a].v;
+                    } else {
+                        for (int d = 0; d < g.nv; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] = R0[d][a].v;
+                    }
+                    if (C.fdMethod <= 0) {
+                        priVars[pv] -= delta + eps;
+                        delta += eps;
+                        IQ qf = computeVIQAt(C, gv[f], priVars[0], priVars[1]);
+                        qd[f] = &qf;
+                        vcfvEvalLocal(C, eid, gv, qd, -1, dt, newtonIteration, Rp, true);
+                        for (int d = 0; d < g.nv; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] -= Rp[d][a].v;
+                    } else {
+                        for (int d = 0; d < g.nv; ++d) for (int a = 0; a < 2; ++a) deriv[d][a] -= R0[d][a].v;
+                    }
+                    qd[f] = q[f];
+                    for (int d = 0; d < g.nv; ++d)
+                        for (int eq = 0; eq < 2; ++eq) jac[d][f][2 * eq + pv] = deriv[d][eq] / delta;
+                }
+            }
+        } else
         for (int f = 0; f < g.nv; ++f) {
             Eval R[8][2];
             vcfvEvalLocal(C, eid, gv, q, f, dt, newtonIteration, R);
@@ -1704,10 +1756,15 @@ void orc_vcfv_apply_initial_solution(orc_vcfv* o) {
     C.sol[1] = C.sol[0];
 }
 void orc_vcfv_advance_time_level(orc_vcfv* o) { o->C.sol[1] = o->C.sol[0]; }
+// kind 0: AD, 1: finite differences with NumericDifferenceMethod `method`
+void orc_vcfv_set_local_linearizer(orc_vcfv* o, int kind, int method) { o->C.fd = kind == 1; o->C.fdMethod = method; }
+// ImmiscibleModel::updateBegin: the reference pressure of the FD pressure weight
+void orc_vcfv_update_begin(orc_vcfv* o) { o->C.refPressure = o->C.sol[0][0]; }
 void orc_vcfv_total_volumes(const orc_vcfv* o, double* out) {
     std::memcpy(out, o->C.totVol.data(), sizeof(double) * o->C.NV);
 }
 int orc_vcfv_linearize(orc_vcfv* o, double dt, int it, double* error) {
+    if (o->C.fd && !(o->C.refPressure > 0)) o->C.refPressure = o->C.sol[0][0];
     try {
         double e = vcfvLinearize(o->C, dt, it);
         if (error) *error = e;
@@ -1740,6 +1797,7 @@ int orc_vcfv_newton_apply(orc_vcfv* o, double dt, const ewg_newton_opts* no, con
         return true;
     };
     int status = 0;
+    C.refPressure = C.sol[0][0];  // ImmiscibleModel::updateBegin before every Newton solve
     try {
         while (proceed()) {
             double e = vcfvLinearize(C, dt, numIterations);

@@ -88,6 +88,8 @@ void orc_vcfv_set_solution(orc_vcfv* c, int time_idx, const double* x);
 void orc_vcfv_get_solution(const orc_vcfv* c, int time_idx, double* x);
 void orc_vcfv_apply_initial_solution(orc_vcfv* c);
 void orc_vcfv_advance_time_level(orc_vcfv* c);
+void orc_vcfv_set_local_linearizer(orc_vcfv* c, int kind, int method);  /* 0 AD, 1 FD */
+void orc_vcfv_update_begin(orc_vcfv* c);
 void orc_vcfv_total_volumes(const orc_vcfv* c, double* out);
 int orc_vcfv_linearize(orc_vcfv* c, double dt, int newton_iteration, double* error);
 void orc_vcfv_get_residual(const orc_vcfv* c, double* r);

@@ -82,6 +82,8 @@ def load():
         "orc_vcfv_get_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_vcfv_apply_initial_solution": (None, [C.c_void_p]),
         "orc_vcfv_advance_time_level": (None, [C.c_void_p]),
+        "orc_vcfv_set_local_linearizer": (None, [C.c_void_p, C.c_int, C.c_int]),
+        "orc_vcfv_update_begin": (None, [C.c_void_p]),
         "orc_vcfv_total_volumes": (None, [C.c_void_p, P(d)]),
         "orc_vcfv_linearize": (C.c_int, [C.c_void_p, d, C.c_int, P(d)]),
         "orc_vcfv_get_residual": (None, [C.c_void_p, P(d)]),
@@ -298,6 +300,12 @@ class VcfvOracle:
 
     def advance_time_level(self):
         self.lib.orc_vcfv_advance_time_level(self.h)
+
+    def set_local_linearizer(self, kind: int, method: int = 1):
+        self.lib.orc_vcfv_set_local_linearizer(self.h, kind, method)
+
+    def update_begin(self):
+        self.lib.orc_vcfv_update_begin(self.h)
 
     def total_volumes(self):
         v = np.zeros(self.n, dtype=np.float64)

@@ -125,3 +125,33 @@ def test_vcfv_hydrostatic_initial_residual(oracle_mod, ewg_mod):
     keep = away & ~corner
     assert np.max(np.abs(r[keep])) < 1e-9 * np.max(np.abs(r))
     assert np.max(np.abs(r[~away])) > 0
+
+
+@pytest.mark.parametrize("method", [1, 0, -1])
+def test_vcfv_fd_local_linearizer_matches_ad(oracle_mod, ewg_mod, method):
+    """lens_immiscible_vcfv_fd: FvBaseFdLocalLinearizer on the vertex-centred stencil gives the AD
+    linearizer's residual and its Jacobian within the difference quotient's error (forward /
+    backward first order, central second order)."""
+    for case in (ewg_mod.vcfv_case(ewg_mod.baseline_case(12, 8)), ewg_mod.vcfv_case(ewg_mod.lens3d_case(6, 5, 4, seed=1))):
+        o = oracle_mod.VcfvOracle(case)
+        o.apply_initial_solution()
+        x = o.get_solution(0)
+        rng = np.random.Generator(np.random.PCG64(0))
+        x[:, 1] = rng.uniform(0.3, 1.0, size=len(x))
+        x[:, 0] += rng.normal(0, 50.0, size=len(x))
+        o.set_solution(1, x)
+        o.set_solution(0, x)
+        o.linearize(250.0, 0)
+        r_ad = o.residual()
+        _, _, J_ad = o.jacobian_bcrs()
+        o.set_local_linearizer(1, method)
+        o.linearize(250.0, 0)
+        assert np.array_equal(o.residual(), r_ad)
+        _, _, J_fd = o.jacobian_bcrs()
+        # central differences are limited by rounding: the element's local residual sums more
+        # flux terms than a cell's (12 SCVFs), divided by 2 eps (eps = 9e-7 Pa for p_w)
+        tol = 5e-5 if method else 2e-5
+        for eq in range(2):
+            for pv in range(2):
+                a, b = J_fd[:, eq, pv], J_ad[:, eq, pv]
+                assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (case.name, eq, pv)
