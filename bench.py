@@ -358,7 +358,17 @@ def run_vcfv(args, rank, pg, torch, ewg):
     nv = g.n
     peak, _ = measured_peak()
     lb = vcfv_lin_bytes(nv)
+    # the finite-difference local linearizer (lens_immiscible_vcfv_fd) on the same state
+    g.set_local_linearizer(ewg.LOCAL_LINEARIZER_FD, 1)
+    g.linearize(250.0)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    for _ in range(3):
+        g.linearize(250.0)
+    fd_ms = max_over_ranks(pg, (time.perf_counter() - t2) / 3 * 1e3)
+    g.set_local_linearizer(ewg.LOCAL_LINEARIZER_AD, 1)
     out = {"grid": f"{args.nx}x{args.ny}x{args.nz} elements, {nv} vertices",
+           "fd_forward_ms_per_linearization": fd_ms,
            "ms_per_linearization": ms, "mvertices_per_s": nv / (ms * 1e-3) / 1e6,
            "algorithmic_bytes": lb, "achieved_gbs": lb / (ms * 1e-3) / 1e9, "frac": lb / (ms * 1e-3) / 1e9 / peak,
            "launches_per_linearization": launches / reps,

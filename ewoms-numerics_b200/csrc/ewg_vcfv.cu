@@ -78,6 +78,11 @@ struct ewg_vcfv {
            *s_y = nullptr, *s_z = nullptr, *s_t = nullptr, *s_dinv = nullptr, *s_red = nullptr;
     double* h_red = nullptr;  // pinned
     long long launches = 0;
+    // LocalLinearizerSplice and NumericDifferenceMethod; the reference pressure of
+    // ImmiscibleModel::updateBegin (p_w of vertex 0) for the FD pressure weight, unset until then
+    int localLinearizer = EWG_LOCAL_LINEARIZER_AD;
+    int fdMethod = 1;
+    double refPressure = -1.0;
 };
 
 namespace ewg {
@@ -440,13 +445,194 @@ __device__ __forceinline__ void vcfv_element(const Phys& P, const VDims& D, cons
         const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
         const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
         const int band = (dx + 1) + 3 * (dy + 1) + (DIM == 3 ? 9 * (dz + 1) : 0);
-#pragma unroll
         // the dz = +1 plane reuses the dz = -1 plane's slots (flushed after the lower elements)
         const int slot = DIM == 3 && band >= 18 ? band - 18 : band;
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[(slot * 4 + e) * kVBlock] += Rd[w][e >> 1][e & 1] * invV;
     }
     if (!isfinite(Rv[0]) || !isfinite(Rv[1])) bad = 1;
+}
+
+// ---- finite-difference local linearizer (lens_immiscible_vcfv_fd) -------------------------------
+//
+// FvBaseFdLocalLinearizer (fvbasefdlocallinearizer.hh:221-237, 393-453) on the vertex-centred
+// stencil: the element's local residual entry of vertex A at the primary variables and, per
+// element vertex w and primary variable, at w's variable deflected by eps = BaseEpsilon /
+// primaryVarWeight (weight 10 / p_ref for the pressure, 1 for the saturation); only w's intensive
+// quantities are re-evaluated, the storage of the previous time level is read from the cache.
+// Values only: the same face arithmetic as the AD kernel.
+
+template <int DIM>
+struct VcfvElemState {
+    double pw[1 << DIM], pn[1 << DIM], lw[1 << DIM], ln[1 << DIM];
+    double SwA;
+};
+
+// local residual entry of vertex A (compile time) in the element, scaled by 1 / control volume
+template <int DIM, int A>
+__device__ __forceinline__ void vcfv_local_value(const Phys& P, const VDims& D, const VGeomDev* __restrict__ geo,
+                                                 const double* __restrict__ kedge, double cst, double invV, int v,
+                                                 const int eidx[3], const VcfvElemState<DIM>& st, double2 so, double KA,
+                                                 int liA, double R[2]) {
+    constexpr int NV = 1 << DIM;
+    constexpr int NE = DIM == 3 ? 12 : 4;
+    const int64_t NVt = D.NV;
+    const int sy = D.nvx, sz = D.nvx * D.nvy;
+    auto gidx = [&](int w) {
+        const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
+        const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
+        return v + dx + sy * dy + sz * dz;
+    };
+    double Rv[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+        const int i = DIM == 3 ? kEdge3[k][0] : kEdge2[k][0];
+        const int j = DIM == 3 ? kEdge3[k][1] : kEdge2[k][1];
+        if (i != A && j != A) continue;
+        const double ns = geo->nsign[k];
+        const double area = geo->area[k];
+        const int gi = gidx(i), gj = gidx(j);
+        const int ax = (i ^ j) == 1 ? 0 : ((i ^ j) == 2 ? 1 : 2);
+        const double Kf = kedge[ax * NVt + (gi < gj ? gi : gj)];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            double g = 0.0;
+#pragma unroll
+            for (int w = 0; w < NV; ++w) g = dadd(g, dmul(a == 0 ? st.pw[w] : st.pn[w], geo->G[k][w]));
+            g = dadd(g, geo->gtab[k][a]);
+            const bool upJ = dmul(g, ns) > 0.0;
+            const double lam = a == 0 ? (upJ ? st.lw[j] : st.lw[i]) : (upJ ? st.ln[j] : st.ln[i]);
+            const double nra = ns * P.rho[a] * area;
+            const double F = g * (Kf * (-lam) * nra);
+            Rv[a] += i == A ? F : -F;
+        }
+    }
+    {
+        const double stw = P.porosity * st.SwA * P.rho[0];
+        const double stn = P.porosity * (1.0 - (0.0 + st.SwA)) * P.rho[1];
+        Rv[0] += (stw - so.x) * cst;
+        Rv[1] += (stn - so.y) * cst;
+    }
+#pragma unroll
+    for (int f = 0; f < 2 * DIM; ++f) {
+        const int ax = f >> 1, sd = f & 1;
+        if (((A >> ax) & 1) != sd) continue;
+        const int nAx = ax == 0 ? D.nex : (ax == 1 ? D.ney : D.nez);
+        if (sd == 0 ? eidx[ax] != 0 : eidx[ax] != nAx - 1) continue;
+        double pos[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pos[d] = d < DIM ? (eidx[d] + geo->bip[f][A][d]) * P.h[d] : 0.0;
+        const double barea = geo->barea[f][A] * 1.0;
+        const bool left = pos[0] < 0.0 + P.eps, right = pos[0] > P.L[0] - P.eps;
+        if (left || right) {
+            const double depth = P.L[1] - pos[1];
+            const double pwB = left ? P.pRef - P.leftScale * P.rho[0] * (-P.g) * depth
+                                    : P.pRef - P.rho[0] * (-P.g) * depth;
+            const double pB[2] = {pwB, pwB + P.bndPc[in_lens(P, pos) ? 1 : 0] - 0.0};
+            const double coef = geo->bcoef[f][A];
+            const double ns = sd ? 1.0 : -1.0;
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const double g = dmul(pB[a] - (a == 0 ? st.pw[A] : st.pn[A]), coef);
+                const bool upB = dmul(g, ns) > 0.0;
+                const double lam = upB ? P.bndLam[liA][a] : (a == 0 ? st.lw[A] : st.ln[A]);
+                Rv[a] += g * (KA * (-lam) * (ns * P.rho[a] * barea));
+            }
+            continue;
+        }
+        const bool upper = pos[1] > P.L[1] - P.eps;
+        bool inlet = upper && pos[0] > P.inletXlo && pos[0] < P.inletXhi;
+        if (DIM == 3) inlet = inlet && pos[2] > P.inletZlo && pos[2] < P.inletZhi;
+        if (inlet) Rv[1] += P.inletRate * barea;
+    }
+    R[0] = Rv[0] * invV;
+    R[1] = Rv[1] * invV;
+}
+
+template <int DIM, int A>
+__device__ __forceinline__ void vcfv_element_fd(const Phys& P, const VDims& D, const VGeomDev* __restrict__ geo,
+                                                const double2* __restrict__ x, const double2* __restrict__ sold,
+                                                const double* __restrict__ perm, const uint8_t* __restrict__ lens,
+                                                const double* __restrict__ iq, const double* __restrict__ kedge,
+                                                double cst, double V, int v, const int eidx[3], double refPressure,
+                                                int method, double r[2], double* acc, int& bad) {
+    constexpr int NV = 1 << DIM;
+    const int64_t NVt = D.NV;
+    const int sy = D.nvx, sz = D.nvx * D.nvy;
+    auto gidx = [&](int w) {
+        const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
+        const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
+        return v + dx + sy * dy + sz * dz;
+    };
+    VcfvElemState<DIM> base;
+    double Sw[NV];
+#pragma unroll
+    for (int w = 0; w < NV; ++w) {
+        const int g = gidx(w);
+        const double2 xw = x[g];
+        base.pw[w] = xw.x;
+        base.pn[w] = xw.x + (iq[g] - 0.0);
+        base.lw[w] = iq[2 * NVt + g];
+        base.ln[w] = iq[4 * NVt + g];
+        Sw[w] = xw.y;
+    }
+    base.SwA = Sw[A];
+    const double2 so = sold[v];
+    const double KA = perm[v];
+    const int liA = lens[v];
+    const double invV = 1.0 / V;
+    double R0[2];
+    vcfv_local_value<DIM, A>(P, D, geo, kedge, cst, invV, v, eidx, base, so, KA, liA, R0);
+    r[0] += R0[0];
+    r[1] += R0[1];
+    if (!isfinite(R0[0]) || !isfinite(R0[1])) bad = 1;
+    const double baseEps = fmax(0.9123e-10, 2.220446049250313e-16 * 1.23e3);
+#pragma unroll
+    for (int w = 0; w < NV; ++w) {
+        const int dx = (w & 1) - (A & 1), dy = ((w >> 1) & 1) - ((A >> 1) & 1);
+        const int dz = DIM == 3 ? ((w >> 2) & 1) - ((A >> 2) & 1) : 0;
+        const int band = (dx + 1) + 3 * (dy + 1) + (DIM == 3 ? 9 * (dz + 1) : 0);
+        const int slot = DIM == 3 && band >= 18 ? band - 18 : band;
+        const int lw_ = lens[gidx(w)];
+#pragma unroll 1
+        for (int pv = 0; pv < 2; ++pv) {
+            const double pvWeight = pv == 0 ? 10 / refPressure : 1.0;
+            const double eps = baseEps / pvWeight;
+            double pri[2] = {base.pw[w], Sw[w]};
+            double delta = 0.0;
+            double deriv[2];
+            // w's state at deflected primary variables
+            auto deflected = [&](double R[2]) {
+                VcfvElemState<DIM> st = base;
+                const IqVals o = intensive_values(P, pri[1], lw_);
+                st.pw[w] = pri[0];
+                st.pn[w] = pri[0] + (o.pc - 0.0);
+                st.lw[w] = o.lw;
+                st.ln[w] = o.ln;
+                if (w == A) st.SwA = pri[1];
+                vcfv_local_value<DIM, A>(P, D, geo, kedge, cst, invV, v, eidx, st, so, KA, liA, R);
+            };
+            double Rp[2];
+            if (method >= 0) {
+                pri[pv] += eps;
+                delta += eps;
+                deflected(Rp);
+                deriv[0] = Rp[0]; deriv[1] = Rp[1];
+            } else {
+                deriv[0] = R0[0]; deriv[1] = R0[1];
+            }
+            if (method <= 0) {
+                pri[pv] -= delta + eps;
+                delta += eps;
+                deflected(Rp);
+                deriv[0] -= Rp[0]; deriv[1] -= Rp[1];
+            } else {
+                deriv[0] -= R0[0]; deriv[1] -= R0[1];
+            }
+            acc[(slot * 4 + pv) * kVBlock] += deriv[0] / delta;
+            acc[(slot * 4 + 2 + pv) * kVBlock] += deriv[1] / delta;
+        }
+    }
 }
 
 // Non-negative doubles compare like their bit patterns as unsigned integers.
@@ -470,14 +656,15 @@ __device__ __forceinline__ void vblock_max(double v, unsigned long long* out) {
 template <int DIM>
 __host__ __device__ constexpr int vcfv_slots() { return DIM == 3 ? 18 : 9; }
 
-template <int DIM>
-__global__ void __launch_bounds__(kVBlock, DIM == 3 ? 6 : 4) kv_assemble(const __grid_constant__ Phys P, VDims D,
+template <int DIM, bool FD>
+__global__ void __launch_bounds__(kVBlock, FD ? 2 : (DIM == 3 ? 6 : 4)) kv_assemble(const __grid_constant__ Phys P, VDims D,
                                                        const VGeomDev* __restrict__ geo,
                                                        const double2* __restrict__ x, const double2* __restrict__ sold,
                                                        const double* __restrict__ perm, const uint8_t* __restrict__ lens,
                                                        const double* __restrict__ iq, const double* __restrict__ kedge,
                                                        const double* __restrict__ totVol,
-                                                       double dt, double2* __restrict__ rOut, double* __restrict__ J,
+                                                       double dt, double refPressure, int method,
+                                                       double2* __restrict__ rOut, double* __restrict__ J,
                                                        unsigned long long* errmax, int* flags) {
     constexpr int NS = vcfv_slots<DIM>();
     extern __shared__ double vacc[];
@@ -499,7 +686,13 @@ __global__ void __launch_bounds__(kVBlock, DIM == 3 ? 6 : 4) kv_assemble(const _
                                  DIM == 3 ? k - (((EO) >> 2) & 1 ? 0 : 1) : 0};                             \
             if (eidx[0] >= 0 && eidx[1] >= 0 && eidx[2] >= 0 && eidx[0] < D.nex && eidx[1] < D.ney &&       \
                 eidx[2] < D.nez)                                                                            \
-                vcfv_element<DIM, A>(P, D, geo, x, sold, perm, lens, iq, kedge, cst, V, v, eidx, r, acc, bad); \
+            {                                                                                               \
+                if (FD)                                                                                     \
+                    vcfv_element_fd<DIM, A>(P, D, geo, x, sold, perm, lens, iq, kedge, cst, V, v, eidx,     \
+                                            refPressure, method, r, acc, bad);                              \
+                else                                                                                        \
+                    vcfv_element<DIM, A>(P, D, geo, x, sold, perm, lens, iq, kedge, cst, V, v, eidx, r, acc, bad); \
+            }                                                                                               \
         }
         EWG_VCFV_ELEM(0) EWG_VCFV_ELEM(1) EWG_VCFV_ELEM(2) EWG_VCFV_ELEM(3)
         if (DIM == 3) {
@@ -592,39 +785,47 @@ __global__ void kv_jacobi(int NV, double w, const double* __restrict__ dinv, con
     }
 }
 
-// per-block partial sums of up to three dot products and one max-norm, in a fixed grid order
+// per-block partial sums of up to two dot products and two max-norms, in a fixed grid order
 constexpr int kVRedBlocks = 296;
 __global__ void __launch_bounds__(kVApi) kv_reduce(int64_t n, const double* __restrict__ a0, const double* __restrict__ b0,
                                                    const double* __restrict__ a1, const double* __restrict__ b1,
-                                                   const double* __restrict__ m, double* __restrict__ part) {
-    double s0 = 0.0, s1 = 0.0, mx = 0.0;
+                                                   const double* __restrict__ m, const double* __restrict__ m2,
+                                                   double* __restrict__ part) {
+    double s0 = 0.0, s1 = 0.0, mx = 0.0, mx2 = 0.0;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         if (a0) s0 += a0[q] * b0[q];
         if (a1) s1 += a1[q] * b1[q];
         if (m) mx = fmax(mx, fabs(m[q]));
+        if (m2) mx2 = fmax(mx2, fabs(m2[q]));
     }
-    __shared__ double sh[3][kVApi / 32];
+    __shared__ double sh[4][kVApi / 32];
     for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_xor_sync(0xffffffffu, s0, o);
         s1 += __shfl_xor_sync(0xffffffffu, s1, o);
         mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mx2 = fmax(mx2, __shfl_xor_sync(0xffffffffu, mx2, o));
     }
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { sh[0][w] = s0; sh[1][w] = s1; sh[2][w] = mx; }
+    if (l == 0) { sh[0][w] = s0; sh[1][w] = s1; sh[2][w] = mx; sh[3][w] = mx2; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-        for (int q = 0; q < kVApi / 32; ++q) { t0 += sh[0][q]; t1 += sh[1][q]; t2 = fmax(t2, sh[2][q]); }
-        part[3 * blockIdx.x] = t0;
-        part[3 * blockIdx.x + 1] = t1;
-        part[3 * blockIdx.x + 2] = t2;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+        for (int q = 0; q < kVApi / 32; ++q) {
+            t0 += sh[0][q]; t1 += sh[1][q]; t2 = fmax(t2, sh[2][q]); t3 = fmax(t3, sh[3][q]);
+        }
+        part[4 * blockIdx.x] = t0;
+        part[4 * blockIdx.x + 1] = t1;
+        part[4 * blockIdx.x + 2] = t2;
+        part[4 * blockIdx.x + 3] = t3;
     }
 }
 __global__ void kv_reduce_final(int nblocks, const double* __restrict__ part, double* __restrict__ out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-        for (int q = 0; q < nblocks; ++q) { t0 += part[3 * q]; t1 += part[3 * q + 1]; t2 = fmax(t2, part[3 * q + 2]); }
-        out[0] = t0; out[1] = t1; out[2] = t2;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+        for (int q = 0; q < nblocks; ++q) {
+            t0 += part[4 * q]; t1 += part[4 * q + 1]; t2 = fmax(t2, part[4 * q + 2]); t3 = fmax(t3, part[4 * q + 3]);
+        }
+        out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3;
     }
 }
 
@@ -660,10 +861,6 @@ __global__ void kv_sub_update(int NV, const double2* __restrict__ dx, double2* _
         x[v] = make_double2(a.x - d.x, a.y - d.y);
     }
 }
-__global__ void kv_changed(int64_t n, const double* __restrict__ c, int* flags) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        if (c[q] != 0.0) { atomicOr(flags, 4); return; }
-}
 
 }  // namespace ewg
 
@@ -687,19 +884,19 @@ ewg_status v_storage(ewg_vcfv* c) {
     return vcheck(c, "kv_storage");
 }
 
-// three reductions in one pass: sums a0.b0 and a1.b1 and max|m|; synchronous read-back
+// one pass of kv_reduce: a0.b0, a1.b1, max|m| and max|m2|; synchronous read-back of the four
 ewg_status v_reduce(ewg_vcfv* c, const double* a0, const double* b0, const double* a1, const double* b1,
-                    const double* m, double out[3]) {
+                    const double* m, const double* m2, double out[4]) {
     const int64_t n = 2 * (int64_t)c->D.NV;
-    kv_reduce<<<kVRedBlocks, kVApi, 0, c->stream>>>(n, a0, b0, a1, b1, m, c->s_red);
+    kv_reduce<<<kVRedBlocks, kVApi, 0, c->stream>>>(n, a0, b0, a1, b1, m, m2, c->s_red);
     ewg_status st = vcheck(c, "kv_reduce");
     if (st) return st;
-    kv_reduce_final<<<1, 32, 0, c->stream>>>(kVRedBlocks, c->s_red, c->s_red + 3 * kVRedBlocks);
+    kv_reduce_final<<<1, 32, 0, c->stream>>>(kVRedBlocks, c->s_red, c->s_red + 4 * kVRedBlocks);
     if ((st = vcheck(c, "kv_reduce_final"))) return st;
-    cudaError_t e = cudaMemcpyAsync(c->h_red, c->s_red + 3 * kVRedBlocks, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaMemcpyAsync(c->h_red, c->s_red + 4 * kVRedBlocks, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return vfail(c, e, "reduce read-back");
-    out[0] = c->h_red[0]; out[1] = c->h_red[1]; out[2] = c->h_red[2];
+    for (int q = 0; q < 4; ++q) out[q] = c->h_red[q];
     return EWG_OK;
 }
 
@@ -712,20 +909,6 @@ ewg_status v_spmv(ewg_vcfv* c, const double* x, double* y) {
 ewg_status v_prec(ewg_vcfv* c, double w, const double* d, double* out) {
     kv_jacobi<<<vgrid(c, c->D.NV), kVApi, 0, c->stream>>>(c->D.NV, w, c->s_dinv, d, out);
     return vcheck(c, "kv_jacobi");
-}
-
-bool v_stagnates(ewg_vcfv* c, const double* change, ewg_status* st) {
-    int flag = 0;
-    cudaError_t e = cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream);
-    if (e == cudaSuccess) {
-        kv_changed<<<vgrid(c, 2 * (int64_t)c->D.NV), kVApi, 0, c->stream>>>(2 * (int64_t)c->D.NV, change, c->d_flags);
-        e = cudaGetLastError();
-        ++c->launches;
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    *st = vfail(c, e, "stagnation check");
-    return (flag & 4) == 0;
 }
 
 }  // namespace
@@ -775,10 +958,10 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
         {(void**)&c->d_errmax, sizeof(unsigned long long)}, {(void**)&c->d_flags, sizeof(int)},
         {(void**)&c->s_b, v2}, {(void**)&c->s_x, v2}, {(void**)&c->s_r, v2}, {(void**)&c->s_r0, v2},
         {(void**)&c->s_v, v2}, {(void**)&c->s_p, v2}, {(void**)&c->s_y, v2}, {(void**)&c->s_z, v2},
-        {(void**)&c->s_t, v2}, {(void**)&c->s_dinv, 2 * v2}, {(void**)&c->s_red, sizeof(double) * (3 * kVRedBlocks + 3)}};
+        {(void**)&c->s_t, v2}, {(void**)&c->s_dinv, 2 * v2}, {(void**)&c->s_red, sizeof(double) * (4 * kVRedBlocks + 4)}};
     for (auto& a : allocs)
         if ((e = cudaMalloc(a.p, a.n)) != cudaSuccess) { ewg_status s = fail(e, "device allocation"); ewg_vcfv_destroy(c); return s; }
-    if ((e = cudaMallocHost(&c->h_red, 3 * sizeof(double))) != cudaSuccess) { ewg_status s = fail(e, "pinned"); ewg_vcfv_destroy(c); return s; }
+    if ((e = cudaMallocHost(&c->h_red, 4 * sizeof(double))) != cudaSuccess) { ewg_status s = fail(e, "pinned"); ewg_vcfv_destroy(c); return s; }
     // vertex lens flags from the vertex positions (isInLens_)
     std::vector<uint8_t> lensH(nv);
     for (int64_t v = 0; v < nv; ++v) {
@@ -801,8 +984,11 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
     if ((e = cudaGetLastError()) != cudaSuccess) { ewg_status s = fail(e, "total volume"); ewg_vcfv_destroy(c); return s; }
     if ((e = boundary_constants(c->P, c->stream)) != cudaSuccess) { ewg_status s = fail(e, "boundary constants"); ewg_vcfv_destroy(c); return s; }
     const int smem = (int)(sizeof(double) * (grid->dim == 3 ? vcfv_slots<3>() : vcfv_slots<2>()) * 4 * kVBlock);
-    e = grid->dim == 3 ? cudaFuncSetAttribute(kv_assemble<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                       : cudaFuncSetAttribute(kv_assemble<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = grid->dim == 3 ? cudaFuncSetAttribute(kv_assemble<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                       : cudaFuncSetAttribute(kv_assemble<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = grid->dim == 3 ? cudaFuncSetAttribute(kv_assemble<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                           : cudaFuncSetAttribute(kv_assemble<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess || (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
         ewg_status s = fail(e, "setup"); ewg_vcfv_destroy(c); return s;
     }
@@ -868,6 +1054,25 @@ ewg_status ewg_vcfv_restore_time_level(ewg_vcfv* c) {
     return vfail(c, e, "restore");
 }
 
+ewg_status ewg_vcfv_set_local_linearizer(ewg_vcfv* c, int32_t kind, int32_t method) {
+    if (!c) return EWG_ERR_INVALID;
+    if (kind != EWG_LOCAL_LINEARIZER_AD && kind != EWG_LOCAL_LINEARIZER_FD) { c->err = "unknown local linearizer"; return EWG_ERR_INVALID; }
+    if (method < -1 || method > 1) { c->err = "NumericDifferenceMethod must be -1, 0 or +1"; return EWG_ERR_INVALID; }
+    c->localLinearizer = kind;
+    c->fdMethod = method;
+    return EWG_OK;
+}
+
+ewg_status ewg_vcfv_update_begin(ewg_vcfv* c) {
+    if (!c) return EWG_ERR_INVALID;
+    double2 v0;
+    cudaError_t e = cudaMemcpyAsync(&v0, c->x0, sizeof(double2), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return vfail(c, e, "update begin");
+    c->refPressure = v0.x;
+    return EWG_OK;
+}
+
 // residual (volumetric) and Jacobian of solution(0); *error = max |r|, NaN/Inf -> EWG_ERR_NONFINITE
 ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error) {
     if (!c || !(dt > 0)) return EWG_ERR_INVALID;
@@ -880,12 +1085,16 @@ ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error) {
     if (st) return st;
     const int blocks = (c->D.NV + kVBlock - 1) / kVBlock;
     const size_t smem = sizeof(double) * (c->P.dim == 3 ? vcfv_slots<3>() : vcfv_slots<2>()) * 4 * kVBlock;
-    if (c->P.dim == 3)
-        kv_assemble<3><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
-                                                              c->totVol, dt, c->r, c->J, c->d_errmax, c->d_flags);
-    else
-        kv_assemble<2><<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
-                                                              c->totVol, dt, c->r, c->J, c->d_errmax, c->d_flags);
+    const bool fd = c->localLinearizer == EWG_LOCAL_LINEARIZER_FD;
+    if (fd && !(c->refPressure > 0)) {
+        // a context that never ran updateBegin takes the reference pressure of the current iterate
+        if ((st = ewg_vcfv_update_begin(c))) return st;
+    }
+    auto k = c->P.dim == 3 ? (fd ? kv_assemble<3, true> : kv_assemble<3, false>)
+                           : (fd ? kv_assemble<2, true> : kv_assemble<2, false>);
+    k<<<blocks, kVBlock, smem, c->stream>>>(c->P, c->D, c->geo, c->x0, c->sold, c->perm, c->lens, c->iq, c->kedge,
+                                            c->totVol, dt, c->refPressure, c->fdMethod, c->r, c->J, c->d_errmax,
+                                            c->d_flags);
     if ((st = vcheck(c, "kv_assemble"))) return st;
     unsigned long long bits = 0;
     int flag = 0;
@@ -952,10 +1161,12 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         (e = cudaMemsetAsync(c->s_v, 0, sizeof(double) * n, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(c->s_p, 0, sizeof(double) * n, s)) != cudaSuccess)
         return vfail(c, e, "solver init");
-    double red[3];
-    if ((st = v_reduce(c, c->s_r0, c->s_r0, nullptr, nullptr, c->s_r, red))) return st;
+    double red[4];
+    if ((st = v_reduce(c, c->s_r0, c->s_r0, nullptr, nullptr, c->s_r, nullptr, red))) return st;
     int sing = 0;
-    if ((e = cudaMemcpy(&sing, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return vfail(c, e, "flags");
+    if ((e = cudaMemcpyAsync(&sing, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return vfail(c, e, "flags");
     if (sing & 2) { c->err = "singular diagonal block"; return EWG_ERR_BREAKDOWN; }
     const double breakdownEps = 2.2250738585072014e-308 * 1e10;
     double r0r0 = red[0];
@@ -977,8 +1188,8 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         if (q) return q;
         kv_residual<<<g, kVApi, 0, s>>>(n, c->s_b, c->s_t, c->s_r);
         if ((q = vcheck(c, "kv_residual"))) return q;
-        double rr[3];
-        if ((q = v_reduce(c, c->s_r, c->s_r, nullptr, nullptr, c->s_r, rr))) return q;
+        double rr[4];
+        if ((q = v_reduce(c, c->s_r, c->s_r, nullptr, nullptr, c->s_r, nullptr, rr))) return q;
         if (rr[2] / fmax(1e-20, initResErr) <= 10 * so->linear_solver_tolerance ||
             rr[2] <= 10 * so->linear_solver_abs_tolerance)
             return EWG_OK;
@@ -996,9 +1207,9 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
     const int maxIt = so->linear_solver_max_iterations;
     int it = 0;
     for (; it < maxIt; ++it) {
-        double rr[3];
+        double rr[4];
         // rho_i = r0hat . r, |r|^2
-        if ((st = v_reduce(c, c->s_r0, c->s_r, c->s_r, c->s_r, nullptr, rr))) return st;
+        if ((st = v_reduce(c, c->s_r0, c->s_r, c->s_r, c->s_r, nullptr, nullptr, rr))) return st;
         double rho_i = rr[0];
         if (so->restart_on_breakdown && fabs(rho_i) <= 1e-12 * sqrt(r0r0) * sqrt(rr[1])) {
             if ((e = cudaMemcpyAsync(c->s_r0, c->s_r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
@@ -1016,16 +1227,16 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         if ((st = vcheck(c, "kv_p_update"))) return st;
         if ((st = v_prec(c, w, c->s_p, c->s_y))) return st;
         if ((st = v_spmv(c, c->s_y, c->s_v))) return st;
-        if ((st = v_reduce(c, c->s_r0, c->s_v, nullptr, nullptr, nullptr, rr))) return st;
+        if ((st = v_reduce(c, c->s_r0, c->s_v, nullptr, nullptr, nullptr, nullptr, rr))) return st;
         if (fabs(rr[0]) <= breakdownEps) { c->err = "BiCGStab breakdown"; return EWG_ERR_BREAKDOWN; }
         alpha = rho_i / rr[0];
         if (fabs(alpha) <= breakdownEps) { c->err = "BiCGStab stagnation"; return EWG_ERR_BREAKDOWN; }
         kv_h_s<<<g, kVApi, 0, s>>>(n, alpha, c->s_y, c->s_v, c->s_x, c->s_r);
         if ((st = vcheck(c, "kv_h_s"))) return st;
-        if ((st = v_reduce(c, nullptr, nullptr, nullptr, nullptr, c->s_r, rr))) return st;
+        // max |s| for the criterion; the update y stagnates when it is all zero
+        if ((st = v_reduce(c, nullptr, nullptr, nullptr, nullptr, c->s_r, c->s_y, rr))) return st;
         resErr = rr[2];
-        bool stag = v_stagnates(c, c->s_y, &st);
-        if (st) return st;
+        bool stag = rr[3] == 0.0;
         if (converged(resErr)) {
             bool goOn;
             if ((st = replace(&goOn))) return st;
@@ -1035,15 +1246,15 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         if (stag || resErr > so->linear_solver_max_error) { *iterations = it; c->err = "BiCGStab failed"; return EWG_ERR_NOT_CONVERGED; }
         if ((st = v_prec(c, w, c->s_r, c->s_z))) return st;
         if ((st = v_spmv(c, c->s_z, c->s_t))) return st;
-        if ((st = v_reduce(c, c->s_t, c->s_t, c->s_t, c->s_r, nullptr, rr))) return st;
+        if ((st = v_reduce(c, c->s_t, c->s_t, c->s_t, c->s_r, nullptr, c->s_z, rr))) return st;
         if (fabs(rr[0]) <= breakdownEps) { c->err = "BiCGStab breakdown"; return EWG_ERR_BREAKDOWN; }
         omega = rr[1] / rr[0];
         if (fabs(omega) <= breakdownEps) { c->err = "BiCGStab stagnation"; return EWG_ERR_BREAKDOWN; }
         kv_axpy<<<g, kVApi, 0, s>>>(n, omega, c->s_z, c->s_x);
         if ((st = vcheck(c, "kv_axpy"))) return st;
-        // the criterion sees s (the reference's aliasing r == s) before r = s - omega t
-        stag = v_stagnates(c, c->s_z, &st);
-        if (st) return st;
+        // the criterion sees s (the reference's aliasing r == s) before r = s - omega t; the
+        // update z stagnates when it is all zero
+        stag = rr[3] == 0.0;
         if (converged(resErr)) {
             bool goOn;
             if ((st = replace(&goOn))) return st;
@@ -1074,7 +1285,9 @@ ewg_status ewg_vcfv_newton_apply(ewg_vcfv* c, double dt, const ewg_newton_opts* 
         if (numIterations >= no->newton_max_iterations) return error * 4.0 < lastError;
         return true;
     };
-    ewg_status status = EWG_OK;
+    // ImmiscibleModel::updateBegin before every Newton solve
+    ewg_status status = ewg_vcfv_update_begin(c);
+    if (status) return status;
     while (proceed()) {
         double err = 0.0;
         ewg_status st = ewg_vcfv_linearize(c, dt, &err);

@@ -401,6 +401,8 @@ def load(path: str = LIB_PATH):
         "ewg_vcfv_apply_initial_solution": (C.c_int, [C.c_void_p]),
         "ewg_vcfv_advance_time_level": (C.c_int, [C.c_void_p]),
         "ewg_vcfv_restore_time_level": (C.c_int, [C.c_void_p]),
+        "ewg_vcfv_set_local_linearizer": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "ewg_vcfv_update_begin": (C.c_int, [C.c_void_p]),
         "ewg_vcfv_linearize": (C.c_int, [C.c_void_p, d, P(d)]),
         "ewg_vcfv_get_residual": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_vcfv_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), C.c_int64, P(d)]),
@@ -842,6 +844,12 @@ class VcfvContext:
 
     def restore_time_level(self):
         self._check(self.lib.ewg_vcfv_restore_time_level(self.h), "restore_time_level")
+
+    def set_local_linearizer(self, kind: int, method: int = 1):
+        self._check(self.lib.ewg_vcfv_set_local_linearizer(self.h, kind, method), "set_local_linearizer")
+
+    def update_begin(self):
+        self._check(self.lib.ewg_vcfv_update_begin(self.h), "update_begin")
 
     def linearize(self, dt) -> float:
         e = C.c_double()

@@ -439,6 +439,11 @@ ewg_status ewg_vcfv_get_solution(ewg_vcfv* c, int32_t time_idx, double* x);
 ewg_status ewg_vcfv_apply_initial_solution(ewg_vcfv* c);
 ewg_status ewg_vcfv_advance_time_level(ewg_vcfv* c);   /* solution(1) = solution(0) */
 ewg_status ewg_vcfv_restore_time_level(ewg_vcfv* c);   /* solution(0) = solution(1) */
+/* LocalLinearizerSplice for the vertex-centred stencil: AD (default) or finite differences with
+ * NumericDifferenceMethod -1/0/+1 (fvbasefdlocallinearizer.hh; lens_immiscible_vcfv_fd). */
+ewg_status ewg_vcfv_set_local_linearizer(ewg_vcfv* c, int32_t kind, int32_t method);
+/* ImmiscibleModel::updateBegin: the FD pressure weight's reference pressure (p_w of vertex 0). */
+ewg_status ewg_vcfv_update_begin(ewg_vcfv* c);
 /* Residual (per unit control volume) and Jacobian of solution(0) against the storage of
  * solution(1); *error = max |r|. */
 ewg_status ewg_vcfv_linearize(ewg_vcfv* c, double dt, double* error);

@@ -91,3 +91,60 @@ def test_vcfv_newton_matches_oracle(ewg_mod, oracle_mod, name):
         g.advance_time_level()
     assert g.launches > 0
     g.close()
+
+
+# finite-difference quotients amplify the last-bit differences of the two evaluations by 1/eps
+FD_RTOL = 1e-4
+
+
+@pytest.mark.parametrize("name", ["baseline_2d", "lens3d_small"])
+@pytest.mark.parametrize("method", [1, 0])
+def test_vcfv_fd_linearization_matches_oracle(ewg_mod, oracle_mod, name, method):
+    """lens_immiscible_vcfv_fd: the FD local linearizer on the device against the oracle's, same
+    deflections (BaseEpsilon / primaryVarWeight with the updateBegin reference pressure)."""
+    case = _cases(ewg_mod)[name]
+    o, x1, x0 = _states(oracle_mod, case)
+    o.set_local_linearizer(1, method)
+    o.set_solution(1, x1)
+    o.set_solution(0, x1)
+    o.linearize(250.0, 0)
+    o.set_solution(0, x0)
+    o.update_begin()
+    o.linearize(250.0, 1)
+    r_ref = o.residual()
+    rp, ci, b_ref = o.jacobian_bcrs()
+    g = ewg_mod.VcfvContext(case)
+    g.set_local_linearizer(1, method)
+    g.set_solution(1, x1)
+    g.set_solution(0, x0)
+    g.update_begin()
+    g.linearize(250.0)
+    ok, err, s = rel_close(g.residual(), r_ref, RTOL)
+    assert ok, (err, s)
+    _, _, b = g.jacobian_bcrs()
+    for row in range(o.n):
+        blk = slice(rp[row], rp[row + 1])
+        ok, err, s = rel_close(b[blk], b_ref[blk], FD_RTOL)
+        assert ok, (row, err, s)
+    g.close()
+
+
+def test_vcfv_fd_newton_matches_oracle(ewg_mod, oracle_mod):
+    case = _cases(ewg_mod)["baseline_2d"]
+    so = ewg_mod.default_solve_opts(precond=ewg_mod.PRECOND_JACOBI, linear_solver_tolerance=1e-10,
+                                    linear_solver_max_iterations=5000)
+    o = oracle_mod.VcfvOracle(case)
+    o.set_local_linearizer(1, 1)
+    o.apply_initial_solution()
+    g = ewg_mod.VcfvContext(case)
+    g.set_local_linearizer(1, 1)
+    g.apply_initial_solution()
+    for step in range(2):
+        st_o, its_o, _, _ = o.newton_apply(250.0, None, so)
+        st_g, its_g, _, _ = g.newton_apply(250.0, None, so)
+        assert st_o == 0 and st_g == 0 and its_g == its_o, (step, its_g, its_o)
+        xo, xg = o.get_solution(0), g.get_solution(0)
+        assert np.max(np.abs(xg[:, 1] - xo[:, 1])) <= 1e-8
+        o.advance_time_level()
+        g.advance_time_level()
+    g.close()
