@@ -107,6 +107,9 @@ public:
     void advanceTimeLevel() { check(ewg_vcfv_advance_time_level(c_), "ewg_vcfv_advance_time_level"); }
     void restoreTimeLevel() { check(ewg_vcfv_restore_time_level(c_), "ewg_vcfv_restore_time_level"); }
     void getSolution(int timeIdx, double* x) { check(ewg_vcfv_get_solution(c_, timeIdx, x), "ewg_vcfv_get_solution"); }
+    void setLocalLinearizer(int kind, int method) {
+        check(ewg_vcfv_set_local_linearizer(c_, kind, method), "ewg_vcfv_set_local_linearizer");
+    }
     // NewtonMethod::apply; returns the status (non-zero: the caller halves the step)
     ewg_status newtonApply(double dt, const ewg_newton_opts& no, const ewg_solve_opts& so, int* its, int* linIts) {
         int32_t a = 0, b = 0;

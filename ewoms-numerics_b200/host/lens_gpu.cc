@@ -255,7 +255,7 @@ std::vector<ewg::VtkMultiWriter::Field> vtkFields(ewg::Context& ctx, const ewg_g
 
 }  // namespace
 
-// lens_immiscible_vcfv_ad: the vertex-centred discretization with P1 gradients, block Jacobi.
+// lens_immiscible_vcfv_ad / _fd: the vertex-centred discretization with P1 gradients, block Jacobi.
 // K per vertex from the lens box at the vertex positions (or PermFile with one value per vertex);
 // VTK output as point data.
 void runVcfv(const Params& p, const ewg_grid& g, const ewg_problem& pr, const std::vector<double>& permCells,
@@ -289,13 +289,17 @@ void runVcfv(const Params& p, const ewg_grid& g, const ewg_problem& pr, const st
         }
     }
     ewg::VcfvContext ctx(g, pr, perm);
+    const std::string ll = p.get("LocalLinearizer");
+    if (ll != "ad" && ll != "fd") throw std::runtime_error("LocalLinearizer must be 'ad' or 'fd'");
+    ctx.setLocalLinearizer(ll == "fd" ? EWG_LOCAL_LINEARIZER_FD : EWG_LOCAL_LINEARIZER_AD, p.i("NumericDifferenceMethod"));
     ctx.applyInitialSolution();
     ewg_newton_opts no;
     ewg_default_newton_opts(&no);
     no.newton_tolerance = p.d("NewtonTolerance");
     no.newton_max_iterations = p.i("NewtonMaxIterations");
     no.newton_max_error = p.d("NewtonMaxError");
-    ewg::VtkMultiWriter vtk(p.get("OutputDir"), "lens_immiscible_vcfv_ad");
+    // LensProblem::name(): lens_immiscible_vcfv_ad for AD, lens_immiscible_vcfv for finite differences
+    ewg::VtkMultiWriter vtk(p.get("OutputDir"), ll == "ad" ? "lens_immiscible_vcfv_ad" : "lens_immiscible_vcfv");
     const bool vtkOut = p.i("EnableVtkOutput") != 0;
     std::vector<double> x(2 * NV);
     auto fields = [&]() {

@@ -163,3 +163,16 @@ def test_driver_vcfv_runs_and_matches_oracle(driver, tmp_path, oracle_mod, ewg_m
     assert np.max(np.abs(x[:, 1] - xo[:, 1])) <= 1e-8
     vtu = (tmp_path / "lens_immiscible_vcfv_ad-00002.vtu").read_text()
     assert "<PointData>" in vtu and 'Name="saturation_n"' in vtu
+
+
+@pytest.mark.gpu
+def test_driver_vcfv_fd_runs(driver, tmp_path):
+    """lens_immiscible_vcfv_fd through the driver: the finite-difference local linearizer on the
+    vertex-centred stencil, two steps, VTK output under the finite-difference name."""
+    out = subprocess.run([driver, "--discretization=vcfv", "--preconditioner=jacobi", "--preset=baseline",
+                          "--cells-x=24", "--cells-y=16", "--end-time=500", "--initial-time-step-size=250",
+                          "--max-time-step-size=250", "--local-linearizer=fd", f"--output-dir={tmp_path}"],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert len([ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]) == 2
+    assert (tmp_path / "lens_immiscible_vcfv-00002.vtu").exists()
