@@ -77,6 +77,8 @@ struct ewg_vcfv {
     double *s_b = nullptr, *s_x = nullptr, *s_r = nullptr, *s_r0 = nullptr, *s_v = nullptr, *s_p = nullptr,
            *s_y = nullptr, *s_z = nullptr, *s_t = nullptr, *s_dinv = nullptr, *s_red = nullptr;
     double* h_red = nullptr;  // pinned
+    double* M = nullptr;      // block ILU(0) factors in the band layout (allocated at the first ILU solve)
+    int precond = EWG_PRECOND_JACOBI;  // preconditioner of the current solve
     long long launches = 0;
     // LocalLinearizerSplice and NumericDifferenceMethod; the reference pressure of
     // ImmiscibleModel::updateBegin (p_w of vertex 0) for the FD pressure weight, unset until then
@@ -775,6 +777,153 @@ __global__ void kv_diag_inverse(VDims D, const double* __restrict__ J, double* _
     }
 }
 
+// ---- block ILU(0) in the parity-colour order ------------------------------------------------------
+//
+// Vertices with the same parities (i & 1, j & 1, k & 1) never share an element, so ordering the
+// vertices by that colour (then lexicographically) gives a block ILU(0) whose rows of one colour
+// are independent: the factorisation and each triangular sweep run colour by colour, all vertices
+// of a colour in parallel. It is dune-istl's bilu0 / bilu_backsolve (the factorisation the reference
+// preconditioner runs, istlpreconditionerwrappers.hh:155-193) on the colour-permuted matrix; the
+// stored diagonal block is its inverse.
+
+struct VColour {
+    int bx, by, bz;       // parity bits of the colour
+    int cx, cy, cz;       // vertices of this colour per axis
+    int count;
+};
+
+__device__ __forceinline__ int v_of_colour(const VDims& D, const VColour& C, int t, int& i, int& j, int& k) {
+    const int ii = t % C.cx, jj = (t / C.cx) % C.cy, kk = t / (C.cx * C.cy);
+    i = 2 * ii + C.bx;
+    j = 2 * jj + C.by;
+    k = 2 * kk + C.bz;
+    return i + D.nvx * (j + D.nvy * k);
+}
+
+// colour of the neighbour at band b of a vertex of colour c
+template <int DIM>
+__device__ __forceinline__ int band_colour(int c, int b) {
+    const int dx = b % 3 - 1, dy = (b / 3) % 3 - 1, dz = DIM == 3 ? b / 9 - 1 : 0;
+    return c ^ ((dx != 0) | ((dy != 0) << 1) | ((dz != 0) << 2));
+}
+template <int DIM>
+__device__ __forceinline__ bool band_in_grid(const VDims& D, int i, int j, int k, int b) {
+    const int dx = b % 3 - 1, dy = (b / 3) % 3 - 1, dz = DIM == 3 ? b / 9 - 1 : 0;
+    const int ii = i + dx, jj = j + dy, kk = k + dz;
+    return ii >= 0 && jj >= 0 && kk >= 0 && ii < D.nvx && jj < D.nvy && kk < D.nvz;
+}
+template <int DIM>
+__device__ __forceinline__ int band_offset(const VDims& D, int b) {
+    const int dx = b % 3 - 1, dy = (b / 3) % 3 - 1, dz = DIM == 3 ? b / 9 - 1 : 0;
+    return dx + D.nvx * (dy + D.nvy * dz);
+}
+
+__device__ __forceinline__ void blk_mul(const double* A, const double* B, double* o) {  // o = A B
+    const double o0 = A[0] * B[0] + A[1] * B[2], o1 = A[0] * B[1] + A[1] * B[3];
+    const double o2 = A[2] * B[0] + A[3] * B[2], o3 = A[2] * B[1] + A[3] * B[3];
+    o[0] = o0; o[1] = o1; o[2] = o2; o[3] = o3;
+}
+
+// factorisation of the rows of colour c (the rows of lower colours are final)
+template <int DIM>
+__global__ void kv_ilu_factor(VDims D, VColour C, int c, const double* __restrict__ J, double* __restrict__ M, int* flags) {
+    constexpr int NB = DIM == 3 ? 27 : 9;
+    constexpr int CB = DIM == 3 ? 13 : 4;
+    const int64_t NV = D.NV;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < C.count; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        const int v = v_of_colour(D, C, t, i, j, k);
+        for (int q = 0; q < NB * 4; ++q) M[q * NV + v] = J[q * NV + v];
+        // eliminate the couplings to lower colours, column order: colour, then index
+        for (int kc = 0; kc < c; ++kc) {
+            for (int b = 0; b < NB; ++b) {
+                if (band_colour<DIM>(c, b) != kc || !band_in_grid<DIM>(D, i, j, k, b)) continue;
+                const int kv = v + band_offset<DIM>(D, b);
+                double Lb[4], Dk[4];
+                for (int e = 0; e < 4; ++e) { Lb[e] = M[(b * 4 + e) * NV + v]; Dk[e] = M[(CB * 4 + e) * NV + kv]; }
+                blk_mul(Lb, Dk, Lb);  // A_vk inv(A_kk)
+                for (int e = 0; e < 4; ++e) M[(b * 4 + e) * NV + v] = Lb[e];
+                const int dxk = b % 3 - 1, dyk = (b / 3) % 3 - 1, dzk = DIM == 3 ? b / 9 - 1 : 0;
+                for (int b2 = 0; b2 < NB; ++b2) {
+                    if (band_colour<DIM>(c, b2) <= kc || !band_in_grid<DIM>(D, i, j, k, b2)) continue;
+                    // column j2 = v + o(b2) in row k: offset o(b2) - o(b) must be a neighbour offset
+                    const int rx = b2 % 3 - 1 - dxk, ry = (b2 / 3) % 3 - 1 - dyk, rz = (DIM == 3 ? b2 / 9 - 1 : 0) - dzk;
+                    if (rx < -1 || rx > 1 || ry < -1 || ry > 1 || rz < -1 || rz > 1) continue;
+                    const int bk = (rx + 1) + 3 * (ry + 1) + (DIM == 3 ? 9 * (rz + 1) : 0);
+                    double Akj[4], B[4];
+                    for (int e = 0; e < 4; ++e) Akj[e] = M[(bk * 4 + e) * NV + kv];
+                    blk_mul(Lb, Akj, B);
+                    for (int e = 0; e < 4; ++e) M[(b2 * 4 + e) * NV + v] -= B[e];
+                }
+            }
+        }
+        // invert the diagonal block in place
+        double a[4];
+        for (int e = 0; e < 4; ++e) a[e] = M[(CB * 4 + e) * NV + v];
+        const double det = a[0] * a[3] - a[1] * a[2];
+        if (det == 0.0 || !isfinite(det)) atomicOr(flags, 2);
+        const double di = 1.0 / det;
+        M[(CB * 4 + 0) * NV + v] = a[3] * di;
+        M[(CB * 4 + 1) * NV + v] = -a[1] * di;
+        M[(CB * 4 + 2) * NV + v] = -a[2] * di;
+        M[(CB * 4 + 3) * NV + v] = a[0] * di;
+    }
+}
+
+// forward sweep of colour c: y_v = d_v - sum over lower colours L_vk y_k
+template <int DIM>
+__global__ void kv_ilu_fwd(VDims D, VColour C, int c, const double* __restrict__ M, const double* __restrict__ d,
+                           double* __restrict__ y) {
+    constexpr int NB = DIM == 3 ? 27 : 9;
+    const int64_t NV = D.NV;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < C.count; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        const int v = v_of_colour(D, C, t, i, j, k);
+        double r0 = d[2 * (int64_t)v], r1 = d[2 * (int64_t)v + 1];
+        for (int kc = 0; kc < c; ++kc)
+            for (int b = 0; b < NB; ++b) {
+                if (band_colour<DIM>(c, b) != kc || !band_in_grid<DIM>(D, i, j, k, b)) continue;
+                const int kv = v + band_offset<DIM>(D, b);
+                const double x0 = y[2 * (int64_t)kv], x1 = y[2 * (int64_t)kv + 1];
+                const double* L = M + (int64_t)b * 4 * NV + v;
+                r0 -= L[0] * x0 + L[NV] * x1;
+                r1 -= L[2 * NV] * x0 + L[3 * NV] * x1;
+            }
+        y[2 * (int64_t)v] = r0;
+        y[2 * (int64_t)v + 1] = r1;
+    }
+}
+
+// backward sweep of colour c (in place): z_v = inv(U_vv) (y_v - sum over higher colours U_vj z_j)
+template <int DIM>
+__global__ void kv_ilu_bwd(VDims D, VColour C, int c, int ncol, const double* __restrict__ M, double* __restrict__ z) {
+    constexpr int NB = DIM == 3 ? 27 : 9;
+    constexpr int CB = DIM == 3 ? 13 : 4;
+    const int64_t NV = D.NV;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < C.count; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        const int v = v_of_colour(D, C, t, i, j, k);
+        double r0 = z[2 * (int64_t)v], r1 = z[2 * (int64_t)v + 1];
+        for (int jc = ncol - 1; jc > c; --jc)
+            for (int b = NB - 1; b >= 0; --b) {
+                if (band_colour<DIM>(c, b) != jc || !band_in_grid<DIM>(D, i, j, k, b)) continue;
+                const int jv = v + band_offset<DIM>(D, b);
+                const double x0 = z[2 * (int64_t)jv], x1 = z[2 * (int64_t)jv + 1];
+                const double* U = M + (int64_t)b * 4 * NV + v;
+                r0 -= U[0] * x0 + U[NV] * x1;
+                r1 -= U[2 * NV] * x0 + U[3 * NV] * x1;
+            }
+        const double* Di = M + (int64_t)CB * 4 * NV + v;
+        z[2 * (int64_t)v] = Di[0] * r0 + Di[NV] * r1;
+        z[2 * (int64_t)v + 1] = Di[2 * NV] * r0 + Di[3 * NV] * r1;
+    }
+}
+
+__global__ void kv_scale(int64_t n, double w, double* __restrict__ x) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        x[q] *= w;
+}
+
 __global__ void kv_jacobi(int NV, double w, const double* __restrict__ dinv, const double* __restrict__ d,
                           double* __restrict__ out) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < NV; v += gridDim.x * blockDim.x) {
@@ -906,7 +1055,61 @@ ewg_status v_spmv(ewg_vcfv* c, const double* x, double* y) {
     return vcheck(c, "kv_spmv");
 }
 
+VColour v_colour(const ewg_vcfv* c, int col) {
+    VColour C;
+    C.bx = col & 1; C.by = (col >> 1) & 1; C.bz = (col >> 2) & 1;
+    C.cx = (c->D.nvx - C.bx + 1) / 2;
+    C.cy = (c->D.nvy - C.by + 1) / 2;
+    C.cz = (c->D.nvz - C.bz + 1) / 2;
+    C.count = C.cx * C.cy * C.cz;
+    return C;
+}
+int v_ncolours(const ewg_vcfv* c) { return c->P.dim == 3 ? 8 : 4; }
+
+// block ILU(0) factorisation of J in the parity-colour order, colour by colour
+ewg_status v_ilu_factor(ewg_vcfv* c) {
+    if (!c->M) {
+        cudaError_t e = cudaMalloc(&c->M, sizeof(double) * c->nb * 4 * (size_t)c->D.NV);
+        if (e != cudaSuccess) return vfail(c, e, "alloc ILU factors");
+        if ((e = cudaMemsetAsync(c->M, 0, sizeof(double) * c->nb * 4 * (size_t)c->D.NV, c->stream)) != cudaSuccess)
+            return vfail(c, e, "zero ILU factors");
+    }
+    for (int col = 0; col < v_ncolours(c); ++col) {
+        const VColour C = v_colour(c, col);
+        if (C.count == 0) continue;
+        if (c->P.dim == 3) kv_ilu_factor<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->J, c->M, c->d_flags);
+        else kv_ilu_factor<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->J, c->M, c->d_flags);
+        ewg_status st = vcheck(c, "kv_ilu_factor");
+        if (st) return st;
+    }
+    return EWG_OK;
+}
+
 ewg_status v_prec(ewg_vcfv* c, double w, const double* d, double* out) {
+    if (c->precond == EWG_PRECOND_ILU0) {
+        const int nc = v_ncolours(c);
+        for (int col = 0; col < nc; ++col) {
+            const VColour C = v_colour(c, col);
+            if (C.count == 0) continue;
+            if (c->P.dim == 3) kv_ilu_fwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
+            else kv_ilu_fwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
+            ewg_status st = vcheck(c, "kv_ilu_fwd");
+            if (st) return st;
+        }
+        for (int col = nc - 1; col >= 0; --col) {
+            const VColour C = v_colour(c, col);
+            if (C.count == 0) continue;
+            if (c->P.dim == 3) kv_ilu_bwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, nc, c->M, out);
+            else kv_ilu_bwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, nc, c->M, out);
+            ewg_status st = vcheck(c, "kv_ilu_bwd");
+            if (st) return st;
+        }
+        if (w != 1.0) {
+            kv_scale<<<vgrid(c, 2 * (int64_t)c->D.NV), kVApi, 0, c->stream>>>(2 * (int64_t)c->D.NV, w, out);
+            return vcheck(c, "kv_scale");
+        }
+        return EWG_OK;
+    }
     kv_jacobi<<<vgrid(c, c->D.NV), kVApi, 0, c->stream>>>(c->D.NV, w, c->s_dinv, d, out);
     return vcheck(c, "kv_jacobi");
 }
@@ -1001,7 +1204,7 @@ void ewg_vcfv_destroy(ewg_vcfv* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* ps[] = {c->x0, c->x1, c->sold, c->r, c->perm, c->totVol, c->kedge, c->iq, c->J, c->lens, c->geo, c->d_errmax,
                   c->d_flags, c->s_b, c->s_x, c->s_r, c->s_r0, c->s_v, c->s_p, c->s_y, c->s_z, c->s_t, c->s_dinv,
-                  c->s_red};
+                  c->s_red, c->M};
     for (void* p : ps) if (p) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1150,9 +1353,14 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
     *iterations = 0;
     cudaError_t e;
     if ((e = cudaMemsetAsync(c->d_flags, 0, sizeof(int), s)) != cudaSuccess) return vfail(c, e, "memset");
-    if (c->P.dim == 3) kv_diag_inverse<3><<<vgrid(c, c->D.NV), kVApi, 0, s>>>(c->D, c->J, c->s_dinv, c->d_flags);
-    else kv_diag_inverse<2><<<vgrid(c, c->D.NV), kVApi, 0, s>>>(c->D, c->J, c->s_dinv, c->d_flags);
-    if ((st = vcheck(c, "kv_diag_inverse"))) return st;
+    c->precond = so->precond;
+    if (so->precond == EWG_PRECOND_ILU0) {
+        if ((st = v_ilu_factor(c))) return st;
+    } else {
+        if (c->P.dim == 3) kv_diag_inverse<3><<<vgrid(c, c->D.NV), kVApi, 0, s>>>(c->D, c->J, c->s_dinv, c->d_flags);
+        else kv_diag_inverse<2><<<vgrid(c, c->D.NV), kVApi, 0, s>>>(c->D, c->J, c->s_dinv, c->d_flags);
+        if ((st = vcheck(c, "kv_diag_inverse"))) return st;
+    }
     // b = r, x = 0, r = b, r0hat = b
     if ((e = cudaMemcpyAsync(c->s_b, c->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(c->s_r, c->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
@@ -1275,7 +1483,8 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
 ewg_status ewg_vcfv_newton_apply(ewg_vcfv* c, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
                                  int32_t* newtonIts, int32_t* linIts, double* errorOut) {
     if (!c || !no || !so || !(dt > 0)) return EWG_ERR_INVALID;
-    if (so->precond != EWG_PRECOND_JACOBI) { c->err = "the vertex-centred path solves with block Jacobi"; return EWG_ERR_INVALID; }
+    if (so->precond != EWG_PRECOND_JACOBI && so->precond != EWG_PRECOND_ILU0) { c->err = "unknown preconditioner"; return EWG_ERR_INVALID; }
+    if (so->precision != EWG_PRECISION_FP64) { c->err = "the vertex-centred solve is FP64"; return EWG_ERR_INVALID; }
     int numIterations = 0, linTotal = 0;
     double error = 1e100, lastError = 1e100;
     auto converged = [&]() { return error <= no->newton_tolerance; };

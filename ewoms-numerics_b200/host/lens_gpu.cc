@@ -255,13 +255,13 @@ std::vector<ewg::VtkMultiWriter::Field> vtkFields(ewg::Context& ctx, const ewg_g
 
 }  // namespace
 
-// lens_immiscible_vcfv_ad / _fd: the vertex-centred discretization with P1 gradients, block Jacobi.
+// lens_immiscible_vcfv_ad / _fd: the vertex-centred discretization with P1 gradients; BiCGStab
+// with block ILU(0) (parity-colour order) or block Jacobi.
 // K per vertex from the lens box at the vertex positions (or PermFile with one value per vertex);
 // VTK output as point data.
 void runVcfv(const Params& p, const ewg_grid& g, const ewg_problem& pr, const std::vector<double>& permCells,
              const ewg_solve_opts& so) {
     (void)permCells;
-    if (so.precond != EWG_PRECOND_JACOBI) throw std::runtime_error("Discretization=vcfv solves with Preconditioner=jacobi");
     const int nz = g.dim == 3 ? g.nz : 1;
     const int nvx = g.nx + 1, nvy = g.ny + 1, nvz = g.dim == 3 ? nz + 1 : 1;
     const int64_t NV = (int64_t)nvx * nvy * nvz;

@@ -423,8 +423,8 @@ void ewg_default_newton_opts(ewg_newton_opts* o);
  * vertex and the lens region is taken at the vertex positions. Replaces, for the vertex-centred
  * type tag, the Linearizer (fvbaselinearizer.hh:401-512, local residual of
  * discretizations/vcfv/vcfvstencil.hh:866-1016 and p1fegradientcalculator.hh:255-290) and the
- * Newton / BiCGStab path with block Jacobi (PreconditionerWrapperJacobi,
- * istlpreconditionerwrappers.hh:145). No red-black constraint on nx. */
+ * Newton / BiCGStab path with block ILU(0) or block Jacobi (istlpreconditionerwrappers.hh:145-193).
+ * No red-black constraint on nx. */
 typedef struct ewg_vcfv ewg_vcfv;
 
 ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, const double* perm, ewg_vcfv** out);
@@ -452,8 +452,9 @@ ewg_status ewg_vcfv_get_residual(ewg_vcfv* c, double* r);
  * vertices of its adjacent elements, columns ascending). */
 ewg_status ewg_vcfv_get_jacobian_bcrs(ewg_vcfv* c, const int32_t* row_ptr, const int32_t* col_idx, int64_t nnzb,
                                       double* blocks);
-/* NewtonMethod::apply at fixed dt with BiCGStab + block Jacobi (sopts->precond must be
- * EWG_PRECOND_JACOBI). */
+/* NewtonMethod::apply at fixed dt with BiCGStab + block ILU(0) (EWG_PRECOND_ILU0: dune-istl's
+ * bilu0 on the matrix ordered by the vertices' parity colour (i&1) + 2 (j&1) + 4 (k&1), then
+ * lexicographically) or block Jacobi; FP64 only. */
 ewg_status ewg_vcfv_newton_apply(ewg_vcfv* c, double dt, const ewg_newton_opts* nopts, const ewg_solve_opts* sopts,
                                  int32_t* newton_iterations, int32_t* linear_iterations, double* error);
 

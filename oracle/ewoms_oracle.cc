@@ -739,6 +739,7 @@ struct Precond {
     double w = 1.0;
     Bcrs F;                         // factor (ILU) in the chosen ordering
     std::vector<int64_t> perm, iperm;  // new index -> old, old -> new
+    std::vector<int8_t> colourOf;      // ORC_ORDER_COLOURS: colour of each row
     std::vector<double> Dinv;        // Jacobi
     std::vector<double> tin, tout;
     void setup(const Ctx& C, const Bcrs& A) {
@@ -750,6 +751,11 @@ struct Precond {
         perm.resize(A.n); iperm.resize(A.n);
         if (ordering == ORC_ORDER_NATURAL) {
             for (int64_t i = 0; i < A.n; ++i) perm[i] = iperm[i] = i;
+        } else if (ordering == ORC_ORDER_COLOURS) {
+            int64_t k = 0;
+            for (int color = 0; color < 8; ++color)
+                for (int64_t c = 0; c < A.n; ++c)
+                    if (colourOf[c] == color) { perm[k] = c; iperm[c] = k; ++k; }
         } else {
             int64_t k = 0;
             for (int color = 0; color < 2; ++color)
@@ -1781,10 +1787,10 @@ void orc_vcfv_get_jacobian_bcrs(const orc_vcfv* o, int32_t* rp, int32_t* ci, dou
     if (b) std::memcpy(b, C.blocks.data(), sizeof(double) * C.blocks.size());
 }
 
-// NewtonMethod::apply at a fixed time-step size with BiCGStab and the block ILU(0) (natural order)
-// or block Jacobi preconditioner of so->precond
+// NewtonMethod::apply at a fixed time-step size with BiCGStab and the block ILU(0) (natural order,
+// or the parity-colour order of the device) or block Jacobi preconditioner of so->precond
 int orc_vcfv_newton_apply(orc_vcfv* o, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
-                          int* newtonIts, int* linIts, double* errorOut) {
+                          int ordering, int* newtonIts, int* linIts, double* errorOut) {
     VCtx& C = o->C;
     static const Ctx kNoGrid{};
     int numIterations = 0, linTotal = 0;
@@ -1806,7 +1812,14 @@ int orc_vcfv_newton_apply(orc_vcfv* o, double dt, const ewg_newton_opts* no, con
             if (error > no->newton_max_error) throw std::runtime_error("Newton: error above NewtonMaxError");
             if (!proceed()) { ++numIterations; break; }
             Bcrs A = vcfvMatrix(C);
-            Precond M; M.kind = so->precond; M.ordering = ORC_ORDER_NATURAL; M.w = so->preconditioner_relaxation;
+            Precond M; M.kind = so->precond; M.ordering = ordering; M.w = so->preconditioner_relaxation;
+            if (ordering == ORC_ORDER_COLOURS) {
+                M.colourOf.resize(C.NV);
+                for (int64_t v = 0; v < C.NV; ++v) {
+                    int64_t id[3]; C.vijk(v, id);
+                    M.colourOf[v] = (int8_t)((id[0] & 1) + 2 * (id[1] & 1) + 4 * (id[2] & 1));
+                }
+            }
             M.setup(kNoGrid, A);
             Criterion crit{so->linear_solver_tolerance, so->linear_solver_abs_tolerance, so->linear_solver_max_error};
             std::vector<double> dx;

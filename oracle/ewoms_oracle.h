@@ -28,6 +28,8 @@ typedef struct orc_ctx orc_ctx;
 /* ordering of the block ILU(0) factorisation */
 #define ORC_ORDER_NATURAL 0   /* dune-istl SeqILU on the lexicographic YaspGrid order */
 #define ORC_ORDER_REDBLACK 1  /* same factorisation on the red-black permuted matrix */
+#define ORC_ORDER_COLOURS 2   /* vertex-centred grids: vertices ordered by the parity colour
+                                 (i&1) + 2 (j&1) + 4 (k&1), then lexicographically */
 
 orc_ctx* orc_create(const ewg_grid* grid, const ewg_problem* problem, const double* perm,
                     int nthreads);
@@ -95,7 +97,7 @@ int orc_vcfv_linearize(orc_vcfv* c, double dt, int newton_iteration, double* err
 void orc_vcfv_get_residual(const orc_vcfv* c, double* r);
 void orc_vcfv_get_jacobian_bcrs(const orc_vcfv* c, int32_t* row_ptr, int32_t* col_idx, double* blocks);
 int orc_vcfv_newton_apply(orc_vcfv* c, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,
-                          int* newton_iterations, int* linear_iterations, double* error);
+                          int ordering, int* newton_iterations, int* linear_iterations, double* error);
 void orc_vcfv_global_storage(const orc_vcfv* c, int time_idx, double* out2);
 void orc_vcfv_boundary_rates(orc_vcfv* c, double* out2);
 void orc_vcfv_geometry(const orc_vcfv* c, int32_t* ij, double* ip, double* nrm, double* area, double* G,

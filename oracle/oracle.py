@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "liboracle.so")
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "ewoms-numerics_b200"))
 import ewg  # noqa: E402  (ABI structs only)
 
-ORDER_NATURAL, ORDER_REDBLACK = 0, 1
+ORDER_NATURAL, ORDER_REDBLACK, ORDER_COLOURS = 0, 1, 2
 
 
 def build(force=False):
@@ -88,7 +88,7 @@ def load():
         "orc_vcfv_linearize": (C.c_int, [C.c_void_p, d, C.c_int, P(d)]),
         "orc_vcfv_get_residual": (None, [C.c_void_p, P(d)]),
         "orc_vcfv_get_jacobian_bcrs": (None, [C.c_void_p, P(i32), P(i32), P(d)]),
-        "orc_vcfv_newton_apply": (C.c_int, [C.c_void_p, d, P(ewg.NewtonOpts), P(ewg.SolveOpts),
+        "orc_vcfv_newton_apply": (C.c_int, [C.c_void_p, d, P(ewg.NewtonOpts), P(ewg.SolveOpts), C.c_int,
                                             P(C.c_int), P(C.c_int), P(d)]),
         "orc_vcfv_global_storage": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_vcfv_boundary_rates": (None, [C.c_void_p, P(d)]),
@@ -330,11 +330,11 @@ class VcfvOracle:
         self.lib.orc_vcfv_get_jacobian_bcrs(self.h, _p(rp, C.c_int32), _p(ci, C.c_int32), _p(b))
         return rp, ci, b
 
-    def newton_apply(self, dt, nopts=None, sopts=None):
+    def newton_apply(self, dt, nopts=None, sopts=None, ordering=ORDER_NATURAL):
         nopts = nopts or ewg.default_newton_opts()
         sopts = sopts or ewg.default_solve_opts()
         its, lin, err = C.c_int(), C.c_int(), C.c_double()
-        st = self.lib.orc_vcfv_newton_apply(self.h, dt, C.byref(nopts), C.byref(sopts), C.byref(its),
+        st = self.lib.orc_vcfv_newton_apply(self.h, dt, C.byref(nopts), C.byref(sopts), ordering, C.byref(its),
                                             C.byref(lin), C.byref(err))
         return st, its.value, lin.value, err.value
 

@@ -133,9 +133,9 @@ def test_driver_fd_linearizer_runs(driver, tmp_path):
     assert len([ln for ln in out.stdout.splitlines() if ln.startswith("Time step")]) == 2
 
 
-def test_driver_vcfv_needs_jacobi(driver):
-    out = subprocess.run([driver, "--discretization=vcfv", "--preconditioner=ilu0"], capture_output=True, text=True)
-    assert out.returncode == 2 and "jacobi" in out.stderr
+def test_driver_rejects_unknown_discretization(driver):
+    out = subprocess.run([driver, "--discretization=box"], capture_output=True, text=True)
+    assert out.returncode == 2 and "Discretization" in out.stderr
 
 
 @pytest.mark.gpu

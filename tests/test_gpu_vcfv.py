@@ -148,3 +148,28 @@ def test_vcfv_fd_newton_matches_oracle(ewg_mod, oracle_mod):
         o.advance_time_level()
         g.advance_time_level()
     g.close()
+
+
+@pytest.mark.parametrize("name", ["baseline_2d", "lens3d_small", "lens3d_odd"])
+def test_vcfv_ilu_newton_matches_oracle(ewg_mod, oracle_mod, name):
+    """Newton with BiCGStab + block ILU(0) in the parity-colour order (the device's) against the
+    oracle's bilu0 on the same permuted matrix: same Newton iteration counts, same states."""
+    case = _cases(ewg_mod)[name]
+    so = ewg_mod.default_solve_opts(precond=ewg_mod.PRECOND_ILU0, linear_solver_tolerance=1e-10,
+                                    linear_solver_max_iterations=5000)
+    o = oracle_mod.VcfvOracle(case)
+    o.apply_initial_solution()
+    g = ewg_mod.VcfvContext(case)
+    g.apply_initial_solution()
+    for step in range(3):
+        st_o, its_o, lin_o, _ = o.newton_apply(250.0, None, so, oracle_mod.ORDER_COLOURS)
+        st_g, its_g, lin_g, _ = g.newton_apply(250.0, None, so)
+        assert st_o == 0 and st_g == 0, (st_o, st_g)
+        assert its_g == its_o, (step, its_g, its_o)
+        assert abs(lin_g - lin_o) <= max(2, 0.1 * lin_o), (step, lin_g, lin_o)
+        xo, xg = o.get_solution(0), g.get_solution(0)
+        assert np.max(np.abs(xg[:, 0] - xo[:, 0])) <= 1e-9 * np.max(np.abs(xo[:, 0]))
+        assert np.max(np.abs(xg[:, 1] - xo[:, 1])) <= 1e-9
+        o.advance_time_level()
+        g.advance_time_level()
+    g.close()
