@@ -257,6 +257,29 @@ def cpu_sample_run(nx, ny, nz, steps, seed=0):
     return case.n_cells, el, cores, its
 
 
+def cpu_vcfv_linearization(n=32, seed=0):
+    """The oracle's vertex-centred linearization on an n^3-element sample of the 3D lens problem
+    at the bench's drained-top state: the element loop runs on one thread (its scatter into shared
+    vertex rows is what the reference serialises with its linearization lock)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ewg
+    import oracle
+    oracle.build()
+    case = ewg.vcfv_case(ewg.lens3d_case(n, n, n, seed=seed), seed=seed)
+    o = oracle.VcfvOracle(case, nthreads=os.cpu_count() or 1)
+    o.apply_initial_solution()
+    x = o.get_solution(0)
+    rng = np.random.default_rng(seed)
+    top = ewg.vertex_positions(case.grid)[1] > 0.8 * case.grid.ly
+    x[top, 1] = 1.0 - rng.uniform(0.0, 0.4, int(top.sum()))
+    o.set_solution(0, x)
+    t0 = time.perf_counter()
+    o.linearize(250.0, 1)
+    el = time.perf_counter() - t0
+    return {"mvertices_per_s": o.n / el / 1e6, "s_per_linearization": el, "cores": 1,
+            "sample": f"oracle vertex-centred AD linearization, {n}^3 elements ({o.n} vertices)"}
+
+
 def cpu_baseline_block(nx=64, ny=64, nz=32):
     n, el, cores, its = cpu_sample_run(nx, ny, nz, 1)
     return {"value": n / el / 1e6, "unit": "Mcells/s", "cores": cores, "kind": "port",
@@ -264,7 +287,7 @@ def cpu_baseline_block(nx=64, ny=64, nz=32):
                       f"and BiCGStab sequential) on a {nx}x{ny}x{nz} sub-grid of the same 3D lens "
                       f"problem, first implicit step (Newton {its[0][0]} its, BiCGStab {its[0][1]} its): "
                       f"{el:.2f} s for {n} cells",
-            "s_per_step": el}
+            "s_per_step": el, "vcfv_linearization": cpu_vcfv_linearization()}
 
 
 # ---------------------------------------------------------------------------------------------
