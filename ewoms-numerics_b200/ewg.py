@@ -265,7 +265,9 @@ def gaussian_log_field(shape, sigma=1.0, corr_cells=8.0, seed=0) -> np.ndarray:
     noise = rng.standard_normal(shape)
     f = np.fft.irfftn(np.fft.rfftn(noise, axes=axes) * np.sqrt(spec), s=shape, axes=axes)
     f -= f.mean()
-    f *= sigma / f.std()
+    sd = f.std()
+    if sd > 0:  # a one-cell field has no variation to scale
+        f *= sigma / sd
     return f
 
 
@@ -329,8 +331,9 @@ def vcfv_case(case: LensCase, seed: int | None = None, sigma: float = 1.0, corr_
         lnk = np.log(9.05e-12) + f
         perm = np.exp(np.where(lens, lnk + np.log(0.1), lnk))
     else:
-        k_lens = float(case.perm[in_lens(g, p)][0])
-        k_out = float(case.perm[~in_lens(g, p)][0])
+        # (K in the lens, K outside) of the 2D presets
+        k_lens, k_out = {"reference": (9.05e-12, 4.6e-10), "baseline": (9.05e-13, 9.05e-12),
+                         "brooks_corey": (9.05e-13, 9.05e-12)}[case.name]
         perm = np.where(lens, k_lens, k_out)
     return LensCase("vcfv_" + case.name, g, p, np.ascontiguousarray(perm, dtype=np.float64), case.dt, case.n_steps)
 

@@ -95,3 +95,24 @@ def test_ensemble_without_device_or_bad_grid_fails_loudly(lib):
         with pytest.raises(ewg.EwgError) as ei:
             ewg.Ensemble([ewg.lens3d_case(8, 4, 4, seed=0)])
         assert ei.value.status == 7
+
+
+def test_vcfv_bad_arguments_and_no_device_fail_loudly(lib):
+    """The vertex-centred context rejects an empty grid with EWG_ERR_INVALID before touching a
+    device and, without a usable B200, reports EWG_ERR_NO_DEVICE instead of running on the CPU;
+    its calls reject a null context."""
+    import ctypes as C
+    import ewg
+    import torch
+    case = ewg.vcfv_case(ewg.baseline_case(4, 4))
+    case.grid.nx = 0
+    with pytest.raises(ewg.EwgError) as ei:
+        ewg.VcfvContext(case)
+    assert ei.value.status == 1
+    e = C.c_double()
+    assert lib.ewg_vcfv_linearize(None, 250.0, C.byref(e)) == 1
+    assert lib.ewg_vcfv_set_local_linearizer(None, 1, 1) == 1
+    if not torch.cuda.is_available():
+        with pytest.raises(ewg.EwgError) as ei:
+            ewg.VcfvContext(ewg.vcfv_case(ewg.baseline_case(4, 4)))
+        assert ei.value.status == 7

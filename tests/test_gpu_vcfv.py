@@ -173,3 +173,35 @@ def test_vcfv_ilu_newton_matches_oracle(ewg_mod, oracle_mod, name):
         o.advance_time_level()
         g.advance_time_level()
     g.close()
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (2, 1), (1, 1, 1), (2, 1, 3)])
+def test_vcfv_minimal_grids_match_oracle(ewg_mod, oracle_mod, shape):
+    """Grids of one or a few elements: every vertex is a corner or edge vertex, every element
+    touches the boundary on most faces."""
+    if len(shape) == 2:
+        base = ewg_mod.baseline_case(*shape)
+    else:
+        base = ewg_mod.lens3d_case(*shape, seed=3)
+    case = ewg_mod.vcfv_case(base)
+    o = oracle_mod.VcfvOracle(case)
+    o.apply_initial_solution()
+    x1 = o.get_solution(0)
+    x0 = x1.copy()
+    x0[:, 1] = np.linspace(0.6, 1.0, len(x0))
+    o.set_solution(1, x1); o.set_solution(0, x1); o.linearize(250.0, 0)
+    o.set_solution(0, x0); e_ref = o.linearize(250.0, 1)
+    rp, ci, b_ref = o.jacobian_bcrs()
+    g = ewg_mod.VcfvContext(case)
+    g.set_solution(1, x1)
+    g.set_solution(0, x0)
+    e = g.linearize(250.0)
+    ok, err, s = rel_close(g.residual(), o.residual(), RTOL)
+    assert ok, (err, s)
+    _, _, b = g.jacobian_bcrs()
+    for row in range(o.n):
+        blk = slice(rp[row], rp[row + 1])
+        ok, err, s = rel_close(b[blk], b_ref[blk], RTOL)
+        assert ok, (row, err, s)
+    assert abs(e - e_ref) <= RTOL * e_ref
+    g.close()
