@@ -870,7 +870,13 @@ __global__ void kv_ilu_factor(VDims D, VColour C, int c, const double* __restric
     }
 }
 
-// forward sweep of colour c: y_v = d_v - sum over lower colours L_vk y_k
+// colour flip of the neighbour at band b: bit a set when the offset along axis a is odd
+template <int DIM>
+__host__ __device__ constexpr int band_flip(int b) {
+    return ((b % 3) != 1) | (((b / 3) % 3 != 1) << 1) | ((DIM == 3 && b / 9 != 1) << 2);
+}
+
+// forward sweep of colour c: y_v = d_v - sum over lower colours L_vk y_k (bands in index order)
 template <int DIM>
 __global__ void kv_ilu_fwd(VDims D, VColour C, int c, const double* __restrict__ M, const double* __restrict__ d,
                            double* __restrict__ y) {
@@ -880,15 +886,15 @@ __global__ void kv_ilu_fwd(VDims D, VColour C, int c, const double* __restrict__
         int i, j, k;
         const int v = v_of_colour(D, C, t, i, j, k);
         double r0 = d[2 * (int64_t)v], r1 = d[2 * (int64_t)v + 1];
-        for (int kc = 0; kc < c; ++kc)
-            for (int b = 0; b < NB; ++b) {
-                if (band_colour<DIM>(c, b) != kc || !band_in_grid<DIM>(D, i, j, k, b)) continue;
-                const int kv = v + band_offset<DIM>(D, b);
-                const double x0 = y[2 * (int64_t)kv], x1 = y[2 * (int64_t)kv + 1];
-                const double* L = M + (int64_t)b * 4 * NV + v;
-                r0 -= L[0] * x0 + L[NV] * x1;
-                r1 -= L[2 * NV] * x0 + L[3 * NV] * x1;
-            }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            if ((c ^ band_flip<DIM>(b)) >= c || !band_in_grid<DIM>(D, i, j, k, b)) continue;
+            const int kv = v + band_offset<DIM>(D, b);
+            const double x0 = y[2 * (int64_t)kv], x1 = y[2 * (int64_t)kv + 1];
+            const double* L = M + (int64_t)b * 4 * NV + v;
+            r0 -= L[0] * x0 + L[NV] * x1;
+            r1 -= L[2 * NV] * x0 + L[3 * NV] * x1;
+        }
         y[2 * (int64_t)v] = r0;
         y[2 * (int64_t)v + 1] = r1;
     }
@@ -896,7 +902,7 @@ __global__ void kv_ilu_fwd(VDims D, VColour C, int c, const double* __restrict__
 
 // backward sweep of colour c (in place): z_v = inv(U_vv) (y_v - sum over higher colours U_vj z_j)
 template <int DIM>
-__global__ void kv_ilu_bwd(VDims D, VColour C, int c, int ncol, const double* __restrict__ M, double* __restrict__ z) {
+__global__ void kv_ilu_bwd(VDims D, VColour C, int c, const double* __restrict__ M, double* __restrict__ z) {
     constexpr int NB = DIM == 3 ? 27 : 9;
     constexpr int CB = DIM == 3 ? 13 : 4;
     const int64_t NV = D.NV;
@@ -904,15 +910,15 @@ __global__ void kv_ilu_bwd(VDims D, VColour C, int c, int ncol, const double* __
         int i, j, k;
         const int v = v_of_colour(D, C, t, i, j, k);
         double r0 = z[2 * (int64_t)v], r1 = z[2 * (int64_t)v + 1];
-        for (int jc = ncol - 1; jc > c; --jc)
-            for (int b = NB - 1; b >= 0; --b) {
-                if (band_colour<DIM>(c, b) != jc || !band_in_grid<DIM>(D, i, j, k, b)) continue;
-                const int jv = v + band_offset<DIM>(D, b);
-                const double x0 = z[2 * (int64_t)jv], x1 = z[2 * (int64_t)jv + 1];
-                const double* U = M + (int64_t)b * 4 * NV + v;
-                r0 -= U[0] * x0 + U[NV] * x1;
-                r1 -= U[2 * NV] * x0 + U[3 * NV] * x1;
-            }
+#pragma unroll
+        for (int b = NB - 1; b >= 0; --b) {
+            if ((c ^ band_flip<DIM>(b)) <= c || !band_in_grid<DIM>(D, i, j, k, b)) continue;
+            const int jv = v + band_offset<DIM>(D, b);
+            const double x0 = z[2 * (int64_t)jv], x1 = z[2 * (int64_t)jv + 1];
+            const double* U = M + (int64_t)b * 4 * NV + v;
+            r0 -= U[0] * x0 + U[NV] * x1;
+            r1 -= U[2 * NV] * x0 + U[3 * NV] * x1;
+        }
         const double* Di = M + (int64_t)CB * 4 * NV + v;
         z[2 * (int64_t)v] = Di[0] * r0 + Di[NV] * r1;
         z[2 * (int64_t)v + 1] = Di[2 * NV] * r0 + Di[3 * NV] * r1;
@@ -1099,8 +1105,8 @@ ewg_status v_prec(ewg_vcfv* c, double w, const double* d, double* out) {
         for (int col = nc - 1; col >= 0; --col) {
             const VColour C = v_colour(c, col);
             if (C.count == 0) continue;
-            if (c->P.dim == 3) kv_ilu_bwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, nc, c->M, out);
-            else kv_ilu_bwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, nc, c->M, out);
+            if (c->P.dim == 3) kv_ilu_bwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
+            else kv_ilu_bwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
             ewg_status st = vcheck(c, "kv_ilu_bwd");
             if (st) return st;
         }
