@@ -1484,6 +1484,24 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
     return EWG_ERR_NOT_CONVERGED;
 }
 
+// ParallelBaseBackend::solve (parallelbasebackend.hh:301-338) on the last linearization: the
+// update dx with J dx = r (dx_out nullable: the update stays on the device)
+ewg_status ewg_vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, double* dx_out, int32_t* iterations) {
+    if (!c || !so) return EWG_ERR_INVALID;
+    if (so->precond != EWG_PRECOND_JACOBI && so->precond != EWG_PRECOND_ILU0) { c->err = "unknown preconditioner"; return EWG_ERR_INVALID; }
+    if (so->precision != EWG_PRECISION_FP64) { c->err = "the vertex-centred solve is FP64"; return EWG_ERR_INVALID; }
+    int it = 0;
+    ewg_status st = vcfv_solve(c, so, &it);
+    if (iterations) *iterations = it;
+    if (st) return st;
+    if (dx_out) {
+        cudaError_t e = cudaMemcpyAsync(dx_out, c->s_x, sizeof(double2) * c->D.NV, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        return vfail(c, e, "get update");
+    }
+    return EWG_OK;
+}
+
 // NewtonMethod::apply at fixed dt (newtonmethod.hh:308-517): linearize, convergence test on the
 // residual max-norm before the solve, BiCGStab + block Jacobi, x -= dx
 ewg_status ewg_vcfv_newton_apply(ewg_vcfv* c, double dt, const ewg_newton_opts* no, const ewg_solve_opts* so,

@@ -409,6 +409,7 @@ def load(path: str = LIB_PATH):
         "ewg_vcfv_linearize": (C.c_int, [C.c_void_p, d, P(d)]),
         "ewg_vcfv_get_residual": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_vcfv_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), C.c_int64, P(d)]),
+        "ewg_vcfv_solve": (C.c_int, [C.c_void_p, P(SolveOpts), P(d), P(C.c_int32)]),
         "ewg_vcfv_newton_apply": (C.c_int, [C.c_void_p, d, P(NewtonOpts), P(SolveOpts), P(C.c_int32),
                                             P(C.c_int32), P(d)]),
         "ewg_net_num_params": (C.c_int64, []),
@@ -870,6 +871,14 @@ class VcfvContext:
         self._check(self.lib.ewg_vcfv_get_jacobian_bcrs(self.h, _ptr(rp, C.c_int32), _ptr(ci, C.c_int32), len(ci),
                                                         _ptr(b)), "get_jacobian_bcrs")
         return rp, ci, b
+
+    def solve(self, sopts=None):
+        """BiCGStab on the last linearization: (status, iterations, dx)."""
+        sopts = sopts or default_solve_opts()
+        dx = self.vec()
+        its = C.c_int32()
+        st = self.lib.ewg_vcfv_solve(self.h, C.byref(sopts), _ptr(dx), C.byref(its))
+        return st, its.value, dx
 
     def newton_apply(self, dt, nopts=None, sopts=None):
         nopts = nopts or default_newton_opts()

@@ -110,6 +110,23 @@ public:
     void setLocalLinearizer(int kind, int method) {
         check(ewg_vcfv_set_local_linearizer(c_, kind, method), "ewg_vcfv_set_local_linearizer");
     }
+    void setSolution(int timeIdx, const double* x) { check(ewg_vcfv_set_solution(c_, timeIdx, x), "ewg_vcfv_set_solution"); }
+    double linearize(double dt) {
+        double err = 0;
+        check(ewg_vcfv_linearize(c_, dt, &err), "ewg_vcfv_linearize");
+        return err;
+    }
+    void getResidual(double* r) { check(ewg_vcfv_get_residual(c_, r), "ewg_vcfv_get_residual"); }
+    void getJacobianBcrs(const int32_t* rowPtr, const int32_t* colIdx, int64_t nnzb, double* blocks) {
+        check(ewg_vcfv_get_jacobian_bcrs(c_, rowPtr, colIdx, nnzb, blocks), "ewg_vcfv_get_jacobian_bcrs");
+    }
+    // returns the status (EWG_ERR_NOT_CONVERGED / EWG_ERR_BREAKDOWN are the caller's to map)
+    ewg_status solve(const ewg_solve_opts& so, double* dx, int* iterations) {
+        int32_t it = 0;
+        ewg_status st = ewg_vcfv_solve(c_, &so, dx, &it);
+        if (iterations) *iterations = it;
+        return st;
+    }
     // NewtonMethod::apply; returns the status (non-zero: the caller halves the step)
     ewg_status newtonApply(double dt, const ewg_newton_opts& no, const ewg_solve_opts& so, int* its, int* linIts) {
         int32_t a = 0, b = 0;

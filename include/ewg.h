@@ -452,6 +452,10 @@ ewg_status ewg_vcfv_get_residual(ewg_vcfv* c, double* r);
  * vertices of its adjacent elements, columns ascending). */
 ewg_status ewg_vcfv_get_jacobian_bcrs(ewg_vcfv* c, const int32_t* row_ptr, const int32_t* col_idx, int64_t nnzb,
                                       double* blocks);
+/* ParallelBaseBackend::solve on the last ewg_vcfv_linearize: BiCGStab for J dx = r with the
+ * preconditioner of sopts (as below); dx_out (nullable) receives the update, natural vertex order.
+ * EWG_ERR_NOT_CONVERGED when BiCGStab fails, EWG_ERR_BREAKDOWN on breakdown. */
+ewg_status ewg_vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* sopts, double* dx_out, int32_t* iterations);
 /* NewtonMethod::apply at fixed dt with BiCGStab + block ILU(0) (EWG_PRECOND_ILU0: dune-istl's
  * bilu0 on the matrix ordered by the vertices' parity colour (i&1) + 2 (j&1) + 4 (k&1), then
  * lexicographically) or block Jacobi; FP64 only. */

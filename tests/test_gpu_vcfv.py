@@ -205,3 +205,29 @@ def test_vcfv_minimal_grids_match_oracle(ewg_mod, oracle_mod, shape):
         assert ok, (row, err, s)
     assert abs(e - e_ref) <= RTOL * e_ref
     g.close()
+
+
+@pytest.mark.parametrize("precond", ["ilu0", "jacobi"])
+def test_vcfv_solve_entry_point(ewg_mod, oracle_mod, precond):
+    """ewg_vcfv_solve (the LinearSolverBackend::solve contract): after a linearization, the update
+    it returns satisfies J dx = r to the requested relative tolerance, checked with the exported
+    BCRS Jacobian."""
+    case = _cases(ewg_mod)["lens3d_small"]
+    _, x1, x0 = _states(oracle_mod, case)
+    g = ewg_mod.VcfvContext(case)
+    g.set_solution(1, x1)
+    g.set_solution(0, x0)
+    g.linearize(250.0)
+    r = g.residual().ravel()
+    rp, ci, b = g.jacobian_bcrs()
+    pc = ewg_mod.PRECOND_ILU0 if precond == "ilu0" else ewg_mod.PRECOND_JACOBI
+    so = ewg_mod.default_solve_opts(precond=pc, linear_solver_tolerance=1e-10, linear_solver_max_iterations=5000)
+    st, its, dx = g.solve(so)
+    assert st == 0 and its > 0
+    dxf = dx.ravel()
+    Jdx = np.zeros_like(r)
+    for row in range(g.n):
+        for q in range(rp[row], rp[row + 1]):
+            Jdx[2 * row:2 * row + 2] += b[q] @ dxf[2 * ci[q]:2 * ci[q] + 2]
+    assert np.max(np.abs(Jdx - r)) <= 1e-8 * np.max(np.abs(r))
+    g.close()
