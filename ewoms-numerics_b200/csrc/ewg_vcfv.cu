@@ -469,6 +469,11 @@ struct VcfvElemState {
     double pw[1 << DIM], pn[1 << DIM], lw[1 << DIM], ln[1 << DIM];
     double SwA;
 };
+// p_c, lambda_w, lambda_n at the primary variables (a pressure deflection keeps them)
+template <int DIM>
+struct VcfvElemIq {
+    double pc[1 << DIM];
+};
 
 // local residual entry of vertex A (compile time) in the element, scaled by 1 / control volume
 template <int DIM, int A>
@@ -567,6 +572,7 @@ __device__ __forceinline__ void vcfv_element_fd(const Phys& P, const VDims& D, c
         return v + dx + sy * dy + sz * dz;
     };
     VcfvElemState<DIM> base;
+    VcfvElemIq<DIM> biq;
     double Sw[NV];
 #pragma unroll
     for (int w = 0; w < NV; ++w) {
@@ -576,6 +582,7 @@ __device__ __forceinline__ void vcfv_element_fd(const Phys& P, const VDims& D, c
         base.pn[w] = xw.x + (iq[g] - 0.0);
         base.lw[w] = iq[2 * NVt + g];
         base.ln[w] = iq[4 * NVt + g];
+        biq.pc[w] = iq[g];
         Sw[w] = xw.y;
     }
     base.SwA = Sw[A];
@@ -606,11 +613,16 @@ __device__ __forceinline__ void vcfv_element_fd(const Phys& P, const VDims& D, c
             // w's state at deflected primary variables
             auto deflected = [&](double R[2]) {
                 VcfvElemState<DIM> st = base;
-                const IqVals o = intensive_values(P, pri[1], lw_);
                 st.pw[w] = pri[0];
-                st.pn[w] = pri[0] + (o.pc - 0.0);
-                st.lw[w] = o.lw;
-                st.ln[w] = o.ln;
+                if (pv == 0) {
+                    // the intensive quantities depend on S_w only: those of the primary variables
+                    st.pn[w] = pri[0] + (biq.pc[w] - 0.0);
+                } else {
+                    const IqVals o = intensive_values(P, pri[1], lw_);
+                    st.pn[w] = pri[0] + (o.pc - 0.0);
+                    st.lw[w] = o.lw;
+                    st.ln[w] = o.ln;
+                }
                 if (w == A) st.SwA = pri[1];
                 vcfv_local_value<DIM, A>(P, D, geo, kedge, cst, invV, v, eidx, st, so, KA, liA, R);
             };
