@@ -284,6 +284,8 @@ __device__ __forceinline__ void fd_local_residual(const Phys& P, int col, int64_
     R[1] /= P.vol;
 }
 
+// (a pressure deflection keeps the intensive quantities of the primary variables, which the
+// callers take from the cache: the same values)
 template <int DIM>
 __device__ __forceinline__ FdState fd_state(const Phys& P, const LawDev& L, double pw, double Sw) {
     const MatOut m = material(L, Sw);
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble_fd(
             if (method >= 0) {
                 pri[pv] += eps;
                 delta += eps;
-                fd_local_residual<DIM>(P, col, h, ci, fd_state<DIM>(P, P.law[li], pri[0], pri[1]), Ki, li, so, dt, x,
+                fd_local_residual<DIM>(P, col, h, ci, (pv == 0 ? FdState{pri[0], pri[1], base.pc, base.lw, base.ln} : fd_state<DIM>(P, P.law[li], pri[0], pri[1])), Ki, li, so, dt, x,
                                        perm, iq, Rp, Fp);
                 dR[0] = Rp[0]; dR[1] = Rp[1];
                 for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] = Fp[q][0]; dF[q][1] = Fp[q][1]; }
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble_fd(
             if (method <= 0) {
                 pri[pv] -= delta + eps;
                 delta += eps;
-                fd_local_residual<DIM>(P, col, h, ci, fd_state<DIM>(P, P.law[li], pri[0], pri[1]), Ki, li, so, dt, x,
+                fd_local_residual<DIM>(P, col, h, ci, (pv == 0 ? FdState{pri[0], pri[1], base.pc, base.lw, base.ln} : fd_state<DIM>(P, P.law[li], pri[0], pri[1])), Ki, li, so, dt, x,
                                        perm, iq, Rp, Fp);
                 dR[0] -= Rp[0]; dR[1] -= Rp[1];
                 for (int q = 0; q < 2 * DIM; ++q) { dF[q][0] -= Fp[q][0]; dF[q][1] -= Fp[q][1]; }
