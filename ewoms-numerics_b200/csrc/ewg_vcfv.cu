@@ -27,6 +27,7 @@
 // Jacobian storage: band-major, band (dx+1) + 3 (dy+1) [+ 9 (dz+1)] for the neighbour at vertex
 // offset (dx, dy, dz), 4 planes per band ([eq][pv]), each plane NV doubles.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1341,6 +1342,21 @@ ewg_status ewg_vcfv_get_residual(ewg_vcfv* c, double* r) {
 ewg_status ewg_vcfv_get_jacobian_bcrs(ewg_vcfv* c, const int32_t* rowPtr, const int32_t* colIdx, int64_t nnzb,
                                       double* blocks) {
     if (!c || !rowPtr || !colIdx || !blocks) return EWG_ERR_INVALID;
+    // every block must be a stored band: the column a vertex of the row's 3x3(x3) neighbourhood
+    if (rowPtr[0] != 0 || rowPtr[c->D.NV] != nnzb) { c->err = "row pointers do not span nnzb blocks"; return EWG_ERR_INVALID; }
+    for (int v = 0; v < c->D.NV; ++v) {
+        if (rowPtr[v + 1] < rowPtr[v]) { c->err = "row pointers decrease"; return EWG_ERR_INVALID; }
+        const int i = v % c->D.nvx, j = (v / c->D.nvx) % c->D.nvy, k = v / (c->D.nvx * c->D.nvy);
+        for (int32_t q = rowPtr[v]; q < rowPtr[v + 1]; ++q) {
+            const int col = colIdx[q];
+            if (col < 0 || col >= c->D.NV) { c->err = "column index out of range"; return EWG_ERR_INVALID; }
+            const int ci = col % c->D.nvx, cj = (col / c->D.nvx) % c->D.nvy, ck = col / (c->D.nvx * c->D.nvy);
+            if (std::abs(ci - i) > 1 || std::abs(cj - j) > 1 || std::abs(ck - k) > 1) {
+                c->err = "the pattern holds a block outside the vertex stencil";
+                return EWG_ERR_INVALID;
+            }
+        }
+    }
     int32_t *dr = nullptr, *dc = nullptr;
     double* db = nullptr;
     cudaError_t e = cudaMalloc(&dr, sizeof(int32_t) * (c->D.NV + 1));

@@ -231,3 +231,21 @@ def test_vcfv_solve_entry_point(ewg_mod, oracle_mod, precond):
             Jdx[2 * row:2 * row + 2] += b[q] @ dxf[2 * ci[q]:2 * ci[q] + 2]
     assert np.max(np.abs(Jdx - r)) <= 1e-8 * np.max(np.abs(r))
     g.close()
+
+
+def test_vcfv_jacobian_export_rejects_foreign_pattern(ewg_mod):
+    """A BCRS pattern with a block outside the vertex stencil is an error, not a read of a band the
+    device does not store."""
+    import ctypes as C
+    case = ewg_mod.vcfv_case(ewg_mod.baseline_case(6, 4))
+    g = ewg_mod.VcfvContext(case)
+    g.apply_initial_solution()
+    g.linearize(250.0)
+    rp, ci = ewg_mod.vcfv_pattern(case.grid)
+    bad = ci.copy()
+    bad[0] = g.n - 1  # row 0 coupled to the far corner
+    blocks = np.zeros((len(ci), 2, 2))
+    st = g.lib.ewg_vcfv_get_jacobian_bcrs(g.h, ewg_mod._ptr(rp, C.c_int32), ewg_mod._ptr(bad, C.c_int32), len(ci),
+                                          ewg_mod._ptr(blocks))
+    assert st == 1
+    g.close()
