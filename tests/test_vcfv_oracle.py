@@ -155,3 +155,15 @@ def test_vcfv_fd_local_linearizer_matches_ad(oracle_mod, ewg_mod, method):
             for pv in range(2):
                 a, b = J_fd[:, eq, pv], J_ad[:, eq, pv]
                 assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (case.name, eq, pv)
+
+
+def test_vcfv_pattern_matches_oracle(oracle_mod, ewg_mod):
+    """The BCRS pattern callers pass to ewg_vcfv_get_jacobian_bcrs (ewg.vcfv_pattern) is the
+    oracle's createMatrix_ pattern: each vertex row holds the vertices of its adjacent elements,
+    columns ascending."""
+    for case in (ewg_mod.vcfv_case(ewg_mod.baseline_case(5, 3)), ewg_mod.vcfv_case(ewg_mod.lens3d_case(3, 4, 2, seed=0))):
+        o = oracle_mod.VcfvOracle(case)
+        rp, ci, _ = o.jacobian_bcrs()
+        rp2, ci2 = ewg_mod.vcfv_pattern(case.grid)
+        assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2)
+        assert all(np.all(np.diff(ci[rp[r]:rp[r + 1]]) > 0) for r in range(o.n))
