@@ -141,6 +141,7 @@ void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p) {
     P.L[0] = g->lx;
     P.L[1] = g->ly;
     P.L[2] = g->dim == 3 ? g->lz : 1.0;
+    P.kOrigin = g->dim == 3 ? g->k_origin : 0;
     const int n[3] = {P.nx, P.ny, P.nz};
     for (int a = 0; a < 3; ++a) P.h[a] = P.L[a] / n[a];
     if (P.dim == 2) {
@@ -200,7 +201,7 @@ __global__ void k_lens_flags(const __grid_constant__ Phys P, uint8_t* __restrict
         const int idx[3] = {ci.i, ci.j, ci.k};
         bool in = true;
         for (int a = 0; a < P.dim; ++a) {
-            double x = (idx[a] + 0.5) * P.h[a];
+            double x = (idx[a] + (a == 2 ? P.kOrigin : 0) + 0.5) * P.h[a];
             if (x < P.lensLo[a] - P.eps || x > P.lensHi[a] + P.eps) in = false;
         }
         lens[s] = in ? 1 : 0;
@@ -415,6 +416,7 @@ ewg_status ewg_create(const ewg_grid* grid, const ewg_problem* problem, const do
         return EWG_ERR_INVALID;
     }
     if ((int64_t)grid->nx * grid->ny * nz >= (int64_t)1 << 31) { g_createError = "grid too large for int32 BCRS indices"; return EWG_ERR_INVALID; }
+    if (grid->dim == 3 && grid->k_origin < 0) { g_createError = "k_origin must be >= 0"; return EWG_ERR_INVALID; }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
         cudaGetLastError();

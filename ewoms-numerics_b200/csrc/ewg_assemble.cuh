@@ -69,8 +69,9 @@ __device__ __forceinline__ void interior_face(const Phys& P, int side, int idxA,
                                               double2 xj, double Kj, double pcj, const double lamj[2],
                                               double R[2], double D[2][2], double Dj[4]) {
     const double h = P.h[AXIS];
-    const double xc = (idxA + 0.5) * h;
-    const double xcj = (idxA + (side ? 1 : -1) + 0.5) * h;
+    const int ia = idxA + (AXIS == 2 ? P.kOrigin : 0);
+    const double xc = (ia + 0.5) * h;
+    const double xcj = (ia + (side ? 1 : -1) + 0.5) * h;
     const double dA = xcj - xc;
     const double distSq = dA * dA;
     const double coef = dA / distSq;
@@ -86,7 +87,7 @@ __device__ __forceinline__ void interior_face(const Phys& P, int side, int idxA,
         const double dgS = a == 0 ? 0.0 : -dpcI * coef;
         if (AXIS == 1) {
             // gravity correction; for the other axes the hydrostatic terms are exactly zero
-            const double xf = (idxA + side) * h;
+            const double xf = (ia + side) * h;
             const double gIn = -P.g * (xc - xf), gEx = -P.g * (xcj - xf);
             const double rho = P.rho[a];
             const double pStatIn = -rho * gIn;
@@ -122,10 +123,10 @@ __device__ __forceinline__ void boundary_face(const Phys& P, int side, const int
                                               const double dlam[2], double R[2], double D[2][2]) {
     double xc[3], xf[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) xc[d] = d < DIM ? (idx[d] + 0.5) * P.h[d] : 0.0;
+    for (int d = 0; d < 3; ++d) xc[d] = d < DIM ? (idx[d] + (d == 2 ? P.kOrigin : 0) + 0.5) * P.h[d] : 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) xf[d] = xc[d];
-    xf[AXIS] = (idx[AXIS] + side) * P.h[AXIS];
+    xf[AXIS] = (idx[AXIS] + (AXIS == 2 ? P.kOrigin : 0) + side) * P.h[AXIS];
     const double area = P.area[AXIS];
     const bool left = xf[0] < 0.0 + P.eps, right = xf[0] > P.L[0] - P.eps;
     if (left || right) {

@@ -1385,8 +1385,8 @@ ewg_status ewg_ensemble_create(int32_t members, const ewg_grid* grids, const ewg
     int64_t tiles = 0;
     for (int m = 0; m < members; ++m) {
         const ewg_grid& g = grids[m];
-        if (g.dim != 3 || g.nx < 2 || (g.nx & 1) || g.ny < 1 || g.nz < 1 || !perms[m]) {
-            g_ensCreateError = "member " + std::to_string(m) + ": ensembles take 3D grids with even nx >= 2 and a permeability field";
+        if (g.dim != 3 || g.nx < 2 || (g.nx & 1) || g.ny < 1 || g.nz < 1 || g.k_origin != 0 || !perms[m]) {
+            g_ensCreateError = "member " + std::to_string(m) + ": ensembles take whole 3D grids (k_origin 0) with even nx >= 2 and a permeability field";
             return EWG_ERR_INVALID;
         }
         const int64_t n = (int64_t)g.nx * g.ny * g.nz;

@@ -91,6 +91,7 @@ struct Phys {
     FastDiv fdNxh, fdNy;     // divisions by nx / 2 and ny in cell_of (N < 2^31)
     double rhoArea[3][2];    // rho_alpha * face area per axis (mass flux per unit velocity)
     double invVol;           // 1 / cell volume
+    int kOrigin;             // global index of plane 0 (z-slab of a decomposed grid), else 0
 };
 
 // Geometry of one interior face seen from a cell, per (axis, cell index along the axis, side):

@@ -453,8 +453,9 @@ void build_face_geo(const Phys& P, std::vector<FaceGeo>& geo) {
             for (int side = 0; side < 2; ++side) {
                 // the operations of interior_face, in the same order
                 const double h = P.h[axis];
-                const double xc = (idx + 0.5) * h;
-                const double xcj = (idx + (side ? 1 : -1) + 0.5) * h;
+                const int ia = idx + (axis == 2 ? P.kOrigin : 0);
+                const double xc = (ia + 0.5) * h;
+                const double xcj = (ia + (side ? 1 : -1) + 0.5) * h;
                 const double dA = xcj - xc;
                 const double distSq = dA * dA;
                 FaceGeo G;
@@ -462,7 +463,7 @@ void build_face_geo(const Phys& P, std::vector<FaceGeo>& geo) {
                 G.dA = dA;
                 G.gt[0] = G.gt[1] = 0.0;
                 if (axis == 1) {
-                    const double xf = (idx + side) * h;
+                    const double xf = (ia + side) * h;
                     const double gIn = -P.g * (xc - xf), gEx = -P.g * (xcj - xf);
                     for (int a = 0; a < 2; ++a) {
                         const double rho = P.rho[a];

@@ -1143,6 +1143,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
     if (grid->dim != 2 && grid->dim != 3) return EWG_ERR_INVALID;
     const int nz = grid->dim == 3 ? grid->nz : 1;
     if (grid->nx < 1 || grid->ny < 1 || nz < 1) return EWG_ERR_INVALID;
+    if (grid->dim == 3 && grid->k_origin != 0) return EWG_ERR_INVALID;  // whole grids only
     const int64_t nv = (int64_t)(grid->nx + 1) * (grid->ny + 1) * (grid->dim == 3 ? nz + 1 : 1);
     if (nv * (grid->dim == 3 ? 27 : 9) * 4 >= ((int64_t)1 << 40) || nv >= ((int64_t)1 << 31) / 2)
         return EWG_ERR_INVALID;

@@ -36,7 +36,7 @@ LOCAL_LINEARIZER_AD, LOCAL_LINEARIZER_FD = 0, 1
 
 class Grid(C.Structure):
     _fields_ = [("dim", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
-                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double)]
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("k_origin", C.c_int32)]
 
     @property
     def n_cells(self) -> int:

@@ -58,6 +58,10 @@ typedef struct ewg_grid {
     int32_t dim;                /* 2 or 3 */
     int32_t nx, ny, nz;         /* nz is ignored (treated as 1) for dim == 2 */
     double lx, ly, lz;          /* extents [m]; lz ignored for dim == 2 */
+    int32_t k_origin;           /* global index of the first z-plane: 0 for a whole grid; for one
+                                   z-slab of a decomposed 3D grid, its first plane, so that plane k
+                                   sits at z = (k_origin + k + 1/2) lz / nz and the lens and inlet
+                                   boxes keep their global coordinates (cell-centred contexts only) */
 } ewg_grid;
 
 typedef enum ewg_law_kind {

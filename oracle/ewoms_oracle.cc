@@ -266,12 +266,16 @@ struct Ctx {
     void ijk(int64_t c, int64_t& i, int64_t& j, int64_t& k) const {
         i = c % n[0]; j = (c / n[0]) % n[1]; k = c / ((int64_t)n[0] * n[1]);
     }
+    // global plane index of plane 0: a z-slab of a decomposed grid keeps the global coordinates
+    int64_t kOrigin = 0;
     void center(int64_t c, double x[3]) const {
         int64_t id[3]; ijk(c, id[0], id[1], id[2]);
+        id[2] += kOrigin;
         for (int a = 0; a < 3; ++a) x[a] = (a < dim) ? (id[a] + 0.5) * h[a] : 0.0;
     }
     void faceCenter(int64_t c, int axis, int side, double x[3]) const {
         int64_t id[3]; ijk(c, id[0], id[1], id[2]);
+        id[2] += kOrigin;
         center(c, x);
         x[axis] = (id[axis] + side) * h[axis];
     }
@@ -1476,6 +1480,7 @@ orc_ctx* orc_create(const ewg_grid* g, const ewg_problem* p, const double* perm,
     C.n[0] = g->nx; C.n[1] = g->ny; C.n[2] = g->dim == 3 ? g->nz : 1;
     C.L[0] = g->lx; C.L[1] = g->ly; C.L[2] = g->dim == 3 ? g->lz : 1.0;
     for (int a = 0; a < 3; ++a) C.h[a] = C.L[a] / C.n[a];
+    C.kOrigin = g->dim == 3 ? g->k_origin : 0;
     C.N = (int64_t)C.n[0] * C.n[1] * C.n[2];
     C.prob = *p;
     C.law[0] = makeLaw(p->outer);

@@ -1,0 +1,138 @@
+"""Domain decomposition into z-slabs (ewoms-numerics_b200/dd.py), host side: the partition, the
+slab problems (same cell size bit for bit, shifted lens and inlet, permeability planes), and the
+ghost-plane exchange between two and three gloo ranks on CPU."""
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def test_partition_covers_the_grid_once(ewg_mod):
+    import dd
+    for nz, world in [(10, 1), (10, 3), (128, 8), (7, 7)]:
+        slabs = dd.partition(nz, world)
+        assert slabs[0].k0 == 0 and slabs[-1].k1 == nz
+        assert all(a.k1 == b.k0 for a, b in zip(slabs, slabs[1:]))
+        sizes = [s.k1 - s.k0 for s in slabs]
+        assert max(sizes) - min(sizes) <= 1
+        assert slabs[0].ghost_lo == 0 and slabs[-1].ghost_hi == 0
+        assert all(s.ghost_lo == 1 for s in slabs[1:]) and all(s.ghost_hi == 1 for s in slabs[:-1])
+    with pytest.raises(ValueError):
+        dd.partition(3, 4)
+
+
+def test_slab_case_keeps_the_cell_and_the_global_geometry(ewg_mod):
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    hz = case.grid.lz / case.grid.nz
+    for s in dd.partition(10, 3):
+        sc = dd.slab_case(case, s)
+        assert sc.grid.lz / sc.grid.nz == hz
+        assert sc.grid.k_origin == s.first
+        assert list(sc.problem.lens_lo) == list(case.problem.lens_lo)
+        assert sc.problem.inlet_z_hi == case.problem.inlet_z_hi
+        plane = 16 * 12
+        assert np.array_equal(sc.perm, case.perm[s.first * plane:(s.first + s.planes) * plane])
+
+
+def test_local_ghost_exchange(ewg_mod):
+    import dd
+    case = ewg_mod.lens3d_case(8, 6, 9, seed=0)
+    slabs = dd.partition(9, 3)
+    xg = np.arange(case.grid.n_cells * 2, dtype=np.float64).reshape(-1, 2)
+    xs = [dd.local_view(xg, case.grid, s) for s in slabs]
+    want = [x.copy() for x in xs]
+    plane = 8 * 6
+    for s, x in zip(slabs, xs):
+        if s.ghost_lo:
+            x[:plane] = -1
+        if s.ghost_hi:
+            x[-plane:] = -1
+    dd.exchange_ghosts_local(xs, case.grid, slabs)
+    assert all(np.array_equal(a, b) for a, b in zip(xs, want))
+
+
+PROBE = r'''
+import os, sys
+sys.path.insert(0, os.path.join(sys.argv[1], "ewoms-numerics_b200"))
+import numpy as np
+import torch.distributed as dist
+import dd, ewg
+dist.init_process_group("gloo")
+rank, world = dist.get_rank(), dist.get_world_size()
+case = ewg.lens3d_case(8, 6, 11, seed=0)
+slabs = dd.partition(11, world)
+s = slabs[rank]
+xg = np.arange(case.grid.n_cells * 2, dtype=np.float64).reshape(-1, 2) * 0.5
+x = dd.local_view(xg, case.grid, s)
+want = x.copy()
+plane = 8 * 6
+if s.ghost_lo: x[:plane] = np.nan
+if s.ghost_hi: x[-plane:] = np.nan
+dd.exchange_ghosts(x, case.grid, s, dist)
+assert np.array_equal(x, want), rank
+dist.barrier()
+dist.destroy_process_group()
+print(f"rank {rank} ok", flush=True)
+'''
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_ghost_exchange_between_gloo_ranks(tmp_path, world):
+    probe = tmp_path / "probe.py"
+    probe.write_text(PROBE)
+    cmd = ["timeout", "-k", "30", "240", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={world}", "--master-addr=127.0.0.1", f"--master-port={_free_port()}", str(probe), ROOT]
+    out = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT,
+                         env=dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert all(f"rank {r} ok" in out.stdout for r in range(world))
+
+
+@pytest.mark.parametrize("world", [2, 3, 5])
+def test_oracle_slab_rows_equal_the_whole_grid(oracle_mod, ewg_mod, world):
+    """The oracle linearizes each slab (plane origin at its first plane, ghost planes filled) and
+    the owned residual and Jacobian rows equal the whole grid's bit for bit: the decomposition
+    changes no operation of a cell's row."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x1 = o.get_solution(0)
+    rng = np.random.default_rng(4)
+    x0 = x1.copy()
+    x0[:, 0] += rng.normal(0, 20.0, len(x0))
+    x0[:, 1] = np.clip(x0[:, 1] - np.abs(rng.normal(0, 0.3, len(x0))), 0.2, 1.0)
+    o.set_solution(1, x1)
+    o.set_solution(0, x0)
+    o.linearize(250.0)
+    r_g = o.residual()
+    rp_g, ci_g, b_g = o.jacobian_bcrs()
+    plane = 16 * 12
+    for s in dd.partition(10, world):
+        sc = dd.slab_case(case, s)
+        ol = oracle_mod.Oracle(sc)
+        ol.set_solution(1, dd.local_view(x1, case.grid, s))
+        ol.set_solution(0, dd.local_view(x0, case.grid, s))
+        ol.linearize(250.0)
+        own = dd.owned_rows(sc.grid, s)
+        assert np.array_equal(ol.residual()[own], r_g[s.k0 * plane:s.k1 * plane])
+        rp, ci, b = ol.jacobian_bcrs()
+        shift = s.first * plane
+        for lr in range(own.start, own.stop):
+            gr = lr + shift
+            assert np.array_equal(ci[rp[lr]:rp[lr + 1]] + shift, ci_g[rp_g[gr]:rp_g[gr + 1]])
+            assert np.array_equal(b[rp[lr]:rp[lr + 1]], b_g[rp_g[gr]:rp_g[gr + 1]])
+        ol.close()
+    o.close()
