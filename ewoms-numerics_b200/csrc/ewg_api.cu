@@ -764,6 +764,35 @@ ewg_status ewg_apply_jacobian(ewg_ctx* ctx, const double* x, double* y) {
     return st;
 }
 
+// a device pointer of this context's device with room for a 16-byte aligned double2 vector
+static bool device_vector_ok(ewg_ctx* ctx, const void* p) {
+    if (!p || ((uintptr_t)p & 15)) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+    return a.device == ctx->device;
+}
+
+ewg_status ewg_device_buffer(ewg_ctx* ctx, int32_t which, double** out) {
+    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+    if (which == EWG_BUFFER_SOLUTION) { *out = (double*)ctx->x0; return EWG_OK; }
+    if (which == EWG_BUFFER_RESIDUAL) { *out = (double*)ctx->r; return EWG_OK; }
+    return EWG_ERR_INVALID;
+}
+
+ewg_status ewg_device_spmv(ewg_ctx* ctx, const double* x, double* y) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    if (!device_vector_ok(ctx, x) || !device_vector_ok(ctx, y)) { ctx->err = "device_spmv: x and y must be aligned device vectors"; return EWG_ERR_INVALID; }
+    if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "device_spmv needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
+    return solver_spmv(ctx, (const double2*)x, (double2*)y);
+}
+
+ewg_status ewg_device_precondition(ewg_ctx* ctx, const ewg_solve_opts* o, const double* b, double* y) {
+    if (check_ctx(ctx) || !o) return EWG_ERR_INVALID;
+    if (!device_vector_ok(ctx, b) || !device_vector_ok(ctx, y)) { ctx->err = "device_precondition: b and y must be aligned device vectors"; return EWG_ERR_INVALID; }
+    return solver_apply_preconditioner(ctx, o, (const double2*)b, (double2*)y);
+}
+
 ewg_status ewg_newton_update(ewg_ctx* ctx) {
     if (check_ctx(ctx)) return EWG_ERR_INVALID;
     int bad = 0;

@@ -169,3 +169,446 @@ class SlabLinearizer:
 
     def close(self):
         self.ctx.close()
+
+
+# ------------------------------------------------------------------------------------------
+# Distributed solve over the slabs: BiCGStab with restricted additive Schwarz
+
+DBL_BREAKDOWN = 2.2250738585072014e-308 * 1e10  # DBL_MIN * 1e10, the solver's breakdown threshold
+ST_RUNNING, ST_CONVERGED, ST_FAILED, ST_BREAKDOWN, ST_MAXITER = 0, 1, 2, 3, 4
+
+
+class SplitLayout:
+    """Row ranges of a slab's device vectors (the context's red-black storage order: plane k of
+    local colour c is the run c*N/2 + k*nx*ny/2 of nx*ny/2 rows). Plane chunks are listed in
+    GLOBAL colour order, (i + j + k_global) & 1, so that two slabs whose first planes differ in
+    parity still pair the same cells."""
+
+    def __init__(self, grid: ewg.Grid, slab: Slab):
+        plane = grid.nx * grid.ny
+        self.half = grid.n_cells // 2
+        self.planeh = plane // 2
+        self.flip = slab.first & 1
+        self.owned = [slice(c * self.half + slab.ghost_lo * self.planeh,
+                            c * self.half + (slab.ghost_lo + slab.k1 - slab.k0) * self.planeh) for c in (0, 1)]
+
+    def plane(self, k: int) -> list[slice]:
+        out = []
+        for g in (0, 1):
+            s = (g ^ self.flip) * self.half + k * self.planeh
+            out.append(slice(s, s + self.planeh))
+        return out
+
+
+class NaturalLayout:
+    """Row ranges of a slab vector in natural order (k slowest)."""
+
+    def __init__(self, grid: ewg.Grid, slab: Slab):
+        self.planesz = grid.nx * grid.ny
+        self.owned = [slice(slab.ghost_lo * self.planesz, (slab.ghost_lo + slab.k1 - slab.k0) * self.planesz)]
+
+    def plane(self, k: int) -> list[slice]:
+        return [slice(k * self.planesz, (k + 1) * self.planesz)]
+
+
+def _bottom_owned(s: Slab) -> int:
+    return s.ghost_lo
+
+
+def _top_owned(s: Slab) -> int:
+    return s.ghost_lo + s.k1 - s.k0 - 1
+
+
+class LocalComm:
+    """All slabs in this process: a ghost exchange copies planes between the slabs' vectors and a
+    reduction combines the slabs' partial values. Used to run the distributed algorithm on one
+    device (no kernel waits on another: every exchange synchronizes the device first)."""
+
+    def exchange(self, parts, vecs):
+        import torch
+        if any(v.is_cuda for v in vecs):
+            torch.cuda.synchronize()
+        for r, (sp, v) in enumerate(zip(parts, vecs)):
+            s, L = sp.slab, sp.layout
+            if s.ghost_lo:
+                lo = parts[r - 1]
+                for d, src in zip(L.plane(0), lo.layout.plane(_top_owned(lo.slab))):
+                    v[d] = vecs[r - 1][src]
+            if s.ghost_hi:
+                hi = parts[r + 1]
+                for d, src in zip(L.plane(s.planes - 1), hi.layout.plane(_bottom_owned(hi.slab))):
+                    v[d] = vecs[r + 1][src]
+        if any(v.is_cuda for v in vecs):
+            torch.cuda.synchronize()
+
+    def sum(self, vals):
+        return [float(x) for x in np.sum(np.array(vals, dtype=np.float64), axis=0)]
+
+    def max(self, vals):
+        return [float(x) for x in np.max(np.array(vals, dtype=np.float64), axis=0)]
+
+
+class TorchComm:
+    """One slab per rank of a torch.distributed process group (rank == slab.rank): a ghost
+    exchange is one plane per neighbour and direction (batch_isend_irecv), a reduction is one
+    all_reduce. NCCL between GPUs, gloo on CPU."""
+
+    def __init__(self, dist):
+        self.dist = dist
+
+    def exchange(self, parts, vecs):
+        import torch
+        dist = self.dist
+        (sp,), (v,) = parts, vecs
+        s, L = sp.slab, sp.layout
+        ops, recv = [], []
+        for flag, peer, send_k, recv_k in ((s.ghost_lo, s.rank - 1, _bottom_owned(s), 0),
+                                           (s.ghost_hi, s.rank + 1, _top_owned(s), s.planes - 1)):
+            if not flag:
+                continue
+            buf = torch.cat([v[c] for c in L.plane(send_k)])
+            into = torch.empty_like(buf)
+            ops.append(dist.P2POp(dist.isend, buf, peer))
+            ops.append(dist.P2POp(dist.irecv, into, peer))
+            recv.append((recv_k, into))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for k, into in recv:
+            o = 0
+            for c in L.plane(k):
+                n = c.stop - c.start
+                v[c] = into[o:o + n]
+                o += n
+
+    def _reduce(self, vals, op):
+        import torch
+        (x,) = vals
+        t = torch.tensor(x, dtype=torch.float64, device=self._device)
+        self.dist.all_reduce(t, op=op)
+        return [float(a) for a in t.tolist()]
+
+    def sum(self, vals):
+        return self._reduce(vals, self.dist.ReduceOp.SUM)
+
+    def max(self, vals):
+        return self._reduce(vals, self.dist.ReduceOp.MAX)
+
+    @property
+    def _device(self):
+        import torch
+        backend = self.dist.get_backend()
+        return torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+
+
+def _owned_dot(L, a, b):
+    return float(sum((a[s] * b[s]).sum() for s in L.owned))
+
+
+def _owned_max(L, a):
+    import torch
+    m = 0.0
+    for s in L.owned:
+        x = a[s].abs()
+        if x.numel():
+            m = max(m, float(torch.nan_to_num(x, nan=float("inf")).max()))
+    return m
+
+
+def _owned_any(L, a):
+    return 1.0 if any(bool((a[s] != 0).any()) for s in L.owned) else 0.0
+
+
+class DeviceSlab:
+    """One slab's device operators for the distributed solve: SpMV and preconditioner of its
+    context on its stream, vectors in the context's storage order."""
+
+    def __init__(self, lin: SlabLinearizer, opts=None):
+        import torch
+        self.lin = lin
+        self.slab = lin.slab
+        self.ctx = lin.ctx
+        self.layout = SplitLayout(lin.case.grid, lin.slab)
+        self.opts = opts or ewg.default_solve_opts()
+        self.stream = torch.cuda.ExternalStream(self.ctx.stream)
+        self.n = self.ctx.n
+
+    def on(self):
+        import torch
+        return torch.cuda.stream(self.stream)
+
+    def zeros(self):
+        import torch
+        return torch.zeros((self.n, 2), dtype=torch.float64, device="cuda")
+
+    def rhs(self):
+        return self.ctx.device_buffer(ewg.BUFFER_RESIDUAL)
+
+    def solution(self):
+        return self.ctx.device_buffer(ewg.BUFFER_SOLUTION)
+
+    def spmv(self, x, y):
+        self.ctx.device_spmv(x, y)
+
+    def precondition(self, b, y):
+        self.ctx.device_precondition(b, y, self.opts)
+
+
+class _Vecs:
+    pass
+
+
+def _bicgstab(parts, comm, opts):
+    """Solve J dx = b over the slabs, b = the owned rows of each slab's rhs(), dx in the slabs'
+    layouts (owned rows meaningful). BiCGStabSolver::apply with CombinedCriterion
+    (linear/bicgstabsolver.hh:116-326, linear/combinedcriterion.hh:112-205) in the same steps
+    and scalar updates as the single-domain device solver, with every dot product and max-norm
+    taken over the owned rows of all slabs (one reduction each) and the preconditioner applied
+    as restricted additive Schwarz: the ghost planes of the preconditioned vector come from the
+    neighbours, each slab applies its own M^-1 (block ILU(0) or Jacobi of the slab matrix,
+    ghost rows included), and only the owned rows are kept. Ghost planes of a vector are
+    refreshed before every SpMV.
+
+    Returns (status, iterations, restarts, final residual, initial residual, [dx per slab])."""
+    import contextlib
+    on = [getattr(p, "on", contextlib.nullcontext) for p in parts]
+    V = []
+    bb_l, bm_l = [], []
+    for p, o in zip(parts, on):
+        with o():
+            v = _Vecs()
+            v.b = p.rhs().clone()
+            v.x, v.v, v.p, v.y, v.z, v.t = (p.zeros() for _ in range(6))
+            v.r = v.b.clone()
+            v.r0 = v.b.clone()
+            bb_l.append([_owned_dot(p.layout, v.b, v.b)])
+            bm_l.append([_owned_max(p.layout, v.b)])
+            V.append(v)
+    (bb,) = comm.sum(bb_l)
+    (bmax,) = comm.max(bm_l)
+    S = dict(resErr=max(bmax, DBL_BREAKDOWN), iter=0, restarts=0, restartPending=0, rho=1.0, alpha=1.0,
+             omega=1.0, r0r0=bb, status=ST_RUNNING, replacements=0, beta=0.0, rho_i=0.0)
+    S["initResErr"] = S["resErr"]
+    relTol, absTol = opts.linear_solver_tolerance, opts.linear_solver_abs_tolerance
+    maxRes, maxIter = opts.linear_solver_max_error, opts.linear_solver_max_iterations
+
+    def criterion(stagnates):
+        red = S["resErr"] / max(1e-20, S["initResErr"])
+        if red <= relTol or S["resErr"] <= absTol:
+            S["status"] = ST_CONVERGED
+        elif stagnates or S["resErr"] > maxRes:
+            S["status"] = ST_FAILED
+
+    def iteration_top(rho_i, rr):
+        if S["iter"] >= maxIter:
+            S["status"] = ST_MAXITER
+            return
+        if opts.restart_on_breakdown and abs(rho_i) <= 1e-12 * math.sqrt(S["r0r0"]) * math.sqrt(rr):
+            S["restartPending"] = 1
+            S["r0r0"] = rr
+            rho_i = rr
+            S["rho"] = S["alpha"] = S["omega"] = 1.0
+            S["restarts"] += 1
+        if abs(S["rho"]) <= DBL_BREAKDOWN or abs(S["omega"]) <= DBL_BREAKDOWN:
+            S["status"] = ST_BREAKDOWN
+            return
+        S["beta"] = (rho_i / S["rho"]) * (S["alpha"] / S["omega"])
+        S["rho"] = rho_i
+        S["rho_i"] = rho_i
+
+    def each(fn):
+        out = []
+        for p, v, o in zip(parts, V, on):
+            with o():
+                out.append(fn(p, v))
+        return out
+
+    def exchange(name):
+        comm.exchange(parts, [getattr(v, name) for v in V])
+
+    if S["resErr"] / max(1e-20, S["initResErr"]) <= relTol or S["resErr"] <= absTol:
+        S["status"] = ST_CONVERGED
+    else:
+        iteration_top(bb, bb)
+    while True:
+        while S["status"] == ST_RUNNING:
+            restart, beta, omega = S["restartPending"], S["beta"], S["omega"]
+
+            def upd_p(p, v):
+                if restart:
+                    v.r0.copy_(v.r)
+                    v.v.zero_()
+                    v.p.zero_()
+                v.p.copy_(v.r + (-beta) * (v.v * omega - v.p))
+            each(upd_p)
+            exchange("p")
+            each(lambda p, v: p.precondition(v.p, v.y))
+            exchange("y")
+            (d,) = comm.sum(each(lambda p, v: (p.spmv(v.y, v.v), [_owned_dot(p.layout, v.r0, v.v)])[1]))
+            S["restartPending"] = 0
+            if abs(d) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
+            S["alpha"] = S["rho_i"] / d
+            if abs(S["alpha"]) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
+            alpha = S["alpha"]
+
+            def upd_hs(p, v):
+                v.x.copy_(v.y * alpha + v.x)
+                v.r.copy_(v.r - v.v * alpha)
+                return [_owned_max(p.layout, v.r), _owned_any(p.layout, v.y)]
+            smax, anyy = comm.max(each(upd_hs))
+            S["resErr"] = smax
+            criterion(anyy == 0.0)
+            if S["status"] != ST_RUNNING:
+                break
+            exchange("r")
+            each(lambda p, v: p.precondition(v.r, v.z))
+            exchange("z")
+            tt, ts = comm.sum(each(lambda p, v: (p.spmv(v.z, v.t),
+                                                 [_owned_dot(p.layout, v.t, v.t), _owned_dot(p.layout, v.t, v.r)])[1]))
+            if abs(tt) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
+            S["omega"] = ts / tt
+            if abs(S["omega"]) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
+            omega = S["omega"]
+
+            def upd_xr(p, v):
+                v.x.copy_(v.x + omega * v.z)
+                m = [_owned_max(p.layout, v.r), _owned_any(p.layout, v.z)]
+                v.r.copy_(v.r + (-omega) * v.t)
+                return m, [_owned_dot(p.layout, v.r0, v.r), _owned_dot(p.layout, v.r, v.r)]
+            res = each(upd_xr)
+            smax, anyz = comm.max([m for m, _ in res])
+            rr0, rr = comm.sum([s for _, s in res])
+            S["resErr"] = smax
+            criterion(anyz == 0.0)
+            if S["status"] != ST_RUNNING:
+                break
+            S["iter"] += 1
+            iteration_top(rr0, rr)
+        if not (S["status"] == ST_CONVERGED and opts.verify_true_residual and S["replacements"] < 3):
+            break
+        # residual replacement: r = r0hat = b - J x; resume if it misses the criterion by 10x
+        exchange("x")
+
+        def true_res(p, v):
+            p.spmv(v.x, v.t)
+            v.r.copy_(v.b - v.t)
+            v.r0.copy_(v.r)
+            v.v.zero_()
+            v.p.zero_()
+            return [_owned_dot(p.layout, v.r, v.r)], [_owned_max(p.layout, v.r)]
+        res = each(true_res)
+        (rr,) = comm.sum([a for a, _ in res])
+        (err,) = comm.max([b for _, b in res])
+        if err / max(1e-20, S["initResErr"]) <= 10 * relTol or err <= 10 * absTol:
+            break
+        S["replacements"] += 1
+        S["restarts"] += 1
+        S["status"] = ST_RUNNING
+        S["resErr"] = err
+        S["restartPending"] = 0
+        S["rho"] = S["alpha"] = S["omega"] = 1.0
+        S["r0r0"] = rr
+        S["iter"] += 1
+        iteration_top(rr, rr)
+    return S["status"], S["iter"], S["restarts"], S["resErr"], S["initResErr"], [v.x for v in V]
+
+
+def _single_stream(parts):
+    """With one slab in this process, all its work (kernels, torch ops, collectives) runs on its
+    context's stream; with several, each slab's work enters its own stream and the exchanges
+    synchronize the device."""
+    import contextlib
+    if len(parts) == 1 and hasattr(parts[0], "on"):
+        return parts[0].on()
+    return contextlib.nullcontext()
+
+
+def distributed_bicgstab(parts, comm, opts):
+    """Distributed BiCGStab over the slabs in `parts` (see _bicgstab)."""
+    with _single_stream(parts):
+        return _bicgstab(parts, comm, opts)
+
+
+class DistributedNewtonReport:
+    def __init__(self):
+        self.iterations = 0
+        self.linear_iterations = 0
+        self.error = 0.0
+        self.status = ewg.EWG_OK
+        self.converged = False
+
+
+def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNewtonReport:
+    """NewtonMethod::apply (newtonmethod.hh:308-517) over the slabs: each iteration linearizes
+    every slab, takes the error as the maximum |r| over all owned rows, solves with
+    distributed_bicgstab, subtracts the update from the owned rows of solution(0) and refreshes
+    the ghost planes from the neighbours. The stopping rules are the single-domain ones
+    (proceed_: at least one iteration, stop when error <= tolerance, past the iteration limit
+    continue only while the error shrinks 4x per iteration). Each part is a DeviceSlab whose
+    context holds solution(0) with consistent ghost planes and the storage of solution(1)."""
+    nopts = nopts or ewg.default_newton_opts()
+    sopts = sopts or ewg.default_solve_opts()
+    rep = DistributedNewtonReport()
+    with _single_stream(parts):
+        error, last = 1e100, 1e100
+        it = 0
+
+        def converged():
+            return error <= nopts.newton_tolerance
+
+        def proceed():
+            if it < 1:
+                return True
+            if converged():
+                return False
+            if it >= nopts.newton_max_iterations:
+                return error * 4.0 < last
+            return True
+
+        while proceed():
+            last = error
+            errs = []
+            for p in parts:
+                with p.on():
+                    p.ctx.linearize(dt)
+                    errs.append([_owned_max(p.layout, p.rhs())])
+            (error,) = comm.max(errs)
+            if error > nopts.newton_max_error:
+                rep.status = ewg.EWG_ERR_MAX_ERROR
+                break
+            if not proceed():
+                it += 1
+                break
+            st, its, _, _, _, dxs = distributed_bicgstab(parts, comm, sopts)
+            rep.linear_iterations += its
+            if st != ST_CONVERGED:
+                rep.status = ewg.EWG_ERR_BREAKDOWN if st == ST_BREAKDOWN else ewg.EWG_ERR_NOT_CONVERGED
+                break
+            bad = []
+            for p, dx in zip(parts, dxs):
+                with p.on():
+                    x = p.solution()
+                    b = 0.0
+                    for sl in p.layout.owned:
+                        b = max(b, 0.0 if bool(dx[sl].isfinite().all()) else 1.0)
+                        x[sl] -= dx[sl]
+                    bad.append([b])
+            if comm.max(bad)[0] != 0.0:
+                rep.status = ewg.EWG_ERR_NONFINITE
+                break
+            comm.exchange(parts, [p.solution() for p in parts])
+            it += 1
+    rep.iterations = it
+    rep.error = error
+    if rep.status == ewg.EWG_OK and not converged():
+        rep.status = ewg.EWG_ERR_NOT_CONVERGED
+    rep.converged = rep.status == ewg.EWG_OK
+    return rep

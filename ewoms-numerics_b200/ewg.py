@@ -24,6 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libewg.so")
 
 EWG_OK = 0
+(EWG_ERR_INVALID, EWG_ERR_CUDA, EWG_ERR_NONFINITE, EWG_ERR_BREAKDOWN, EWG_ERR_NOT_CONVERGED, EWG_ERR_TIMEOUT,
+ EWG_ERR_NO_DEVICE, EWG_ERR_MAX_ERROR) = range(1, 9)
 STATUS_NAMES = {0: "EWG_OK", 1: "EWG_ERR_INVALID", 2: "EWG_ERR_CUDA", 3: "EWG_ERR_NONFINITE",
                 4: "EWG_ERR_BREAKDOWN", 5: "EWG_ERR_NOT_CONVERGED", 6: "EWG_ERR_TIMEOUT",
                 7: "EWG_ERR_NO_DEVICE", 8: "EWG_ERR_MAX_ERROR"}
@@ -389,6 +391,9 @@ def load(path: str = LIB_PATH):
         "ewg_default_solve_opts": (None, [P(SolveOpts)]),
         "ewg_default_newton_opts": (None, [P(NewtonOpts)]),
         "ewg_get_stream": (C.c_void_p, [C.c_void_p]),
+        "ewg_device_buffer": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_void_p)]),
+        "ewg_device_spmv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ewg_device_precondition": (C.c_int, [C.c_void_p, P(SolveOpts), C.c_void_p, C.c_void_p]),
         "ewg_profile_num_kernels": (C.c_int32, []),
         "ewg_profile_kernel_name": (C.c_char_p, [C.c_int32]),
         "ewg_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -461,6 +466,17 @@ class EwgError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
         self.status = status
+
+
+BUFFER_SOLUTION, BUFFER_RESIDUAL = 0, 1
+
+
+class _DeviceVector:
+    """__cuda_array_interface__ of an N x 2 float64 device vector owned by a context."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n, 2), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3, "strides": None, "stream": None}
 
 
 class Context:
@@ -608,6 +624,34 @@ class Context:
     def stream(self) -> int:
         """The cudaStream_t (as an integer handle) all work of this context runs on."""
         return self.lib.ewg_get_stream(self.h)
+
+    # ---- device-order vectors (N x 2 float64 torch tensors in the context's storage order) ----
+
+    def device_buffer(self, which: int):
+        """A torch view of the solution(0) (BUFFER_SOLUTION) or residual (BUFFER_RESIDUAL) device
+        vector; it aliases the context's memory and is valid until close()."""
+        import torch
+        p = C.c_void_p()
+        self._check(self.lib.ewg_device_buffer(self.h, which, C.byref(p)), "device_buffer")
+        return torch.as_tensor(_DeviceVector(p.value, self.n), device="cuda")
+
+    def _device_args(self, *ts):
+        for t in ts:
+            if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()
+                    and tuple(t.shape) == (self.n, 2)):
+                raise ValueError("device vectors are contiguous N x 2 float64 CUDA tensors")
+        return [C.c_void_p(t.data_ptr()) for t in ts]
+
+    def device_spmv(self, x, y):
+        """y = J x on the context's stream (device storage order)."""
+        xp, yp = self._device_args(x, y)
+        self._check(self.lib.ewg_device_spmv(self.h, xp, yp), "device_spmv")
+
+    def device_precondition(self, b, y, opts: SolveOpts | None = None):
+        """y = M^-1 b on the context's stream (device storage order)."""
+        opts = opts or default_solve_opts()
+        bp, yp = self._device_args(b, y)
+        self._check(self.lib.ewg_device_precondition(self.h, C.byref(opts), bp, yp), "device_precondition")
 
     def profile_enable(self, on=True, period=1):
         """Time kernel launches with CUDA events: every `period`-th launch of each class."""

@@ -252,6 +252,27 @@ ewg_status ewg_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* opts, co
 /* y = J x with the current Jacobian (natural order host vectors). */
 ewg_status ewg_apply_jacobian(ewg_ctx* ctx, const double* x, double* y);
 
+/* ---- device-order vectors (callers that keep their Krylov vectors on the device) --------
+ * A device vector is N x 2 doubles in the context's storage order: cell c = i + nx (j + ny k)
+ * of colour col = (i + j + k) & 1 sits at entry col * N/2 + c/2, so each z-plane of one colour
+ * is a contiguous run of nx*ny/2 entries. Pointers are device memory on the context's device
+ * (checked: anything else is EWG_ERR_INVALID), 16-byte aligned; the work is ordered on
+ * ewg_get_stream and the calls return without synchronizing. This is the interface of the
+ * solve distributed over z-slabs (overlapping Schwarz BiCGStab, parallelbasebackend.hh:301-338
+ * with the overlap of overlappingbcrsmatrix.hh). */
+typedef enum ewg_buffer {
+    EWG_BUFFER_SOLUTION = 0,    /* solution(0), read and written by the caller between calls */
+    EWG_BUFFER_RESIDUAL = 1     /* residual of the last linearization */
+} ewg_buffer;
+/* The device address of one of the context's vectors (valid until ewg_destroy). */
+ewg_status ewg_device_buffer(ewg_ctx* ctx, int32_t which, double** out);
+/* y = J x with the FP64 Jacobian of the last linearization. */
+ewg_status ewg_device_spmv(ewg_ctx* ctx, const double* x, double* y);
+/* y = M^-1 b with the preconditioner opts->precond of the last linearization's FP64 Jacobian
+ * (factorized at the first call after a linearization). */
+ewg_status ewg_device_precondition(ewg_ctx* ctx, const ewg_solve_opts* opts, const double* b,
+                                   double* y);
+
 /* ---- Newton (NewtonMethod::apply, newtonmethod.hh:308-517) -------------------------- */
 
 /* x(0) -= dx after checking that dx is finite (newtonmethod.hh:743-809). */

@@ -116,3 +116,15 @@ def test_vcfv_bad_arguments_and_no_device_fail_loudly(lib):
         with pytest.raises(ewg.EwgError) as ei:
             ewg.VcfvContext(ewg.vcfv_case(ewg.baseline_case(4, 4)))
         assert ei.value.status == 7
+
+
+def test_device_vector_calls_reject_bad_arguments(lib):
+    """The device-order vector calls reject a null context, an unknown buffer and null vectors
+    with EWG_ERR_INVALID before touching a device."""
+    import ctypes as C
+    import ewg
+    p = C.c_void_p()
+    assert lib.ewg_device_buffer(None, ewg.BUFFER_SOLUTION, C.byref(p)) == 1
+    assert lib.ewg_device_spmv(None, None, None) == 1
+    opts = ewg.default_solve_opts()
+    assert lib.ewg_device_precondition(None, C.byref(opts), None, None) == 1

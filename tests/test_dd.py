@@ -136,3 +136,158 @@ def test_oracle_slab_rows_equal_the_whole_grid(oracle_mod, ewg_mod, world):
             assert np.array_equal(b[rp[lr]:rp[lr + 1]], b_g[rp_g[gr]:rp_g[gr + 1]])
         ol.close()
     o.close()
+
+
+# ---- the distributed BiCGStab's host logic, driven by the oracle as the slabs' operators ----
+
+class OracleSlab:
+    """One slab's operators for dd.distributed_bicgstab backed by the oracle (natural-order CPU
+    tensors), so the distributed algorithm's host logic runs without a device."""
+
+    def __init__(self, oracle_mod, case, slab, x0, x1, dt, opts):
+        import dd
+        sc = dd.slab_case(case, slab)
+        self.o = oracle_mod.Oracle(sc)
+        self.o.set_solution(1, dd.local_view(x1, case.grid, slab))
+        self.o.set_solution(0, dd.local_view(x0, case.grid, slab))
+        self.o.linearize(dt)
+        self.slab, self.layout, self.n, self.opts = slab, dd.NaturalLayout(sc.grid, slab), sc.grid.n_cells, opts
+
+    def zeros(self):
+        import torch
+        return torch.zeros((self.n, 2), dtype=torch.float64)
+
+    def rhs(self):
+        import torch
+        return torch.from_numpy(self.o.residual())
+
+    def spmv(self, x, y):
+        import torch
+        y.copy_(torch.from_numpy(self.o.apply_jacobian(x.numpy())))
+
+    def precondition(self, b, y):
+        import torch
+        y.copy_(torch.from_numpy(self.o.apply_preconditioner(b.numpy(), self.opts)))
+
+
+def _perturbed_state(oracle_mod, case):
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    x1 = o.get_solution(0)
+    rng = np.random.default_rng(4)
+    x0 = x1.copy()
+    x0[:, 0] += rng.normal(0, 20.0, len(x0))
+    x0[:, 1] = np.clip(x0[:, 1] - np.abs(rng.normal(0, 0.3, len(x0))), 0.2, 1.0)
+    o.set_solution(1, x1)
+    o.set_solution(0, x0)
+    o.linearize(250.0)
+    return o, x0, x1
+
+
+def _solve_opts(ewg_mod):
+    opts = ewg_mod.default_solve_opts(linear_solver_tolerance=1e-9)
+    opts.verify_true_residual = 1
+    return opts
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 5])
+def test_distributed_bicgstab_solves_the_whole_grid(oracle_mod, ewg_mod, world):
+    """The slabs' distributed BiCGStab (restricted additive Schwarz, global reductions) returns
+    an update whose owned rows, put together, solve the whole grid's J dx = r."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    og, x0, x1 = _perturbed_state(oracle_mod, case)
+    r_g = og.residual()
+    opts = _solve_opts(ewg_mod)
+    slabs = dd.partition(10, world)
+    parts = [OracleSlab(oracle_mod, case, s, x0, x1, 250.0, opts) for s in slabs]
+    st, its, _, res, init, dxs = dd.distributed_bicgstab(parts, dd.LocalComm(), opts)
+    assert st == dd.ST_CONVERGED and its > 0
+    plane = 16 * 12
+    dx = np.concatenate([d.numpy()[p.layout.owned[0]] for d, p in zip(dxs, parts)])
+    assert dx.shape == (case.grid.n_cells, 2)
+    true = np.max(np.abs(r_g - og.apply_jacobian(dx)))
+    assert true <= 10 * 1e-9 * np.max(np.abs(r_g)), (true, np.max(np.abs(r_g)))
+    assert init == np.max(np.abs(r_g))
+
+
+DIST_PROBE = r'''
+import os, sys
+root = sys.argv[1]
+sys.path[:0] = [os.path.join(root, "ewoms-numerics_b200"), os.path.join(root, "oracle"), os.path.join(root, "tests")]
+import numpy as np
+import torch.distributed as dist
+import dd, ewg, oracle
+from test_dd import OracleSlab, _perturbed_state, _solve_opts
+dist.init_process_group("gloo")
+rank, world = dist.get_rank(), dist.get_world_size()
+case = ewg.lens3d_case(16, 12, 10, seed=2)
+og, x0, x1 = _perturbed_state(oracle, case)
+opts = _solve_opts(ewg)
+s = dd.partition(10, world)[rank]
+part = OracleSlab(oracle, case, s, x0, x1, 250.0, opts)
+st, its, _, res, init, (dx,) = dd.distributed_bicgstab([part], dd.TorchComm(dist), opts)
+got = [None] * world
+dist.all_gather_object(got, (st, its, dx.numpy()[part.layout.owned[0]]))
+assert len({(a, b) for a, b, _ in got}) == 1, got
+if rank == 0:
+    dxg = np.concatenate([d for _, _, d in got])
+    r_g = og.residual()
+    true = np.max(np.abs(r_g - og.apply_jacobian(dxg)))
+    assert st == dd.ST_CONVERGED and true <= 10 * 1e-9 * np.max(np.abs(r_g)), (st, true)
+dist.barrier()
+dist.destroy_process_group()
+print(f"rank {rank} ok its={its}", flush=True)
+'''
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_bicgstab_between_gloo_ranks(tmp_path, world):
+    """The same solve with one slab per gloo rank: ghost planes over P2P messages, reductions
+    over all_reduce; every rank ends with the same status and iteration count."""
+    probe = tmp_path / "probe.py"
+    probe.write_text(DIST_PROBE)
+    cmd = ["timeout", "-k", "30", "300", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={world}", "--master-addr=127.0.0.1", f"--master-port={_free_port()}", str(probe), ROOT]
+    out = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT,
+                         env=dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stdout[-3000:] + out.stderr[-3000:]
+    assert all(f"rank {r} ok" in out.stdout for r in range(world))
+
+
+def _to_split(x_nat, grid):
+    """Natural -> the device storage order (entry col * N/2 + c/2, col = (i + j + k) & 1)."""
+    n = grid.n_cells
+    c = np.arange(n)
+    i, j, k = c % grid.nx, (c // grid.nx) % grid.ny, c // (grid.nx * grid.ny)
+    out = np.empty_like(x_nat)
+    out[((i + j + k) & 1) * (n // 2) + (c >> 1)] = x_nat
+    return out
+
+
+def test_split_layout_ghost_exchange(ewg_mod):
+    """Ghost planes exchanged in the device storage order (plane chunks in global colour order)
+    hold the same cells as an exchange in natural order, also between slabs whose first planes
+    differ in parity (there the local colours of a plane are swapped)."""
+    import types
+    import dd
+    import torch
+    case = ewg_mod.lens3d_case(8, 6, 11, seed=0)
+    xg = np.arange(case.grid.n_cells * 2, dtype=np.float64).reshape(-1, 2) * 0.25
+    for world in (2, 3, 4):
+        slabs = dd.partition(11, world)
+        assert len({s.first & 1 for s in slabs}) == 2 or world == 2
+        parts, vecs, want = [], [], []
+        for s in slabs:
+            g = dd.slab_case(case, s).grid
+            nat = dd.local_view(xg, case.grid, s)
+            spl = torch.from_numpy(_to_split(nat, g))
+            L = dd.SplitLayout(g, s)
+            want.append(spl.clone())
+            for k in ([0] if s.ghost_lo else []) + ([s.planes - 1] if s.ghost_hi else []):
+                for c in L.plane(k):
+                    spl[c] = -7.0
+            parts.append(types.SimpleNamespace(slab=s, layout=L))
+            vecs.append(spl)
+        dd.LocalComm().exchange(parts, vecs)
+        assert all(torch.equal(a, b) for a, b in zip(vecs, want))
