@@ -247,6 +247,17 @@ class LocalComm:
     def max(self, vals):
         return [float(x) for x in np.max(np.array(vals, dtype=np.float64), axis=0)]
 
+    def reduce(self, vals, nsum):
+        """vals: one 1-D tensor of partials per slab, the first nsum summed over the slabs and the
+        rest maximised. One host read per slab."""
+        rows = np.array([v.tolist() for v in vals], dtype=np.float64)
+        return _combine(rows, nsum)
+
+
+def _combine(rows, nsum):
+    return ([float(x) for x in np.sum(rows[:, :nsum], axis=0)],
+            [float(x) for x in np.max(rows[:, nsum:], axis=0)])
+
 
 class TorchComm:
     """One slab per rank of a torch.distributed process group (rank == slab.rank): a ghost
@@ -294,6 +305,17 @@ class TorchComm:
     def max(self, vals):
         return self._reduce(vals, self.dist.ReduceOp.MAX)
 
+    def reduce(self, vals, nsum):
+        """One all_gather of this rank's partials (a 1-D tensor, the first nsum summed and the rest
+        maximised over the ranks); every rank combines the same gathered rows in rank order, so
+        all ranks take the same branches."""
+        import torch
+        (x,) = vals
+        x = x.to(self._device)
+        g = [torch.empty_like(x) for _ in range(self.dist.get_world_size())]
+        self.dist.all_gather(g, x)
+        return _combine(np.array(torch.stack(g).tolist(), dtype=np.float64), nsum)
+
     @property
     def _device(self):
         import torch
@@ -301,22 +323,36 @@ class TorchComm:
         return torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
 
 
-def _owned_dot(L, a, b):
-    return float(sum((a[s] * b[s]).sum() for s in L.owned))
+# Partials over a slab's owned rows as device tensors (no host read); a reduction point stacks
+# them into one vector, so a slab reads its partials back once and the ranks combine them in one
+# collective.
+
+def _dev_dot(L, a, b):
+    return sum((a[s] * b[s]).sum() for s in L.owned)
 
 
-def _owned_max(L, a):
+def _dev_max(L, a):
     import torch
-    m = 0.0
+    m = a.new_zeros(())
     for s in L.owned:
         x = a[s].abs()
         if x.numel():
-            m = max(m, float(torch.nan_to_num(x, nan=float("inf")).max()))
+            m = torch.maximum(m, torch.nan_to_num(x, nan=float("inf")).max())
     return m
 
 
-def _owned_any(L, a):
-    return 1.0 if any(bool((a[s] != 0).any()) for s in L.owned) else 0.0
+def _dev_any(L, a):
+    import torch
+    f = a.new_zeros(())
+    for s in L.owned:
+        if a[s].numel():
+            f = torch.maximum(f, (a[s] != 0).any().to(a.dtype))
+    return f
+
+
+def _pack(sums, maxes):
+    import torch
+    return torch.stack(list(sums) + list(maxes))
 
 
 class DeviceSlab:
@@ -363,11 +399,14 @@ def _bicgstab(parts, comm, opts):
     layouts (owned rows meaningful). BiCGStabSolver::apply with CombinedCriterion
     (linear/bicgstabsolver.hh:116-326, linear/combinedcriterion.hh:112-205) in the same steps
     and scalar updates as the single-domain device solver, with every dot product and max-norm
-    taken over the owned rows of all slabs (one reduction each) and the preconditioner applied
+    taken over the owned rows of all slabs and the preconditioner applied
     as restricted additive Schwarz: the ghost planes of the preconditioned vector come from the
     neighbours, each slab applies its own M^-1 (block ILU(0) or Jacobi of the slab matrix,
     ghost rows included), and only the owned rows are kept. Ghost planes of a vector are
-    refreshed before every SpMV.
+    refreshed before every SpMV. The partials of an iteration meet in three reductions, each one
+    host read per slab and one collective: <r0,v>; the half-step max-norm and stagnation flag
+    together with <t,t> and <t,s> (z and t are computed before the half-step check and left
+    unused when it ends the solve); the full-step max-norm and flag with <r0,r> and <r,r>.
 
     Returns (status, iterations, restarts, final residual, initial residual, [dx per slab])."""
     import contextlib
@@ -381,11 +420,9 @@ def _bicgstab(parts, comm, opts):
             v.x, v.v, v.p, v.y, v.z, v.t = (p.zeros() for _ in range(6))
             v.r = v.b.clone()
             v.r0 = v.b.clone()
-            bb_l.append([_owned_dot(p.layout, v.b, v.b)])
-            bm_l.append([_owned_max(p.layout, v.b)])
+            bb_l.append(_pack([_dev_dot(p.layout, v.b, v.b)], [_dev_max(p.layout, v.b)]))
             V.append(v)
-    (bb,) = comm.sum(bb_l)
-    (bmax,) = comm.max(bm_l)
+    (bb,), (bmax,) = comm.reduce(bb_l, 1)
     S = dict(resErr=max(bmax, DBL_BREAKDOWN), iter=0, restarts=0, restartPending=0, rho=1.0, alpha=1.0,
              omega=1.0, r0r0=bb, status=ST_RUNNING, replacements=0, beta=0.0, rho_i=0.0)
     S["initResErr"] = S["resErr"]
@@ -444,7 +481,7 @@ def _bicgstab(parts, comm, opts):
             exchange("p")
             each(lambda p, v: p.precondition(v.p, v.y))
             exchange("y")
-            (d,) = comm.sum(each(lambda p, v: (p.spmv(v.y, v.v), [_owned_dot(p.layout, v.r0, v.v)])[1]))
+            (d,), _ = comm.reduce(each(lambda p, v: (p.spmv(v.y, v.v), _pack([_dev_dot(p.layout, v.r0, v.v)], []))[1]), 1)
             S["restartPending"] = 0
             if abs(d) <= DBL_BREAKDOWN:
                 S["status"] = ST_BREAKDOWN
@@ -458,17 +495,21 @@ def _bicgstab(parts, comm, opts):
             def upd_hs(p, v):
                 v.x.copy_(v.y * alpha + v.x)
                 v.r.copy_(v.r - v.v * alpha)
-                return [_owned_max(p.layout, v.r), _owned_any(p.layout, v.y)]
-            smax, anyy = comm.max(each(upd_hs))
+                v.half = [_dev_max(p.layout, v.r), _dev_any(p.layout, v.y)]
+            each(upd_hs)
+            # the half-step check travels with <t,t> and <t,s>: z = M^-1 s and t = J z are
+            # computed before it is known, and left unused when the half step ends the solve
+            exchange("r")
+            each(lambda p, v: p.precondition(v.r, v.z))
+            exchange("z")
+            (tt, ts), (smax, anyy) = comm.reduce(
+                each(lambda p, v: (p.spmv(v.z, v.t),
+                                   _pack([_dev_dot(p.layout, v.t, v.t), _dev_dot(p.layout, v.t, v.r)],
+                                         v.half))[1]), 2)
             S["resErr"] = smax
             criterion(anyy == 0.0)
             if S["status"] != ST_RUNNING:
                 break
-            exchange("r")
-            each(lambda p, v: p.precondition(v.r, v.z))
-            exchange("z")
-            tt, ts = comm.sum(each(lambda p, v: (p.spmv(v.z, v.t),
-                                                 [_owned_dot(p.layout, v.t, v.t), _owned_dot(p.layout, v.t, v.r)])[1]))
             if abs(tt) <= DBL_BREAKDOWN:
                 S["status"] = ST_BREAKDOWN
                 break
@@ -480,12 +521,10 @@ def _bicgstab(parts, comm, opts):
 
             def upd_xr(p, v):
                 v.x.copy_(v.x + omega * v.z)
-                m = [_owned_max(p.layout, v.r), _owned_any(p.layout, v.z)]
+                m = [_dev_max(p.layout, v.r), _dev_any(p.layout, v.z)]
                 v.r.copy_(v.r + (-omega) * v.t)
-                return m, [_owned_dot(p.layout, v.r0, v.r), _owned_dot(p.layout, v.r, v.r)]
-            res = each(upd_xr)
-            smax, anyz = comm.max([m for m, _ in res])
-            rr0, rr = comm.sum([s for _, s in res])
+                return _pack([_dev_dot(p.layout, v.r0, v.r), _dev_dot(p.layout, v.r, v.r)], m)
+            (rr0, rr), (smax, anyz) = comm.reduce(each(upd_xr), 2)
             S["resErr"] = smax
             criterion(anyz == 0.0)
             if S["status"] != ST_RUNNING:
@@ -503,10 +542,8 @@ def _bicgstab(parts, comm, opts):
             v.r0.copy_(v.r)
             v.v.zero_()
             v.p.zero_()
-            return [_owned_dot(p.layout, v.r, v.r)], [_owned_max(p.layout, v.r)]
-        res = each(true_res)
-        (rr,) = comm.sum([a for a, _ in res])
-        (err,) = comm.max([b for _, b in res])
+            return _pack([_dev_dot(p.layout, v.r, v.r)], [_dev_max(p.layout, v.r)])
+        (rr,), (err,) = comm.reduce(each(true_res), 1)
         if err / max(1e-20, S["initResErr"]) <= 10 * relTol or err <= 10 * absTol:
             break
         S["replacements"] += 1
@@ -554,6 +591,7 @@ def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNe
     (proceed_: at least one iteration, stop when error <= tolerance, past the iteration limit
     continue only while the error shrinks 4x per iteration). Each part is a DeviceSlab whose
     context holds solution(0) with consistent ghost planes and the storage of solution(1)."""
+    import torch
     nopts = nopts or ewg.default_newton_opts()
     sopts = sopts or ewg.default_solve_opts()
     rep = DistributedNewtonReport()
@@ -579,8 +617,8 @@ def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNe
             for p in parts:
                 with p.on():
                     p.ctx.linearize(dt)
-                    errs.append([_owned_max(p.layout, p.rhs())])
-            (error,) = comm.max(errs)
+                    errs.append(_pack([], [_dev_max(p.layout, p.rhs())]))
+            _, (error,) = comm.reduce(errs, 0)
             if error > nopts.newton_max_error:
                 rep.status = ewg.EWG_ERR_MAX_ERROR
                 break
@@ -596,12 +634,12 @@ def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNe
             for p, dx in zip(parts, dxs):
                 with p.on():
                     x = p.solution()
-                    b = 0.0
+                    b = x.new_zeros(())
                     for sl in p.layout.owned:
-                        b = max(b, 0.0 if bool(dx[sl].isfinite().all()) else 1.0)
+                        b = torch.maximum(b, (~dx[sl].isfinite()).any().to(x.dtype))
                         x[sl] -= dx[sl]
-                    bad.append([b])
-            if comm.max(bad)[0] != 0.0:
+                    bad.append(_pack([], [b]))
+            if comm.reduce(bad, 0)[1][0] != 0.0:
                 rep.status = ewg.EWG_ERR_NONFINITE
                 break
             comm.exchange(parts, [p.solution() for p in parts])

@@ -211,6 +211,39 @@ def test_distributed_bicgstab_solves_the_whole_grid(oracle_mod, ewg_mod, world):
     assert init == np.max(np.abs(r_g))
 
 
+class CountingComm:
+    """LocalComm that counts the reductions (one collective each between ranks)."""
+
+    def __init__(self, dd):
+        self.inner, self.reductions = dd.LocalComm(), 0
+
+    def exchange(self, parts, vecs):
+        self.inner.exchange(parts, vecs)
+
+    def reduce(self, vals, nsum):
+        self.reductions += 1
+        return self.inner.reduce(vals, nsum)
+
+
+@pytest.mark.parametrize("verify", [0, 1])
+def test_distributed_bicgstab_takes_three_reductions_per_iteration(oracle_mod, ewg_mod, verify):
+    """Every BiCGStab iteration's dot products and max-norms meet in three reductions: <r0,v>;
+    the half-step check with <t,t>, <t,s>; the full-step check with <r0,r>, <r,r>. Besides
+    them: one for ||b|| at the start, one per true-residual check."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    og, x0, x1 = _perturbed_state(oracle_mod, case)
+    opts = _solve_opts(ewg_mod)
+    opts.verify_true_residual = verify
+    parts = [OracleSlab(oracle_mod, case, s, x0, x1, 250.0, opts) for s in dd.partition(10, 3)]
+    comm = CountingComm(dd)
+    st, its, restarts, _, _, _ = dd.distributed_bicgstab(parts, comm, opts)
+    assert st == dd.ST_CONVERGED and its == 27
+    # the converging iteration ends after its second (half step) or third (full step) reduction
+    # without adding to the count
+    assert comm.reductions - 1 - 3 * its - verify * (1 + restarts) in (2, 3), comm.reductions
+
+
 DIST_PROBE = r'''
 import os, sys
 root = sys.argv[1]
