@@ -1,6 +1,7 @@
 """Domain decomposition into z-slabs (ewoms-numerics_b200/dd.py), host side: the partition, the
-slab problems (same cell size bit for bit, shifted lens and inlet, permeability planes), and the
-ghost-plane exchange between two and three gloo ranks on CPU."""
+slab problems (same cell size bit for bit, shifted lens and inlet, permeability planes), the
+ghost-plane exchange between two and three gloo ranks on CPU, and the distributed BiCGStab and
+Newton driven by the oracle as the slabs' operators (in one process and on gloo ranks)."""
 import os
 import socket
 import subprocess
@@ -170,6 +171,43 @@ class OracleSlab:
         y.copy_(torch.from_numpy(self.o.apply_preconditioner(b.numpy(), self.opts)))
 
 
+class OracleNewtonSlab(OracleSlab):
+    """OracleSlab whose state solution(0) is a CPU tensor in natural order that
+    dd.distributed_newton updates in place; linearize() hands it to the oracle first, with the
+    Newton iteration number (the oracle takes the old-time-level storage at iteration 0)."""
+
+    def __init__(self, oracle_mod, case, slab, x0, x1, opts):
+        import dd
+        import torch
+        sc = dd.slab_case(case, slab)
+        self.o = oracle_mod.Oracle(sc)
+        self.o.set_solution(1, dd.local_view(x1, case.grid, slab))
+        self.x = torch.from_numpy(np.ascontiguousarray(dd.local_view(x0, case.grid, slab)))
+        self.slab, self.layout, self.n, self.opts = slab, dd.NaturalLayout(sc.grid, slab), sc.grid.n_cells, opts
+        self.ctx = self
+        self.iteration = 0
+
+    def on(self):
+        import contextlib
+        return contextlib.nullcontext()
+
+    def linearize(self, dt):
+        self.o.set_solution(0, self.x.numpy())
+        self.o.linearize(dt, self.iteration)
+        self.iteration += 1
+
+    def solution(self):
+        return self.x
+
+
+def _stepped_state(oracle_mod, case, steps):
+    """The state after `steps` implicit-Euler steps of the single-domain oracle."""
+    o = oracle_mod.Oracle(case)
+    o.apply_initial_solution()
+    o.run(steps, 250.0)
+    return o
+
+
 def _perturbed_state(oracle_mod, case):
     o = oracle_mod.Oracle(case)
     o.apply_initial_solution()
@@ -244,6 +282,84 @@ def test_distributed_bicgstab_takes_three_reductions_per_iteration(oracle_mod, e
     assert comm.reductions - 1 - 3 * its - verify * (1 + restarts) in (2, 3), comm.reductions
 
 
+def _check_newton_state(x_dd, x_sd):
+    dp = np.max(np.abs(x_dd[:, 0] - x_sd[:, 0])) / np.max(np.abs(x_sd[:, 0]))
+    ds = np.max(np.abs(x_dd[:, 1] - x_sd[:, 1]))
+    assert dp <= 1e-7 and ds <= 1e-5, (dp, ds)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_distributed_newton_matches_the_single_domain(oracle_mod, ewg_mod, world):
+    """One implicit-Euler step by dd.distributed_newton over oracle slabs: it converges, its
+    error is the whole grid's residual max-norm at the final state (the owned rows are the whole
+    grid's rows), and the state agrees with the single-domain oracle Newton's (the linear solves
+    differ within their tolerance: block ILU(0) of the whole grid against restricted additive
+    Schwarz over the slabs)."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    o = _stepped_state(oracle_mod, case, 2)
+    x1 = o.get_solution(0)
+    sopts = ewg_mod.default_solve_opts()
+    parts = [OracleNewtonSlab(oracle_mod, case, s, x1, x1, sopts) for s in dd.partition(10, world)]
+    rep = dd.distributed_newton(parts, dd.LocalComm(), 250.0, None, sopts)
+    assert rep.converged and rep.iterations >= 1, (rep.status, rep.iterations, rep.error)
+    x_dd = np.concatenate([p.x.numpy()[p.layout.owned[0]] for p in parts])
+    # the whole grid linearized as the slabs were: old storage recycled at iteration 0 from x1
+    ow = oracle_mod.Oracle(case)
+    ow.set_solution(1, x1)
+    ow.set_solution(0, x1)
+    ow.linearize(250.0, 0)
+    ow.set_solution(0, x_dd)
+    ow.linearize(250.0, 1)
+    assert np.max(np.abs(ow.residual())) == rep.error
+    ow.close()
+    o.set_solution(1, x1)
+    o.set_solution(0, x1)
+    rc, ni, li, e = o.newton_apply(250.0)
+    assert rc == 0
+    _check_newton_state(x_dd, o.get_solution(0))
+
+
+def _newton_slabs(oracle_mod, ewg_mod, world):
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    x1 = _stepped_state(oracle_mod, case, 1).get_solution(0)
+    sopts = ewg_mod.default_solve_opts()
+    return [OracleNewtonSlab(oracle_mod, case, s, x1, x1, sopts) for s in dd.partition(10, world)], sopts
+
+
+def test_distributed_newton_stops_on_a_nonfinite_update(oracle_mod, ewg_mod, monkeypatch):
+    """A solve that reports convergence but leaves a non-finite entry in one slab's update ends
+    the distributed Newton with EWG_ERR_NONFINITE (the flag is a maximum over all slabs)."""
+    import dd
+    parts, sopts = _newton_slabs(oracle_mod, ewg_mod, 3)
+    solve = dd.distributed_bicgstab
+
+    def poisoned(parts, comm, opts):
+        out = solve(parts, comm, opts)
+        out[5][2][parts[2].layout.owned[0].start, 1] = float("nan")
+        return out
+    monkeypatch.setattr(dd, "distributed_bicgstab", poisoned)
+    rep = dd.distributed_newton(parts, dd.LocalComm(), 250.0, None, sopts)
+    assert rep.status == ewg_mod.EWG_ERR_NONFINITE and not rep.converged and rep.iterations == 0
+
+
+def test_distributed_newton_stops_when_a_slab_preconditioner_breaks(oracle_mod, ewg_mod):
+    """A NaN out of one slab's preconditioner makes the global residual max-norm infinite, so the
+    distributed BiCGStab fails on every slab's side and Newton ends with EWG_ERR_NOT_CONVERGED."""
+    import dd
+    parts, sopts = _newton_slabs(oracle_mod, ewg_mod, 2)
+    bad = parts[1]
+    apply = bad.precondition
+
+    def poisoned(b, y):
+        apply(b, y)
+        y[bad.layout.owned[0].start] = float("nan")
+    bad.precondition = poisoned
+    rep = dd.distributed_newton(parts, dd.LocalComm(), 250.0, None, sopts)
+    assert rep.status == ewg_mod.EWG_ERR_NOT_CONVERGED and not rep.converged
+
+
 DIST_PROBE = r'''
 import os, sys
 root = sys.argv[1]
@@ -277,9 +393,56 @@ print(f"rank {rank} ok its={its}", flush=True)
 @pytest.mark.parametrize("world", [2, 3])
 def test_distributed_bicgstab_between_gloo_ranks(tmp_path, world):
     """The same solve with one slab per gloo rank: ghost planes over P2P messages, reductions
-    over all_reduce; every rank ends with the same status and iteration count."""
+    over all_gather; every rank ends with the same status and iteration count."""
     probe = tmp_path / "probe.py"
     probe.write_text(DIST_PROBE)
+    cmd = ["timeout", "-k", "30", "300", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={world}", "--master-addr=127.0.0.1", f"--master-port={_free_port()}", str(probe), ROOT]
+    out = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT,
+                         env=dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stdout[-3000:] + out.stderr[-3000:]
+    assert all(f"rank {r} ok" in out.stdout for r in range(world))
+
+
+NEWTON_PROBE = r'''
+import os, sys
+root = sys.argv[1]
+sys.path[:0] = [os.path.join(root, "ewoms-numerics_b200"), os.path.join(root, "oracle"), os.path.join(root, "tests")]
+import numpy as np
+import torch.distributed as dist
+import dd, ewg, oracle
+from test_dd import OracleNewtonSlab, _stepped_state, _check_newton_state
+dist.init_process_group("gloo")
+rank, world = dist.get_rank(), dist.get_world_size()
+case = ewg.lens3d_case(16, 12, 10, seed=2)
+o = _stepped_state(oracle, case, 2)
+x1 = o.get_solution(0)
+sopts = ewg.default_solve_opts()
+part = OracleNewtonSlab(oracle, case, dd.partition(10, world)[rank], x1, x1, sopts)
+rep = dd.distributed_newton([part], dd.TorchComm(dist), 250.0, None, sopts)
+got = [None] * world
+dist.all_gather_object(got, (rep.status, rep.iterations, rep.linear_iterations, rep.error,
+                             part.x.numpy()[part.layout.owned[0]]))
+assert len({g[:4] for g in got}) == 1, [g[:4] for g in got]
+if rank == 0:
+    assert rep.converged, (rep.status, rep.iterations, rep.error)
+    o.set_solution(1, x1)
+    o.set_solution(0, x1)
+    assert o.newton_apply(250.0)[0] == 0
+    _check_newton_state(np.concatenate([g[4] for g in got]), o.get_solution(0))
+dist.barrier()
+dist.destroy_process_group()
+print(f"rank {rank} ok newton={rep.iterations} linear={rep.linear_iterations}", flush=True)
+'''
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_newton_between_gloo_ranks(tmp_path, world):
+    """One implicit-Euler step by Newton with one slab per gloo rank: every rank ends with the
+    same status, iteration counts and error, and the gathered state agrees with the
+    single-domain oracle Newton's."""
+    probe = tmp_path / "probe.py"
+    probe.write_text(NEWTON_PROBE)
     cmd = ["timeout", "-k", "30", "300", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
            f"--nproc-per-node={world}", "--master-addr=127.0.0.1", f"--master-port={_free_port()}", str(probe), ROOT]
     out = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT,
