@@ -241,15 +241,13 @@ class LocalComm:
         if any(v.is_cuda for v in vecs):
             torch.cuda.synchronize()
 
-    def sum(self, vals):
-        return [float(x) for x in np.sum(np.array(vals, dtype=np.float64), axis=0)]
-
-    def max(self, vals):
-        return [float(x) for x in np.max(np.array(vals, dtype=np.float64), axis=0)]
-
     def reduce(self, vals, nsum):
         """vals: one 1-D tensor of partials per slab, the first nsum summed over the slabs and the
-        rest maximised. One host read per slab."""
+        rest maximised. One host read per slab. The partials were computed on the slabs' own
+        (non-blocking) streams, so the device is synchronized before they are read."""
+        import torch
+        if any(v.is_cuda for v in vals):
+            torch.cuda.synchronize()
         rows = np.array([v.tolist() for v in vals], dtype=np.float64)
         return _combine(rows, nsum)
 
@@ -262,7 +260,7 @@ def _combine(rows, nsum):
 class TorchComm:
     """One slab per rank of a torch.distributed process group (rank == slab.rank): a ghost
     exchange is one plane per neighbour and direction (batch_isend_irecv), a reduction is one
-    all_reduce. NCCL between GPUs, gloo on CPU."""
+    all_gather of the ranks' partials. NCCL between GPUs, gloo on CPU."""
 
     def __init__(self, dist):
         self.dist = dist
@@ -291,19 +289,6 @@ class TorchComm:
                 n = c.stop - c.start
                 v[c] = into[o:o + n]
                 o += n
-
-    def _reduce(self, vals, op):
-        import torch
-        (x,) = vals
-        t = torch.tensor(x, dtype=torch.float64, device=self._device)
-        self.dist.all_reduce(t, op=op)
-        return [float(a) for a in t.tolist()]
-
-    def sum(self, vals):
-        return self._reduce(vals, self.dist.ReduceOp.SUM)
-
-    def max(self, vals):
-        return self._reduce(vals, self.dist.ReduceOp.MAX)
 
     def reduce(self, vals, nsum):
         """One all_gather of this rank's partials (a 1-D tensor, the first nsum summed and the rest
