@@ -222,11 +222,22 @@ def _top_owned(s: Slab) -> int:
 class LocalComm:
     """All slabs in this process: a ghost exchange copies planes between the slabs' vectors and a
     reduction combines the slabs' partial values. Used to run the distributed algorithm on one
-    device (no kernel waits on another: every exchange synchronizes the device first)."""
+    device. No kernel waits on another: the plane copies run on the current stream after it has
+    waited for every slab's stream, and the slabs' streams wait for the copies (a host
+    synchronization instead where a slab has no stream)."""
 
     def exchange(self, parts, vecs):
         import torch
-        if any(v.is_cuda for v in vecs):
+        if not any(sp.slab.ghost_lo or sp.slab.ghost_hi for sp in parts):
+            return
+        cuda = any(v.is_cuda for v in vecs)
+        streams = [getattr(sp, "stream", None) for sp in parts]
+        ordered = cuda and all(st is not None for st in streams)
+        if ordered:
+            cur = torch.cuda.current_stream()
+            for st in streams:
+                cur.wait_stream(st)
+        elif cuda:
             torch.cuda.synchronize()
         for r, (sp, v) in enumerate(zip(parts, vecs)):
             s, L = sp.slab, sp.layout
@@ -238,7 +249,10 @@ class LocalComm:
                 hi = parts[r + 1]
                 for d, src in zip(L.plane(s.planes - 1), hi.layout.plane(_bottom_owned(hi.slab))):
                     v[d] = vecs[r + 1][src]
-        if any(v.is_cuda for v in vecs):
+        if ordered:
+            for st in streams:
+                st.wait_stream(cur)
+        elif cuda:
             torch.cuda.synchronize()
 
     def reduce(self, vals, nsum):
@@ -253,8 +267,11 @@ class LocalComm:
 
 
 def _combine(rows, nsum):
+    """Sums of the first nsum columns, maxima of the rest; a NaN maximum reads as infinity, so a
+    non-finite residual fails the convergence tests instead of passing them silently."""
+    maxes = np.max(rows[:, nsum:], axis=0)
     return ([float(x) for x in np.sum(rows[:, :nsum], axis=0)],
-            [float(x) for x in np.max(rows[:, nsum:], axis=0)])
+            [math.inf if math.isnan(x) else float(x) for x in maxes])
 
 
 class TorchComm:
@@ -313,26 +330,17 @@ class TorchComm:
 # collective.
 
 def _dev_dot(L, a, b):
-    return sum((a[s] * b[s]).sum() for s in L.owned)
+    import torch
+    return sum(torch.vdot(a[s].reshape(-1), b[s].reshape(-1)) for s in L.owned)
 
 
 def _dev_max(L, a):
+    """max |a| over the owned rows (NaN propagates; the host reads it as infinity)."""
     import torch
-    m = a.new_zeros(())
-    for s in L.owned:
-        x = a[s].abs()
-        if x.numel():
-            m = torch.maximum(m, torch.nan_to_num(x, nan=float("inf")).max())
-    return m
-
-
-def _dev_any(L, a):
-    import torch
-    f = a.new_zeros(())
-    for s in L.owned:
-        if a[s].numel():
-            f = torch.maximum(f, (a[s] != 0).any().to(a.dtype))
-    return f
+    ms = [torch.linalg.vector_norm(a[s], float("inf")) for s in L.owned if a[s].numel()]
+    if not ms:
+        return a.new_zeros(())
+    return ms[0] if len(ms) == 1 else torch.stack(ms).amax()
 
 
 def _pack(sums, maxes):
@@ -389,12 +397,14 @@ def _bicgstab(parts, comm, opts):
     neighbours, each slab applies its own M^-1 (block ILU(0) or Jacobi of the slab matrix,
     ghost rows included), and only the owned rows are kept. Ghost planes of a vector are
     refreshed before every SpMV. The partials of an iteration meet in three reductions, each one
-    host read per slab and one collective: <r0,v>; the half-step max-norm and stagnation flag
+    host read per slab and one collective: <r0,v>; the half-step max-norms of s and y
     together with <t,t> and <t,s> (z and t are computed before the half-step check and left
-    unused when it ends the solve); the full-step max-norm and flag with <r0,r> and <r,r>.
+    unused when it ends the solve); the full-step max-norms of s and z with <r0,r> and <r,r>.
+    A zero max-norm of y or z is the stagnation test.
 
     Returns (status, iterations, restarts, final residual, initial residual, [dx per slab])."""
     import contextlib
+    import torch
     on = [getattr(p, "on", contextlib.nullcontext) for p in parts]
     V = []
     bb_l, bm_l = [], []
@@ -461,7 +471,7 @@ def _bicgstab(parts, comm, opts):
                     v.r0.copy_(v.r)
                     v.v.zero_()
                     v.p.zero_()
-                v.p.copy_(v.r + (-beta) * (v.v * omega - v.p))
+                v.p.sub_(v.v, alpha=omega).mul_(beta).add_(v.r)
             each(upd_p)
             exchange("p")
             each(lambda p, v: p.precondition(v.p, v.y))
@@ -478,21 +488,21 @@ def _bicgstab(parts, comm, opts):
             alpha = S["alpha"]
 
             def upd_hs(p, v):
-                v.x.copy_(v.y * alpha + v.x)
-                v.r.copy_(v.r - v.v * alpha)
-                v.half = [_dev_max(p.layout, v.r), _dev_any(p.layout, v.y)]
+                v.x.add_(v.y, alpha=alpha)
+                v.r.sub_(v.v, alpha=alpha)
+                v.half = [_dev_max(p.layout, v.r), _dev_max(p.layout, v.y)]
             each(upd_hs)
             # the half-step check travels with <t,t> and <t,s>: z = M^-1 s and t = J z are
             # computed before it is known, and left unused when the half step ends the solve
             exchange("r")
             each(lambda p, v: p.precondition(v.r, v.z))
             exchange("z")
-            (tt, ts), (smax, anyy) = comm.reduce(
+            (tt, ts), (smax, ymax) = comm.reduce(
                 each(lambda p, v: (p.spmv(v.z, v.t),
                                    _pack([_dev_dot(p.layout, v.t, v.t), _dev_dot(p.layout, v.t, v.r)],
                                          v.half))[1]), 2)
             S["resErr"] = smax
-            criterion(anyy == 0.0)
+            criterion(ymax == 0.0)  # the update y stagnates when it is all zero
             if S["status"] != ST_RUNNING:
                 break
             if abs(tt) <= DBL_BREAKDOWN:
@@ -505,13 +515,13 @@ def _bicgstab(parts, comm, opts):
             omega = S["omega"]
 
             def upd_xr(p, v):
-                v.x.copy_(v.x + omega * v.z)
-                m = [_dev_max(p.layout, v.r), _dev_any(p.layout, v.z)]
-                v.r.copy_(v.r + (-omega) * v.t)
+                v.x.add_(v.z, alpha=omega)
+                m = [_dev_max(p.layout, v.r), _dev_max(p.layout, v.z)]
+                v.r.sub_(v.t, alpha=omega)
                 return _pack([_dev_dot(p.layout, v.r0, v.r), _dev_dot(p.layout, v.r, v.r)], m)
-            (rr0, rr), (smax, anyz) = comm.reduce(each(upd_xr), 2)
+            (rr0, rr), (smax, zmax) = comm.reduce(each(upd_xr), 2)
             S["resErr"] = smax
-            criterion(anyz == 0.0)
+            criterion(zmax == 0.0)
             if S["status"] != ST_RUNNING:
                 break
             S["iter"] += 1
@@ -523,7 +533,7 @@ def _bicgstab(parts, comm, opts):
 
         def true_res(p, v):
             p.spmv(v.x, v.t)
-            v.r.copy_(v.b - v.t)
+            torch.sub(v.b, v.t, out=v.r)
             v.r0.copy_(v.r)
             v.v.zero_()
             v.p.zero_()
@@ -635,3 +645,79 @@ def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNe
         rep.status = ewg.EWG_ERR_NOT_CONVERGED
     rep.converged = rep.status == ewg.EWG_OK
     return rep
+
+
+def main(argv=None) -> None:
+    """Times one implicit-Euler step of the 3D lens problem on one device: the single-domain
+    Newton (ewg_newton_apply) and distributed_newton over 1, 2, ... z-slabs held as separate
+    contexts in this process (LocalComm). Both start from the state after one warm-up step, each
+    form runs the step once untimed and once timed; the time is host wall clock between device
+    synchronizations (the distributed loop is host-orchestrated over several streams). Prints one
+    JSON line per form, with the final state's distance from the single-domain step.
+
+    python ewoms-numerics_b200/dd.py --grid 128,128,64 --slabs 1,2,4"""
+    import argparse
+    import json
+    import time
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", default="128,128,64")
+    ap.add_argument("--slabs", default="1,2,4")
+    ap.add_argument("--dt", type=float, default=250.0)
+    ap.add_argument("--linear-tol", type=float, default=1e-3)
+    a = ap.parse_args(argv)
+    nx, ny, nz = (int(v) for v in a.grid.split(","))
+    case = ewg.lens3d_case(nx, ny, nz, seed=0)
+    sopts = ewg.default_solve_opts(linear_solver_tolerance=a.linear_tol)
+    ctx = ewg.Context(case)
+    ctx.apply_initial_solution()
+    st, _ = ctx.newton_apply(a.dt, None, sopts)
+    if st:
+        raise RuntimeError(f"warm-up step failed: {ewg.STATUS_NAMES.get(st, st)}")
+    ctx.advance_time_level()
+    x1 = ctx.get_solution(0)
+    cfg = {"grid": [nx, ny, nz], "cells": case.grid.n_cells, "dt": a.dt, "linear_tol": a.linear_tol}
+
+    def single():
+        ctx.set_solution(1, x1)
+        ctx.set_solution(0, x1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, rep = ctx.newton_apply(a.dt, None, sopts)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, st, rep.iterations, rep.linear_iterations
+    single()
+    t, st, ni, li = single()
+    x_sd = ctx.get_solution(0)
+    print(json.dumps({"form": "single-domain", "s_per_step": t, "status": st, "newton_its": ni,
+                      "bicgstab_its": li, "ms_per_bicgstab_it": 1e3 * t / max(li, 1), **cfg}), flush=True)
+    plane = nx * ny
+    for world in (int(w) for w in a.slabs.split(",")):
+        parts = [DeviceSlab(SlabLinearizer(case, s), sopts) for s in partition(nz, world)]
+
+        def run():
+            for p in parts:
+                p.lin.set_state(local_view(x1, case.grid, p.slab), local_view(x1, case.grid, p.slab))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rep = distributed_newton(parts, LocalComm(), a.dt, None, sopts)
+            torch.cuda.synchronize()
+            return time.perf_counter() - t0, rep
+        run()
+        t, rep = run()
+        x = np.empty_like(x_sd)
+        for p in parts:
+            x[p.slab.k0 * plane:p.slab.k1 * plane] = p.ctx.get_solution(0)[p.lin.own]
+        dp = float(np.max(np.abs(x[:, 0] - x_sd[:, 0])) / np.max(np.abs(x_sd[:, 0])))
+        ds = float(np.max(np.abs(x[:, 1] - x_sd[:, 1])))
+        print(json.dumps({"form": f"z-slabs x{world}", "s_per_step": t, "status": rep.status,
+                          "newton_its": rep.iterations, "bicgstab_its": rep.linear_iterations,
+                          "ms_per_bicgstab_it": 1e3 * t / max(rep.linear_iterations, 1),
+                          "pw_rel_diff": dp, "sn_abs_diff": ds, **cfg}), flush=True)
+        for p in parts:
+            p.lin.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
