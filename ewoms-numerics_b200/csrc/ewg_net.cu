@@ -671,9 +671,8 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* n, double dt, int32_t* usedG
 //
 // ewg_net_forward_noalloc runs the same four k_conv3d launches as the forward pass of
 // ewg_net_eval_host, for callers that must not allocate device memory: a host simulator that
-// hands all of the device's memory to its own arena up front, code that runs while another
-// thread captures a CUDA graph in global capture mode (cudaMalloc is illegal then), and time-step
-// loops that cannot afford the device-wide synchronisation of cudaMalloc / cudaFree. The caller
+// hands all of the device's memory to its own arena up front, and time-step loops that cannot
+// afford the device-wide synchronisation of cudaMalloc / cudaFree. The caller
 // passes the FP32 parameters, the features and the output on the device; the BF16 weights, the
 // 16-channel BF16 features and two 32-channel activation buffers live in one file-scope device
 // array of fixed size, which every GPU that loads this library holds until the process exits.

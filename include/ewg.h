@@ -324,8 +324,7 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* net, double dt, int32_t* use
 
 /* Forward pass of the guess network that allocates no memory (no reference counterpart). For
  * callers that cannot call cudaMalloc: a host simulator whose own arena owns the device's memory,
- * code running while a CUDA graph is captured in global mode (cudaMalloc is illegal then), and
- * step loops that cannot take the device-wide synchronisation of cudaMalloc / cudaFree.
+ * and step loops that cannot take the device-wide synchronisation of cudaMalloc / cudaFree.
  *   params    device, FP32, the layout of ewg_net_get_params (ewg_net_num_params() floats)
  *   features  device, FP32 [B][D][H][W][5];  outputs  device, FP32 [B][D][H][W][2]
  *   stream    cudaStream_t the work is enqueued on (NULL: the legacy default stream); the call
