@@ -191,6 +191,12 @@ class SplitLayout:
         self.flip = slab.first & 1
         self.owned = [slice(c * self.half + slab.ghost_lo * self.planeh,
                             c * self.half + (slab.ghost_lo + slab.k1 - slab.k0) * self.planeh) for c in (0, 1)]
+        self._own = slice(self.owned[0].start, self.owned[0].stop)
+
+    def owned_view(self, a):
+        """The owned rows of both colours as one strided view (colour, row, component): the two
+        colours' owned runs start at the same offset within their halves."""
+        return a.view(2, self.half, 2)[:, self._own]
 
     def plane(self, k: int) -> list[slice]:
         out = []
@@ -206,6 +212,9 @@ class NaturalLayout:
     def __init__(self, grid: ewg.Grid, slab: Slab):
         self.planesz = grid.nx * grid.ny
         self.owned = [slice(slab.ghost_lo * self.planesz, (slab.ghost_lo + slab.k1 - slab.k0) * self.planesz)]
+
+    def owned_view(self, a):
+        return a[self.owned[0]]
 
     def plane(self, k: int) -> list[slice]:
         return [slice(k * self.planesz, (k + 1) * self.planesz)]
@@ -330,17 +339,14 @@ class TorchComm:
 # collective.
 
 def _dev_dot(L, a, b):
-    import torch
-    return sum(torch.vdot(a[s].reshape(-1), b[s].reshape(-1)) for s in L.owned)
+    return (L.owned_view(a) * L.owned_view(b)).sum()
 
 
 def _dev_max(L, a):
     """max |a| over the owned rows (NaN propagates; the host reads it as infinity)."""
     import torch
-    ms = [torch.linalg.vector_norm(a[s], float("inf")) for s in L.owned if a[s].numel()]
-    if not ms:
-        return a.new_zeros(())
-    return ms[0] if len(ms) == 1 else torch.stack(ms).amax()
+    o = L.owned_view(a)
+    return torch.linalg.vector_norm(o, float("inf")) if o.numel() else a.new_zeros(())
 
 
 def _pack(sums, maxes):

@@ -487,3 +487,20 @@ def test_split_layout_ghost_exchange(ewg_mod):
             vecs.append(spl)
         dd.LocalComm().exchange(parts, vecs)
         assert all(torch.equal(a, b) for a, b in zip(vecs, want))
+
+
+def test_split_layout_owned_view_is_the_owned_rows(ewg_mod):
+    """SplitLayout.owned_view covers exactly the rows of both colours' owned runs, so the
+    distributed solve's norms and dot products see every owned cell once and no ghost cell."""
+    import dd
+    import torch
+    case = ewg_mod.lens3d_case(8, 6, 11, seed=0)
+    for world in (1, 2, 3, 4):
+        for s in dd.partition(11, world):
+            g = dd.slab_case(case, s).grid
+            L = dd.SplitLayout(g, s)
+            a = torch.arange(g.n_cells * 2, dtype=torch.float64).reshape(-1, 2)
+            want = torch.cat([a[o] for o in L.owned])
+            got = L.owned_view(a).reshape(-1, 2)
+            assert torch.equal(got, want), (world, s)
+            assert got.shape[0] == (s.k1 - s.k0) * 8 * 6
