@@ -1470,26 +1470,28 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         if ((st = vcheck(c, "kv_p_update"))) return st;
         if ((st = v_prec(c, w, c->s_p, c->s_y))) return st;
         if ((st = v_spmv(c, c->s_y, c->s_v))) return st;
-        if ((st = v_reduce(c, c->s_r0, c->s_v, nullptr, nullptr, nullptr, nullptr, rr))) return st;
+        // r0hat . v, and max |y|: the update y stagnates when it is all zero
+        if ((st = v_reduce(c, c->s_r0, c->s_v, nullptr, nullptr, c->s_y, nullptr, rr))) return st;
+        const bool stagY = rr[2] == 0.0;
         if (fabs(rr[0]) <= breakdownEps) { c->err = "BiCGStab breakdown"; return EWG_ERR_BREAKDOWN; }
         alpha = rho_i / rr[0];
         if (fabs(alpha) <= breakdownEps) { c->err = "BiCGStab stagnation"; return EWG_ERR_BREAKDOWN; }
         kv_h_s<<<g, kVApi, 0, s>>>(n, alpha, c->s_y, c->s_v, c->s_x, c->s_r);
         if ((st = vcheck(c, "kv_h_s"))) return st;
-        // max |s| for the criterion; the update y stagnates when it is all zero
-        if ((st = v_reduce(c, nullptr, nullptr, nullptr, nullptr, c->s_r, c->s_y, rr))) return st;
+        // z = M^-1 s and t = J z come before the half-step check, so that max |s| for the
+        // criterion shares one read-back with t.t, t.s and max |z|; when the half step ends the
+        // solve (or replaces the residual), z and t are left unused
+        if ((st = v_prec(c, w, c->s_r, c->s_z))) return st;
+        if ((st = v_spmv(c, c->s_z, c->s_t))) return st;
+        if ((st = v_reduce(c, c->s_t, c->s_t, c->s_t, c->s_r, c->s_r, c->s_z, rr))) return st;
         resErr = rr[2];
-        bool stag = rr[3] == 0.0;
         if (converged(resErr)) {
             bool goOn;
             if ((st = replace(&goOn))) return st;
             if (!goOn) { *iterations = it; return EWG_OK; }
             continue;
         }
-        if (stag || resErr > so->linear_solver_max_error) { *iterations = it; c->err = "BiCGStab failed"; return EWG_ERR_NOT_CONVERGED; }
-        if ((st = v_prec(c, w, c->s_r, c->s_z))) return st;
-        if ((st = v_spmv(c, c->s_z, c->s_t))) return st;
-        if ((st = v_reduce(c, c->s_t, c->s_t, c->s_t, c->s_r, nullptr, c->s_z, rr))) return st;
+        if (stagY || resErr > so->linear_solver_max_error) { *iterations = it; c->err = "BiCGStab failed"; return EWG_ERR_NOT_CONVERGED; }
         if (fabs(rr[0]) <= breakdownEps) { c->err = "BiCGStab breakdown"; return EWG_ERR_BREAKDOWN; }
         omega = rr[1] / rr[0];
         if (fabs(omega) <= breakdownEps) { c->err = "BiCGStab stagnation"; return EWG_ERR_BREAKDOWN; }
@@ -1497,7 +1499,7 @@ static ewg_status vcfv_solve(ewg_vcfv* c, const ewg_solve_opts* so, int* iterati
         if ((st = vcheck(c, "kv_axpy"))) return st;
         // the criterion sees s (the reference's aliasing r == s) before r = s - omega t; the
         // update z stagnates when it is all zero
-        stag = rr[3] == 0.0;
+        const bool stag = rr[3] == 0.0;
         if (converged(resErr)) {
             bool goOn;
             if ((st = replace(&goOn))) return st;
