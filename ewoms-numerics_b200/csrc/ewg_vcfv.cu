@@ -81,6 +81,16 @@ struct ewg_vcfv {
     double* M = nullptr;      // block ILU(0) factors in the band layout (allocated at the first ILU solve)
     int precond = EWG_PRECOND_JACOBI;  // preconditioner of the current solve
     long long launches = 0;
+    // the ILU(0) application (colour sweeps, relaxation) captured once per input / output / w:
+    // the solve applies it to p -> y and s -> z, so two graphs serve every iteration
+    struct PrecGraph {
+        const double* d = nullptr;
+        double* out = nullptr;
+        double w = 0.0;
+        int kernels = 0;
+        cudaGraphExec_t exec = nullptr;
+    } precGraphs[2];
+    int precGraphNext = 0;
     // LocalLinearizerSplice and NumericDifferenceMethod; the reference pressure of
     // ImmiscibleModel::updateBegin (p_w of vertex 0) for the FD pressure weight, unset until then
     int localLinearizer = EWG_LOCAL_LINEARIZER_AD;
@@ -1104,33 +1114,77 @@ ewg_status v_ilu_factor(ewg_vcfv* c) {
     return EWG_OK;
 }
 
-ewg_status v_prec(ewg_vcfv* c, double w, const double* d, double* out) {
-    if (c->precond == EWG_PRECOND_ILU0) {
-        const int nc = v_ncolours(c);
-        for (int col = 0; col < nc; ++col) {
-            const VColour C = v_colour(c, col);
-            if (C.count == 0) continue;
-            if (c->P.dim == 3) kv_ilu_fwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
-            else kv_ilu_fwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
-            ewg_status st = vcheck(c, "kv_ilu_fwd");
-            if (st) return st;
-        }
-        for (int col = nc - 1; col >= 0; --col) {
-            const VColour C = v_colour(c, col);
-            if (C.count == 0) continue;
-            if (c->P.dim == 3) kv_ilu_bwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
-            else kv_ilu_bwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
-            ewg_status st = vcheck(c, "kv_ilu_bwd");
-            if (st) return st;
-        }
-        if (w != 1.0) {
-            kv_scale<<<vgrid(c, 2 * (int64_t)c->D.NV), kVApi, 0, c->stream>>>(2 * (int64_t)c->D.NV, w, out);
-            return vcheck(c, "kv_scale");
-        }
-        return EWG_OK;
+// the ILU(0) application as direct launches on the context's stream
+ewg_status v_ilu_apply(ewg_vcfv* c, double w, const double* d, double* out) {
+    const int nc = v_ncolours(c);
+    for (int col = 0; col < nc; ++col) {
+        const VColour C = v_colour(c, col);
+        if (C.count == 0) continue;
+        if (c->P.dim == 3) kv_ilu_fwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
+        else kv_ilu_fwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, d, out);
+        ewg_status st = vcheck(c, "kv_ilu_fwd");
+        if (st) return st;
     }
-    kv_jacobi<<<vgrid(c, c->D.NV), kVApi, 0, c->stream>>>(c->D.NV, w, c->s_dinv, d, out);
-    return vcheck(c, "kv_jacobi");
+    for (int col = nc - 1; col >= 0; --col) {
+        const VColour C = v_colour(c, col);
+        if (C.count == 0) continue;
+        if (c->P.dim == 3) kv_ilu_bwd<3><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
+        else kv_ilu_bwd<2><<<vgrid(c, C.count), kVApi, 0, c->stream>>>(c->D, C, col, c->M, out);
+        ewg_status st = vcheck(c, "kv_ilu_bwd");
+        if (st) return st;
+    }
+    if (w != 1.0) {
+        kv_scale<<<vgrid(c, 2 * (int64_t)c->D.NV), kVApi, 0, c->stream>>>(2 * (int64_t)c->D.NV, w, out);
+        return vcheck(c, "kv_scale");
+    }
+    return EWG_OK;
+}
+
+// y = M^-1 d. Block ILU(0) replays a CUDA graph of its 2 x (colours) sweep launches: the
+// factors, colour tables and vectors keep their addresses for the context's lifetime, so a graph
+// captured for (d, out, w) stays valid; the first application of a pair captures it.
+ewg_status v_prec(ewg_vcfv* c, double w, const double* d, double* out) {
+    if (c->precond != EWG_PRECOND_ILU0) {
+        kv_jacobi<<<vgrid(c, c->D.NV), kVApi, 0, c->stream>>>(c->D.NV, w, c->s_dinv, d, out);
+        return vcheck(c, "kv_jacobi");
+    }
+    for (auto& g : c->precGraphs) {
+        if (g.exec && g.d == d && g.out == out && g.w == w) {
+            c->launches += g.kernels;
+            return vfail(c, cudaGraphLaunch(g.exec, c->stream), "ILU graph launch");
+        }
+    }
+    ewg_vcfv::PrecGraph* slot = nullptr;
+    for (auto& g : c->precGraphs) if (!g.exec) { slot = &g; break; }
+    if (!slot) {
+        slot = &c->precGraphs[c->precGraphNext];
+        c->precGraphNext ^= 1;
+        cudaGraphExecDestroy(slot->exec);
+        slot->exec = nullptr;
+    }
+    const long long before = c->launches;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return vfail(c, e, "ILU graph capture");
+    ewg_status st = v_ilu_apply(c, w, d, out);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(c->stream, &graph);
+    const int kernels = (int)(c->launches - before);
+    c->launches = before;
+    if (st || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return st ? st : vfail(c, e, "ILU graph capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return vfail(c, e, "ILU graph instantiate");
+    slot->d = d;
+    slot->out = out;
+    slot->w = w;
+    slot->kernels = kernels;
+    slot->exec = exec;
+    c->launches += kernels;
+    return vfail(c, cudaGraphLaunch(exec, c->stream), "ILU graph launch");
 }
 
 }  // namespace
@@ -1222,6 +1276,7 @@ ewg_status ewg_vcfv_create(const ewg_grid* grid, const ewg_problem* problem, con
 void ewg_vcfv_destroy(ewg_vcfv* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& g : c->precGraphs) if (g.exec) cudaGraphExecDestroy(g.exec);
     void* ps[] = {c->x0, c->x1, c->sold, c->r, c->perm, c->totVol, c->kedge, c->iq, c->J, c->lens, c->geo, c->d_errmax,
                   c->d_flags, c->s_b, c->s_x, c->s_r, c->s_r0, c->s_v, c->s_p, c->s_y, c->s_z, c->s_t, c->s_dinv,
                   c->s_red, c->M};
