@@ -264,6 +264,31 @@ class LocalComm:
         elif cuda:
             torch.cuda.synchronize()
 
+    def reduce_device(self, vals, parts=None):
+        """The sum over the slabs of one partial tensor each, left on the device (no host read).
+        With several slabs the sum runs on the current stream after it has waited for every
+        slab's stream, and the slabs' streams wait for the sum (device synchronizations instead
+        where a slab has no stream)."""
+        import torch
+        if len(vals) == 1:
+            return vals[0]
+        cuda = any(v.is_cuda for v in vals)
+        streams = [getattr(sp, "stream", None) for sp in (parts or [])]
+        ordered = cuda and len(streams) == len(vals) and all(st is not None for st in streams)
+        if ordered:
+            cur = torch.cuda.current_stream()
+            for st in streams:
+                cur.wait_stream(st)
+        elif cuda:
+            torch.cuda.synchronize()
+        out = torch.stack(vals).sum(0)
+        if ordered:
+            for st in streams:
+                st.wait_stream(cur)
+        elif cuda:
+            torch.cuda.synchronize()
+        return out
+
     def reduce(self, vals, nsum):
         """vals: one 1-D tensor of partials per slab, the first nsum summed over the slabs and the
         rest maximised. One host read per slab. The partials were computed on the slabs' own
@@ -315,6 +340,16 @@ class TorchComm:
                 n = c.stop - c.start
                 v[c] = into[o:o + n]
                 o += n
+
+    def reduce_device(self, vals, parts=None):
+        """The sum over the ranks of this rank's partial tensor, left on the device: one
+        all_gather, summed in rank order, so every rank holds the same bits."""
+        import torch
+        (x,) = vals
+        x = x.to(self._device).reshape(1)
+        g = [torch.empty_like(x) for _ in range(self.dist.get_world_size())]
+        self.dist.all_gather(g, x)
+        return torch.stack(g).sum(0).reshape(())
 
     def reduce(self, vals, nsum):
         """One all_gather of this rank's partials (a 1-D tensor, the first nsum summed and the rest
@@ -402,11 +437,12 @@ def _bicgstab(parts, comm, opts):
     as restricted additive Schwarz: the ghost planes of the preconditioned vector come from the
     neighbours, each slab applies its own M^-1 (block ILU(0) or Jacobi of the slab matrix,
     ghost rows included), and only the owned rows are kept. Ghost planes of a vector are
-    refreshed before every SpMV. The partials of an iteration meet in three reductions, each one
-    host read per slab and one collective: <r0,v>; the half-step max-norms of s and y
-    together with <t,t> and <t,s> (z and t are computed before the half-step check and left
-    unused when it ends the solve); the full-step max-norms of s and z with <r0,r> and <r,r>.
-    A zero max-norm of y or z is the stagnation test.
+    refreshed before every SpMV. The partials of an iteration meet in three reductions, one
+    collective each: <r0,v> stays on the device (alpha = rho_i / <r0,v> is formed there); the
+    half-step max-norms of s and y together with <t,t>, <t,s> and <r0,v> (z and t are computed
+    before the half-step check and left unused when it ends the solve), one host read per slab;
+    the full-step max-norms of s and z with <r0,r> and <r,r>, one host read per slab. A zero
+    max-norm of y or z is the stagnation test.
 
     Returns (status, iterations, restarts, final residual, initial residual, [dx per slab])."""
     import contextlib
@@ -482,31 +518,38 @@ def _bicgstab(parts, comm, opts):
             exchange("p")
             each(lambda p, v: p.precondition(v.p, v.y))
             exchange("y")
-            (d,), _ = comm.reduce(each(lambda p, v: (p.spmv(v.y, v.v), _pack([_dev_dot(p.layout, v.r0, v.v)], []))[1]), 1)
+            # <r0,v> stays on the device: alpha = rho_i / <r0,v> is formed there, and <r0,v> reaches
+            # the host with the next read-back, where the breakdown tests run (x and r have moved
+            # by then, which a breakdown makes moot)
+            d_dev = comm.reduce_device(each(lambda p, v: (p.spmv(v.y, v.v), _dev_dot(p.layout, v.r0, v.v))[1]),
+                                       parts)
             S["restartPending"] = 0
-            if abs(d) <= DBL_BREAKDOWN:
-                S["status"] = ST_BREAKDOWN
-                break
-            S["alpha"] = S["rho_i"] / d
-            if abs(S["alpha"]) <= DBL_BREAKDOWN:
-                S["status"] = ST_BREAKDOWN
-                break
-            alpha = S["alpha"]
+            rho_i = S["rho_i"]
 
             def upd_hs(p, v):
-                v.x.add_(v.y, alpha=alpha)
-                v.r.sub_(v.v, alpha=alpha)
-                v.half = [_dev_max(p.layout, v.r), _dev_max(p.layout, v.y)]
+                alpha_dev = rho_i / d_dev
+                v.x.addcmul_(v.y, alpha_dev)
+                v.r.addcmul_(v.v, alpha_dev, value=-1.0)
+                # exactly one slab (the bottom one) carries <r0,v> in its sums
+                v.half = ([d_dev if p.slab.k0 == 0 else torch.zeros_like(d_dev)],
+                          [_dev_max(p.layout, v.r), _dev_max(p.layout, v.y)])
             each(upd_hs)
             # the half-step check travels with <t,t> and <t,s>: z = M^-1 s and t = J z are
             # computed before it is known, and left unused when the half step ends the solve
             exchange("r")
             each(lambda p, v: p.precondition(v.r, v.z))
             exchange("z")
-            (tt, ts), (smax, ymax) = comm.reduce(
+            (tt, ts, d), (smax, ymax) = comm.reduce(
                 each(lambda p, v: (p.spmv(v.z, v.t),
-                                   _pack([_dev_dot(p.layout, v.t, v.t), _dev_dot(p.layout, v.t, v.r)],
-                                         v.half))[1]), 2)
+                                   _pack([_dev_dot(p.layout, v.t, v.t), _dev_dot(p.layout, v.t, v.r)] + v.half[0],
+                                         v.half[1]))[1]), 3)
+            if abs(d) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
+            S["alpha"] = rho_i / d
+            if abs(S["alpha"]) <= DBL_BREAKDOWN:
+                S["status"] = ST_BREAKDOWN
+                break
             S["resErr"] = smax
             criterion(ymax == 0.0)  # the update y stagnates when it is all zero
             if S["status"] != ST_RUNNING:

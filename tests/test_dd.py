@@ -250,10 +250,11 @@ def test_distributed_bicgstab_solves_the_whole_grid(oracle_mod, ewg_mod, world):
 
 
 class CountingComm:
-    """LocalComm that counts the reductions (one collective each between ranks)."""
+    """LocalComm that counts the reductions (one collective each between ranks): those read back
+    to the host and those left on the device."""
 
     def __init__(self, dd):
-        self.inner, self.reductions = dd.LocalComm(), 0
+        self.inner, self.reductions, self.device_reductions = dd.LocalComm(), 0, 0
 
     def exchange(self, parts, vecs):
         self.inner.exchange(parts, vecs)
@@ -262,12 +263,17 @@ class CountingComm:
         self.reductions += 1
         return self.inner.reduce(vals, nsum)
 
+    def reduce_device(self, vals, parts=None):
+        self.device_reductions += 1
+        return self.inner.reduce_device(vals, parts)
+
 
 @pytest.mark.parametrize("verify", [0, 1])
 def test_distributed_bicgstab_takes_three_reductions_per_iteration(oracle_mod, ewg_mod, verify):
-    """Every BiCGStab iteration's dot products and max-norms meet in three reductions: <r0,v>;
-    the half-step check with <t,t>, <t,s>; the full-step check with <r0,r>, <r,r>. Besides
-    them: one for ||b|| at the start, one per true-residual check."""
+    """Every BiCGStab iteration's dot products and max-norms meet in three reductions: <r0,v> on
+    the device; the half-step check with <t,t>, <t,s> and <r0,v>; the full-step check with
+    <r0,r>, <r,r>; only the last two are read back to the host. Besides them: one for ||b|| at
+    the start, one per true-residual check."""
     import dd
     case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
     og, x0, x1 = _perturbed_state(oracle_mod, case)
@@ -277,9 +283,10 @@ def test_distributed_bicgstab_takes_three_reductions_per_iteration(oracle_mod, e
     comm = CountingComm(dd)
     st, its, restarts, _, _, _ = dd.distributed_bicgstab(parts, comm, opts)
     assert st == dd.ST_CONVERGED and its == 27
-    # the converging iteration ends after its second (half step) or third (full step) reduction
+    # the converging iteration ends after its first (half step) or second (full step) host read
     # without adding to the count
-    assert comm.reductions - 1 - 3 * its - verify * (1 + restarts) in (2, 3), comm.reductions
+    assert comm.reductions - 1 - 2 * its - verify * (1 + restarts) in (1, 2), comm.reductions
+    assert comm.device_reductions == its + 1
 
 
 def _check_newton_state(x_dd, x_sd):
