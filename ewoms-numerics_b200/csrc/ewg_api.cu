@@ -617,6 +617,16 @@ ewg_status ewg_update_begin(ewg_ctx* ctx) {
     return update_reference_pressure(ctx, true);
 }
 
+ewg_status ewg_set_reference_pressure(ewg_ctx* ctx, double p_ref) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    if (!(p_ref > 0) || !std::isfinite(p_ref)) {
+        ctx->err = "set_reference_pressure: p_ref must be positive and finite";
+        return EWG_ERR_INVALID;
+    }
+    ctx->refPressure = p_ref;
+    return EWG_OK;
+}
+
 ewg_status ewg_get_intensive_quantities(ewg_ctx* ctx, double* out) {
     if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
     ewg_status st = launch_intensive(ctx, ctx->x0);

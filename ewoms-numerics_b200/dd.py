@@ -151,6 +151,12 @@ class SlabLinearizer:
         self.ctx.set_solution(1, x_old_local)
         self.ctx.set_solution(0, x_local)
 
+    def set_reference_pressure(self, p_ref: float):
+        """The finite-difference linearizer's reference pressure: pass the whole grid's (p_w of
+        global cell 0, known to the bottom slab), so the slab's deflections are the whole
+        grid's."""
+        self.ctx.set_reference_pressure(p_ref)
+
     def linearize(self, dt: float) -> float:
         """Linearizes the slab; returns max |r| over the owned rows (the Newton error's share)."""
         self.ctx.linearize(dt)

@@ -376,6 +376,7 @@ def load(path: str = LIB_PATH):
         "ewg_linearize": (C.c_int, [C.c_void_p, d, P(LinReport)]),
         "ewg_set_local_linearizer": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
         "ewg_update_begin": (C.c_int, [C.c_void_p]),
+        "ewg_set_reference_pressure": (C.c_int, [C.c_void_p, C.c_double]),
         "ewg_get_intensive_quantities": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_get_residual": (C.c_int, [C.c_void_p, P(d)]),
         "ewg_get_jacobian_bcrs": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(d)]),
@@ -541,6 +542,10 @@ class Context:
     def update_begin(self):
         """ImmiscibleModel::updateBegin: records the FD linearizer's reference pressure."""
         self._check(self.lib.ewg_update_begin(self.h), "update_begin")
+
+    def set_reference_pressure(self, p_ref: float):
+        """updateBegin with the caller's reference pressure (a slab takes the whole grid's)."""
+        self._check(self.lib.ewg_set_reference_pressure(self.h, float(p_ref)), "set_reference_pressure")
 
     def intensive_quantities(self):
         """N x {p_cnw, lambda_w, lambda_n} of solution(0), natural order."""

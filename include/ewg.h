@@ -215,6 +215,12 @@ ewg_status ewg_set_local_linearizer(ewg_ctx* ctx, int32_t kind, int32_t numeric_
  * (fvbasediscretization.hh:1242); ewg_newton_apply does so itself, and a context that never ran it
  * takes p_ref from solution(0) at its first finite-difference linearization. */
 ewg_status ewg_update_begin(ewg_ctx* ctx);
+/* The same step with p_ref given by the caller (immisciblemodel.hh:278-293 reads p_w of the
+ * grid's first DOF): a z-slab of a decomposed grid passes the whole grid's value, p_w of global
+ * cell 0, so that its finite-difference deflections, and with them its owned Jacobian rows, equal
+ * the whole grid's. p_ref must be positive and finite; it holds until the next ewg_update_begin
+ * (ewg_newton_apply runs one). */
+ewg_status ewg_set_reference_pressure(ewg_ctx* ctx, double p_ref);
 
 /* linearizeDomain() at the current iterate with time-step size dt: residual r(x) and Jacobian
  * dr/dx into device buffers (fvbaselinearizer.hh:166-197, 401-512). */

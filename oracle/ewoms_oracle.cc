@@ -1522,6 +1522,8 @@ void orc_apply_initial_solution(orc_ctx* o) {
 void orc_advance_time_level(orc_ctx* o) { o->C.sol[1] = o->C.sol[0]; }
 
 void orc_update_begin(orc_ctx* o) { o->C.refPressure = o->C.sol[0][0]; }
+// updateBegin with the caller's reference pressure (a z-slab takes the whole grid's)
+void orc_set_reference_pressure(orc_ctx* o, double p) { o->C.refPressure = p; }
 int orc_linearize(orc_ctx* o, double dt, int it, double* error) {
     // a context that never ran updateBegin takes the reference pressure of the current iterate
     if (o->C.fd && !(o->C.refPressure > 0)) o->C.refPressure = o->C.sol[0][0];

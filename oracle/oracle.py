@@ -54,6 +54,7 @@ def load():
         "orc_set_recycle_first_iteration_storage": (None, [C.c_void_p, C.c_int]),
         "orc_set_local_linearizer": (None, [C.c_void_p, C.c_int, C.c_int]),
         "orc_update_begin": (None, [C.c_void_p]),
+        "orc_set_reference_pressure": (None, [C.c_void_p, C.c_double]),
         "orc_set_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_get_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_apply_initial_solution": (None, [C.c_void_p]),
@@ -145,6 +146,10 @@ class Oracle:
     def update_begin(self):
         """ImmiscibleModel::updateBegin: the reference pressure for the FD pressure weight."""
         self.lib.orc_update_begin(self.h)
+
+    def set_reference_pressure(self, p_ref):
+        """updateBegin with the caller's reference pressure (a z-slab takes the whole grid's)."""
+        self.lib.orc_set_reference_pressure(self.h, float(p_ref))
 
     def set_solution(self, t, x):
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)

@@ -139,6 +139,48 @@ def test_oracle_slab_rows_equal_the_whole_grid(oracle_mod, ewg_mod, world):
     o.close()
 
 
+@pytest.mark.parametrize("method", [1, 0])
+def test_oracle_fd_slab_rows_equal_the_whole_grid(oracle_mod, ewg_mod, method):
+    """With the finite-difference linearizer (forward and central differences) the slabs' owned
+    rows equal the whole grid's bit for bit once every slab takes the whole grid's reference
+    pressure (p_w of global cell 0); with its own (p_w of its first cell) a slab above the first
+    deflects the pressure by a different step."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    og, x0, x1 = _perturbed_state(oracle_mod, case)
+    o = oracle_mod.Oracle(case)
+    o.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+    o.set_solution(1, x1)
+    o.set_solution(0, x0)
+    o.update_begin()
+    o.linearize(250.0)
+    r_g = o.residual()
+    rp_g, ci_g, b_g = o.jacobian_bcrs()
+    plane = 16 * 12
+    for given in (True, False):
+        same = []
+        for s in dd.partition(10, 3):
+            sc = dd.slab_case(case, s)
+            ol = oracle_mod.Oracle(sc)
+            ol.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+            ol.set_solution(1, dd.local_view(x1, case.grid, s))
+            ol.set_solution(0, dd.local_view(x0, case.grid, s))
+            if given:
+                ol.set_reference_pressure(x0[0, 0])
+            else:
+                ol.update_begin()
+            ol.linearize(250.0)
+            own = dd.owned_rows(sc.grid, s)
+            assert np.array_equal(ol.residual()[own], r_g[s.k0 * plane:s.k1 * plane])
+            rp, ci, b = ol.jacobian_bcrs()
+            shift = s.first * plane
+            same.append(all(np.array_equal(b[rp[lr]:rp[lr + 1]], b_g[rp_g[lr + shift]:rp_g[lr + shift + 1]])
+                            for lr in range(own.start, own.stop)))
+            ol.close()
+        assert all(same) if given else not all(same[1:])
+    o.close()
+
+
 # ---- the distributed BiCGStab's host logic, driven by the oracle as the slabs' operators ----
 
 class OracleSlab:

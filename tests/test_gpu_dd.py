@@ -50,6 +50,42 @@ def test_slab_linearization_equals_single_domain(ewg_mod, world):
     ctx.close()
 
 
+@pytest.mark.parametrize("method", [1, 0])
+def test_fd_slab_linearization_equals_single_domain(ewg_mod, method):
+    """The finite-difference linearizer (forward and central) on device slabs: with the whole
+    grid's reference pressure (p_w of global cell 0) every slab's owned residual and Jacobian rows
+    equal the single-domain FD linearization's bit for bit."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    ctx = ewg_mod.Context(case)
+    ctx.apply_initial_solution()
+    x1 = ctx.get_solution(0)
+    rng = np.random.default_rng(5)
+    x0 = x1.copy()
+    x0[:, 0] += rng.normal(0, 20.0, len(x0))
+    x0[:, 1] = np.clip(x0[:, 1] - np.abs(rng.normal(0, 0.2, len(x0))), 0.3, 1.0)
+    ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+    ctx.set_solution(1, x1)
+    ctx.set_solution(0, x0)
+    ctx.update_begin()
+    ctx.linearize(250.0)
+    r_g = ctx.residual()
+    rp_g, ci_g, b_g = ctx.jacobian_bcrs()
+    for s in dd.partition(case.grid.nz, 3):
+        lin = dd.SlabLinearizer(case, s)
+        lin.ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, method)
+        lin.set_state(dd.local_view(x0, case.grid, s), dd.local_view(x1, case.grid, s))
+        lin.set_reference_pressure(x0[0, 0])
+        lin.linearize(250.0)
+        rows, rp, ci, b = lin.owned_jacobian()
+        assert np.array_equal(lin.owned_residual(), r_g[rows])
+        for lr, gr in zip(range(lin.own.start, lin.own.stop), rows):
+            assert np.array_equal(ci[rp[lr]:rp[lr + 1]], ci_g[rp_g[gr]:rp_g[gr + 1]]), gr
+            assert np.array_equal(b[rp[lr]:rp[lr + 1]], b_g[rp_g[gr]:rp_g[gr + 1]]), gr
+        lin.close()
+    ctx.close()
+
+
 def _state_after_steps(ewg_mod, case, steps):
     ctx = ewg_mod.Context(case)
     ctx.apply_initial_solution()
