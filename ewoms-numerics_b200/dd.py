@@ -634,7 +634,9 @@ class DistributedNewtonReport:
 
 
 def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNewtonReport:
-    """NewtonMethod::apply (newtonmethod.hh:308-517) over the slabs: each iteration linearizes
+    """NewtonMethod::apply (newtonmethod.hh:308-517) over the slabs, after updateBegin (every
+    slab takes the whole grid's reference pressure for the finite-difference linearizer): each
+    iteration linearizes
     every slab, takes the error as the maximum |r| over all owned rows, solves with
     distributed_bicgstab, subtracts the update from the owned rows of solution(0) and refreshes
     the ghost planes from the neighbours. The stopping rules are the single-domain ones
@@ -661,6 +663,17 @@ def distributed_newton(parts, comm, dt, nopts=None, sopts=None) -> DistributedNe
                 return error * 4.0 < last
             return True
 
+        # updateBegin before the solve, as ewg_newton_apply does: every slab takes the whole
+        # grid's reference pressure, p_w of global cell 0 (position 0 of the bottom slab's
+        # solution(0) in either storage order); only the finite-difference linearizer reads it
+        refs = []
+        for p in parts:
+            with p.on():
+                x = p.solution()
+                refs.append(_pack([x[0, 0] if p.slab.k0 == 0 else x.new_zeros(())], []))
+        (p_ref,), _ = comm.reduce(refs, 1)
+        for p in parts:
+            p.ctx.set_reference_pressure(p_ref)
         while proceed():
             last = error
             errs = []

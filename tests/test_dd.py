@@ -238,6 +238,9 @@ class OracleNewtonSlab(OracleSlab):
         self.o.linearize(dt, self.iteration)
         self.iteration += 1
 
+    def set_reference_pressure(self, p_ref):
+        self.o.set_reference_pressure(p_ref)
+
     def solution(self):
         return self.x
 
@@ -384,6 +387,30 @@ def test_distributed_newton_matches_the_single_domain(oracle_mod, ewg_mod, world
     ow.linearize(250.0, 1)
     assert np.max(np.abs(ow.residual())) == rep.error
     ow.close()
+    o.set_solution(1, x1)
+    o.set_solution(0, x1)
+    rc, ni, li, e = o.newton_apply(250.0)
+    assert rc == 0
+    _check_newton_state(x_dd, o.get_solution(0))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_fd_newton_matches_the_single_domain(oracle_mod, ewg_mod, world):
+    """Newton over slabs that linearize with finite differences (distributed_newton hands every
+    slab the whole grid's reference pressure; the row-level tests pin its effect): the step
+    converges and agrees with the single-domain oracle's FD Newton."""
+    import dd
+    case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
+    o = _stepped_state(oracle_mod, case, 2)
+    x1 = o.get_solution(0)
+    sopts = ewg_mod.default_solve_opts()
+    parts = [OracleNewtonSlab(oracle_mod, case, s, x1, x1, sopts) for s in dd.partition(10, world)]
+    for p in parts:
+        p.o.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, 1)
+    rep = dd.distributed_newton(parts, dd.LocalComm(), 250.0, None, sopts)
+    assert rep.converged, (rep.status, rep.iterations, rep.error)
+    x_dd = np.concatenate([p.x.numpy()[p.layout.owned[0]] for p in parts])
+    o.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, 1)
     o.set_solution(1, x1)
     o.set_solution(0, x1)
     rc, ni, li, e = o.newton_apply(250.0)
