@@ -340,16 +340,29 @@ ewg_status ensure_capacity(ewg_net* n, int64_t V) {
     return EWG_OK;
 }
 
+// The dynamic shared-memory limit of one k_conv3d instance (its weights, up to 55,296 B, are above
+// the 48 KB default). The attribute belongs to the current device, so ewg_net_create sets it for
+// the device the net lives on.
+template <int CIN, int COUT, int EPI>
+cudaError_t conv_smem_attr() {
+    return cudaFuncSetAttribute(k_conv3d<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(__nv_bfloat16) * kTaps * COUT * CIN));
+}
+
+cudaError_t conv_smem_attrs() {
+    cudaError_t e = conv_smem_attr<16, 32, EPI_BIAS_RELU>();
+    if (!e) e = conv_smem_attr<32, 32, EPI_BIAS_RELU>();
+    if (!e) e = conv_smem_attr<32, 8, EPI_BIAS>();
+    if (!e) e = conv_smem_attr<16, 32, EPI_MASK>();
+    if (!e) e = conv_smem_attr<32, 32, EPI_MASK>();
+    return e;
+}
+
 template <int CIN, int COUT, int EPI>
 void launch_conv(ewg_net* n, const VolDims& d, const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias,
                  const __nv_bfloat16* mask, int maskC, void* out, int outC) {
     const size_t smem = sizeof(__nv_bfloat16) * kTaps * COUT * CIN;
     auto k = k_conv3d<CIN, COUT, EPI>;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
     const int64_t tiles = (d.V() + 15) / 16;
     int64_t blocks = (tiles + 3) / 4;
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -413,6 +426,7 @@ ewg_status ewg_net_create(uint64_t seed, ewg_net** out) {
     ewg_net* n = new ewg_net();
     cudaGetDevice(&n->device);
     cudaError_t e = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking);
+    if (!e) e = conv_smem_attrs();
     int64_t off = 0;
     for (int l = 0; l < kNetLayers; ++l) {
         n->wOff[l] = off; off += layer_w(l);

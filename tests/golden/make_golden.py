@@ -1,8 +1,16 @@
-"""Generate the committed golden fixtures of the 2D lens problem (48 x 32) from the CPU oracle.
+"""Generate the committed golden fixtures of the lens problem from the CPU oracle.
+
+lens2d_golden.npz: the 2D lens problem (48 x 32), linearizations and 10-step runs of both presets,
+material-law values. lens3d_golden.npz: 10 implicit-Euler steps (dt 250 s, Newton tolerance 1e-8,
+BiCGStab + natural-order block ILU(0), linear tolerance 1e-10) of the 3D lens problem on
+32 x 32 x 16 and 64 x 64 x 32 grids with seeded log-normal permeability; each entry stores the
+permeability field it was run with, so the GPU test runs on the same bits wherever numpy's
+transcendental functions round differently.
 
 The reference itself cannot be built here (DUNE / ewoms-material are absent) and ships no golden
 vectors, so these fixtures pin the oracle restatement against regressions and give the GPU tests
-inputs and outputs that do not need the oracle at run time. Run:  python tests/golden/make_golden.py
+inputs and outputs that do not need the oracle at run time.
+Run:  python tests/golden/make_golden.py [--2d] [--3d]   (both when no flag is given)
 """
 import os
 import sys
@@ -47,6 +55,30 @@ def run10(case, ordering):
     return o.get_solution(0), np.array(steps, dtype=np.int32)
 
 
+# (tag, grid shape, permeability seed, correlation length in cells) of the 3D fixtures
+CASES_3D = (("g32x32x16", (32, 32, 16), 7, 4.0), ("g64x64x32", (64, 64, 32), 8, 8.0))
+
+
+def case_3d(shape, seed, corr_cells):
+    return ewg.lens3d_case(*shape, seed=seed, corr_cells=corr_cells)
+
+
+def main_3d():
+    out = {}
+    for tag, shape, seed, corr in CASES_3D:
+        case = case_3d(shape, seed, corr)
+        o = oracle.Oracle(case, nthreads=os.cpu_count() or 1)
+        o.apply_initial_solution()
+        steps = o.run(10, 250.0, ordering=oracle.ORDER_NATURAL)
+        out[f"{tag}_perm"] = case.perm
+        out[f"{tag}_run10_x"] = o.get_solution(0)
+        out[f"{tag}_run10_steps"] = np.array(steps, dtype=np.int32)
+        print(tag, steps)
+    path = os.path.join(HERE, "lens3d_golden.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 def main():
     out = {}
     for name, mk in (("baseline", ewg.baseline_case), ("reference", ewg.reference_case)):
@@ -70,4 +102,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    flags = set(sys.argv[1:])
+    if not flags or "--2d" in flags:
+        main()
+    if not flags or "--3d" in flags:
+        main_3d()
