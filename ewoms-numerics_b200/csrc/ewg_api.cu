@@ -284,6 +284,7 @@ ewg_status to_split(ewg_ctx* ctx, const double* host, double2* dev) {
     const size_t bytes = sizeof(double2) * ctx->P.N;
     if ((e = cudaMemcpyAsync(ctx->d_stage, host, bytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "H2D");
+    ctx->h2dBytes += bytes;
     EWG_LAUNCH(ctx, K_LAYOUT, k_natural_to_split, lgrid(ctx, (const void*)k_natural_to_split), kApiBlock, ctx->P, ctx->d_stage, dev);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "natural_to_split");
     return cuda_fail(ctx, cudaStreamSynchronize(ctx->stream), "sync H2D");
@@ -296,6 +297,7 @@ ewg_status from_split(ewg_ctx* ctx, const double2* dev, double* host) {
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "split_to_natural");
     if ((e = cudaMemcpyAsync(host, ctx->d_stage, bytes, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "D2H");
+    ctx->d2hBytes += bytes;
     return cuda_fail(ctx, cudaStreamSynchronize(ctx->stream), "sync D2H");
 }
 
@@ -639,6 +641,7 @@ ewg_status ewg_get_intensive_quantities(ewg_ctx* ctx, double* out) {
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) ctx->d2hBytes += bytes;
     cudaFree(d);
     return cuda_fail(ctx, e, "intensive quantities");
 }
@@ -671,8 +674,10 @@ ewg_status ewg_get_jacobian_bcrs(ewg_ctx* ctx, int32_t* rowPtr, int32_t* colIdx,
     const Phys& P = ctx->P;
     if (rowPtr && (e = cudaMemcpyAsync(rowPtr, ctx->d_rowPtr, sizeof(int32_t) * (P.N + 1), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "rowptr");
+    if (rowPtr) ctx->d2hBytes += sizeof(int32_t) * (P.N + 1);
     if (colIdx && (e = cudaMemcpyAsync(colIdx, ctx->d_colIdx, sizeof(int32_t) * ctx->nnzb, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
         return cuda_fail(ctx, e, "colidx");
+    if (colIdx) ctx->d2hBytes += sizeof(int32_t) * ctx->nnzb;
     if (!blocks) return cuda_fail(ctx, cudaStreamSynchronize(ctx->stream), "sync pattern");
     if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "BCRS export needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
     double* tmp = nullptr;
@@ -682,6 +687,7 @@ ewg_status ewg_get_jacobian_bcrs(ewg_ctx* ctx, int32_t* rowPtr, int32_t* colIdx,
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(blocks, tmp, sizeof(double) * 4 * ctx->nnzb, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) ctx->d2hBytes += sizeof(double) * 4 * ctx->nnzb;
     cudaFree(tmp);
     return cuda_fail(ctx, e, "export blocks");
 }
@@ -703,6 +709,7 @@ ewg_status ewg_set_matrix_bcrs(ewg_ctx* ctx, const int32_t* rowPtr, const int32_
     // and the legacy stream does not order the non-blocking context stream
     e = cudaMemcpyAsync(tmp, blocks, sizeof(double) * 4 * ctx->nnzb, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
+        ctx->h2dBytes += sizeof(double) * 4 * ctx->nnzb;
         EWG_LAUNCH(ctx, K_BCRS, k_bcrs_blocks<false>, lgrid(ctx, (const void*)k_bcrs_blocks<false>), kApiBlock, P, ctx->d_rowPtr, ctx->d_colIdx, ctx->J, tmp, ctx->d_flags);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -716,6 +723,14 @@ ewg_status ewg_set_matrix_bcrs(ewg_ctx* ctx, const int32_t* rowPtr, const int32_
 ewg_status ewg_set_residual(ewg_ctx* ctx, const double* b) {
     if (check_ctx(ctx) || !b) return EWG_ERR_INVALID;
     return to_split(ctx, b, ctx->r);
+}
+
+ewg_status ewg_transfer_counters(ewg_ctx* ctx, int32_t reset, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    if (h2d_bytes) *h2d_bytes = ctx->h2dBytes;
+    if (d2h_bytes) *d2h_bytes = ctx->d2hBytes;
+    if (reset) ctx->h2dBytes = ctx->d2hBytes = 0;
+    return EWG_OK;
 }
 
 ewg_status ewg_residual_norm(ewg_ctx* ctx, const double* x, double dt, double* maxNorm) {

@@ -239,6 +239,9 @@ struct ewg_ctx {
     // host staging
     double* h_pinned = nullptr;
     size_t h_pinnedBytes = 0;
+    // bytes copied between the caller's host buffers and the device by the entry points
+    // (ewg_transfer_counters); the library's own control reads are not counted
+    uint64_t h2dBytes = 0, d2hBytes = 0;
     ewg::Profiler prof;
 };
 

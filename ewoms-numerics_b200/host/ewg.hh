@@ -80,6 +80,10 @@ public:
         return rep;
     }
     void getUpdate(double* dx) const { check(ewg_get_update(ctx_, dx), "ewg_get_update"); }
+    // bytes copied between host buffers and the device by this context's entry points
+    void transferCounters(bool reset, uint64_t* h2d, uint64_t* d2h) {
+        check(ewg_transfer_counters(ctx_, reset ? 1 : 0, h2d, d2h), "ewg_transfer_counters");
+    }
     void newtonUpdate() { check(ewg_newton_update(ctx_), "ewg_newton_update"); }
     double residualNorm(const double* x, double dt) {
         double v = 0;

@@ -11,11 +11,19 @@
 // LinearSolverMaxError, PreconditionerRelaxation; two are new: GpuPreconditioner (ilu0 | jacobi)
 // and GpuLinearSolverPrecision (fp64 | mixed).
 //
-// With GpuEcfvLinearizer the Jacobian and residual are already on the device and setMatrix /
-// setResidual only mark them current. With the CPU linearizer setMatrix uploads the BCRS matrix
-// (structured pattern) and setResidual the residual. solve() returns false when BiCGStab does not
-// converge and throws Ewoms::NumericalIssue on breakdown, like BiCGStabSolver::apply
-// (bicgstabsolver.hh:196-197, 228-232, 284-288). This header compiles inside an eWoms build.
+// The backend solves on the device context of the model's linearizer, which must be
+// GpuEcfvLinearizer (it calls linearizer().context()). What setMatrix and setResidual move:
+// * setMatrix(M) with the linearizer's GpuSparseMatrixAdapter: nothing, unless a host consumer
+//   changed blocks since the linearization, in which case the host copy is uploaded first.
+//   Any other SparseMatrixAdapter (IstlSparseMatrixAdapter) is uploaded from M.istlMatrix().
+// * setResidual(b) with the linearizer's own residual() object (what NewtonMethod::apply passes,
+//   newtonmethod.hh:371-373): nothing, the device residual is the one it was downloaded from.
+//   Any other vector is uploaded. getResidual(b) downloads the device residual into any vector
+//   but the linearizer's own.
+// solve() returns false when BiCGStab does not converge and throws Ewoms::NumericalIssue on
+// breakdown, like BiCGStabSolver::apply (bicgstabsolver.hh:196-197, 228-232, 284-288); the update
+// is the only vector it downloads. This header compiles inside an eWoms build; the repository
+// compiles it against a stand-in of the property system in tests/dropin/.
 #ifndef EWOMS_GPU_BICGSTAB_BACKEND_HH
 #define EWOMS_GPU_BICGSTAB_BACKEND_HH
 
@@ -26,6 +34,7 @@
 #include <vector>
 
 #include "ewg.hh"
+#include "gpusparsematrixadapter.hh"
 
 BEGIN_PROPERTIES
 NEW_PROP_TAG(GpuPreconditioner);
@@ -70,18 +79,33 @@ public:
 
     void setResidual(const Vector& b)
     {
-        if (deviceSystem_())
-            return;  // the GPU linearizer wrote it on the device
+        if (&b == &simulator_.model().linearizer().residual())
+            return;  // downloaded from the device residual by the linearization
         pack_(b, host_);
         ctx_()->setResidual(host_.data());
     }
 
-    void getResidual(Vector& b) const { (void)b; }
+    void getResidual(Vector& b) const
+    {
+        if (&b == &simulator_.model().linearizer().residual())
+            return;
+        host_.resize(2 * b.size());
+        ctx_()->getResidual(host_.data());
+        for (size_t i = 0; i < b.size(); ++i) {
+            b[i][0] = host_[2 * i];
+            b[i][1] = host_[2 * i + 1];
+        }
+    }
 
     void setMatrix(const SparseMatrixAdapter& M)
     {
-        if (deviceSystem_())
-            return;
+        if constexpr (Linear::IsGpuSparseMatrixAdapter<SparseMatrixAdapter>::value) {
+            if (M.deviceContext() == ctx_()) {
+                // device-resident: upload only what a host consumer changed
+                const_cast<SparseMatrixAdapter&>(M).uploadIfHostNewer();
+                return;
+            }
+        }
         const auto& A = M.istlMatrix();
         std::vector<int32_t> rowPtr(A.N() + 1, 0), colIdx;
         std::vector<double> blocks;
@@ -133,7 +157,6 @@ public:
 
 private:
     ewg::Context* ctx_() const { return simulator_.model().linearizer().context(); }
-    bool deviceSystem_() const { return true; }
 
     static void pack_(const Vector& v, std::vector<double>& out)
     {
@@ -145,7 +168,7 @@ private:
     }
 
     const Simulator& simulator_;
-    std::vector<double> host_;
+    mutable std::vector<double> host_;
     size_t lastIterations_ = 0;
 };
 

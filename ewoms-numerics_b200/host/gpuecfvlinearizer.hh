@@ -3,6 +3,8 @@
 // structured grid, backed by libewg.so.
 //
 //   SET_TYPE_PROP(LensProblemEcfvAd, Linearizer, Ewoms::GpuEcfvLinearizer<TypeTag>);
+//   SET_TYPE_PROP(LensProblemEcfvAd, SparseMatrixAdapter,
+//                 Ewoms::Linear::GpuSparseMatrixAdapter<Block, Dune::BCRSMatrix<Block>>);
 //
 // The public interface is FvBaseLinearizer's: registerParameters, init, eraseMatrix, linearize,
 // linearizeDomain, linearizeAuxiliaryEquations, finalize, jacobian, residual, constraintsMap.
@@ -10,23 +12,36 @@
 // fvbaselinearizer.hh:183-196, so the Newton method and FvBaseProblem::timeIntegration react as
 // they do to a CPU linearization failure.
 //
+// Where the data lives. The device keeps its own copy of solution(0) / solution(1);
+// linearizeDomain uploads solution(0) every Newton iteration and solution(1) at the first
+// iteration of a time step, and downloads the residual, which NewtonMethod::preSolve_ reads on the
+// host (newtonmethod.hh:650-685). The Jacobian stays on the device: with GpuSparseMatrixAdapter
+// as the SparseMatrixAdapter, jacobian() returns the adapter bound to the device context, and the
+// Newton method passes it to the backend's prepare / setMatrix (newtonmethod.hh:371-374, :408)
+// without a copy; only a host consumer that reads or changes blocks makes it export (once per
+// linearization). With any other SparseMatrixAdapter (IstlSparseMatrixAdapter), jacobian() exports
+// the whole matrix into it after every linearization, which is correct but moves nnzb x 32 bytes
+// per Newton iteration.
+//
 // Requirements checked in init(): a structured grid (StructuredGridVanguard; cell index
 // i + nx (j + ny k)), even CellsX, an isotropic intrinsic permeability, the lens problem's
-// boundary types. The device keeps its own copy of solution(0) / solution(1); linearizeDomain
-// uploads solution(0) every Newton iteration and solution(1) at the first iteration of a time
-// step. This header compiles inside an eWoms build (it uses the property system); it is not
-// built in this repository, whose tests drive the same C ABI through ewg.hh and lens_gpu.cc.
+// boundary types. This header compiles inside an eWoms build (it uses the property system); the
+// repository compiles it against a stand-in of the property system in tests/dropin/, which replays
+// NewtonMethod::apply's calls on it.
 #ifndef EWOMS_GPU_ECFV_LINEARIZER_HH
 #define EWOMS_GPU_ECFV_LINEARIZER_HH
 
 #include <ewoms/common/exceptions.hh>
 #include <ewoms/common/propertysystem.hh>
 
+#include <iostream>
 #include <map>
 #include <memory>
+#include <set>
 #include <vector>
 
 #include "ewg.hh"
+#include "gpusparsematrixadapter.hh"
 
 namespace Ewoms {
 
@@ -42,6 +57,7 @@ class GpuEcfvLinearizer
     using Constraints = GET_PROP_TYPE(TypeTag, Constraints);
     using GridView = GET_PROP_TYPE(TypeTag, GridView);
     enum { dimWorld = GridView::dimensionworld };
+    static constexpr bool deviceMatrix = Linear::IsGpuSparseMatrixAdapter<SparseMatrixAdapter>::value;
 
 public:
     GpuEcfvLinearizer() = default;
@@ -53,6 +69,7 @@ public:
     void init(Simulator& simulator)
     {
         simulatorPtr_ = &simulator;
+        jacobian_.reset();
         ctx_.reset();
     }
 
@@ -83,6 +100,8 @@ public:
             ctx_->getResidual(hostR_.data());
             unpackResidual_(hostR_, residual_);
             jacobianValid_ = false;
+            if constexpr (deviceMatrix)
+                jacobian_->markDeviceCurrent();
         }
         catch (const std::exception& e) {
             std::cout << "rank " << simulatorPtr_->gridView().comm().rank()
@@ -97,8 +116,8 @@ public:
     void linearizeAuxiliaryEquations() {}
     void finalize() {}
 
-    // The BCRS view is exported from the device only when a caller asks for it; the GPU backend
-    // never does (it solves on the device copy).
+    // With GpuSparseMatrixAdapter: the device-resident matrix (no copy). Otherwise the matrix is
+    // exported from the device into the adapter once per linearization.
     const SparseMatrixAdapter& jacobian() const { exportJacobian_(); return *jacobian_; }
     SparseMatrixAdapter& jacobian() { exportJacobian_(); return *jacobian_; }
 
@@ -131,6 +150,12 @@ private:
         hostX_.resize(2 * n);
         hostR_.resize(2 * n);
         residual_.resize(n);
+        if constexpr (deviceMatrix) {
+            // FvBaseLinearizer::createMatrix_ reserves the stencil pattern; the device assembles
+            // exactly that pattern, so the adapter takes it from the device on its first export
+            jacobian_.reset(new SparseMatrixAdapter(*simulatorPtr_));
+            jacobian_->bindDevice(ctx_.get());
+        }
     }
 
     template <class SolutionVector>
@@ -151,6 +176,17 @@ private:
     }
 
     void exportJacobian_() const
+    {
+        if constexpr (deviceMatrix) {
+            if (!jacobian_)
+                throw std::logic_error("GpuEcfvLinearizer::jacobian() before the first linearization");
+            // the adapter stays on the device and exports itself on host access
+        }
+        else
+            exportToHostAdapter_();
+    }
+
+    void exportToHostAdapter_() const
     {
         if (jacobianValid_)
             return;

@@ -252,6 +252,12 @@ ewg_status ewg_set_residual(ewg_ctx* ctx, const double* b);
 ewg_status ewg_solve(ewg_ctx* ctx, const ewg_solve_opts* opts, ewg_solve_report* report);
 /* The last solution update dx (N x 2, natural). */
 ewg_status ewg_get_update(ewg_ctx* ctx, double* dx);
+/* Bytes the entry points of this context copied between the caller's host buffers and the device
+ * since creation or the last reset (solution, residual, update, matrix and intensive-quantity
+ * transfers; the library's own status and norm reads of a few bytes are not counted). reset != 0
+ * zeroes the counters after reading. No reference counterpart: it makes the host<->device traffic of
+ * a drop-in Newton iteration observable (the reference keeps everything in host memory). */
+ewg_status ewg_transfer_counters(ewg_ctx* ctx, int32_t reset, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 /* Apply the preconditioner once, y = M^-1 b (natural order host vectors). For parity tests. */
 ewg_status ewg_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* opts, const double* b,
                                     double* y);
