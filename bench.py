@@ -161,7 +161,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-# algorithmic bytes per kernel launch (FP64 s = 8, FP32 s = 4); see DESIGN.md
+# algorithmic bytes per kernel launch (FP64 s = 8, FP32 s = 4)
 
 
 def mixed_opts(ewg):
@@ -242,21 +242,6 @@ NCU_TRAFFIC = {
 # CPU baseline: the oracle restatement on the host cores
 
 
-def cpu_sample_run(nx, ny, nz, steps, seed=0):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ewg
-    import oracle
-    oracle.build()
-    case = ewg.lens3d_case(nx, ny, nz, seed=seed)
-    cores = os.cpu_count() or 1
-    o = oracle.Oracle(case, nthreads=cores)
-    o.apply_initial_solution()
-    t0 = time.perf_counter()
-    its = o.run(steps, 250.0)
-    el = time.perf_counter() - t0
-    return case.n_cells, el, cores, its
-
-
 def cpu_vcfv_linearization(n=32, seed=0):
     """The oracle's vertex-centred linearization on an n^3-element sample of the 3D lens problem
     at the bench's drained-top state: the element loop runs on one thread (its scatter into shared
@@ -280,14 +265,75 @@ def cpu_vcfv_linearization(n=32, seed=0):
             "sample": f"oracle vertex-centred AD linearization, {n}^3 elements ({o.n} vertices)"}
 
 
-def cpu_baseline_block(nx=64, ny=64, nz=32):
-    n, el, cores, its = cpu_sample_run(nx, ny, nz, 1)
-    return {"value": n / el / 1e6, "unit": "Mcells/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (CPU restatement, element loop on {cores} threads, natural-order ILU0 "
-                      f"and BiCGStab sequential) on a {nx}x{ny}x{nz} sub-grid of the same 3D lens "
-                      f"problem, first implicit step (Newton {its[0][0]} its, BiCGStab {its[0][1]} its): "
-                      f"{el:.2f} s for {n} cells",
-            "s_per_step": el, "vcfv_linearization": cpu_vcfv_linearization()}
+def cpu_phases_full(case, x, dt=250.0, its=8):
+    """The oracle on the bench's own problem and state: one AD linearization with the element loop
+    on all host cores (the reference's ThreadsPerProcess tasklets), and natural-order block ILU(0)
+    + BiCGStab (sequential, as one reference rank runs dune-istl): a solve capped at 1 iteration
+    and one capped at 1 + its iterations give the factorization time and the time per iteration."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ewg
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    o = oracle.Oracle(case, nthreads=cores)
+    o.set_solution(1, x)
+    o.set_solution(0, x)
+    o.linearize(dt, 0)  # first iteration of the step: the storage cache of solution(1)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.linearize(dt, 1)
+    t_lin = time.perf_counter() - t0
+    capped = dict(linear_solver_tolerance=1e-30, linear_solver_abs_tolerance=0.0, restart_on_breakdown=1,
+                  verify_true_residual=0)
+    t0 = time.perf_counter()
+    o.solve(ewg.default_solve_opts(linear_solver_max_iterations=1, **capped))
+    t_1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rc, _, it, _ = o.solve(ewg.default_solve_opts(linear_solver_max_iterations=1 + its, **capped))
+    t_k = time.perf_counter() - t0
+    o.close()
+    t_it = (t_k - t_1) / its
+    return {"cores": cores, "threads_linearization": cores, "threads_solve": 1,
+            "s_per_linearization": t_lin, "s_per_bicgstab_iteration": t_it,
+            "s_ilu_factorization": max(t_1 - t_it, 0.0), "s_context_setup": t_setup,
+            "iterations_timed": it}
+
+
+def cpu_baseline_block(case, x, gpu, steps_its):
+    """cpu_baseline on the bench workload itself (same grid, permeability and state): per-phase CPU
+    times, the GPU/CPU ratio of each phase, and a time step composed from them with the Newton and
+    BiCGStab iteration counts of the timed GPU steps."""
+    N = case.n_cells
+    ph = cpu_phases_full(case, x)
+    n_newton = float(np.mean([a for a, _ in steps_its]))
+    n_bicg = float(np.mean([b for _, b in steps_its]))
+    # a step: one linearization and one ILU(0) factorization per Newton iteration, one BiCGStab
+    # iteration per counted iteration (the last linearization of a step is not solved)
+    s_step = n_newton * ph["s_per_linearization"] + (n_newton - 1) * ph["s_ilu_factorization"] + \
+        n_bicg * ph["s_per_bicgstab_iteration"]
+    value = N / s_step / 1e6
+    phases = {
+        "linearization": {"cpu_mcells_per_s": N / ph["s_per_linearization"] / 1e6,
+                          "gpu_mcells_per_s": gpu.get("lin_mcells_per_s"),
+                          "gpu_over_cpu": (gpu["lin_mcells_per_s"] / (N / ph["s_per_linearization"] / 1e6))
+                          if gpu.get("lin_mcells_per_s") else None},
+        "bicgstab_iteration": {"cpu_iterations_per_s": 1.0 / ph["s_per_bicgstab_iteration"],
+                               "cpu_cell_iterations_per_s": N / ph["s_per_bicgstab_iteration"],
+                               "gpu_iterations_per_s": gpu.get("bicg_iterations_per_s"),
+                               "gpu_over_cpu": (gpu["bicg_iterations_per_s"] * ph["s_per_bicgstab_iteration"])
+                               if gpu.get("bicg_iterations_per_s") else None},
+    }
+    return {"value": value, "unit": "Mcells/s", "cores": ph["cores"], "kind": "port",
+            "sample": (f"oracle (CPU restatement of the reference path) on the same {case.grid.nx}x{case.grid.ny}x"
+                       f"{case.grid.nz} problem and state as the timed GPU steps: one AD linearization "
+                       f"(element loop on {ph['cores']} threads) and {ph['iterations_timed'] - 1} + 1 "
+                       f"natural-order block-ILU(0) BiCGStab iterations (sequential, as one reference rank); "
+                       f"value = cells / composed step time, the step composed of {n_newton:.1f} "
+                       f"linearizations, {n_newton - 1:.1f} ILU(0) factorizations and {n_bicg:.0f} BiCGStab "
+                       f"iterations (the means of the timed GPU steps, red-black ILU(0))"),
+            "s_per_step_composed": s_step, "phases": ph, "gpu_over_cpu": phases,
+            "vcfv_linearization": cpu_vcfv_linearization()}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -682,7 +728,9 @@ def run_ours(args, rank, world, local, pg):
     launches = int(sum(v[1] for v in prof.values()))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_block()
+        gpu_phase = {"lin_mcells_per_s": lin["mcells_per_s"] if lin else None,
+                     "bicg_iterations_per_s": bicg["iterations_per_s"] if bicg else None}
+        cpu = cpu_baseline_block(case, x_plain, gpu_phase, [(r.iterations, r.linear_iterations) for r in reps])
     line = {
         "metric": METRIC, "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "s_per_step": ms / args.steps / 1e3,
