@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "ewg.hh"
+#include "restart.hh"
 #include "vtkwriter.hh"
 
 namespace {
@@ -42,6 +43,11 @@ struct Params {
         {"EnableVtkOutput", "1"},      {"OutputDir", "."},
         {"LocalLinearizer", "ad"},     {"NumericDifferenceMethod", "1"},
         {"Discretization", "ecfv"},
+        // Simulator::run restarts from <OutputDir>/<name>_time=<RestartTime>_rank=0.ers when
+        // RestartTime > -1e30 (utils/simulator.hh:669-688); a restart file is written after every
+        // RestartFileInterval-th time step (FvBaseProblem::shouldWriteRestartFile writes every
+        // 10th, fvbaseproblem.hh:611-615; 0: none)
+        {"RestartTime", "-1e35"},      {"RestartFileInterval", "10"},
     };
     std::string get(const std::string& k) const {
         auto it = values.find(k);
@@ -392,17 +398,42 @@ int main(int argc, char** argv) {
         if (ll != "ad" && ll != "fd") throw std::runtime_error("LocalLinearizer must be 'ad' or 'fd'");
         ctx.setLocalLinearizer(ll == "fd" ? EWG_LOCAL_LINEARIZER_FD : EWG_LOCAL_LINEARIZER_AD,
                                p.i("NumericDifferenceMethod"));
-        ctx.applyInitialSolution();
         // LensProblem::name(): lens_<model>_<discretization>[_ad]
-        ewg::VtkMultiWriter vtk(p.get("OutputDir"), ll == "ad" ? "lens_immiscible_ecfv_ad" : "lens_immiscible_ecfv");
+        const std::string simName = ll == "ad" ? "lens_immiscible_ecfv_ad" : "lens_immiscible_ecfv";
+        ewg::VtkMultiWriter vtk(p.get("OutputDir"), simName);
         const bool vtkOut = p.i("EnableVtkOutput") != 0;
-        if (vtkOut) vtk.write(0.0, g, vtkFields(ctx, g, pr, perm));
+        const int64_t N = ctx.numCells();
+        ewg::SimulatorState sim;
+        const double restartTime = p.d("RestartTime");
+        if (restartTime > -1e30) {
+            // Simulator::run: deserialize the simulator, the problem (its VTK writer) and the model
+            ewg::Restart res;
+            res.deserializeBegin(p.get("OutputDir"), simName, restartTime, g);
+            std::printf("Deserialize from file '%s'\n", res.fileNameUsed().c_str());
+            res.deserializeSimulator(sim);
+            if (vtkOut) {
+                int num = 0;
+                int64_t pos = 0;
+                std::string coll;
+                res.deserializeVtkWriter(num, coll, pos);
+                vtk.restore(num, coll);
+            }
+            std::vector<double> x(2 * N);
+            res.deserializeCells(x.data(), N);
+            res.deserializeEnd();
+            ctx.setSolution(0, x.data());
+            ctx.setSolution(1, x.data());  // EcfvDiscretization::deserialize: solution(1) = solution(0)
+        } else {
+            ctx.applyInitialSolution();
+            if (vtkOut) vtk.write(0.0, g, vtkFields(ctx, g, pr, perm));
+        }
         const double endTime = p.d("EndTime");
         const double maxDt = p.d("MaxTimeStepSize");
         const int maxDivisions = p.i("MaxTimeStepDivisions");
         const int target = p.i("NewtonTargetIterations");
-        double t = 0.0, dt = std::min(p.d("InitialTimeStepSize"), maxDt);
-        int step = 0;
+        const int restartInterval = p.i("RestartFileInterval");
+        double t = sim.time, dt = std::min(p.d("InitialTimeStepSize"), maxDt);
+        int step = sim.timeStepIdx;
         double tLin = 0, tSolve = 0, tUpdate = 0;
         auto wall0 = std::chrono::steady_clock::now();
         while (t < endTime * (1 - 1e-12)) {
@@ -447,6 +478,20 @@ int main(int argc, char** argv) {
             double next = n > target ? dt / (1.0 + double(n - target) / target)
                                      : dt * (1.0 + double(target - n) / target / 1.2);
             dt = std::min(maxDt, next);
+            if (restartInterval > 0 && step > 0 && step % restartInterval == 0) {
+                // Simulator::serialize (utils/simulator.hh:923-937)
+                sim.time = t;
+                sim.timeStepIdx = step;
+                ewg::Restart res;
+                res.serializeBegin(p.get("OutputDir"), simName, t, g);
+                std::printf("Serialize to file '%s', next time step size: %g\n", res.fileNameUsed().c_str(), dt);
+                res.serializeSimulator(sim);
+                if (vtkOut) res.serializeVtkWriter(vtk.writerNum(), vtk.collection(), vtk.collectionWritePos());
+                std::vector<double> x(2 * N);
+                ctx.getSolution(0, x.data());
+                res.serializeCells(x.data(), N);
+                res.serializeEnd();
+            }
         }
         double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
         double tot = tLin + tSolve + tUpdate;

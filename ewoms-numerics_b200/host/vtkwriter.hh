@@ -106,17 +106,54 @@ public:
         if (!o) throw std::runtime_error("error writing '" + path + "'");
     }
 
+    // ---- restart (VtkMultiWriter::serialize / deserialize, io/vtkmultiwriter.hh:409-476) -------
+
+    // index of the next file, the collection's text, and where its next entry goes (before the
+    // closing tags, where the reference's open collection stream stands)
+    int writerNum() const { return index_; }
+    std::string collection() const { return pvdText(); }
+    int64_t collectionWritePos() const {
+        const std::string t = pvdText();
+        return (int64_t)(t.size() - std::string(kPvdTail).size());
+    }
+
+    // Restores the writer from a restart file: the file index and the collection's entries
+    // (parsed back from its text), and rewrites the collection file.
+    void restore(int writerNum, const std::string& collection) {
+        index_ = writerNum;
+        steps_.clear();
+        std::istringstream in(collection);
+        std::string line;
+        while (std::getline(in, line)) {
+            const std::string ts = "timestep=\"", fs = "file=\"";
+            const size_t a = line.find(ts), b = line.find(fs);
+            if (a == std::string::npos || b == std::string::npos) continue;
+            const size_t ae = line.find('"', a + ts.size()), be = line.find('"', b + fs.size());
+            steps_.emplace_back(std::stod(line.substr(a + ts.size(), ae - a - ts.size())),
+                                line.substr(b + fs.size(), be - b - fs.size()));
+        }
+        writePvd();
+    }
+
 private:
-    void writePvd() const {
-        const std::string path = dir_ + "/" + name_ + ".pvd";
-        std::ofstream o(path);
-        if (!o) throw std::runtime_error("cannot open '" + path + "' for writing");
+    static constexpr const char* kPvdTail = " </Collection>\n</VTKFile>\n";
+
+    std::string pvdText() const {
+        std::ostringstream o;
         o << std::setprecision(16);
         o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"Collection\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
           << " <Collection>\n";
         for (const auto& s : steps_)
             o << "   <DataSet timestep=\"" << s.first << "\" group=\"\" part=\"0\" file=\"" << s.second << "\"/>\n";
-        o << " </Collection>\n</VTKFile>\n";
+        o << kPvdTail;
+        return o.str();
+    }
+
+    void writePvd() const {
+        const std::string path = dir_ + "/" + name_ + ".pvd";
+        std::ofstream o(path);
+        if (!o) throw std::runtime_error("cannot open '" + path + "' for writing");
+        o << pvdText();
     }
 
     std::string dir_, name_;
