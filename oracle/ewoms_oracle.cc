@@ -20,6 +20,7 @@
 #include "ewoms_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -760,6 +761,22 @@ struct Precond {
             for (int color = 0; color < 8; ++color)
                 for (int64_t c = 0; c < A.n; ++c)
                     if (colourOf[c] == color) { perm[k] = c; iperm[c] = k; ++k; }
+        } else if (ordering == ORC_ORDER_BOX8) {
+            // 2x2x2 boxes in eight colours: a cell's colour is bit 1 of (i, j, k), its place in
+            // its box bit 0; colour-major, then box (i/4, j/4, k/4) in natural order, then the
+            // cell's place in the box (x fastest). Boxes of one colour are never adjacent.
+            std::vector<std::array<int64_t, 4>> key((size_t)A.n);
+            const int64_t nbx = (C.n[0] + 3) / 4, nby = (C.n[1] + 3) / 4;
+            for (int64_t c = 0; c < A.n; ++c) {
+                int64_t i, j, kk; C.ijk(c, i, j, kk);
+                const int64_t colour = ((i >> 1) & 1) | (((j >> 1) & 1) << 1) | (((kk >> 1) & 1) << 2);
+                const int64_t box = (i >> 2) + nbx * ((j >> 2) + nby * (kk >> 2));
+                const int64_t q = (i & 1) | ((j & 1) << 1) | ((kk & 1) << 2);
+                key[(size_t)c] = {colour, box, q, c};
+            }
+            for (int64_t c = 0; c < A.n; ++c) perm[c] = c;
+            std::sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return key[(size_t)a] < key[(size_t)b]; });
+            for (int64_t k = 0; k < A.n; ++k) iperm[perm[k]] = k;
         } else {
             int64_t k = 0;
             for (int color = 0; color < 2; ++color)
@@ -1523,7 +1540,16 @@ void orc_advance_time_level(orc_ctx* o) { o->C.sol[1] = o->C.sol[0]; }
 
 void orc_update_begin(orc_ctx* o) { o->C.refPressure = o->C.sol[0][0]; }
 // updateBegin with the caller's reference pressure (a z-slab takes the whole grid's)
-void orc_set_reference_pressure(orc_ctx* o, double p) { o->C.refPressure = p; }
+// updateBegin with a caller-given reference pressure; like ewg_set_reference_pressure it rejects a
+// value that is not positive and finite (returns 1 and leaves the stored pressure unchanged)
+int orc_set_reference_pressure(orc_ctx* o, double p) {
+    if (!(p > 0) || !std::isfinite(p)) {
+        o->C.err = "set_reference_pressure: p_ref must be positive and finite";
+        return 1;
+    }
+    o->C.refPressure = p;
+    return 0;
+}
 int orc_linearize(orc_ctx* o, double dt, int it, double* error) {
     // a context that never ran updateBegin takes the reference pressure of the current iterate
     if (o->C.fd && !(o->C.refPressure > 0)) o->C.refPressure = o->C.sol[0][0];

@@ -30,6 +30,8 @@ typedef struct orc_ctx orc_ctx;
 #define ORC_ORDER_REDBLACK 1  /* same factorisation on the red-black permuted matrix */
 #define ORC_ORDER_COLOURS 2   /* vertex-centred grids: vertices ordered by the parity colour
                                  (i&1) + 2 (j&1) + 4 (k&1), then lexicographically */
+#define ORC_ORDER_BOX8 3      /* 3D cell grids: 2x2x2 boxes in eight colours (bit 1 of i, j, k),
+                                 colour-major, boxes (i/4, j/4, k/4) natural, x-fastest inside */
 
 orc_ctx* orc_create(const ewg_grid* grid, const ewg_problem* problem, const double* perm,
                     int nthreads);

@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "liboracle.so")
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "ewoms-numerics_b200"))
 import ewg  # noqa: E402  (ABI structs only)
 
-ORDER_NATURAL, ORDER_REDBLACK, ORDER_COLOURS = 0, 1, 2
+ORDER_NATURAL, ORDER_REDBLACK, ORDER_COLOURS, ORDER_BOX8 = 0, 1, 2, 3
 
 
 def build(force=False):
@@ -54,7 +54,7 @@ def load():
         "orc_set_recycle_first_iteration_storage": (None, [C.c_void_p, C.c_int]),
         "orc_set_local_linearizer": (None, [C.c_void_p, C.c_int, C.c_int]),
         "orc_update_begin": (None, [C.c_void_p]),
-        "orc_set_reference_pressure": (None, [C.c_void_p, C.c_double]),
+        "orc_set_reference_pressure": (C.c_int, [C.c_void_p, C.c_double]),
         "orc_set_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_get_solution": (None, [C.c_void_p, C.c_int, P(d)]),
         "orc_apply_initial_solution": (None, [C.c_void_p]),
@@ -149,7 +149,8 @@ class Oracle:
 
     def set_reference_pressure(self, p_ref):
         """updateBegin with the caller's reference pressure (a z-slab takes the whole grid's)."""
-        self.lib.orc_set_reference_pressure(self.h, float(p_ref))
+        if self.lib.orc_set_reference_pressure(self.h, float(p_ref)):
+            raise ValueError(self.err())
 
     def set_solution(self, t, x):
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.n, 2)

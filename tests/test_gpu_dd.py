@@ -162,21 +162,38 @@ def test_distributed_bicgstab_on_device_slabs(ewg_mod, world):
 
 
 @pytest.mark.parametrize("world", [2, 3])
-def test_distributed_newton_step(ewg_mod, world):
+@pytest.mark.parametrize("local", ["ad", "fd_forward"])
+def test_distributed_newton_step(ewg_mod, world, local):
     """One implicit-Euler step solved by Newton over the slabs: it converges, its final error is
     the whole grid's residual max-norm at the assembled state (owned rows are the whole grid's
     rows; the residual-only evaluation may contract differently, hence 1e-10), and the state
-    agrees with the single-domain Newton's."""
+    agrees with the single-domain Newton's. With the forward-difference local linearizer every
+    slab must take the whole grid's reference pressure (the updateBegin reduction of
+    distributed_newton reads p_w of global cell 0 from the bottom slab's split-order storage) for
+    its deflections, and so its Jacobian rows, to be the single domain's."""
     import dd
     case = ewg_mod.lens3d_case(16, 12, 10, seed=2)
     ctx = _state_after_steps(ewg_mod, case, 2)
     x1 = ctx.get_solution(0)
     sopts = ewg_mod.default_solve_opts()
     parts = _device_slabs(dd, case, x1, x1, world, sopts)
+    if local == "fd_forward":
+        ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, 1)
+        for p in parts:
+            p.ctx.set_local_linearizer(ewg_mod.LOCAL_LINEARIZER_FD, 1)
     rep = dd.distributed_newton(parts, dd.LocalComm(), 250.0, None, sopts)
     assert rep.converged, (rep.status, rep.iterations, rep.error)
     x_dd = _gather_owned(dd, case, parts)
-    whole = ctx.residual_norm(x_dd, 250.0)
+    if local == "ad":
+        whole = ctx.residual_norm(x_dd, 250.0)
+    else:
+        # the finite-difference linearizer's residual comes from its own kernel: linearize the whole
+        # grid at the assembled state with the slabs' reference pressure (p_w of global cell 0 at
+        # the start of the step) and the same old time level
+        ctx.set_reference_pressure(x1[0, 0])
+        ctx.set_solution(0, x_dd)
+        whole = ctx.linearize(250.0).error
+        ctx.set_solution(0, x1)
     assert abs(whole - rep.error) <= 1e-10 * rep.error, (whole, rep.error)
     st, srep = ctx.newton_apply(250.0, None, sopts)
     assert st == 0
