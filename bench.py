@@ -180,11 +180,37 @@ def geometry(n):
     return N, F
 
 
-def kernel_bytes(name, N, F, s_mat=8, s_vec=8):
-    """Bytes a launch must move at minimum in the band / red-black layout (no index arrays):
-    every matrix block and vector entry it needs read once, every output written once."""
+def cross_box_faces(n):
+    """Interior faces between two 2x2x2 boxes of the box-8-colour order (the rest lie inside a box)."""
+    nx, ny, nz = n
+    return (nx // 2 - 1) * ny * nz + nx * (ny // 2 - 1) * nz + nx * ny * (nz // 2 - 1)
+
+
+def kernel_bytes(name, N, F, s_mat=8, s_vec=8, b8=False, Fx=None):
+    """Bytes a launch must move at minimum in the band layout (no index arrays): every matrix
+    block and vector entry it needs read once, every output written once. b8: the solve runs its
+    ILU(0) in the box-8-colour order (Fx = faces between boxes): per sweep eight colour launches,
+    and the SpMV after a preconditioner application reads only the earlier neighbours' blocks."""
     Nh = N // 2
     blk, vec = 4 * s_mat, 2 * s_vec
+    if b8:
+        Fx = F // 2 if Fx is None else Fx
+        table8 = {
+            # forward, per colour: L blocks of the earlier neighbours, d in, w out, the earlier
+            # neighbours' w across box faces (within a box they stay in registers)
+            "b8_forward": (F * blk + N * vec * 2 + Fx * vec) / 8,
+            # backward, per colour: blocks of the later neighbours, inverted pivots, w in, y out,
+            # the later neighbours' y across box faces
+            "b8_backward": (F * blk + N * blk + N * vec * 2 + Fx * vec) / 8,
+            # v = relax w + E y + sum of the earlier neighbours' blocks times y; r0hat (or s) for
+            # the dot products
+            "bicg_spmv_alpha": F * blk + N * blk + N * vec * 4,
+            "bicg_spmv_omega": F * blk + N * blk + N * vec * 4,
+            # the Jacobian into box-8 order (7 bands) and a vector conversion
+            "b8_layout": None,
+        }
+        if name in table8:
+            return table8[name]
     table = {
         # linearization: x, storage(old), K, lens flag in; the iq cache out (6 doubles)
         "intensive": N * (16 + 1) + N * 48,
@@ -375,12 +401,12 @@ def run_reference(args, rank, world, pg):
     print(json.dumps(line), flush=True)
 
 
-def ensemble_cases(ewg, members, seed=3):
+def ensemble_cases(ewg, members, seed=3, sizes=(32, 48, 64, 96, 128)):
     """Batched-ensemble workload: seeded lens realizations with cube grids drawn from
     {32, 48, 64, 96, 128}^3, sigma in [0.5, 1.5], correlation length in [4, 12] cells and
     dt in {100, 250, 500} s."""
     rng = np.random.default_rng(seed)
-    sizes = rng.choice([32, 48, 64, 96, 128], size=members)
+    sizes = rng.choice(list(sizes), size=members)
     cases, dts = [], []
     for m in range(members):
         n = int(sizes[m])
@@ -461,8 +487,16 @@ def run_vcfv(args, rank, pg, torch, ewg):
 def run_ensemble(args, rank, pg, torch, ewg):
     """The batched ensemble form: every member advances one implicit step per timed step (its own
     dt, FP64 residual / update / Newton test, FP32 Jacobian, ILU(0) and BiCGStab), all members in
-    the same launches with the BiCGStab iteration replayed from a CUDA graph."""
-    cases, dts = ensemble_cases(ewg, args.ensemble_members, seed=3 + rank)
+    the same launches with the BiCGStab iteration replayed from a CUDA graph. Under torchrun the
+    one ensemble is sharded: every rank draws the same member list and advances the members the
+    greedy cost balance assigns to it (shard.py); only the timing and the counts are reduced."""
+    import shard
+    world = pg.get_world_size() if pg is not None else 1
+    all_cases, all_dts = ensemble_cases(ewg, args.ensemble_members, seed=3)
+    costs = [shard.member_cost(c.n_cells, dt) for c, dt in zip(all_cases, all_dts)]
+    assignment = shard.assign_members(costs, world)
+    mine = assignment[rank]
+    cases, dts = [all_cases[m] for m in mine], [all_dts[m] for m in mine]
     so = ewg.default_solve_opts(precision=ewg.PRECISION_MIXED, linear_solver_tolerance=1e-3,
                                 verify_true_residual=0)
     ens = ewg.Ensemble(cases, precision=ewg.PRECISION_MIXED)
@@ -486,11 +520,15 @@ def run_ensemble(args, rank, pg, torch, ewg):
     ms = max_over_ranks(pg, e0.elapsed_time(e1))
     cells = ens.total_cells
     total = sum_over_ranks(pg, float(cells))
+    all_cells = sum(c.n_cells for c in all_cases)
     newton = [r.newton_iterations / args.ensemble_steps for reps, _ in stats for r in reps]
     out = {
-        "workload": f"{len(cases)} lens realizations, cube grids from {{32,48,64,96,128}}^3, {cells} cells, "
+        "workload": f"{len(all_cases)} lens realizations, cube grids from {{32,48,64,96,128}}^3, {all_cells} cells, "
                     f"dt from {{100,250,500}} s, mixed precision (FP32 inner BiCGStab to rel 1e-3, Newton tol 1e-8)",
-        "members": len(cases), "cells": cells, "steps": args.ensemble_steps,
+        "members": len(all_cases), "cells": all_cells, "steps": args.ensemble_steps,
+        "sharding": {"ranks": world, "members_per_rank": [len(a) for a in assignment],
+                     "cost_imbalance": shard.imbalance(costs, assignment),
+                     "scaling": "strong (one ensemble split across the ranks by cost)"},
         "s_per_step": ms / args.ensemble_steps / 1e3,
         "mcells_steps_per_s": total * args.ensemble_steps / (ms * 1e-3) / 1e6,
         "newton_iterations_per_step_mean": float(np.mean(newton)),
@@ -697,7 +735,9 @@ def run_ours(args, rank, world, local, pg):
     s = 4 if mixed else 8
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dname, (dms, dn) = dom
-    db = kernel_bytes(dname, N, F, s_mat=s, s_vec=s)
+    b8 = "b8_forward" in prof
+    Fx = cross_box_faces((nx, ny, nz))
+    db = kernel_bytes(dname, N, F, s_mat=s, s_vec=s, b8=b8, Fx=Fx)
     avg_ms = dms / dn
     achieved = db / (avg_ms * 1e-3) / 1e9 if db else None
     traffic = NCU_TRAFFIC.get(dname) if not mixed else None
@@ -715,13 +755,14 @@ def run_ours(args, rank, world, local, pg):
         lin = {"ms_per_linearization": lin_avg, "mcells_per_s": N / (lin_avg * 1e-3) / 1e6,
                "algorithmic_bytes": lb, "achieved_gbs": lb / (lin_avg * 1e-3) / 1e9,
                "frac": lb / (lin_avg * 1e-3) / 1e9 / peak, "launches": n_lin}
-    it_kernels = ("bicg_p", "ilu_black_apply", "ilu_red_apply", "jacobi_apply", "bicg_spmv_alpha",
-                  "bicg_hs", "bicg_spmv_omega", "bicg_xr")
+    it_kernels = ("bicg_p", "ilu_black_apply", "ilu_red_apply", "jacobi_apply", "b8_forward", "b8_backward",
+                  "bicg_spmv_alpha", "bicg_hs", "bicg_spmv_omega", "bicg_xr")
     n_it = prof.get("bicg_xr", (0, 0))[1]
     bicg = None
     if n_it:
         t_it = sum(prof.get(k, (0, 0))[0] for k in it_kernels) / n_it
-        b_it = sum((kernel_bytes(k, N, F, s, s) or 0) * prof.get(k, (0, 0))[1] for k in it_kernels) / n_it
+        b_it = sum((kernel_bytes(k, N, F, s, s, b8=b8, Fx=Fx) or 0) * prof.get(k, (0, 0))[1]
+                   for k in it_kernels) / n_it
         bicg = {"ms_per_iteration": t_it, "iterations_per_s": 1e3 / t_it, "algorithmic_bytes": b_it,
                 "achieved_gbs": b_it / (t_it * 1e-3) / 1e9, "frac": b_it / (t_it * 1e-3) / 1e9 / peak,
                 "iterations": n_it}

@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
+#include <string>
 #include <vector>
 
 #include "ewg_internal.cuh"
@@ -28,7 +30,7 @@ const char* const kKernelNames[K_NUM_KERNELS] = {
     "diag_inverse", "ilu_black_factor", "ilu_black_apply", "ilu_red_apply", "jacobi_apply",
     "spmv", "bicg_init", "bicg_p", "bicg_spmv_alpha", "bicg_hs", "bicg_spmv_omega", "bicg_xr",
     "to_float", "defect_accumulate", "defect_residual", "newton_update", "bcrs",
-    "bicg_true_residual"};
+    "bicg_true_residual", "b8_layout", "b8_factor", "b8_forward", "b8_backward"};
 
 void prof_flush(ewg_ctx* ctx) {
     Profiler& pr = ctx->prof;
@@ -351,6 +353,7 @@ void ewg_default_solve_opts(ewg_solve_opts* o) {
     o->check_interval = 0;
     o->restart_on_breakdown = 1;
     o->verify_true_residual = 1;
+    o->ilu_ordering = EWG_ILU_ORDER_AUTO;
 }
 
 void* ewg_get_stream(ewg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -816,6 +819,64 @@ ewg_status ewg_device_precondition(ewg_ctx* ctx, const ewg_solve_opts* o, const 
     if (check_ctx(ctx) || !o) return EWG_ERR_INVALID;
     if (!device_vector_ok(ctx, b) || !device_vector_ok(ctx, y)) { ctx->err = "device_precondition: b and y must be aligned device vectors"; return EWG_ERR_INVALID; }
     return solver_apply_preconditioner(ctx, o, (const double2*)b, (double2*)y);
+}
+
+static ewg_status slab_args_ok(ewg_ctx* ctx, std::initializer_list<const void*> vecs, const void* out, const char* what) {
+    for (const void* v : vecs)
+        if (!device_vector_ok(ctx, (const double*)v)) {
+            ctx->err = std::string(what) + ": vectors must be aligned device vectors";
+            return EWG_ERR_INVALID;
+        }
+    if (out && ((uintptr_t)out % sizeof(double)) != 0) {
+        ctx->err = std::string(what) + ": misaligned output";
+        return EWG_ERR_INVALID;
+    }
+    return EWG_OK;
+}
+
+ewg_status ewg_device_bicg_p(ewg_ctx* ctx, double* p, const double* r, double* r0, double* v, double beta, double omega,
+                             int32_t restart) {
+    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+    ewg_status st = slab_args_ok(ctx, {p, r, r0, v}, nullptr, "device_bicg_p");
+    if (st) return st;
+    return solver_slab(ctx, 0, (double2*)p, (double2*)r, (double2*)r0, (double2*)v, nullptr, nullptr, beta, omega,
+                       restart, 0, 0, nullptr);
+}
+
+ewg_status ewg_device_bicg_spmv_dot(ewg_ctx* ctx, const double* x, double* y, const double* w, int64_t lo, int64_t hi,
+                                    double* out) {
+    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+    if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "device_bicg_spmv_dot needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
+    ewg_status st = slab_args_ok(ctx, {x, y, w}, out, "device_bicg_spmv_dot");
+    if (st) return st;
+    return solver_slab(ctx, 1, (double2*)x, (double2*)y, (double2*)w, nullptr, nullptr, nullptr, 0, 0, 0, lo, hi, out);
+}
+
+ewg_status ewg_device_bicg_hs(ewg_ctx* ctx, double* x, const double* y, double* r, const double* v, double rho_i,
+                              const double* denom, int64_t lo, int64_t hi, double* out) {
+    if (check_ctx(ctx) || !out || !denom) return EWG_ERR_INVALID;
+    ewg_status st = slab_args_ok(ctx, {x, y, r, v}, out, "device_bicg_hs");
+    if (st) return st;
+    return solver_slab(ctx, 2, (double2*)x, (double2*)y, (double2*)r, (double2*)v, nullptr, denom, rho_i, 0, 0, lo, hi,
+                       out);
+}
+
+ewg_status ewg_device_bicg_spmv_dot2(ewg_ctx* ctx, const double* z, double* t, const double* s, int64_t lo, int64_t hi,
+                                     double* out) {
+    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+    if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "device_bicg_spmv_dot2 needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
+    ewg_status st = slab_args_ok(ctx, {z, t, s}, out, "device_bicg_spmv_dot2");
+    if (st) return st;
+    return solver_slab(ctx, 3, (double2*)z, (double2*)t, (double2*)s, nullptr, nullptr, nullptr, 0, 0, 0, lo, hi, out);
+}
+
+ewg_status ewg_device_bicg_xr(ewg_ctx* ctx, double* x, const double* z, double* r, const double* t, const double* r0,
+                              double omega, int64_t lo, int64_t hi, double* out) {
+    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+    ewg_status st = slab_args_ok(ctx, {x, z, r, t, r0}, out, "device_bicg_xr");
+    if (st) return st;
+    return solver_slab(ctx, 4, (double2*)x, (double2*)z, (double2*)r, (double2*)t, (const double2*)r0, nullptr, omega, 0,
+                       0, lo, hi, out);
 }
 
 ewg_status ewg_newton_update(ewg_ctx* ctx) {

@@ -92,6 +92,11 @@ struct Phys {
     double rhoArea[3][2];    // rho_alpha * face area per axis (mass flux per unit velocity)
     double invVol;           // 1 / cell volume
     int kOrigin;             // global index of plane 0 (z-slab of a decomposed grid), else 0
+    // box-8-colour solver order (3D grids with nx, ny, nz multiples of 4; see ewg_box8.cuh)
+    int b8ok;                // 1 if the grid has that order
+    int nbx, nby, nbz;       // 4x4x4 superblocks per axis
+    int64_t Nb;              // N / 64: cells per group = superblocks
+    FastDiv fdNbx, fdNby, fdNb;
 };
 
 // Geometry of one interior face seen from a cell, per (axis, cell index along the axis, side):
@@ -119,6 +124,14 @@ inline void set_index_constants(Phys& P) {
     P.nb = 1 + 2 * P.dim;
     P.fdNxh = make_fastdiv((uint32_t)P.nxh);
     P.fdNy = make_fastdiv((uint32_t)P.ny);
+    P.b8ok = P.dim == 3 && P.nx % 4 == 0 && P.ny % 4 == 0 && P.nz % 4 == 0 && P.N >= 64 ? 1 : 0;
+    P.nbx = P.nx / 4;
+    P.nby = P.ny / 4;
+    P.nbz = P.nz / 4;
+    P.Nb = P.N / 64;
+    P.fdNbx = make_fastdiv((uint32_t)(P.nbx > 0 ? P.nbx : 1));
+    P.fdNby = make_fastdiv((uint32_t)(P.nby > 0 ? P.nby : 1));
+    P.fdNb = make_fastdiv((uint32_t)(P.Nb > 0 ? P.Nb : 1));
 }
 
 struct CellIdx {
@@ -180,6 +193,7 @@ enum KernelId {
     K_SPMV, K_BICG_INIT, K_BICG_P, K_BICG_SPMV_ALPHA, K_BICG_HS, K_BICG_SPMV_OMEGA, K_BICG_XR,
     K_TO_FLOAT, K_DEFECT_ACCUMULATE, K_DEFECT_RESIDUAL, K_NEWTON_UPDATE, K_BCRS,
     K_BICG_TRUE_RESIDUAL,
+    K_B8_LAYOUT, K_B8_FACTOR, K_B8_FORWARD, K_B8_BACKWARD,
     K_NUM_KERNELS
 };
 extern const char* const kKernelNames[K_NUM_KERNELS];
@@ -213,7 +227,7 @@ struct ewg_ctx {
     double refPressure = -1.0;               // ImmiscibleModel::updateBegin's reference pressure (unset)
     bool jacFromLinearizer = false;          // J/r valid
     bool iluValid = false;
-    int iluKind = -1, iluPrecision = -1;
+    int iluKind = -1, iluPrecision = -1, iluOrder = -1;
     // host copy of the reference BCRS pattern
     int64_t nnzb = 0;
     int32_t* d_rowPtr = nullptr;             // device BCRS pattern (for export / import)
@@ -289,6 +303,8 @@ ewg_status solver_solve(ewg_ctx* ctx, const ewg_solve_opts* o, ewg_solve_report*
 ewg_status solver_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* o, const double2* b,
                                        double2* y);
 ewg_status solver_spmv(ewg_ctx* ctx, const double2* x, double2* y);
+ewg_status solver_slab(ewg_ctx* ctx, int kind, double2* a, double2* b, double2* c, double2* d, const double2* e,
+                       const double* s0, double s1, double s2, int flag, int64_t lo, int64_t hi, double* out);
 ewg_status solver_newton_update(ewg_ctx* ctx, int* nonfinite);
 void solver_free(ewg_ctx* ctx);
 

@@ -429,9 +429,85 @@ class DeviceSlab:
     def precondition(self, b, y):
         self.ctx.device_precondition(b, y, self.opts)
 
+    # the fused kernels of one slab-iteration (ewg_device_bicg_*): vector updates with their
+    # owned-row reductions in one pass each, results left on the device
+    def _reduction_slots(self):
+        import torch
+        if not hasattr(self, "_red"):
+            self._red = torch.zeros(16, dtype=torch.float64, device="cuda")
+        lo, hi = self.layout._own.start, self.layout._own.stop
+        return self._red, lo, hi
+
+    def bicg_p(self, v, beta, omega, restart):
+        self.ctx.device_bicg_p(v.p, v.r, v.r0, v.v, beta, omega, restart)
+
+    def bicg_spmv_dot(self, x, y, w):
+        red, lo, hi = self._reduction_slots()
+        out = red[0:1]
+        self.ctx.device_bicg_spmv_dot(x, y, w, lo, hi, out)
+        return out[0]
+
+    def bicg_hs(self, v, rho_i, denom):
+        red, lo, hi = self._reduction_slots()
+        out = red[2:4]
+        self.ctx.device_bicg_hs(v.x, v.y, v.r, v.v, rho_i, denom, lo, hi, out)
+        return [out[0], out[1]]
+
+    def bicg_spmv_dot2(self, z, t, s):
+        red, lo, hi = self._reduction_slots()
+        out = red[4:6]
+        self.ctx.device_bicg_spmv_dot2(z, t, s, lo, hi, out)
+        return [out[0], out[1]]
+
+    def bicg_xr(self, v, omega):
+        red, lo, hi = self._reduction_slots()
+        out = red[8:12]
+        self.ctx.device_bicg_xr(v.x, v.z, v.r, v.t, v.r0, omega, lo, hi, out)
+        return out.clone()
+
 
 class _Vecs:
     pass
+
+
+class _TorchOps:
+    """The fused steps of one slab's BiCGStab iteration written with torch operations, for slabs
+    without device kernels (the CPU oracle slabs of the tests). DeviceSlab runs the same steps as
+    single kernels (ewg_device_bicg_*), each with its owned-row reductions."""
+
+    def __init__(self, p):
+        self.p = p
+
+    def bicg_p(self, v, beta, omega, restart):
+        if restart:
+            v.r0.copy_(v.r)
+            v.v.zero_()
+            v.p.zero_()
+        v.p.sub_(v.v, alpha=omega).mul_(beta).add_(v.r)
+
+    def bicg_spmv_dot(self, x, y, w):
+        self.p.spmv(x, y)
+        return _dev_dot(self.p.layout, w, y)
+
+    def bicg_hs(self, v, rho_i, denom):
+        alpha_dev = rho_i / denom
+        v.x.addcmul_(v.y, alpha_dev)
+        v.r.addcmul_(v.v, alpha_dev, value=-1.0)
+        return [_dev_max(self.p.layout, v.r), _dev_max(self.p.layout, v.y)]
+
+    def bicg_spmv_dot2(self, z, t, s):
+        self.p.spmv(z, t)
+        return [_dev_dot(self.p.layout, t, t), _dev_dot(self.p.layout, t, s)]
+
+    def bicg_xr(self, v, omega):
+        v.x.add_(v.z, alpha=omega)
+        m = [_dev_max(self.p.layout, v.r), _dev_max(self.p.layout, v.z)]
+        v.r.sub_(v.t, alpha=omega)
+        return _pack([_dev_dot(self.p.layout, v.r0, v.r), _dev_dot(self.p.layout, v.r, v.r)], m)
+
+
+def _ops(p):
+    return p if hasattr(p, "bicg_xr") else _TorchOps(p)
 
 
 def _bicgstab(parts, comm, opts):
@@ -514,31 +590,21 @@ def _bicgstab(parts, comm, opts):
         while S["status"] == ST_RUNNING:
             restart, beta, omega = S["restartPending"], S["beta"], S["omega"]
 
-            def upd_p(p, v):
-                if restart:
-                    v.r0.copy_(v.r)
-                    v.v.zero_()
-                    v.p.zero_()
-                v.p.sub_(v.v, alpha=omega).mul_(beta).add_(v.r)
-            each(upd_p)
+            each(lambda p, v: _ops(p).bicg_p(v, beta, omega, restart))
             exchange("p")
             each(lambda p, v: p.precondition(v.p, v.y))
             exchange("y")
             # <r0,v> stays on the device: alpha = rho_i / <r0,v> is formed there, and <r0,v> reaches
             # the host with the next read-back, where the breakdown tests run (x and r have moved
             # by then, which a breakdown makes moot)
-            d_dev = comm.reduce_device(each(lambda p, v: (p.spmv(v.y, v.v), _dev_dot(p.layout, v.r0, v.v))[1]),
-                                       parts)
+            d_dev = comm.reduce_device(each(lambda p, v: _ops(p).bicg_spmv_dot(v.y, v.v, v.r0)), parts)
             S["restartPending"] = 0
             rho_i = S["rho_i"]
 
             def upd_hs(p, v):
-                alpha_dev = rho_i / d_dev
-                v.x.addcmul_(v.y, alpha_dev)
-                v.r.addcmul_(v.v, alpha_dev, value=-1.0)
+                m = _ops(p).bicg_hs(v, rho_i, d_dev)
                 # exactly one slab (the bottom one) carries <r0,v> in its sums
-                v.half = ([d_dev if p.slab.k0 == 0 else torch.zeros_like(d_dev)],
-                          [_dev_max(p.layout, v.r), _dev_max(p.layout, v.y)])
+                v.half = ([d_dev if p.slab.k0 == 0 else torch.zeros_like(d_dev)], m)
             each(upd_hs)
             # the half-step check travels with <t,t> and <t,s>: z = M^-1 s and t = J z are
             # computed before it is known, and left unused when the half step ends the solve
@@ -546,9 +612,7 @@ def _bicgstab(parts, comm, opts):
             each(lambda p, v: p.precondition(v.r, v.z))
             exchange("z")
             (tt, ts, d), (smax, ymax) = comm.reduce(
-                each(lambda p, v: (p.spmv(v.z, v.t),
-                                   _pack([_dev_dot(p.layout, v.t, v.t), _dev_dot(p.layout, v.t, v.r)] + v.half[0],
-                                         v.half[1]))[1]), 3)
+                each(lambda p, v: _pack(_ops(p).bicg_spmv_dot2(v.z, v.t, v.r) + v.half[0], v.half[1])), 3)
             if abs(d) <= DBL_BREAKDOWN:
                 S["status"] = ST_BREAKDOWN
                 break
@@ -569,12 +633,7 @@ def _bicgstab(parts, comm, opts):
                 break
             omega = S["omega"]
 
-            def upd_xr(p, v):
-                v.x.add_(v.z, alpha=omega)
-                m = [_dev_max(p.layout, v.r), _dev_max(p.layout, v.z)]
-                v.r.sub_(v.t, alpha=omega)
-                return _pack([_dev_dot(p.layout, v.r0, v.r), _dev_dot(p.layout, v.r, v.r)], m)
-            (rr0, rr), (smax, zmax) = comm.reduce(each(upd_xr), 2)
+            (rr0, rr), (smax, zmax) = comm.reduce(each(lambda p, v: _ops(p).bicg_xr(v, omega)), 2)
             S["resErr"] = smax
             criterion(zmax == 0.0)
             if S["status"] != ST_RUNNING:
@@ -733,10 +792,14 @@ def main(argv=None) -> None:
     ap.add_argument("--slabs", default="1,2,4")
     ap.add_argument("--dt", type=float, default=250.0)
     ap.add_argument("--linear-tol", type=float, default=1e-3)
+    # one ILU(0) order for every form, so that the forms differ only in the decomposition (the
+    # box-8 order needs slab plane counts divisible by 4, which ghost planes rarely give)
+    ap.add_argument("--ilu-ordering", default="redblack", choices=["redblack", "box8", "auto"])
     a = ap.parse_args(argv)
     nx, ny, nz = (int(v) for v in a.grid.split(","))
     case = ewg.lens3d_case(nx, ny, nz, seed=0)
-    sopts = ewg.default_solve_opts(linear_solver_tolerance=a.linear_tol)
+    order = {"redblack": ewg.ILU_ORDER_REDBLACK, "box8": ewg.ILU_ORDER_BOX8, "auto": ewg.ILU_ORDER_AUTO}[a.ilu_ordering]
+    sopts = ewg.default_solve_opts(linear_solver_tolerance=a.linear_tol, ilu_ordering=order)
     ctx = ewg.Context(case)
     ctx.apply_initial_solution()
     st, _ = ctx.newton_apply(a.dt, None, sopts)
@@ -744,7 +807,8 @@ def main(argv=None) -> None:
         raise RuntimeError(f"warm-up step failed: {ewg.STATUS_NAMES.get(st, st)}")
     ctx.advance_time_level()
     x1 = ctx.get_solution(0)
-    cfg = {"grid": [nx, ny, nz], "cells": case.grid.n_cells, "dt": a.dt, "linear_tol": a.linear_tol}
+    cfg = {"grid": [nx, ny, nz], "cells": case.grid.n_cells, "dt": a.dt, "linear_tol": a.linear_tol,
+           "ilu_ordering": a.ilu_ordering}
 
     def single():
         ctx.set_solution(1, x1)

@@ -33,6 +33,8 @@ STATUS_NAMES = {0: "EWG_OK", 1: "EWG_ERR_INVALID", 2: "EWG_ERR_CUDA", 3: "EWG_ER
 LAW_VG, LAW_BC = 0, 1
 PRECOND_ILU0, PRECOND_JACOBI = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+# ewg_ilu_ordering: row order of the block ILU(0) (BOX8 needs a 3D grid with dimensions divisible by 4)
+ILU_ORDER_AUTO, ILU_ORDER_REDBLACK, ILU_ORDER_BOX8 = 0, 1, 2
 LOCAL_LINEARIZER_AD, LOCAL_LINEARIZER_FD = 0, 1
 
 
@@ -76,7 +78,8 @@ class SolveOpts(C.Structure):
                 ("preconditioner_relaxation", C.c_double),
                 ("defect_tolerance", C.c_double), ("inner_tolerance", C.c_double),
                 ("max_defect_iterations", C.c_int32), ("check_interval", C.c_int32),
-                ("restart_on_breakdown", C.c_int32), ("verify_true_residual", C.c_int32)]
+                ("restart_on_breakdown", C.c_int32), ("verify_true_residual", C.c_int32),
+                ("ilu_ordering", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -130,7 +133,7 @@ def default_solve_opts(**kw) -> SolveOpts:
                   linear_solver_max_error=1e7, linear_solver_max_iterations=1000,
                   preconditioner_relaxation=1.0, defect_tolerance=0.0, inner_tolerance=1e-4,
                   max_defect_iterations=50, check_interval=0, restart_on_breakdown=1,
-                  verify_true_residual=1)
+                  verify_true_residual=1, ilu_ordering=ILU_ORDER_AUTO)
     for k, v in kw.items():
         setattr(o, k, v)
     return o
@@ -395,6 +398,17 @@ def load(path: str = LIB_PATH):
         "ewg_device_buffer": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_void_p)]),
         "ewg_device_spmv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "ewg_device_precondition": (C.c_int, [C.c_void_p, P(SolveOpts), C.c_void_p, C.c_void_p]),
+        "ewg_device_bicg_p": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                        C.c_double, C.c_int32]),
+        "ewg_device_bicg_spmv_dot": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                               C.c_int64, C.c_void_p]),
+        "ewg_device_bicg_hs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                         C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+        "ewg_device_bicg_spmv_dot2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                                C.c_int64, C.c_void_p]),
+        "ewg_device_bicg_xr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_int64, C.c_int64, C.c_void_p]),
+        "ewg_transfer_counters": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_uint64), P(C.c_uint64)]),
         "ewg_profile_num_kernels": (C.c_int32, []),
         "ewg_profile_kernel_name": (C.c_char_p, [C.c_int32]),
         "ewg_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -658,6 +672,39 @@ class Context:
         bp, yp = self._device_args(b, y)
         self._check(self.lib.ewg_device_precondition(self.h, C.byref(opts), bp, yp), "device_precondition")
 
+    # fused kernels of one slab's BiCGStab iteration (dd.distributed_bicgstab); device tensors
+    # (N x 2 float64), owned rows [lo, hi) of each colour half, `out` a float64 device tensor
+
+    def device_bicg_p(self, p, r, r0, v, beta, omega, restart):
+        a = self._device_args(p, r, r0, v)
+        self._check(self.lib.ewg_device_bicg_p(self.h, *a, float(beta), float(omega), int(restart)), "device_bicg_p")
+
+    def device_bicg_spmv_dot(self, x, y, w, lo, hi, out):
+        a = self._device_args(x, y, w)
+        self._check(self.lib.ewg_device_bicg_spmv_dot(self.h, *a, int(lo), int(hi), C.c_void_p(out.data_ptr())),
+                    "device_bicg_spmv_dot")
+
+    def device_bicg_hs(self, x, y, r, v, rho_i, denom, lo, hi, out):
+        a = self._device_args(x, y, r, v)
+        self._check(self.lib.ewg_device_bicg_hs(self.h, *a, float(rho_i), C.c_void_p(denom.data_ptr()), int(lo),
+                                                int(hi), C.c_void_p(out.data_ptr())), "device_bicg_hs")
+
+    def device_bicg_spmv_dot2(self, z, t, s, lo, hi, out):
+        a = self._device_args(z, t, s)
+        self._check(self.lib.ewg_device_bicg_spmv_dot2(self.h, *a, int(lo), int(hi), C.c_void_p(out.data_ptr())),
+                    "device_bicg_spmv_dot2")
+
+    def device_bicg_xr(self, x, z, r, t, r0, omega, lo, hi, out):
+        a = self._device_args(x, z, r, t, r0)
+        self._check(self.lib.ewg_device_bicg_xr(self.h, *a, float(omega), int(lo), int(hi),
+                                                C.c_void_p(out.data_ptr())), "device_bicg_xr")
+
+    def transfer_counters(self, reset=False):
+        """(host->device, device->host) bytes of this context's entry points (ewg_transfer_counters)."""
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.ewg_transfer_counters(self.h, int(reset), C.byref(h2d), C.byref(d2h)), "transfer_counters")
+        return h2d.value, d2h.value
+
     def profile_enable(self, on=True, period=1):
         """Time kernel launches with CUDA events: every `period`-th launch of each class."""
         self._check(self.lib.ewg_profile_enable(self.h, int(period) if on else 0), "profile_enable")
@@ -676,6 +723,18 @@ class Context:
                 out[self.lib.ewg_profile_kernel_name(k).decode()] = (ms.value, n.value)
         return out
 
+    def save_restart(self, output_dir: str, sim_name: str, sim: "SimulatorState") -> str:
+        """Simulator::serialize of this context's solution(0) (restart file name returned)."""
+        return write_restart(output_dir, sim_name, self.case.grid, self.get_solution(0), sim)
+
+    def load_restart(self, output_dir: str, sim_name: str, t: float) -> "SimulatorState":
+        """Restart from the file written at time t: solution(0) from the file and solution(1) =
+        solution(0) (EcfvDiscretization::deserialize); returns the simulator state."""
+        sim, x, _ = read_restart(output_dir, sim_name, t, self.case.grid)
+        self.set_solution(0, x)
+        self.set_solution(1, x)
+        return sim
+
     def run(self, n_steps, dt, nopts=None, sopts=None, max_divisions=10):
         """Simulator time loop at a fixed step size with FvBaseProblem::timeIntegration's halving
         retry (fvbaseproblem.hh:507-550). Returns the per-step Newton reports."""
@@ -693,6 +752,138 @@ class Context:
             self.advance_time_level()
             reports.append(rep)
         return reports
+
+
+# ------------------------------------------------------------------------------------------
+# restart files (io/restart.hh:36-271; the C++ driver's host/restart.hh writes the same files)
+
+
+@dataclass
+class SimulatorState:
+    """Simulator's serialized state (utils/simulator.hh:944-952)."""
+    episode_idx: int = 0
+    episode_start_time: float = 0.0
+    episode_length: float = 1e100
+    start_time: float = 0.0
+    time: float = 0.0
+    time_step_idx: int = 0
+
+
+def _g20(v: float) -> str:
+    """A double as an ostream with precision 20 prints it (%.20g)."""
+    return "%.20g" % v
+
+
+def _ostream_default(v: float) -> str:
+    """A double as an ostream with its default precision (6) prints it (%g)."""
+    return "%g" % v
+
+
+def restart_grid_counts(grid: Grid):
+    """(elements, codim dim-1 entities, vertices) of the structured grid."""
+    nx, ny = grid.nx, grid.ny
+    if grid.dim == 2:
+        return nx * ny, nx * (ny + 1) + (nx + 1) * ny, (nx + 1) * (ny + 1)
+    nz = grid.nz
+    return (nx * ny * nz, nx * (ny + 1) * (nz + 1) + (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz,
+            (nx + 1) * (ny + 1) * (nz + 1))
+
+
+def restart_cookie(grid: Grid, num_cpus: int = 1, rank: int = 0) -> str:
+    """magicRestartCookie_ (restart.hh:42-62); the grid name is the reference's literal 'blubb'."""
+    ne, ned, nv = restart_grid_counts(grid)
+    return (f"eWoms restart file: gridName='blubb' numCPUs={num_cpus} myRank={rank} "
+            f"numElements={ne} numEdges={ned} numVertices={nv}")
+
+
+def restart_file_name(output_dir: str, sim_name: str, t: float, rank: int = 0) -> str:
+    """restartFileName_ (restart.hh:67-83): <dir>/<simName>_time=<t>_rank=<rank>.ers."""
+    d = "" if output_dir == "." else (output_dir if not output_dir or output_dir.endswith("/") else output_dir + "/")
+    return f"{d}{sim_name}_time={_ostream_default(t)}_rank={rank}.ers"
+
+
+def write_restart(output_dir: str, sim_name: str, grid: Grid, x: np.ndarray, sim: SimulatorState,
+                  vtk: tuple | None = None, num_cpus: int = 1, rank: int = 0) -> str:
+    """Simulator::serialize: cookie, Simulator section, the VTK writer's section when given
+    (writer index, collection text, write position), and solution(0) of every cell (natural order).
+    Returns the file name."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1, 2)
+    path = restart_file_name(output_dir, sim_name, sim.time, rank)
+    parts = [restart_cookie(grid, num_cpus, rank), "\n", "\n", "Simulator\n",
+             f"{sim.episode_idx} {_g20(sim.episode_start_time)} {_g20(sim.episode_length)} "
+             f"{_g20(sim.start_time)} {_g20(sim.time)} {sim.time_step_idx} ", "\n"]
+    if vtk is not None:
+        num, coll, pos = vtk
+        parts += ["VTKMultiWriter\n", f"{num}\n", f"{len(coll.encode())}  {pos}\n", coll, "\n"]
+    parts.append("Entities: Codim 0\n")
+    parts.append("".join(f"{_g20(a)} {_g20(b)} \n" for a, b in x))
+    parts.append("\n")
+    with open(path, "w") as f:
+        f.write("".join(parts))
+    return path
+
+
+def read_restart(output_dir: str, sim_name: str, t: float, grid: Grid, vtk: bool = False,
+                 num_cpus: int = 1, rank: int = 0):
+    """Simulator::run with RestartTime = t: (SimulatorState, solution(0) as N x 2, the VTK
+    section (index, collection, write position) or None). Raises like Restart::deserialize* on a
+    missing or empty file, a wrong cookie, a short section or unread values."""
+    path = restart_file_name(output_dir, sim_name, t, rank)
+    try:
+        with open(path, "rb") as f:
+            data = f.read()
+    except OSError as e:
+        raise RuntimeError(f"Restart file '{path}' could not be opened properly") from e
+    if not data:
+        raise RuntimeError(f"Restart file '{path}' is empty")
+    pos = 0
+
+    def line():
+        nonlocal pos
+        if pos >= len(data):
+            raise RuntimeError("Encountered unexpected EOF in restart file.")
+        e = data.find(b"\n", pos)
+        e = len(data) if e < 0 else e
+        ln = data[pos:e].decode()
+        pos = e + 1
+        return ln
+
+    def section_begin(cookie):
+        if line() != cookie:
+            raise RuntimeError(f"Could not start section '{cookie}'")
+
+    def section_end():
+        if line().strip():
+            raise RuntimeError("Encountered unread values while deserializing")
+
+    section_begin(restart_cookie(grid, num_cpus, rank))
+    section_end()
+    section_begin("Simulator")
+    vals = line().split()
+    if len(vals) != 6:
+        raise RuntimeError("Encountered unread values while deserializing" if len(vals) > 6 else
+                           "Restart file is corrupted (Simulator section)")
+    # the values and the section's end share one line (the writer ends the section right after them)
+    sim = SimulatorState(int(vals[0]), float(vals[1]), float(vals[2]), float(vals[3]), float(vals[4]), int(vals[5]))
+    vtk_state = None
+    if vtk:
+        section_begin("VTKMultiWriter")
+        num = int(line().split()[0])
+        ln, wpos = (int(v) for v in line().split())
+        coll = data[pos:pos + ln].decode()
+        pos += ln
+        section_end()
+        vtk_state = (num, coll, wpos)
+    section_begin("Entities: Codim 0")
+    n = grid.n_cells
+    x = np.empty((n, 2))
+    for c in range(n):
+        v = line().split()
+        if len(v) < 2:
+            raise RuntimeError(f"Could not deserialize degree of freedom {c}")
+        x[c, 0], x[c, 1] = float(v[0]), float(v[1])
+    section_end()
+    return sim, x, vtk_state
 
 
 # ------------------------------------------------------------------------------------------
