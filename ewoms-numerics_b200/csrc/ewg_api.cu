@@ -834,49 +834,67 @@ static ewg_status slab_args_ok(ewg_ctx* ctx, std::initializer_list<const void*> 
     return EWG_OK;
 }
 
-ewg_status ewg_device_bicg_p(ewg_ctx* ctx, double* p, const double* r, double* r0, double* v, double beta, double omega,
-                             int32_t restart) {
-    if (check_ctx(ctx)) return EWG_ERR_INVALID;
+static bool device_ptr_ok(ewg_ctx* ctx, const void* p) {
+    if (!p || ((uintptr_t)p & 7)) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == ctx->device;
+}
+
+ewg_status ewg_device_bicg_p(ewg_ctx* ctx, double* p, const double* r, double* r0, double* v, const void* state) {
+    if (check_ctx(ctx) || !device_ptr_ok(ctx, state)) return EWG_ERR_INVALID;
     ewg_status st = slab_args_ok(ctx, {p, r, r0, v}, nullptr, "device_bicg_p");
     if (st) return st;
-    return solver_slab(ctx, 0, (double2*)p, (double2*)r, (double2*)r0, (double2*)v, nullptr, nullptr, beta, omega,
-                       restart, 0, 0, nullptr);
+    return solver_slab(ctx, 0, (double2*)p, (double2*)r, (double2*)r0, (double2*)v, nullptr, state, 0, 0, nullptr);
 }
 
 ewg_status ewg_device_bicg_spmv_dot(ewg_ctx* ctx, const double* x, double* y, const double* w, int64_t lo, int64_t hi,
-                                    double* out) {
-    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+                                    const void* state, double* out) {
+    if (check_ctx(ctx) || !out || (state && !device_ptr_ok(ctx, state))) return EWG_ERR_INVALID;
     if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "device_bicg_spmv_dot needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
     ewg_status st = slab_args_ok(ctx, {x, y, w}, out, "device_bicg_spmv_dot");
     if (st) return st;
-    return solver_slab(ctx, 1, (double2*)x, (double2*)y, (double2*)w, nullptr, nullptr, nullptr, 0, 0, 0, lo, hi, out);
+    return solver_slab(ctx, 1, (double2*)x, (double2*)y, (double2*)w, nullptr, nullptr, state, lo, hi, out);
 }
 
-ewg_status ewg_device_bicg_hs(ewg_ctx* ctx, double* x, const double* y, double* r, const double* v, double rho_i,
-                              const double* denom, int64_t lo, int64_t hi, double* out) {
-    if (check_ctx(ctx) || !out || !denom) return EWG_ERR_INVALID;
+ewg_status ewg_device_bicg_hs(ewg_ctx* ctx, double* x, const double* y, double* r, const double* v, int64_t lo,
+                              int64_t hi, const void* state, double* out) {
+    if (check_ctx(ctx) || !out || !device_ptr_ok(ctx, state)) return EWG_ERR_INVALID;
     ewg_status st = slab_args_ok(ctx, {x, y, r, v}, out, "device_bicg_hs");
     if (st) return st;
-    return solver_slab(ctx, 2, (double2*)x, (double2*)y, (double2*)r, (double2*)v, nullptr, denom, rho_i, 0, 0, lo, hi,
-                       out);
+    return solver_slab(ctx, 2, (double2*)x, (double2*)y, (double2*)r, (double2*)v, nullptr, state, lo, hi, out);
 }
 
 ewg_status ewg_device_bicg_spmv_dot2(ewg_ctx* ctx, const double* z, double* t, const double* s, int64_t lo, int64_t hi,
-                                     double* out) {
-    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+                                     const void* state, double* out) {
+    if (check_ctx(ctx) || !out || (state && !device_ptr_ok(ctx, state))) return EWG_ERR_INVALID;
     if (ctx->jacPrecision != EWG_PRECISION_FP64) { ctx->err = "device_bicg_spmv_dot2 needs the FP64 Jacobian"; return EWG_ERR_INVALID; }
     ewg_status st = slab_args_ok(ctx, {z, t, s}, out, "device_bicg_spmv_dot2");
     if (st) return st;
-    return solver_slab(ctx, 3, (double2*)z, (double2*)t, (double2*)s, nullptr, nullptr, nullptr, 0, 0, 0, lo, hi, out);
+    return solver_slab(ctx, 3, (double2*)z, (double2*)t, (double2*)s, nullptr, nullptr, state, lo, hi, out);
 }
 
 ewg_status ewg_device_bicg_xr(ewg_ctx* ctx, double* x, const double* z, double* r, const double* t, const double* r0,
-                              double omega, int64_t lo, int64_t hi, double* out) {
-    if (check_ctx(ctx) || !out) return EWG_ERR_INVALID;
+                              int64_t lo, int64_t hi, const void* state, double* out) {
+    if (check_ctx(ctx) || !out || !device_ptr_ok(ctx, state)) return EWG_ERR_INVALID;
     ewg_status st = slab_args_ok(ctx, {x, z, r, t, r0}, out, "device_bicg_xr");
     if (st) return st;
-    return solver_slab(ctx, 4, (double2*)x, (double2*)z, (double2*)r, (double2*)t, (const double2*)r0, nullptr, omega, 0,
-                       0, lo, hi, out);
+    return solver_slab(ctx, 4, (double2*)x, (double2*)z, (double2*)r, (double2*)t, (const double2*)r0, state, lo, hi,
+                       out);
+}
+
+int32_t ewg_device_bicg_state_size(void) { return solver_slab_state_size(); }
+
+ewg_status ewg_device_bicg_state(ewg_ctx* ctx, int32_t stage, void* state, const double* red, const ewg_solve_opts* o) {
+    if (check_ctx(ctx) || !device_ptr_ok(ctx, state) || !device_ptr_ok(ctx, red)) return EWG_ERR_INVALID;
+    if (stage == 0 && !o) { ctx->err = "device_bicg_state: stage 0 needs the solve options"; return EWG_ERR_INVALID; }
+    return solver_slab_state(ctx, stage, state, red, o);
+}
+
+ewg_status ewg_device_bicg_state_read(ewg_ctx* ctx, const void* state, int32_t* status, int32_t* iterations,
+                                      int32_t* restarts, double* res, double* init) {
+    if (check_ctx(ctx) || !device_ptr_ok(ctx, state)) return EWG_ERR_INVALID;
+    return solver_slab_state_read(ctx, state, status, iterations, restarts, res, init);
 }
 
 ewg_status ewg_newton_update(ewg_ctx* ctx) {

@@ -304,7 +304,11 @@ ewg_status solver_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* o, co
                                        double2* y);
 ewg_status solver_spmv(ewg_ctx* ctx, const double2* x, double2* y);
 ewg_status solver_slab(ewg_ctx* ctx, int kind, double2* a, double2* b, double2* c, double2* d, const double2* e,
-                       const double* s0, double s1, double s2, int flag, int64_t lo, int64_t hi, double* out);
+                       const void* state, int64_t lo, int64_t hi, double* out);
+ewg_status solver_slab_state(ewg_ctx* ctx, int stage, void* state, const double* red, const ewg_solve_opts* o);
+int32_t solver_slab_state_size();
+ewg_status solver_slab_state_read(ewg_ctx* ctx, const void* state, int32_t* status, int32_t* iterations,
+                                  int32_t* restarts, double* res, double* init);
 ewg_status solver_newton_update(ewg_ctx* ctx, int* nonfinite);
 void solver_free(ewg_ctx* ctx);
 

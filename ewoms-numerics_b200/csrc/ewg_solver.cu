@@ -454,11 +454,12 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_true_residu
 // ---- one slab's BiCGStab iteration in a distributed solve ---------------------------------------
 //
 // The same fused updates as the kernels above, for dd.distributed_bicgstab: vectors are device
-// vectors in the context's storage order, scalars come from the host or from device memory (the
-// cross-slab reduction of <r0,v>), and every reduction runs over the slab's owned rows -- rows
-// [lo, hi) of each colour half -- and ends, deterministically, in a small device array `out` that
-// the caller combines across slabs. Rows outside [lo, hi) (ghost planes) are updated too; the
-// exchange overwrites them.
+// vectors in the context's storage order, the scalars (alpha, omega, beta, the restart flag) come
+// from a BiState in device memory that k_slab_state advances from the reductions combined over
+// all slabs, and every reduction runs over the slab's owned rows -- rows [lo, hi) of each colour
+// half -- and ends, deterministically, in a small device array `out`. Rows outside [lo, hi)
+// (ghost planes) are updated too; the exchange overwrites them. Once the state has left RUNNING
+// every kernel returns at once, so the host reads the status only every few iterations.
 
 __device__ __forceinline__ bool owned_row(const Phys& P, int64_t s, int64_t lo, int64_t hi) {
     const int64_t h = s >= P.Nh ? s - P.Nh : s;
@@ -468,7 +469,10 @@ __device__ __forceinline__ bool owned_row(const Phys& P, int64_t s, int64_t lo, 
 // p = r + beta (p - omega v); on a restart r0 = r and v = p = 0 first
 __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_p(const __grid_constant__ Phys P, double2* __restrict__ p,
                                                        const double2* __restrict__ r, double2* __restrict__ r0,
-                                                       double2* __restrict__ v, double beta, double omega, int restart) {
+                                                       double2* __restrict__ v, const BiState* __restrict__ st) {
+    if (st->status != ST_RUNNING) return;
+    const double beta = st->beta, omega = st->omega;
+    const bool restart = st->restartPending != 0;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
         const double2 rs = r[s];
         double2 vs = v[s], ps = p[s];
@@ -478,10 +482,11 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_p(const __g
             ps = vs;
             v[s] = vs;
         }
-        // torch's p.sub_(v, alpha=omega).mul_(beta).add_(r) order
-        double t0 = ps.x - omega * vs.x, t1 = ps.y - omega * vs.y;
-        t0 *= beta; t1 *= beta;
-        p[s] = make_double2(t0 + rs.x, t1 + rs.y);
+        // (omega v - p)(-beta) + r, the order of k_bicg_p
+        double t0 = vs.x * omega, t1 = vs.y * omega;
+        t0 -= ps.x; t1 -= ps.y;
+        t0 *= -beta; t1 *= -beta;
+        p[s] = make_double2(rs.x + t0, rs.y + t1);
     }
 }
 
@@ -490,7 +495,9 @@ template <int MODE>
 __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_spmv_dot(const __grid_constant__ Phys P, const double* __restrict__ A,
                                                               const double2* __restrict__ x, double2* __restrict__ y,
                                                               const double2* __restrict__ w, int64_t lo, int64_t hi,
-                                                              double* partials, unsigned* counter, double* out) {
+                                                              const BiState* __restrict__ st, double* partials,
+                                                              unsigned* counter, double* out) {
+    if (st && st->status != ST_RUNNING) return;
     double red[1] = {0.0};
     const SpmvExtra ex{nullptr, nullptr, 1.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
@@ -511,7 +518,9 @@ template <int MODE>
 __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_spmv_dot2(const __grid_constant__ Phys P, const double* __restrict__ A,
                                                                const double2* __restrict__ z, double2* __restrict__ t,
                                                                const double2* __restrict__ sres, int64_t lo, int64_t hi,
-                                                               double* partials, unsigned* counter, double* out) {
+                                                               const BiState* __restrict__ st, double* partials,
+                                                               unsigned* counter, double* out) {
+    if (st && st->status != ST_RUNNING) return;
     double red[2] = {0.0, 0.0};
     const SpmvExtra ex{nullptr, nullptr, 1.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
@@ -528,19 +537,20 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_spmv_dot2(c
     if (grid_reduce<2, 0>(red, partials, counter, o) && threadIdx.x == 0) { out[0] = o[0]; out[1] = o[1]; }
 }
 
-// alpha = rho_i / *denom; x += alpha y; r -= alpha v; out = {max |r|, max |y|} over owned rows
+// x += alpha y (h); r -= alpha v (s); out = {max |s|, max |y|} over owned rows
 __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_hs(const __grid_constant__ Phys P, double2* __restrict__ x,
                                                         const double2* __restrict__ y, double2* __restrict__ r,
-                                                        const double2* __restrict__ v, double rho_i,
-                                                        const double* __restrict__ denom, int64_t lo, int64_t hi,
-                                                        double* partials, unsigned* counter, double* out) {
-    const double alpha = rho_i / *denom;
+                                                        const double2* __restrict__ v, int64_t lo, int64_t hi,
+                                                        const BiState* __restrict__ st, double* partials,
+                                                        unsigned* counter, double* out) {
+    if (st->status != ST_RUNNING) return;
+    const double alpha = st->alpha;
     double red[2] = {0.0, 0.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
         const double2 ys = y[s], vs = v[s];
         double2 xs = x[s], rs = r[s];
-        xs.x += ys.x * alpha; xs.y += ys.y * alpha;
-        rs.x -= vs.x * alpha; rs.y -= vs.y * alpha;
+        xs.x = ys.x * alpha + xs.x; xs.y = ys.y * alpha + xs.y;
+        rs.x = rs.x - vs.x * alpha; rs.y = rs.y - vs.y * alpha;
         x[s] = xs;
         r[s] = rs;
         if (owned_row(P, s, lo, hi)) {
@@ -552,25 +562,27 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_hs(const __
     if (grid_reduce<0, 2>(red, partials, counter, o) && threadIdx.x == 0) { out[0] = o[0]; out[1] = o[1]; }
 }
 
-// x += omega z; then {max |r|, max |z|} over owned rows (r before its update); r -= omega t;
-// out = {r0 . r, r . r, max |r|, max |z|}
+// x += omega z; then {max |s|, max |z|} over owned rows (r still holds s); r += -omega t;
+// out = {r0 . r, r . r, max |s|, max |z|}
 __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_xr(const __grid_constant__ Phys P, double2* __restrict__ x,
                                                         const double2* __restrict__ z, double2* __restrict__ r,
                                                         const double2* __restrict__ t, const double2* __restrict__ r0,
-                                                        double omega, int64_t lo, int64_t hi, double* partials,
-                                                        unsigned* counter, double* out) {
+                                                        int64_t lo, int64_t hi, const BiState* __restrict__ st,
+                                                        double* partials, unsigned* counter, double* out) {
+    if (st->status != ST_RUNNING) return;
+    const double omega = st->omega;
     double red[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
         const double2 zs = z[s], ts = t[s];
         double2 xs = x[s], rs = r[s];
-        xs.x += omega * zs.x; xs.y += omega * zs.y;
+        xs.x = xs.x + omega * zs.x; xs.y = xs.y + omega * zs.y;
         x[s] = xs;
         const bool own = owned_row(P, s, lo, hi);
         if (own) {
             red[2] = fmax(red[2], fmax(absn(rs.x), absn(rs.y)));
             red[3] = fmax(red[3], fmax(absn(zs.x), absn(zs.y)));
         }
-        rs.x -= omega * ts.x; rs.y -= omega * ts.y;
+        rs.x = rs.x + (-omega) * ts.x; rs.y = rs.y + (-omega) * ts.y;
         r[s] = rs;
         if (own) {
             const double2 rh = r0[s];
@@ -581,6 +593,77 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_slab_xr(const __
     double o[4];
     if (grid_reduce<2, 2>(red, partials, counter, o) && threadIdx.x == 0)
         for (int k = 0; k < 4; ++k) out[k] = o[k];
+}
+
+// One scalar step of the distributed BiCGStab on the reductions combined over all slabs, the
+// decisions the single-domain kernels take in their last block (BiCGStabSolver::apply,
+// CombinedCriterion, bicgstabsolver.hh:191-322, combinedcriterion.hh:112-205).
+//   0 start  red = {b.b, max|b|}            setInitial, then the top of the first iteration
+//   1 alpha  red = {r0.v}                    alpha = rho_i / r0.v, breakdown tests
+//   2 half   red = {t.t, t.s, max|s|, max|y|}  criterion on s (y all zero: stagnation), omega
+//   3 full   red = {r0.r, r.r, max|s|, max|z|} criterion on s, next iteration's top
+//   4 true   red = {r.r, max|r|}             after convergence, on r = b - J x: resume from x when
+//                                             the true residual misses the criterion by 10x
+__global__ void k_slab_state(int stage, BiState* st, const double* __restrict__ red, double relTol, double absTol,
+                             double maxRes, int maxIter, int restartOnBreakdown) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double breakdownEps = DBL_MIN * 1e10;
+    if (stage == 0) {
+        memset(st, 0, sizeof(BiState));
+        st->relTol = relTol; st->absTol = absTol; st->maxRes = maxRes; st->maxIter = maxIter;
+        st->restartOnBreakdown = restartOnBreakdown;
+        st->resErr = fmax(red[1], breakdownEps);
+        st->initResErr = st->resErr;
+        st->lastResErr = st->resErr;
+        st->rho = 1.0; st->alpha = 1.0; st->omega = 1.0;
+        st->r0r0 = red[0];
+        st->status = ST_RUNNING;
+        if (st->resErr / fmax(1e-20, st->initResErr) <= relTol || st->resErr <= absTol) { st->status = ST_CONVERGED; return; }
+        iteration_top(st, red[0], red[0]);
+        return;
+    }
+    if (stage == 4) {
+        if (st->status != ST_CONVERGED) return;
+        const double err = red[1];
+        if (err / fmax(1e-20, st->initResErr) <= 10 * st->relTol || err <= 10 * st->absTol) return;
+        st->replacements += 1;
+        st->restarts += 1;
+        st->status = ST_RUNNING;
+        st->lastResErr = st->resErr;
+        st->resErr = err;
+        st->stagnates = 0;
+        st->restartPending = 0;
+        st->rho = 1.0; st->alpha = 1.0; st->omega = 1.0;
+        st->r0r0 = red[0];
+        st->iter += 1;
+        iteration_top(st, red[0], red[0]);
+        return;
+    }
+    if (st->status != ST_RUNNING) return;
+    if (stage == 1) {
+        st->restartPending = 0;
+        const double denom = red[0];
+        if (fabs(denom) <= breakdownEps) { st->status = ST_BREAKDOWN; return; }
+        st->alpha = st->rho_i / denom;
+        if (fabs(st->alpha) <= breakdownEps) st->status = ST_BREAKDOWN;
+    } else if (stage == 2) {
+        st->lastResErr = st->resErr;
+        st->resErr = red[2];
+        st->stagnates = red[3] == 0.0;
+        criterion_check(st);
+        if (st->status != ST_RUNNING) return;
+        if (fabs(red[0]) <= breakdownEps) { st->status = ST_BREAKDOWN; return; }
+        st->omega = red[1] / red[0];
+        if (fabs(st->omega) <= breakdownEps) st->status = ST_BREAKDOWN;
+    } else if (stage == 3) {
+        st->lastResErr = st->resErr;
+        st->resErr = red[2];
+        st->stagnates = red[3] == 0.0;
+        criterion_check(st);
+        if (st->status != ST_RUNNING) return;
+        st->iter += 1;
+        iteration_top(st, red[0], red[1]);
+    }
 }
 
 // ---- mixed precision: defect correction ----------------------------------------------------
@@ -900,7 +983,10 @@ static ewg_status bicgstab(ewg_ctx* ctx, KrylovWs<T>& w, const ewg_solve_opts* o
     double* part = sw->partials;
     unsigned* cnt = sw->counter;
     EWG_LAUNCH(ctx, K_BICG_INIT, k_bicg_init<T>, G, kSolBlock, P, w.b, w.x, w.r, w.r0, w.v, w.p, sw->st, part, cnt);
-    int interval = o->check_interval > 0 ? o->check_interval : (P.N >= (1 << 20) ? 1 : 8);
+    // host status reads: every kernel launched after the solve has ended returns at once, so a few
+    // iterations' launches past convergence cost microseconds, while a read per iteration leaves
+    // the device idle for a host round trip every iteration
+    int interval = o->check_interval > 0 ? o->check_interval : (P.N >= (1 << 20) ? 4 : 8);
     const int* status = &sw->st->status;
     const double relax = o->preconditioner_relaxation;
     const SpmvExtra ex{b8 ? (const void*)w.E8 : nullptr, b8 ? (const void*)w.W : nullptr, relax};
@@ -1072,31 +1158,58 @@ ewg_status solver_apply_preconditioner(ewg_ctx* ctx, const ewg_solve_opts* o, co
 }
 
 // One slab-iteration kernel of the distributed BiCGStab (kind: 0 p-update, 1 SpMV + dot,
-// 2 h/s update, 3 SpMV + two dots, 4 x/r update); vectors in the split order, out on the device.
+// 2 h/s update, 3 SpMV + two dots, 4 x/r update); vectors in the split order, out on the device,
+// st the device state (may be null for kinds 1 and 3: no status test).
 ewg_status solver_slab(ewg_ctx* ctx, int kind, double2* a, double2* b, double2* c, double2* d, const double2* e,
-                       const double* s0, double s1, double s2, int flag, int64_t lo, int64_t hi, double* out) {
+                       const void* stv, int64_t lo, int64_t hi, double* out) {
     ewg_status st = ensure_ws(ctx, false);
     if (st) return st;
     SolverWs* sw = ws_of(ctx);
     const Phys& P = ctx->P;
     const int G = sw->gridRed;
+    const BiState* bs = (const BiState*)stv;
     if (lo < 0 || hi < lo || hi > P.Nh) {
         ctx->err = "slab kernel: owned row range outside the colour half";
         return EWG_ERR_INVALID;
     }
     switch (kind) {
-        case 0: EWG_LAUNCH(ctx, K_BICG_P, k_slab_p, G, kSolBlock, P, a, b, c, d, s1, s2, flag); break;
-        case 1: EWG_LAUNCH(ctx, K_BICG_SPMV_ALPHA, k_slab_spmv_dot<0>, G, kSolBlock, P, ctx->J, a, b, c, lo, hi,
+        case 0: EWG_LAUNCH(ctx, K_BICG_P, k_slab_p, G, kSolBlock, P, a, b, c, d, bs); break;
+        case 1: EWG_LAUNCH(ctx, K_BICG_SPMV_ALPHA, k_slab_spmv_dot<0>, G, kSolBlock, P, ctx->J, a, b, c, lo, hi, bs,
                            sw->partials, sw->counter, out); break;
-        case 2: EWG_LAUNCH(ctx, K_BICG_HS, k_slab_hs, G, kSolBlock, P, a, b, c, d, s1, s0, lo, hi, sw->partials,
+        case 2: EWG_LAUNCH(ctx, K_BICG_HS, k_slab_hs, G, kSolBlock, P, a, b, c, d, lo, hi, bs, sw->partials,
                            sw->counter, out); break;
-        case 3: EWG_LAUNCH(ctx, K_BICG_SPMV_OMEGA, k_slab_spmv_dot2<0>, G, kSolBlock, P, ctx->J, a, b, c, lo, hi,
+        case 3: EWG_LAUNCH(ctx, K_BICG_SPMV_OMEGA, k_slab_spmv_dot2<0>, G, kSolBlock, P, ctx->J, a, b, c, lo, hi, bs,
                            sw->partials, sw->counter, out); break;
-        case 4: EWG_LAUNCH(ctx, K_BICG_XR, k_slab_xr, G, kSolBlock, P, a, b, c, d, e, s1, lo, hi, sw->partials,
+        case 4: EWG_LAUNCH(ctx, K_BICG_XR, k_slab_xr, G, kSolBlock, P, a, b, c, d, e, lo, hi, bs, sw->partials,
                            sw->counter, out); break;
         default: ctx->err = "slab kernel: unknown kind"; return EWG_ERR_INVALID;
     }
     return cuda_fail(ctx, cudaGetLastError(), "slab kernel");
+}
+
+ewg_status solver_slab_state(ewg_ctx* ctx, int stage, void* state, const double* red, const ewg_solve_opts* o) {
+    if (stage < 0 || stage > 4) { ctx->err = "slab state: unknown stage"; return EWG_ERR_INVALID; }
+    k_slab_state<<<1, 32, 0, ctx->stream>>>(stage, (BiState*)state, red, o ? o->linear_solver_tolerance : 0.0,
+                                            o ? o->linear_solver_abs_tolerance : 0.0,
+                                            o ? o->linear_solver_max_error : 0.0,
+                                            o ? o->linear_solver_max_iterations : 0, o ? o->restart_on_breakdown : 0);
+    return cuda_fail(ctx, cudaGetLastError(), "slab state");
+}
+
+int32_t solver_slab_state_size() { return (int32_t)sizeof(BiState); }
+
+ewg_status solver_slab_state_read(ewg_ctx* ctx, const void* state, int32_t* status, int32_t* iterations,
+                                  int32_t* restarts, double* res, double* init) {
+    BiState h;
+    cudaError_t e = cudaMemcpyAsync(&h, state, sizeof(BiState), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "read slab state");
+    if (status) *status = h.status;
+    if (iterations) *iterations = h.iter;
+    if (restarts) *restarts = h.restarts;
+    if (res) *res = h.resErr;
+    if (init) *init = h.initResErr;
+    return EWG_OK;
 }
 
 ewg_status solver_spmv(ewg_ctx* ctx, const double2* x, double2* y) {

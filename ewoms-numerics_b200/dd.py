@@ -295,6 +295,30 @@ class LocalComm:
             torch.cuda.synchronize()
         return out
 
+    def reduce_device_mixed(self, vals, nsum, parts=None):
+        """One 1-D partial tensor per slab combined on the device: the first nsum entries summed
+        over the slabs (in slab order), the rest maximised; no host read."""
+        import torch
+        if len(vals) == 1:
+            return vals[0]
+        cuda = any(v.is_cuda for v in vals)
+        streams = [getattr(sp, "stream", None) for sp in (parts or [])]
+        ordered = cuda and len(streams) == len(vals) and all(st is not None for st in streams)
+        if ordered:
+            cur = torch.cuda.current_stream()
+            for st in streams:
+                cur.wait_stream(st)
+        elif cuda:
+            torch.cuda.synchronize()
+        g = torch.stack(vals)
+        out = torch.cat([g[:, :nsum].sum(0), g[:, nsum:].amax(0)])
+        if ordered:
+            for st in streams:
+                st.wait_stream(cur)
+        elif cuda:
+            torch.cuda.synchronize()
+        return out
+
     def reduce(self, vals, nsum):
         """vals: one 1-D tensor of partials per slab, the first nsum summed over the slabs and the
         rest maximised. One host read per slab. The partials were computed on the slabs' own
@@ -356,6 +380,17 @@ class TorchComm:
         g = [torch.empty_like(x) for _ in range(self.dist.get_world_size())]
         self.dist.all_gather(g, x)
         return torch.stack(g).sum(0).reshape(())
+
+    def reduce_device_mixed(self, vals, nsum, parts=None):
+        """This rank's partials combined over the ranks on the device (one all_gather, combined in
+        rank order): the first nsum entries summed, the rest maximised."""
+        import torch
+        (x,) = vals
+        x = x.to(self._device).reshape(-1)
+        g = [torch.empty_like(x) for _ in range(self.dist.get_world_size())]
+        self.dist.all_gather(g, x)
+        st = torch.stack(g)
+        return torch.cat([st[:, :nsum].sum(0), st[:, nsum:].amax(0)])
 
     def reduce(self, vals, nsum):
         """One all_gather of this rank's partials (a 1-D tensor, the first nsum summed and the rest
@@ -430,40 +465,43 @@ class DeviceSlab:
         self.ctx.device_precondition(b, y, self.opts)
 
     # the fused kernels of one slab-iteration (ewg_device_bicg_*): vector updates with their
-    # owned-row reductions in one pass each, results left on the device
+    # owned-row reductions in one pass each, scalars from the device state, results on the device
     def _reduction_slots(self):
         import torch
         if not hasattr(self, "_red"):
             self._red = torch.zeros(16, dtype=torch.float64, device="cuda")
-        lo, hi = self.layout._own.start, self.layout._own.stop
-        return self._red, lo, hi
+        return self._red, self.layout._own.start, self.layout._own.stop
 
-    def bicg_p(self, v, beta, omega, restart):
-        self.ctx.device_bicg_p(v.p, v.r, v.r0, v.v, beta, omega, restart)
+    def new_state(self):
+        import torch
+        return torch.zeros(self.ctx.lib.ewg_device_bicg_state_size(), dtype=torch.uint8, device="cuda")
 
-    def bicg_spmv_dot(self, x, y, w):
+    def dev_p(self, v, state):
+        self.ctx.device_bicg_p(v.p, v.r, v.r0, v.v, state)
+
+    def dev_spmv_dot(self, x, y, w, state):
         red, lo, hi = self._reduction_slots()
         out = red[0:1]
-        self.ctx.device_bicg_spmv_dot(x, y, w, lo, hi, out)
-        return out[0]
+        self.ctx.device_bicg_spmv_dot(x, y, w, lo, hi, state, out)
+        return out
 
-    def bicg_hs(self, v, rho_i, denom):
+    def dev_hs(self, v, state):
         red, lo, hi = self._reduction_slots()
         out = red[2:4]
-        self.ctx.device_bicg_hs(v.x, v.y, v.r, v.v, rho_i, denom, lo, hi, out)
-        return [out[0], out[1]]
+        self.ctx.device_bicg_hs(v.x, v.y, v.r, v.v, lo, hi, state, out)
+        return out
 
-    def bicg_spmv_dot2(self, z, t, s):
+    def dev_spmv_dot2(self, z, t, s, state):
         red, lo, hi = self._reduction_slots()
         out = red[4:6]
-        self.ctx.device_bicg_spmv_dot2(z, t, s, lo, hi, out)
-        return [out[0], out[1]]
+        self.ctx.device_bicg_spmv_dot2(z, t, s, lo, hi, state, out)
+        return out
 
-    def bicg_xr(self, v, omega):
+    def dev_xr(self, v, state):
         red, lo, hi = self._reduction_slots()
         out = red[8:12]
-        self.ctx.device_bicg_xr(v.x, v.z, v.r, v.t, v.r0, omega, lo, hi, out)
-        return out.clone()
+        self.ctx.device_bicg_xr(v.x, v.z, v.r, v.t, v.r0, lo, hi, state, out)
+        return out
 
 
 class _Vecs:
@@ -507,7 +545,7 @@ class _TorchOps:
 
 
 def _ops(p):
-    return p if hasattr(p, "bicg_xr") else _TorchOps(p)
+    return _TorchOps(p)
 
 
 def _bicgstab(parts, comm, opts):
@@ -667,6 +705,85 @@ def _bicgstab(parts, comm, opts):
     return S["status"], S["iter"], S["restarts"], S["resErr"], S["initResErr"], [v.x for v in V]
 
 
+def _bicgstab_device(parts, comm, opts, check_every=4):
+    """_bicgstab with every scalar on the device, for slabs with device kernels (DeviceSlab): the
+    fused kernels (ewg_device_bicg_*) update the vectors and reduce over the owned rows, the
+    reductions are combined over the slabs on the device (comm.reduce_device_mixed, one collective
+    each), and each slab's copy of the BiCGStab state takes the same scalar step on them
+    (ewg_device_bicg_state). The host reads the state every check_every iterations; kernels
+    launched after the solve has ended return at once. Same steps, tests and results as
+    _bicgstab (the dot products are summed in another order)."""
+    import torch
+    V = []
+    for p in parts:
+        with p.on():
+            v = _Vecs()
+            v.b = p.rhs().clone()
+            v.x, v.v, v.p, v.y, v.z, v.t = (p.zeros() for _ in range(6))
+            v.r = v.b.clone()
+            v.r0 = v.b.clone()
+            v.state = p.new_state()
+            V.append(v)
+
+    def each(fn):
+        out = []
+        for p, v in zip(parts, V):
+            with p.on():
+                out.append(fn(p, v))
+        return out
+
+    def exchange(name):
+        comm.exchange(parts, [getattr(v, name) for v in V])
+
+    def combine(vals, nsum):
+        return comm.reduce_device_mixed(vals, nsum, parts)
+
+    def stage(k, red, o=None):
+        each(lambda p, v: p.ctx.device_bicg_state(k, v.state, red, o))
+
+    def read():
+        return parts[0].ctx.device_bicg_state_read(V[0].state)
+
+    stage(0, combine(each(lambda p, v: _pack([_dev_dot(p.layout, v.b, v.b)], [_dev_max(p.layout, v.b)])), 1), opts)
+    replacements = 0
+    while True:
+        st = read()
+        while st[0] == ST_RUNNING:
+            for _ in range(check_every):
+                each(lambda p, v: p.dev_p(v, v.state))
+                exchange("p")
+                each(lambda p, v: p.precondition(v.p, v.y))
+                exchange("y")
+                stage(1, combine(each(lambda p, v: p.dev_spmv_dot(v.y, v.v, v.r0, v.state)), 1))
+                each(lambda p, v: setattr(v, "half", p.dev_hs(v, v.state)))
+                exchange("r")
+                each(lambda p, v: p.precondition(v.r, v.z))
+                exchange("z")
+                # {t.t, t.s} with the half step's {max|s|, max|y|}, joined on each slab's stream
+                stage(2, combine(each(lambda p, v: torch.cat([p.dev_spmv_dot2(v.z, v.t, v.r, v.state), v.half])), 2))
+                stage(3, combine(each(lambda p, v: p.dev_xr(v, v.state)), 2))
+            st = read()
+        if not (st[0] == ST_CONVERGED and opts.verify_true_residual and replacements < 3):
+            break
+        # residual replacement: r = r0hat = b - J x; resume if it misses the criterion by 10x
+        exchange("x")
+
+        def true_res(p, v):
+            p.spmv(v.x, v.t)
+            torch.sub(v.b, v.t, out=v.r)
+            v.r0.copy_(v.r)
+            v.v.zero_()
+            v.p.zero_()
+            return _pack([_dev_dot(p.layout, v.r, v.r)], [_dev_max(p.layout, v.r)])
+        stage(4, combine(each(true_res), 1))
+        st = read()
+        if st[0] != ST_RUNNING:
+            break
+        replacements += 1
+    status, its, restarts, res, init = st
+    return status, its, restarts, res, init, [v.x for v in V]
+
+
 def _single_stream(parts):
     """With one slab in this process, all its work (kernels, torch ops, collectives) runs on its
     context's stream; with several, each slab's work enters its own stream and the exchanges
@@ -678,8 +795,11 @@ def _single_stream(parts):
 
 
 def distributed_bicgstab(parts, comm, opts):
-    """Distributed BiCGStab over the slabs in `parts` (see _bicgstab)."""
+    """Distributed BiCGStab over the slabs in `parts`: device-resident (_bicgstab_device) when
+    every slab has device kernels, else with the scalars on the host (_bicgstab)."""
     with _single_stream(parts):
+        if parts and all(isinstance(p, DeviceSlab) for p in parts) and hasattr(comm, "reduce_device_mixed"):
+            return _bicgstab_device(parts, comm, opts)
         return _bicgstab(parts, comm, opts)
 
 

@@ -398,16 +398,19 @@ def load(path: str = LIB_PATH):
         "ewg_device_buffer": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_void_p)]),
         "ewg_device_spmv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "ewg_device_precondition": (C.c_int, [C.c_void_p, P(SolveOpts), C.c_void_p, C.c_void_p]),
-        "ewg_device_bicg_p": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
-                                        C.c_double, C.c_int32]),
+        "ewg_device_bicg_p": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ewg_device_bicg_spmv_dot": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
-                                               C.c_int64, C.c_void_p]),
-        "ewg_device_bicg_hs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
-                                         C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+                                               C.c_int64, C.c_void_p, C.c_void_p]),
+        "ewg_device_bicg_hs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                         C.c_int64, C.c_void_p, C.c_void_p]),
         "ewg_device_bicg_spmv_dot2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
-                                                C.c_int64, C.c_void_p]),
+                                                C.c_int64, C.c_void_p, C.c_void_p]),
         "ewg_device_bicg_xr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                         C.c_double, C.c_int64, C.c_int64, C.c_void_p]),
+                                         C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
+        "ewg_device_bicg_state_size": (C.c_int32, []),
+        "ewg_device_bicg_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, P(SolveOpts)]),
+        "ewg_device_bicg_state_read": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_int32), P(C.c_int32),
+                                                 P(C.c_int32), P(C.c_double), P(C.c_double)]),
         "ewg_transfer_counters": (C.c_int, [C.c_void_p, C.c_int32, P(C.c_uint64), P(C.c_uint64)]),
         "ewg_profile_num_kernels": (C.c_int32, []),
         "ewg_profile_kernel_name": (C.c_char_p, [C.c_int32]),
@@ -673,31 +676,50 @@ class Context:
         self._check(self.lib.ewg_device_precondition(self.h, C.byref(opts), bp, yp), "device_precondition")
 
     # fused kernels of one slab's BiCGStab iteration (dd.distributed_bicgstab); device tensors
-    # (N x 2 float64), owned rows [lo, hi) of each colour half, `out` a float64 device tensor
+    # (N x 2 float64), owned rows [lo, hi) of each colour half, `out` a float64 device tensor,
+    # `state` the device state (a uint8 tensor of ewg_device_bicg_state_size() bytes)
 
-    def device_bicg_p(self, p, r, r0, v, beta, omega, restart):
+    @staticmethod
+    def _ptr_of(t):
+        return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(None)
+
+    def device_bicg_p(self, p, r, r0, v, state):
         a = self._device_args(p, r, r0, v)
-        self._check(self.lib.ewg_device_bicg_p(self.h, *a, float(beta), float(omega), int(restart)), "device_bicg_p")
+        self._check(self.lib.ewg_device_bicg_p(self.h, *a, self._ptr_of(state)), "device_bicg_p")
 
-    def device_bicg_spmv_dot(self, x, y, w, lo, hi, out):
+    def device_bicg_spmv_dot(self, x, y, w, lo, hi, state, out):
         a = self._device_args(x, y, w)
-        self._check(self.lib.ewg_device_bicg_spmv_dot(self.h, *a, int(lo), int(hi), C.c_void_p(out.data_ptr())),
-                    "device_bicg_spmv_dot")
+        self._check(self.lib.ewg_device_bicg_spmv_dot(self.h, *a, int(lo), int(hi), self._ptr_of(state),
+                                                      self._ptr_of(out)), "device_bicg_spmv_dot")
 
-    def device_bicg_hs(self, x, y, r, v, rho_i, denom, lo, hi, out):
+    def device_bicg_hs(self, x, y, r, v, lo, hi, state, out):
         a = self._device_args(x, y, r, v)
-        self._check(self.lib.ewg_device_bicg_hs(self.h, *a, float(rho_i), C.c_void_p(denom.data_ptr()), int(lo),
-                                                int(hi), C.c_void_p(out.data_ptr())), "device_bicg_hs")
+        self._check(self.lib.ewg_device_bicg_hs(self.h, *a, int(lo), int(hi), self._ptr_of(state), self._ptr_of(out)),
+                    "device_bicg_hs")
 
-    def device_bicg_spmv_dot2(self, z, t, s, lo, hi, out):
+    def device_bicg_spmv_dot2(self, z, t, s, lo, hi, state, out):
         a = self._device_args(z, t, s)
-        self._check(self.lib.ewg_device_bicg_spmv_dot2(self.h, *a, int(lo), int(hi), C.c_void_p(out.data_ptr())),
-                    "device_bicg_spmv_dot2")
+        self._check(self.lib.ewg_device_bicg_spmv_dot2(self.h, *a, int(lo), int(hi), self._ptr_of(state),
+                                                       self._ptr_of(out)), "device_bicg_spmv_dot2")
 
-    def device_bicg_xr(self, x, z, r, t, r0, omega, lo, hi, out):
+    def device_bicg_xr(self, x, z, r, t, r0, lo, hi, state, out):
         a = self._device_args(x, z, r, t, r0)
-        self._check(self.lib.ewg_device_bicg_xr(self.h, *a, float(omega), int(lo), int(hi),
-                                                C.c_void_p(out.data_ptr())), "device_bicg_xr")
+        self._check(self.lib.ewg_device_bicg_xr(self.h, *a, int(lo), int(hi), self._ptr_of(state), self._ptr_of(out)),
+                    "device_bicg_xr")
+
+    def device_bicg_state(self, stage, state, red, opts=None):
+        o = C.byref(opts) if opts is not None else None
+        self._check(self.lib.ewg_device_bicg_state(self.h, int(stage), self._ptr_of(state), self._ptr_of(red), o),
+                    "device_bicg_state")
+
+    def device_bicg_state_read(self, state):
+        """(status, iterations, restarts, residual, initial residual) of a distributed solve's state."""
+        st, it, rs = C.c_int32(), C.c_int32(), C.c_int32()
+        res, ini = C.c_double(), C.c_double()
+        self._check(self.lib.ewg_device_bicg_state_read(self.h, self._ptr_of(state), C.byref(st), C.byref(it),
+                                                        C.byref(rs), C.byref(res), C.byref(ini)),
+                    "device_bicg_state_read")
+        return st.value, it.value, rs.value, res.value, ini.value
 
     def transfer_counters(self, reset=False):
         """(host->device, device->host) bytes of this context's entry points (ewg_transfer_counters)."""

@@ -306,26 +306,47 @@ ewg_status ewg_device_precondition(ewg_ctx* ctx, const ewg_solve_opts* opts, con
  * products over the locally owned rows, overlappingscalarproduct.hh:64-80). All vectors are device
  * vectors in this context's storage order (N x 2 doubles); each kernel updates all N rows and
  * reduces over the owned rows only -- rows [own_lo, own_hi) of each of the two colour halves --
- * deterministically into `out`, a device array the caller combines across slabs. Scalars are
- * host values except the denominator of alpha, which is read from device memory (the cross-slab
- * sum of <r0,v>), so no host read is needed between the kernels.
- *   bicg_p:         p = r + beta (p - omega v); restart != 0: r0 = r, v = p = 0 first
- *   bicg_spmv_dot:  y = J x; out[0] = sum_owned w . y
- *   bicg_hs:        alpha = rho_i / *denom; x += alpha y; r -= alpha v;
- *                   out = {max_owned |r|, max_owned |y|} (NaN counts as infinity)
- *   bicg_spmv_dot2: t = J z; out = {t . t, t . s} over owned rows
+ * deterministically into `out`, a device array the caller combines across slabs. The scalars
+ * (alpha, omega, beta, the restart flag) are read from `state`, a device BiCGStab state that
+ * ewg_device_bicg_state advances from the combined reductions, so no host read is needed between
+ * the kernels; once the state has left "running" every kernel returns at once.
+ *   bicg_p:         p = r + beta (p - omega v); on a restart r0 = r, v = p = 0 first
+ *   bicg_spmv_dot:  y = J x; out[0] = sum_owned w . y          (state may be NULL: no status test)
+ *   bicg_hs:        x += alpha y; r -= alpha v; out = {max_owned |r|, max_owned |y|}
+ *                   (NaN counts as infinity)
+ *   bicg_spmv_dot2: t = J z; out = {t . t, t . s} over owned rows (state may be NULL)
  *   bicg_xr:        x += omega z; out[2..3] = {max |r|, max |z|} with r before its update;
  *                   r -= omega t; out[0..1] = {r0 . r, r . r} over owned rows */
-ewg_status ewg_device_bicg_p(ewg_ctx* ctx, double* p, const double* r, double* r0, double* v, double beta,
-                             double omega, int32_t restart);
+ewg_status ewg_device_bicg_p(ewg_ctx* ctx, double* p, const double* r, double* r0, double* v, const void* state);
 ewg_status ewg_device_bicg_spmv_dot(ewg_ctx* ctx, const double* x, double* y, const double* w, int64_t own_lo,
-                                    int64_t own_hi, double* out);
-ewg_status ewg_device_bicg_hs(ewg_ctx* ctx, double* x, const double* y, double* r, const double* v, double rho_i,
-                              const double* denom, int64_t own_lo, int64_t own_hi, double* out);
+                                    int64_t own_hi, const void* state, double* out);
+ewg_status ewg_device_bicg_hs(ewg_ctx* ctx, double* x, const double* y, double* r, const double* v,
+                              int64_t own_lo, int64_t own_hi, const void* state, double* out);
 ewg_status ewg_device_bicg_spmv_dot2(ewg_ctx* ctx, const double* z, double* t, const double* s, int64_t own_lo,
-                                     int64_t own_hi, double* out);
+                                     int64_t own_hi, const void* state, double* out);
 ewg_status ewg_device_bicg_xr(ewg_ctx* ctx, double* x, const double* z, double* r, const double* t,
-                              const double* r0, double omega, int64_t own_lo, int64_t own_hi, double* out);
+                              const double* r0, int64_t own_lo, int64_t own_hi, const void* state, double* out);
+/* The device state of a distributed BiCGStab: ewg_device_bicg_state_size() bytes of device memory
+ * the caller owns (one per slab; every slab's copy takes the same steps on the same reductions).
+ * ewg_device_bicg_state runs one scalar step on the context's stream, on `red`, the reductions
+ * combined over all slabs (device doubles):
+ *   stage 0  red = {b.b, max|b|}: CombinedCriterion::setInitial and the top of the first iteration
+ *            (tolerances, maximum error and iterations, restart option from opts)
+ *   stage 1  red = {r0.v}: alpha = rho_i / r0.v, breakdown tests
+ *   stage 2  red = {t.t, t.s, max|s|, max|y|}: the half-step criterion on s (y all zero:
+ *            stagnation), omega = t.s / t.t, breakdown tests
+ *   stage 3  red = {r0.r, r.r, max|s|, max|z|}: the full-step criterion, the next iteration's top
+ *            (restart on breakdown, beta, rho, the iteration limit)
+ *   stage 4  red = {r.r, max|r|} of r = b - J x after convergence: resume from x when the true
+ *            residual misses the criterion by more than 10x (residual replacement)
+ * ewg_device_bicg_state_read copies status (ewg_status-like: 0 running, 1 converged, 2 failed,
+ * 3 breakdown, 4 iteration limit), iterations, restarts and the current and initial residual
+ * max-norms to the host (one small synchronous read). */
+int32_t ewg_device_bicg_state_size(void);
+ewg_status ewg_device_bicg_state(ewg_ctx* ctx, int32_t stage, void* state, const double* red,
+                                 const ewg_solve_opts* opts);
+ewg_status ewg_device_bicg_state_read(ewg_ctx* ctx, const void* state, int32_t* status, int32_t* iterations,
+                                      int32_t* restarts, double* residual, double* initial_residual);
 
 /* ---- Newton (NewtonMethod::apply, newtonmethod.hh:308-517) -------------------------- */
 
