@@ -11,6 +11,13 @@ int b8_grid(ewg_ctx* ctx, const void* kernel) {
     return (int)(need < g ? (need > 0 ? need : 1) : g);
 }
 
+// sweeps: one block per tile of 32 superblocks, at most the resident blocks of one wave
+int b8_sweep_grid(ewg_ctx* ctx, const void* kernel) {
+    int g = grid_size_for(ctx, kernel, kB8Block);
+    const int64_t need = (ctx->P.Nb + 31) / 32;
+    return (int)(need < g ? (need > 0 ? need : 1) : g);
+}
+
 template <typename T, int C>
 void factor_colour(ewg_ctx* ctx, const T* A8, T* Dinv8, T* L8, T* E8, int* bad) {
     auto kfn = k_b8_factor<T, C>;
@@ -21,14 +28,14 @@ template <typename T, int C>
 void forward_colour(ewg_ctx* ctx, const T* L8, const typename V2T<T>::type* d, typename V2T<T>::type* y,
                     const int* status) {
     auto kfn = k_b8_forward<T, T, C>;
-    EWG_LAUNCH(ctx, K_B8_FORWARD, kfn, b8_grid(ctx, (const void*)kfn), kSolBlock, ctx->P, L8, d, y, status);
+    EWG_LAUNCH(ctx, K_B8_FORWARD, kfn, b8_sweep_grid(ctx, (const void*)kfn), kB8Block, ctx->P, L8, d, y, status);
 }
 
 template <typename T, int C>
 void backward_colour(ewg_ctx* ctx, const T* A8, const T* Dinv8, const typename V2T<T>::type* w,
                      typename V2T<T>::type* y, const int* status, double relax) {
     auto kfn = k_b8_backward<T, T, C>;
-    EWG_LAUNCH(ctx, K_B8_BACKWARD, kfn, b8_grid(ctx, (const void*)kfn), kSolBlock, ctx->P, A8, Dinv8, w, y, status,
+    EWG_LAUNCH(ctx, K_B8_BACKWARD, kfn, b8_sweep_grid(ctx, (const void*)kfn), kB8Block, ctx->P, A8, Dinv8, w, y, status,
                relax);
 }
 

@@ -4,8 +4,8 @@
 // (i, j, k) -- colour = ((i >> 1) & 1) | ((j >> 1) & 1) << 1 | ((k >> 1) & 1) << 2 -- so two boxes
 // of one colour never share a face. The ILU order is colour-major; inside a box the cells follow
 // the natural order q = (i & 1) | (j & 1) << 1 | (k & 1) << 2 (x fastest). Boxes of one colour are
-// independent, so a colour's boxes are factorized and swept in parallel, each by one thread that
-// walks its eight cells in order. The factorization is dune-istl's bilu0_decomposition and the
+// independent, so a colour's boxes are factorized and swept in parallel: the factorization by one
+// thread per box that walks its eight cells in order, the sweeps by one warp per place. The factorization is dune-istl's bilu0_decomposition and the
 // sweeps its bilu_backsolve on the matrix permuted to this order (the oracle's ORC_ORDER_BOX8
 // runs exactly that on the CPU). On the 3D lens problem this order needs about a third fewer
 // BiCGStab iterations than the red-black order (64x64x32: 658 against 998 in the first step;
@@ -210,160 +210,258 @@ __global__ void __launch_bounds__(kSolBlock) k_b8_factor(const __grid_constant__
     }
 }
 
-// ---- forward sweep: w_c = d_c - sum_{k earlier} L_ck w_k ------------------------------------------
+// ---- sweeps: one warp per place, one lane per box ---------------------------------------------------
+//
+// A block of kB8Block threads takes 32 consecutive superblocks b0 .. b0 + 31 of one colour: warp q
+// holds place q of the 32 boxes, lane l the box of superblock b0 + l, so every load and store of a
+// warp touches 32 consecutive positions of one group. Inside a box the dependencies of the sweeps
+// form the 3-cube of the places (a place depends on the places that differ from it in one bit and
+// come earlier), so the eight places run in four levels -- forward by the number of set bits of q,
+// backward by the number of clear bits -- with the box's finished values passed through shared
+// memory and one block barrier between levels. Every load of a cell (its vector entry, the blocks
+// and the other colours' values) is issued before the levels; a level only adds the terms of the
+// same box.
+//
+// Summation order. In ascending ILU order the neighbours of a cell are: the boxes of earlier
+// colours, then the cells of the same box by place, then the boxes of later colours (the key
+// group = colour * 8 + place, B8FaceOrder). The forward sweep subtracts its terms in ascending
+// order and the backward sweep in descending order, so the terms of other boxes come first in
+// both and the terms of the same box last -- exactly the split into "before the levels" and "in a
+// level", which keeps each cell's sums in bilu_backsolve's column order.
 
-template <typename TM, typename TV, int C, int Q, int AXIS, int SIDE>
-__device__ __forceinline__ void b8_forward_face(const Phys& P, const TM* __restrict__ L,
-                                                const typename V2T<TV>::type* __restrict__ w, int64_t b,
-                                                const Box8Pos& bp, int64_t pos, const double (&wBox)[8][2],
-                                                double& r0, double& r1) {
+constexpr int kB8Block = 256;  // 8 places x 32 boxes
+
+// Inside a box each cell has one neighbour per axis (place bit flipped): an earlier one where the
+// place bit is set, a later one where it is clear. The blocks of these faces are indexed by axis.
+
+// forward, before the levels: the terms of earlier colours, and the blocks of the same box
+template <typename TM, typename TV, int C, int Q, int R>
+__device__ __forceinline__ void b8_fwd_far(const Phys& P, const TM* __restrict__ L,
+                                           const typename V2T<TV>::type* __restrict__ w, int64_t b, const Box8Pos& bp,
+                                           int64_t pos, double& r0, double& r1, double (&Lin)[3][4]) {
+    using O = B8FaceOrder<C, Q>;
+    constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
     if (!NB::earlier) return;
+    if (NB::inBox) {
+        load_block(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lin[AXIS]);
+        return;
+    }
     const int64_t n = b8_nbr_pos<C, Q, AXIS, SIDE>(P, b, bp);
     if (n < 0) return;
     double Lb[4];
     load_block(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lb);
-    double x0, x1;
-    if (NB::inBox) {
-        x0 = wBox[NB::nQ][0];
-        x1 = wBox[NB::nQ][1];
-    } else {
-        const auto wk = w[n];
-        x0 = (double)wk.x;
-        x1 = (double)wk.y;
-    }
+    const auto wk = w[n];
+    const double x0 = (double)wk.x, x1 = (double)wk.y;
     r0 -= Lb[0] * x0; r0 -= Lb[1] * x1;
     r1 -= Lb[2] * x0; r1 -= Lb[3] * x1;
 }
 
 template <typename TM, typename TV, int C, int Q>
-__device__ __forceinline__ void b8_forward_cell(const Phys& P, const TM* __restrict__ L,
-                                                const typename V2T<TV>::type* __restrict__ d,
-                                                typename V2T<TV>::type* __restrict__ w, int64_t b,
-                                                const Box8Pos& bp, double (&wBox)[8][2]) {
-    const int64_t pos = (int64_t)(C * 8 + Q) * P.Nb + b;
-    const auto ds = d[pos];
-    double r0 = (double)ds.x, r1 = (double)ds.y;
-    using O = B8FaceOrder<C, Q>;
-    b8_forward_face<TM, TV, C, Q, (O::dir(0) >> 1), (O::dir(0) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    b8_forward_face<TM, TV, C, Q, (O::dir(1) >> 1), (O::dir(1) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    b8_forward_face<TM, TV, C, Q, (O::dir(2) >> 1), (O::dir(2) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    b8_forward_face<TM, TV, C, Q, (O::dir(3) >> 1), (O::dir(3) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    b8_forward_face<TM, TV, C, Q, (O::dir(4) >> 1), (O::dir(4) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    b8_forward_face<TM, TV, C, Q, (O::dir(5) >> 1), (O::dir(5) & 1)>(P, L, w, b, bp, pos, wBox, r0, r1);
-    typename V2T<TV>::type o;
-    o.x = (TV)r0;
-    o.y = (TV)r1;
-    w[pos] = o;
-    // later cells of the box read the stored (rounded) value, as the reference's vector holds it
-    wBox[Q][0] = (double)o.x;
-    wBox[Q][1] = (double)o.y;
+__device__ __forceinline__ void b8_fwd_far_all(const Phys& P, const TM* __restrict__ L,
+                                               const typename V2T<TV>::type* __restrict__ w, int64_t b, int64_t pos,
+                                               double& r0, double& r1, double (&Lin)[3][4]) {
+    const Box8Pos bp = b8_box(P, (uint32_t)b);
+    b8_fwd_far<TM, TV, C, Q, 0>(P, L, w, b, bp, pos, r0, r1, Lin);
+    b8_fwd_far<TM, TV, C, Q, 1>(P, L, w, b, bp, pos, r0, r1, Lin);
+    b8_fwd_far<TM, TV, C, Q, 2>(P, L, w, b, bp, pos, r0, r1, Lin);
+    b8_fwd_far<TM, TV, C, Q, 3>(P, L, w, b, bp, pos, r0, r1, Lin);
+    b8_fwd_far<TM, TV, C, Q, 4>(P, L, w, b, bp, pos, r0, r1, Lin);
+    b8_fwd_far<TM, TV, C, Q, 5>(P, L, w, b, bp, pos, r0, r1, Lin);
 }
 
+// forward, in its level: the terms of the same box, ascending
+template <int C, int Q, int R>
+__device__ __forceinline__ void b8_fwd_near(const double2 (&S)[8][32], int lane, const double (&Lin)[3][4], double& r0,
+                                            double& r1) {
+    using O = B8FaceOrder<C, Q>;
+    constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
+    using NB = B8Nbr<C, Q, AXIS, SIDE>;
+    if (!NB::earlier || !NB::inBox) return;
+    const double2 v = S[NB::nQ][lane];
+    r0 -= Lin[AXIS][0] * v.x; r0 -= Lin[AXIS][1] * v.y;
+    r1 -= Lin[AXIS][2] * v.x; r1 -= Lin[AXIS][3] * v.y;
+}
+
+template <int C, int Q>
+__device__ __forceinline__ void b8_fwd_near_all(const double2 (&S)[8][32], int lane, const double (&Lin)[3][4],
+                                                double& r0, double& r1) {
+    b8_fwd_near<C, Q, 0>(S, lane, Lin, r0, r1);
+    b8_fwd_near<C, Q, 1>(S, lane, Lin, r0, r1);
+    b8_fwd_near<C, Q, 2>(S, lane, Lin, r0, r1);
+    b8_fwd_near<C, Q, 3>(S, lane, Lin, r0, r1);
+    b8_fwd_near<C, Q, 4>(S, lane, Lin, r0, r1);
+    b8_fwd_near<C, Q, 5>(S, lane, Lin, r0, r1);
+}
+
+#define EWG_B8_PLACE_SWITCH(q, CALL) \
+    switch (q) {                     \
+    case 0: CALL(0); break;          \
+    case 1: CALL(1); break;          \
+    case 2: CALL(2); break;          \
+    case 3: CALL(3); break;          \
+    case 4: CALL(4); break;          \
+    case 5: CALL(5); break;          \
+    case 6: CALL(6); break;          \
+    default: CALL(7); break;         \
+    }
+
+// forward sweep of colour C: w_c = d_c - sum_{k earlier} L_ck w_k
 template <typename TM, typename TV, int C>
-__global__ void __launch_bounds__(kSolBlock, EWG_B8_SWEEP_BLOCKS) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
+__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
                                                            const typename V2T<TV>::type* __restrict__ d,
                                                            typename V2T<TV>::type* __restrict__ w,
                                                            const int* __restrict__ status) {
-    if (status && *status != ST_RUNNING) return;
-    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < P.Nb; b += (int64_t)gridDim.x * blockDim.x) {
-        const Box8Pos bp = b8_box(P, (uint32_t)b);
-        double wBox[8][2];
-        b8_forward_cell<TM, TV, C, 0>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 1>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 2>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 3>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 4>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 5>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 6>(P, L, d, w, b, bp, wBox);
-        b8_forward_cell<TM, TV, C, 7>(P, L, d, w, b, bp, wBox);
+    if (status && *status != ST_RUNNING) return;  // uniform over the grid
+    __shared__ double2 S[8][32];
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    const int level = __popc(q);
+    const int64_t nTiles = (P.Nb + 31) >> 5;
+    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+        const int64_t b = tile * 32 + lane;
+        const bool valid = b < P.Nb;
+        const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+        double r0 = 0.0, r1 = 0.0, Lin[3][4];
+        if (valid) {
+            const auto ds = d[pos];
+            r0 = (double)ds.x;
+            r1 = (double)ds.y;
+#define EWG_B8_CALL(Q) b8_fwd_far_all<TM, TV, C, Q>(P, L, w, b, pos, r0, r1, Lin)
+            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+        }
+#pragma unroll
+        for (int lev = 0; lev < 4; ++lev) {
+            if (lev > 0) __syncthreads();
+            if (lev == level) {
+#define EWG_B8_CALL(Q) b8_fwd_near_all<C, Q>(S, lane, Lin, r0, r1)
+                EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+                typename V2T<TV>::type o;
+                o.x = (TV)r0;
+                o.y = (TV)r1;
+                if (valid) w[pos] = o;
+                // later places read the stored (rounded) value, as the reference's vector holds it
+                S[q][lane] = make_double2((double)o.x, (double)o.y);
+            }
+        }
+        __syncthreads();  // S is reused by the next tile
     }
 }
 
-// ---- backward sweep: y_c = inv(D'_c) (w_c - sum_{k later} A_ck y_k), output relax * y ---------------
-// w stays in its own vector (the preconditioned SpMV reads it again). The stored outputs of later
-// colours are relax * y; the coupling term works on unscaled y, as the reference's backward solve
-// runs before its final scaling.
-
-template <typename TM, typename TV, int C, int Q, int AXIS, int SIDE>
-__device__ __forceinline__ void b8_backward_face(const Phys& P, const TM* __restrict__ A,
-                                                 const typename V2T<TV>::type* __restrict__ y, int64_t b,
-                                                 const Box8Pos& bp, int64_t pos, const double (&yBox)[8][2],
-                                                 double winv, double& r0, double& r1) {
+// backward, before the levels: the terms of later colours, and the blocks of the same box
+template <typename TM, typename TV, int C, int Q, int R>
+__device__ __forceinline__ void b8_bwd_far(const Phys& P, const TM* __restrict__ A,
+                                           const typename V2T<TV>::type* __restrict__ y, int64_t b, const Box8Pos& bp,
+                                           int64_t pos, double winv, double& r0, double& r1, double (&Ain)[3][4]) {
+    using O = B8FaceOrder<C, Q>;
+    constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
     if (NB::earlier) return;
+    if (NB::inBox) {
+        load_block(A, P.N, band_of(AXIS, SIDE), pos, Ain[AXIS]);
+        return;
+    }
     const int64_t n = b8_nbr_pos<C, Q, AXIS, SIDE>(P, b, bp);
     if (n < 0) return;
     double Ab[4];
     load_block(A, P.N, band_of(AXIS, SIDE), pos, Ab);
-    double x0, x1;
-    if (NB::inBox) {
-        x0 = yBox[NB::nQ][0];
-        x1 = yBox[NB::nQ][1];
-    } else {
-        const auto yk = y[n];
-        x0 = (double)yk.x;
-        x1 = (double)yk.y;
-        if (winv != 1.0) { x0 *= winv; x1 *= winv; }
-    }
+    const auto yk = y[n];
+    double x0 = (double)yk.x, x1 = (double)yk.y;
+    if (winv != 1.0) { x0 *= winv; x1 *= winv; }
     r0 -= Ab[0] * x0; r0 -= Ab[1] * x1;
     r1 -= Ab[2] * x0; r1 -= Ab[3] * x1;
 }
 
+// descending columns, as bilu_backsolve's backward loop
 template <typename TM, typename TV, int C, int Q>
-__device__ __forceinline__ void b8_backward_cell(const Phys& P, const TM* __restrict__ A, const TM* __restrict__ Dinv,
-                                                 const typename V2T<TV>::type* __restrict__ wv,
-                                                 typename V2T<TV>::type* __restrict__ y, int64_t b,
-                                                 const Box8Pos& bp, double w, double winv, double (&yBox)[8][2]) {
-    const int64_t pos = (int64_t)(C * 8 + Q) * P.Nb + b;
-    const auto ws = wv[pos];
-    double r0 = (double)ws.x, r1 = (double)ws.y;
-    // descending columns, as bilu_backsolve's backward loop
-    using O = B8FaceOrder<C, Q>;
-    b8_backward_face<TM, TV, C, Q, (O::dir(5) >> 1), (O::dir(5) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    b8_backward_face<TM, TV, C, Q, (O::dir(4) >> 1), (O::dir(4) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    b8_backward_face<TM, TV, C, Q, (O::dir(3) >> 1), (O::dir(3) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    b8_backward_face<TM, TV, C, Q, (O::dir(2) >> 1), (O::dir(2) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    b8_backward_face<TM, TV, C, Q, (O::dir(1) >> 1), (O::dir(1) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    b8_backward_face<TM, TV, C, Q, (O::dir(0) >> 1), (O::dir(0) & 1)>(P, A, y, b, bp, pos, yBox, winv, r0, r1);
-    double Di[4];
-    load_block(Dinv, P.N, 0, pos, Di);
-    const double u0 = Di[0] * r0 + Di[1] * r1, u1 = Di[2] * r0 + Di[3] * r1;
-    typename V2T<TV>::type o;
-    o.x = (TV)(w * u0);
-    o.y = (TV)(w * u1);
-    y[pos] = o;
-    // the unscaled value as a later-colour reader recovers it from the stored one
-    if (w == 1.0) {
-        yBox[Q][0] = (double)o.x;
-        yBox[Q][1] = (double)o.y;
-    } else {
-        yBox[Q][0] = (double)o.x * winv;
-        yBox[Q][1] = (double)o.y * winv;
-    }
+__device__ __forceinline__ void b8_bwd_far_all(const Phys& P, const TM* __restrict__ A,
+                                               const typename V2T<TV>::type* __restrict__ y, int64_t b, int64_t pos,
+                                               double winv, double& r0, double& r1, double (&Ain)[3][4]) {
+    const Box8Pos bp = b8_box(P, (uint32_t)b);
+    b8_bwd_far<TM, TV, C, Q, 5>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
+    b8_bwd_far<TM, TV, C, Q, 4>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
+    b8_bwd_far<TM, TV, C, Q, 3>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
+    b8_bwd_far<TM, TV, C, Q, 2>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
+    b8_bwd_far<TM, TV, C, Q, 1>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
+    b8_bwd_far<TM, TV, C, Q, 0>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
 }
 
+template <int C, int Q, int R>
+__device__ __forceinline__ void b8_bwd_near(const double2 (&S)[8][32], int lane, const double (&Ain)[3][4], double& r0,
+                                            double& r1) {
+    using O = B8FaceOrder<C, Q>;
+    constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
+    using NB = B8Nbr<C, Q, AXIS, SIDE>;
+    if (NB::earlier || !NB::inBox) return;
+    const double2 v = S[NB::nQ][lane];
+    r0 -= Ain[AXIS][0] * v.x; r0 -= Ain[AXIS][1] * v.y;
+    r1 -= Ain[AXIS][2] * v.x; r1 -= Ain[AXIS][3] * v.y;
+}
+
+template <int C, int Q>
+__device__ __forceinline__ void b8_bwd_near_all(const double2 (&S)[8][32], int lane, const double (&Ain)[3][4],
+                                                double& r0, double& r1) {
+    b8_bwd_near<C, Q, 5>(S, lane, Ain, r0, r1);
+    b8_bwd_near<C, Q, 4>(S, lane, Ain, r0, r1);
+    b8_bwd_near<C, Q, 3>(S, lane, Ain, r0, r1);
+    b8_bwd_near<C, Q, 2>(S, lane, Ain, r0, r1);
+    b8_bwd_near<C, Q, 1>(S, lane, Ain, r0, r1);
+    b8_bwd_near<C, Q, 0>(S, lane, Ain, r0, r1);
+}
+
+// backward sweep of colour C: y_c = inv(D'_c) (w_c - sum_{k later} A_ck y_k), output relax * y.
+// w stays in its own vector (the preconditioned SpMV reads it again). The stored outputs of later
+// colours are relax * y; the coupling term works on unscaled y, as the reference's backward solve
+// runs before its final scaling.
 template <typename TM, typename TV, int C>
-__global__ void __launch_bounds__(kSolBlock, EWG_B8_SWEEP_BLOCKS) k_b8_backward(const __grid_constant__ Phys P, const TM* __restrict__ A,
+__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                             const TM* __restrict__ Dinv,
                                                             const typename V2T<TV>::type* __restrict__ wv,
                                                             typename V2T<TV>::type* __restrict__ y,
                                                             const int* __restrict__ status, double w) {
-    if (status && *status != ST_RUNNING) return;
+    if (status && *status != ST_RUNNING) return;  // uniform over the grid
+    __shared__ double2 S[8][32];
     const double winv = 1.0 / w;
-    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < P.Nb; b += (int64_t)gridDim.x * blockDim.x) {
-        const Box8Pos bp = b8_box(P, (uint32_t)b);
-        double yBox[8][2];
-        b8_backward_cell<TM, TV, C, 7>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 6>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 5>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 4>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 3>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 2>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 1>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
-        b8_backward_cell<TM, TV, C, 0>(P, A, Dinv, wv, y, b, bp, w, winv, yBox);
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    const int level = 3 - __popc(q);
+    const int64_t nTiles = (P.Nb + 31) >> 5;
+    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+        const int64_t b = tile * 32 + lane;
+        const bool valid = b < P.Nb;
+        const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+        double r0 = 0.0, r1 = 0.0, Ain[3][4], Di[4] = {0.0, 0.0, 0.0, 0.0};
+        if (valid) {
+            const auto ws = wv[pos];
+            r0 = (double)ws.x;
+            r1 = (double)ws.y;
+#define EWG_B8_CALL(Q) b8_bwd_far_all<TM, TV, C, Q>(P, A, y, b, pos, winv, r0, r1, Ain)
+            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+            load_block(Dinv, P.N, 0, pos, Di);
+        }
+#pragma unroll
+        for (int lev = 0; lev < 4; ++lev) {
+            if (lev > 0) __syncthreads();
+            if (lev == level) {
+#define EWG_B8_CALL(Q) b8_bwd_near_all<C, Q>(S, lane, Ain, r0, r1)
+                EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+                const double u0 = Di[0] * r0 + Di[1] * r1, u1 = Di[2] * r0 + Di[3] * r1;
+                typename V2T<TV>::type o;
+                o.x = (TV)(w * u0);
+                o.y = (TV)(w * u1);
+                if (valid) y[pos] = o;
+                // the unscaled value as a later-colour reader recovers it from the stored one
+                if (w == 1.0) S[q][lane] = make_double2((double)o.x, (double)o.y);
+                else S[q][lane] = make_double2((double)o.x * winv, (double)o.y * winv);
+            }
+        }
+        __syncthreads();  // S is reused by the next tile
     }
 }
+
+#undef EWG_B8_PLACE_SWITCH
 
 // ---- SpMV row in box-8 order ---------------------------------------------------------------------
 //
