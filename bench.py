@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-scheduler", default="device", choices=["device", "host"],
+                    help="device: Newton / step decisions on the device, supersteps in a CUDA graph WHILE node")
     ap.add_argument("--no-vcfv", action="store_true")
     return ap.parse_args()
 
@@ -508,7 +510,8 @@ def run_ensemble(args, rank, pg, torch, ewg):
     shapes = ens.autotune(dts, so)
     tune_s = time.perf_counter() - t0
     ens.apply_initial_solution()
-    ens.advance(1, dts, sopts=so)  # warm-up step
+    dev = args.ensemble_scheduler == "device"
+    ens.advance(1, dts, sopts=so, device=dev)  # warm-up step
     stream = torch.cuda.ExternalStream(ens.stream)
     torch.cuda.synchronize()
     barrier(pg)
@@ -516,7 +519,7 @@ def run_ensemble(args, rank, pg, torch, ewg):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     # every member advances ensemble_steps steps at its own pace
-    st, reps, sts = ens.advance(args.ensemble_steps, dts, sopts=so)
+    st, reps, sts = ens.advance(args.ensemble_steps, dts, sopts=so, device=dev)
     e1.record(stream)
     torch.cuda.synchronize()
     stats = [(reps, sts)]
@@ -537,13 +540,17 @@ def run_ensemble(args, rank, pg, torch, ewg):
         "newton_iterations_per_step_mean": float(np.mean(newton)),
         "newton_iterations_per_step_max": float(np.max(newton)),
         "halvings": int(sum(r.halvings for reps, _ in stats for r in reps)),
+        "scheduler": ("device: every decision on the device, supersteps inside a CUDA graph WHILE node"
+                      if dev else "host: decisions on the host between supersteps"),
         "rounds": [s.rounds for _, s in stats], "linear_iterations": [s.linear_iterations for _, s in stats],
-        # BiCGStab work actually done: cells x iterations summed over members, and the HBM rate it
-        # implies at the FP32 per-iteration bytes of the single-problem kernels (s = 4)
+        "supersteps": [s.supersteps for _, s in stats],
+        # BiCGStab work actually done: cells x iterations summed over members, per second of BiCGStab
+        # time (host scheduler) or of the whole advance (device scheduler: phases not timed apart)
         "bicgstab_cell_iterations_per_s": sum(s.cell_iterations for _, s in stats) / sum(s.t_solve for _, s in stats),
-        "phase_s": {"linearize": sum(s.t_linearize for _, s in stats) / len(stats),
-                    "solve": sum(s.t_solve for _, s in stats) / len(stats),
-                    "update": sum(s.t_update for _, s in stats) / len(stats)},
+        "phase_s": ({"advance": sum(s.t_solve for _, s in stats) / len(stats)} if dev else
+                    {"linearize": sum(s.t_linearize for _, s in stats) / len(stats),
+                     "solve": sum(s.t_solve for _, s in stats) / len(stats),
+                     "update": sum(s.t_update for _, s in stats) / len(stats)}),
         "launch_shapes": shapes, "autotune_s": tune_s,
     }
     ens.close()

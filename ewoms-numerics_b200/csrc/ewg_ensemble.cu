@@ -657,6 +657,29 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_xr(ENS_ARGS, typen
     }
 }
 
+// state of the device scheduler (ewg_ensemble_advance_device)
+struct RunD {  // MemberRun on the device
+    int phase, numIt;
+    double error, lastError, dt0, h;
+    int stepsLeft, halvingsStep, lastStatus, newton, linear, halvings;
+    int fail, accept;  // the member's failed / accepted entry, cleared by the next settle
+};
+
+struct SchedD {
+    long long supersteps;  // supersteps run so far
+    long long limit;       // the WHILE loop stops after this many (set by the host per launch)
+    int active;            // a member is linearizing or solving
+    int error;             // EWG_ERR_TIMEOUT: a member's BiCGStab never left running
+    int rounds;            // supersteps that linearized a member
+    int linearIterations;
+    double cellIterations;  // sums of integers below 2^53: exact in any order
+};
+
+struct NewtonD {
+    double tol, maxError;
+    int maxIt;
+};
+
 }  // namespace ewg
 
 // ---- host side ----------------------------------------------------------------------------------
@@ -723,6 +746,14 @@ struct ewg_ensemble {
     // BiCGStab chunk graph
     cudaGraphExec_t graphExec = nullptr;
     double relaxation = 1.0;
+    // device scheduler of ewg_ensemble_advance_device (allocated on its first call)
+    ewg::RunD* dRun = nullptr;
+    ewg::SchedD* dSched = nullptr;
+    int* dPrefix = nullptr;
+    int2* dTilesAll = nullptr;
+    int *maskF = nullptr, *maskA = nullptr, *maskS = nullptr;
+    ewg::RunD* hRun = nullptr;
+    ewg::SchedD* hSched = nullptr;
 };
 
 namespace {
@@ -1107,6 +1138,7 @@ ewg_status ensemble_advance(ewg_ensemble* e, int steps, const double* dt, const 
     };
     const int maxSupersteps = 10000000;
     for (int ss = 0; ss < maxSupersteps; ++ss) {
+        S.supersteps += 1;
         // ---- (1) linearization and the Newton decisions that follow it
         std::vector<int> lin;
         for (int m = 0; m < M; ++m)
@@ -1233,6 +1265,400 @@ ewg_status ensemble_advance(ewg_ensemble* e, int steps, const double* dt, const 
     return EWG_OK;
 }
 
+// ---- Newton decisions on the device ---------------------------------------------------------------
+//
+// ensemble_advance_device runs the supersteps of ensemble_advance with every per-member decision
+// taken on the device by single-block scheduling kernels (kd_*), and captures one whole superstep as
+// the body of a CUDA graph WHILE node: one graph launch runs supersteps until no member is active,
+// without returning to the host. The work kernels, their order and the member set of every launch
+// are those of ensemble_advance (the tile lists are compacted on the device in member order, as
+// set_tiles does on the host), so both advance the members to the same bits.
+
+__device__ __forceinline__ bool d_converged(const RunD& n, const NewtonD& no) { return n.error <= no.tol; }
+// NewtonMethod::proceed_ (newtonmethod.hh:620-636), as ensemble_advance's proceed
+__device__ __forceinline__ bool d_proceed(const RunD& n, const NewtonD& no) {
+    if (n.numIt < 1) return true;
+    if (d_converged(n, no)) return false;
+    if (n.numIt >= no.maxIt) return n.error * 4.0 < n.lastError;
+    return true;
+}
+__device__ __forceinline__ void d_fail(RunD& n, int status) {
+    n.lastStatus = status;
+    n.fail = 1;
+}
+
+// tile list of the members with sel[m] != 0, in member order (set_tiles); one block
+__global__ void kd_tiles(const EnsMember* __restrict__ mem, const int2* __restrict__ allTiles, int M,
+                         const int* __restrict__ sel, int* __restrict__ prefix, int2* __restrict__ out,
+                         int* __restrict__ outN) {
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int m = 0; m < M; ++m) {
+            prefix[m] = n;
+            if (sel[m]) n += mem[m].ntiles;
+        }
+        *outN = n;
+    }
+    __syncthreads();
+    for (int m = 0; m < M; ++m) {
+        if (!sel[m]) continue;
+        const int t0 = mem[m].tile0, nt = mem[m].ntiles, o = prefix[m];
+        for (int k = threadIdx.x; k < nt; k += blockDim.x) out[o + k] = allTiles[t0 + k];
+    }
+}
+
+// (1) the members that linearize: mask, their step sizes, cleared error maxima and flags
+__global__ void kd_lin_begin(RunD* __restrict__ run, int M, int* __restrict__ mask, double* __restrict__ dtArr,
+                             unsigned long long* __restrict__ errmax, int* __restrict__ flags, SchedD* __restrict__ sch) {
+    int any = 0;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        RunD& n = run[m];
+        const int sel = n.phase == PH_LIN;
+        if (sel) {
+            n.lastError = n.error;
+            dtArr[m] = n.h;
+        }
+        mask[m] = sel;
+        errmax[m] = 0ull;
+        flags[m] = 0;
+        any |= sel;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0 && any) sch->rounds += 1;
+}
+
+// (1) Newton decisions after the linearization; mask becomes the members that need a correction
+__global__ void kd_lin_decide(RunD* __restrict__ run, int M, int* __restrict__ mask,
+                              const unsigned long long* __restrict__ errmax, const int* __restrict__ flags,
+                              int* __restrict__ flagsF, NewtonD no) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        flagsF[m] = 0;
+        if (!mask[m]) continue;
+        RunD& n = run[m];
+        int solve = 0;
+        if (flags[m] & 1) {
+            d_fail(n, EWG_ERR_NONFINITE);
+        } else {
+            n.lastError = n.error;
+            n.error = __longlong_as_double((long long)errmax[m]);
+            if (n.error > no.maxError) {
+                d_fail(n, EWG_ERR_MAX_ERROR);
+            } else if (!d_proceed(n, no)) {
+                ++n.numIt;
+                if (d_converged(n, no)) n.accept = 1;
+                else d_fail(n, EWG_ERR_NOT_CONVERGED);
+            } else {
+                solve = 1;
+            }
+        }
+        mask[m] = solve;
+    }
+}
+
+// (2) after the preconditioner setup: a singular diagonal block fails the member, the others solve
+__global__ void kd_factor_decide(RunD* __restrict__ run, int M, int* __restrict__ mask, const int* __restrict__ flagsF) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        if (!mask[m]) continue;
+        if (flagsF[m] & 4) {
+            d_fail(run[m], EWG_ERR_BREAKDOWN);
+            mask[m] = 0;
+        } else {
+            run[m].phase = PH_SOLVE;
+        }
+    }
+}
+
+// settle, part 1: the failed and the accepted members as masks (their levels are reset / advanced)
+__global__ void kd_settle_masks(const RunD* __restrict__ run, int M, int* __restrict__ maskF, int* __restrict__ maskA) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        maskF[m] = run[m].fail;
+        maskA[m] = run[m].accept;
+    }
+}
+
+// settle, part 2: retry with half the step, or the next step (ensemble_advance's settle)
+__global__ void kd_settle(RunD* __restrict__ run, int M, int maxDiv) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        RunD& n = run[m];
+        if (n.fail) {
+            n.fail = 0;
+            n.halvingsStep += 1;
+            if (n.halvingsStep >= maxDiv) {
+                n.phase = PH_FAILED;
+            } else {
+                n.h *= 0.5;
+                n.numIt = 0;
+                n.error = n.lastError = 1e100;
+                n.phase = PH_LIN;
+            }
+        }
+        if (n.accept) {
+            n.accept = 0;
+            n.newton += n.numIt;
+            n.halvings += n.halvingsStep;
+            n.lastStatus = EWG_OK;
+            if (--n.stepsLeft == 0) {
+                n.phase = PH_DONE;
+            } else {
+                n.h = n.dt0;
+                n.halvingsStep = 0;
+                n.numIt = 0;
+                n.error = n.lastError = 1e100;
+                n.phase = PH_LIN;
+            }
+        }
+    }
+}
+
+// (3) the members whose BiCGStab runs this superstep
+__global__ void kd_solve_select(const RunD* __restrict__ run, int M, int* __restrict__ maskS) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) maskS[m] = run[m].phase == PH_SOLVE;
+}
+
+// (4) after the BiCGStab iterations: members whose solve ended take the Newton update (mask) or fail
+__global__ void kd_solve_decide(RunD* __restrict__ run, int M, const int* __restrict__ maskS,
+                                const BiState* __restrict__ st, const EnsMember* __restrict__ mem, int* __restrict__ mask,
+                                int* __restrict__ flagsU, int maxIter, SchedD* __restrict__ sch) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        flagsU[m] = 0;
+        int upd = 0;
+        if (maskS[m]) {
+            const BiState& b = st[m];
+            if (b.status == ST_RUNNING) {
+                if (b.iter > maxIter + 8) atomicExch(&sch->error, (int)EWG_ERR_TIMEOUT);
+            } else {
+                RunD& n = run[m];
+                n.linear += b.iter;
+                atomicAdd(&sch->linearIterations, b.iter);
+                atomicAdd(&sch->cellIterations, (double)mem[m].P.N * b.iter);
+                if (b.status == ST_CONVERGED) upd = 1;
+                else d_fail(n, b.status == ST_BREAKDOWN ? EWG_ERR_BREAKDOWN : EWG_ERR_NOT_CONVERGED);
+                n.phase = PH_LIN;  // provisional; settle or the update decision decides
+            }
+        }
+        mask[m] = upd;
+    }
+}
+
+// (4) after the Newton update: the loop-top test of NewtonMethod::apply (while (proceed_()))
+__global__ void kd_update_decide(RunD* __restrict__ run, int M, const int* __restrict__ mask,
+                                 const int* __restrict__ flagsU, NewtonD no) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        if (!mask[m]) continue;
+        RunD& n = run[m];
+        if (flagsU[m] & 2) {
+            d_fail(n, EWG_ERR_NONFINITE);
+            continue;
+        }
+        ++n.numIt;
+        if (!d_proceed(n, no)) {
+            if (d_converged(n, no)) n.accept = 1;
+            else d_fail(n, EWG_ERR_NOT_CONVERGED);
+        }
+    }
+}
+
+// end of a superstep: another one while a member is active, no member timed out and the launch's
+// superstep bound is not reached
+__global__ void kd_superstep_end(const RunD* __restrict__ run, int M, SchedD* __restrict__ sch,
+                                 cudaGraphConditionalHandle loop) {
+    int act = 0;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) act |= run[m].phase == PH_LIN || run[m].phase == PH_SOLVE;
+    act = __syncthreads_or(act);
+    if (threadIdx.x == 0) {
+        sch->active = act;
+        sch->supersteps += 1;
+        const bool more = act && sch->error == 0 && sch->supersteps < sch->limit;
+        cudaGraphSetConditional(loop, more ? 1u : 0u);
+    }
+}
+
+// supersteps per graph launch: the host reads the scheduler state between launches
+constexpr long long kSuperstepsPerLaunch = 4096;
+
+ewg_status ensure_sched(ewg_ensemble* e) {
+    if (e->dRun) return EWG_OK;
+    const int M = e->M;
+    cudaError_t c = cudaMalloc(&e->dRun, sizeof(RunD) * M);
+    if (c == cudaSuccess) c = cudaMalloc(&e->dSched, sizeof(SchedD));
+    if (c == cudaSuccess) c = cudaMalloc(&e->dPrefix, sizeof(int) * M);
+    if (c == cudaSuccess) c = cudaMalloc(&e->maskF, sizeof(int) * M);
+    if (c == cudaSuccess) c = cudaMalloc(&e->maskA, sizeof(int) * M);
+    if (c == cudaSuccess) c = cudaMalloc(&e->maskS, sizeof(int) * M);
+    if (c == cudaSuccess) c = cudaMalloc(&e->dTilesAll, sizeof(int2) * std::max(1, e->nTiles));
+    if (c == cudaSuccess) c = cudaMallocHost(&e->hRun, sizeof(RunD) * M);
+    if (c == cudaSuccess) c = cudaMallocHost(&e->hSched, sizeof(SchedD));
+    if (c == cudaSuccess && e->nTiles > 0)
+        c = cudaMemcpyAsync(e->dTilesAll, e->hTiles.data(), sizeof(int2) * e->nTiles, cudaMemcpyHostToDevice, e->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
+    return ens_fail(e, c, "allocate device scheduler");
+}
+
+void kd_tile_list(ewg_ensemble* e, const int* sel, ewg_ensemble::TileList& tl) {
+    kd_tiles<<<1, 256, 0, e->stream>>>(e->dm, e->dTilesAll, e->M, sel, e->dPrefix, tl.d, tl.dn);
+}
+
+// settle on the device: levels of the failed (x0 = x1) and accepted (x1 = x0) members, then their
+// next attempt or step
+void kd_settle_all(ewg_ensemble* e) {
+    cudaStream_t s = e->stream;
+    kd_settle_masks<<<1, 256, 0, s>>>(e->dRun, e->M, e->maskF, e->maskA);
+    kd_tile_list(e, e->maskF, e->tlA);
+    ke_levels<<<e->grid[EC_CELL], kEnsTile, 0, s>>>(e->dm, e->tlA.d, e->tlA.dn, e->maskF, 2, e->x0, e->x1, e->sold);
+    kd_tile_list(e, e->maskA, e->tlA);
+    ke_levels<<<e->grid[EC_CELL], kEnsTile, 0, s>>>(e->dm, e->tlA.d, e->tlA.dn, e->maskA, 1, e->x0, e->x1, e->sold);
+    kd_settle<<<1, 256, 0, s>>>(e->dRun, e->M, e->maxDiv);
+}
+
+// one superstep of ensemble_advance, every launch on the ensemble stream (captured into the body)
+template <typename T>
+void superstep_device(ewg_ensemble* e, const NewtonD& nd, const ewg_solve_opts* so, cudaGraphConditionalHandle loop) {
+    cudaStream_t s = e->stream;
+    const int M = e->M;
+    // (1) linearization and the Newton decisions that follow it
+    kd_lin_begin<<<1, 256, 0, s>>>(e->dRun, M, e->mask, e->dtArr, e->errmax, e->flags, e->dSched);
+    kd_tile_list(e, e->mask, e->tlA);
+    Ops<T>::intensive(e);
+    Ops<T>::assemble(e, true);
+    kd_lin_decide<<<1, 256, 0, s>>>(e->dRun, M, e->mask, e->errmax, e->flags, e->flagsF, nd);
+    // (2) preconditioner setup and BiCGStab start of the members that need a correction
+    kd_tile_list(e, e->mask, e->tlA);
+    Ops<T>::factor(e);
+    kd_factor_decide<<<1, 256, 0, s>>>(e->dRun, M, e->mask, e->flagsF);
+    kd_tile_list(e, e->mask, e->tlA);
+    ke_bicg_arm<<<(M + 127) / 128, 128, 0, s>>>(e->mask, M, bicg_template(so), e->st);
+    Ops<T>::rhs_init(e);
+    kd_settle_all(e);
+    // (3) every running BiCGStab advances by check_interval iterations
+    kd_solve_select<<<1, 256, 0, s>>>(e->dRun, M, e->maskS);
+    kd_tile_list(e, e->maskS, e->tlB);
+    for (int k = 0; k < e->checkInterval; ++k) Ops<T>::iteration(e);
+    // (4) Newton update of the members whose solve ended
+    kd_solve_decide<<<1, 256, 0, s>>>(e->dRun, M, e->maskS, e->st, e->dm, e->mask, e->flagsU,
+                                      so->linear_solver_max_iterations, e->dSched);
+    kd_tile_list(e, e->mask, e->tlA);
+    Ops<T>::update(e);
+    kd_update_decide<<<1, 256, 0, s>>>(e->dRun, M, e->mask, e->flagsU, nd);
+    kd_settle_all(e);
+    kd_superstep_end<<<1, 256, 0, s>>>(e->dRun, M, e->dSched, loop);
+}
+
+// graph: one WHILE node whose body is a superstep
+template <typename T>
+ewg_status build_device_advance(ewg_ensemble* e, const NewtonD& nd, const ewg_solve_opts* so, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    cudaError_t c = cudaGraphCreate(&g, 0);
+    if (c != cudaSuccess) return ens_fail(e, c, "create graph");
+    cudaGraphConditionalHandle loop = 0;
+    c = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (c == cudaSuccess) c = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    if (c == cudaSuccess)
+        c = cudaStreamBeginCaptureToGraph(e->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+    if (c == cudaSuccess) {
+        superstep_device<T>(e, nd, so, loop);
+        cudaGraph_t body = nullptr;
+        const cudaError_t launch = cudaGetLastError();
+        c = cudaStreamEndCapture(e->stream, &body);
+        if (c == cudaSuccess) c = launch;
+    }
+    if (c == cudaSuccess) c = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    return ens_fail(e, c, "device advance graph");
+}
+
+// ensemble_advance with the decisions on the device: the host starts the graph, reads the
+// scheduler state between launches (every kSuperstepsPerLaunch supersteps) and the members' runs at
+// the end. Stats: t_solve is the device time of the whole advance (phases are not timed apart).
+template <typename T>
+ewg_status ensemble_advance_device(ewg_ensemble* e, int steps, const double* dt, const ewg_newton_opts* no,
+                                   const ewg_solve_opts* so, ewg_ensemble_report* rep, ewg_ensemble_stats* stats) {
+    const int M = e->M;
+    for (int m = 0; m < M; ++m)
+        if (!(dt[m] > 0)) { e->err = "dt must be positive"; return EWG_ERR_INVALID; }
+    ewg_status s = ensure_sched(e);
+    if (s) return s;
+    cudaError_t c;
+    for (int m = 0; m < M; ++m) {
+        RunD& n = e->hRun[m];
+        memset(&n, 0, sizeof(n));
+        n.phase = PH_LIN;
+        n.error = n.lastError = 1e100;
+        n.dt0 = n.h = dt[m];
+        n.stepsLeft = steps;
+        n.lastStatus = EWG_OK;
+        memset(&e->hSt[m], 0, sizeof(BiState));
+        e->hSt[m].status = ST_IDLE;
+    }
+    memset(e->hSched, 0, sizeof(SchedD));
+    e->hSched->limit = kSuperstepsPerLaunch;
+    if ((c = cudaMemcpyAsync(e->st, e->hSt, sizeof(BiState) * M, cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+        (c = cudaMemcpyAsync(e->dRun, e->hRun, sizeof(RunD) * M, cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+        (c = cudaMemcpyAsync(e->dSched, e->hSched, sizeof(SchedD), cudaMemcpyHostToDevice, e->stream)) != cudaSuccess)
+        return ens_fail(e, c, "upload scheduler state");
+    const NewtonD nd{no->newton_tolerance, no->newton_max_error, no->newton_max_iterations};
+    cudaGraphExec_t exec = nullptr;
+    if ((s = build_device_advance<T>(e, nd, so, &exec))) return s;
+    auto done = [&](ewg_status r) {
+        cudaGraphExecDestroy(exec);
+        return r;
+    };
+    cudaEventRecord(e->ev0, e->stream);
+    const long long maxSupersteps = 10000000;
+    for (;;) {
+        if ((c = cudaGraphLaunch(exec, e->stream)) != cudaSuccess) return done(ens_fail(e, c, "graph launch"));
+        if ((s = sync_read(e, e->hSched, e->dSched, sizeof(SchedD), "read scheduler state"))) return done(s);
+        if (e->hSched->error) {
+            e->err = "ensemble bicgstab: a member never left RUNNING";
+            return done((ewg_status)e->hSched->error);
+        }
+        if (!e->hSched->active) break;
+        if (e->hSched->supersteps >= maxSupersteps) {
+            e->err = "ensemble advance: superstep limit reached";
+            return done(EWG_ERR_TIMEOUT);
+        }
+        e->hSched->limit = e->hSched->supersteps + kSuperstepsPerLaunch;
+        if ((c = cudaMemcpyAsync(&e->dSched->limit, &e->hSched->limit, sizeof(long long), cudaMemcpyHostToDevice,
+                                 e->stream)) != cudaSuccess)
+            return done(ens_fail(e, c, "upload superstep bound"));
+    }
+    cudaEventRecord(e->ev1, e->stream);
+    if ((s = sync_read(e, e->hRun, e->dRun, sizeof(RunD) * M, "read member runs"))) return done(s);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    bool allOk = true;
+    for (int m = 0; m < M; ++m) {
+        const RunD& n = e->hRun[m];
+        if (rep) {
+            rep[m].status = n.phase == PH_DONE ? EWG_OK : n.lastStatus;
+            rep[m].newton_iterations = n.phase == PH_DONE ? n.newton : n.numIt;
+            rep[m].linear_iterations = n.linear;
+            rep[m].halvings = n.halvings + (n.phase == PH_DONE ? 0 : n.halvingsStep);
+            rep[m].dt = n.h;
+            rep[m].error = n.error;
+        }
+        allOk = allOk && n.phase == PH_DONE;
+    }
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->rounds = e->hSched->rounds;
+        stats->linear_iterations = e->hSched->linearIterations;
+        stats->cell_iterations = e->hSched->cellIterations;
+        stats->t_solve = ms * 1e-3;
+        stats->supersteps = (int32_t)e->hSched->supersteps;
+    }
+    if (!allOk) {
+        e->err = "a member's time step failed after the allowed halvings";
+        return done(EWG_ERR_NOT_CONVERGED);
+    }
+    return done(EWG_OK);
+}
+
 // Time every launch shape of each kernel class on the current state and keep the fastest.
 template <typename T>
 ewg_status autotune(ewg_ensemble* e, const double* dt, const ewg_solve_opts* so) {
@@ -1344,10 +1770,11 @@ void ewg_ensemble_destroy(ewg_ensemble* e) {
     if (e->graphExec) cudaGraphExecDestroy(e->graphExec);
     void* ps[] = {e->dm, e->x0, e->x1, e->sold, e->r, e->stage, e->perm, e->lens, e->iq, e->geo, e->J,
                   e->Dinv, e->L, e->kx, e->kr, e->kr0, e->kv, e->kp, e->ky, e->kz, e->kb, e->partials, e->counters,
-                  e->st, e->stSave, e->mask, e->errmax, e->flags, e->flagsF, e->flagsU, e->dtArr};
+                  e->st, e->stSave, e->mask, e->errmax, e->flags, e->flagsF, e->flagsU, e->dtArr,
+                  e->dRun, e->dSched, e->dPrefix, e->dTilesAll, e->maskF, e->maskA, e->maskS};
     for (void* p : ps)
         if (p) cudaFree(p);
-    void* hs[] = {e->hSt, e->hMask, e->hErr, e->hFlags, e->hFlagsF, e->hFlagsU, e->hDt};
+    void* hs[] = {e->hSt, e->hMask, e->hErr, e->hFlags, e->hFlagsF, e->hFlagsU, e->hDt, e->hRun, e->hSched};
     for (void* p : hs)
         if (p) cudaFreeHost(p);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -1615,6 +2042,15 @@ ewg_status ewg_ensemble_advance(ewg_ensemble* e, int32_t steps, const double* dt
     if (so->precond != EWG_PRECOND_ILU0) { e->err = "ensembles use the block ILU(0) preconditioner"; return EWG_ERR_INVALID; }
     return e->precision == EWG_PRECISION_MIXED ? ensemble_advance<float>(e, steps, dt, no, so, reports, stats)
                                                : ensemble_advance<double>(e, steps, dt, no, so, reports, stats);
+}
+
+ewg_status ewg_ensemble_advance_device(ewg_ensemble* e, int32_t steps, const double* dt, const ewg_newton_opts* no,
+                                       const ewg_solve_opts* so, ewg_ensemble_report* reports,
+                                       ewg_ensemble_stats* stats) {
+    if (check_ens(e) || !dt || !no || !so || steps < 1) return EWG_ERR_INVALID;
+    if (so->precond != EWG_PRECOND_ILU0) { e->err = "ensembles use the block ILU(0) preconditioner"; return EWG_ERR_INVALID; }
+    return e->precision == EWG_PRECISION_MIXED ? ensemble_advance_device<float>(e, steps, dt, no, so, reports, stats)
+                                               : ensemble_advance_device<double>(e, steps, dt, no, so, reports, stats);
 }
 
 ewg_status ewg_ensemble_step(ewg_ensemble* e, const double* dt, const ewg_newton_opts* no, const ewg_solve_opts* so,

@@ -118,7 +118,8 @@ class EnsembleReport(C.Structure):
 
 class EnsembleStats(C.Structure):
     _fields_ = [("rounds", C.c_int32), ("linear_iterations", C.c_int32), ("t_linearize", C.c_double),
-                ("t_solve", C.c_double), ("t_update", C.c_double), ("cell_iterations", C.c_double)]
+                ("t_solve", C.c_double), ("t_update", C.c_double), ("cell_iterations", C.c_double),
+                ("supersteps", C.c_int32)]
 
 
 ENSEMBLE_KERNEL_CLASSES = ("intensive", "assemble", "factor", "cell", "ilu_black", "ilu_red",
@@ -471,6 +472,8 @@ def load(path: str = LIB_PATH):
                                         P(EnsembleStats)]),
         "ewg_ensemble_advance": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(NewtonOpts), P(SolveOpts),
                                            P(EnsembleReport), P(EnsembleStats)]),
+        "ewg_ensemble_advance_device": (C.c_int, [C.c_void_p, C.c_int32, P(d), P(NewtonOpts), P(SolveOpts),
+                                                  P(EnsembleReport), P(EnsembleStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -1251,16 +1254,18 @@ class Ensemble:
         """One implicit step of every member (own dt each). Returns (status, reports, stats)."""
         return self.advance(1, dt, nopts, sopts, check)
 
-    def advance(self, steps, dt, nopts=None, sopts=None, check=True):
+    def advance(self, steps, dt, nopts=None, sopts=None, check=True, device=False):
         """`steps` implicit steps of every member, each at its own pace. Returns (status, reports,
-        stats); reports sum the iterations over each member's accepted steps."""
+        stats); reports sum the iterations over each member's accepted steps. device=True takes
+        every decision on the device (ewg_ensemble_advance_device: the supersteps run inside one
+        CUDA graph WHILE node); the results are the same bits."""
         d = self._dt(dt)
         nopts = nopts or default_newton_opts()
         sopts = sopts or default_solve_opts()
         reps = (EnsembleReport * self.M)()
         stats = EnsembleStats()
-        st = self.lib.ewg_ensemble_advance(self.h, int(steps), _ptr(d), C.byref(nopts), C.byref(sopts), reps,
-                                           C.byref(stats))
+        fn = self.lib.ewg_ensemble_advance_device if device else self.lib.ewg_ensemble_advance
+        st = fn(self.h, int(steps), _ptr(d), C.byref(nopts), C.byref(sopts), reps, C.byref(stats))
         if check:
             self._check(st, "advance")
         return st, list(reps), stats

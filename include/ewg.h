@@ -451,6 +451,8 @@ typedef struct ewg_ensemble_stats {
     int32_t linear_iterations;  /* BiCGStab iterations summed over members */
     double t_linearize, t_solve, t_update;  /* device seconds per phase */
     double cell_iterations;     /* sum over members of cells x BiCGStab iterations */
+    int32_t supersteps;         /* supersteps run (each: linearize, decide, start solves, check_interval
+                                   BiCGStab iterations, update) */
 } ewg_ensemble_stats;
 
 void ewg_default_ensemble_opts(ewg_ensemble_opts* opts);
@@ -493,6 +495,16 @@ ewg_status ewg_ensemble_step(ewg_ensemble* ens, const double* dt, const ewg_newt
  * Newton / BiCGStab iterations and halvings over the member's accepted steps). */
 ewg_status ewg_ensemble_advance(ewg_ensemble* ens, int32_t steps, const double* dt, const ewg_newton_opts* nopts,
                                 const ewg_solve_opts* sopts, ewg_ensemble_report* reports, ewg_ensemble_stats* stats);
+/* ewg_ensemble_advance with every Newton, step-size and BiCGStab-stop decision taken on the device:
+ * one superstep (linearization, decisions, preconditioner setup, check_interval BiCGStab
+ * iterations, Newton update, step acceptance or halving) is the body of a CUDA graph WHILE node,
+ * and a launch of that graph runs supersteps until no member is active, reading nothing back to
+ * the host; the host reads the scheduler state every 4096 supersteps. Same launches and member
+ * sets as ewg_ensemble_advance, so the results are the same bits. stats->t_solve holds the device
+ * time of the whole advance (t_linearize and t_update are 0: the phases are not timed apart). */
+ewg_status ewg_ensemble_advance_device(ewg_ensemble* ens, int32_t steps, const double* dt,
+                                       const ewg_newton_opts* nopts, const ewg_solve_opts* sopts,
+                                       ewg_ensemble_report* reports, ewg_ensemble_stats* stats);
 
 /* ---- instrumentation (no reference counterpart; the analogue of the reference's phase timers,
  * newtonmethod.hh:488-500) --------------------------------------------------------------- */

@@ -171,3 +171,61 @@ def test_ensemble_step_halving(ewg_mod):
         assert np.max(np.abs(xe[:, 1] - x[:, 1])) <= 1e-8
         ctx.close()
     ens.close()
+
+
+def _advance_pair(ewg, cases, dts, steps, precision, so, no=None, max_divisions=10, check_interval=4):
+    out = []
+    for device in (False, True):
+        ens = ewg.Ensemble(cases, precision=precision, check_interval=check_interval, max_divisions=max_divisions)
+        ens.apply_initial_solution()
+        st, reps, stats = ens.advance(steps, dts, nopts=no, sopts=so, check=False, device=device)
+        xs = [(ens.get_solution(m, 0), ens.get_solution(m, 1)) for m in range(len(cases))]
+        ens.close()
+        out.append((st, reps, stats, xs))
+    return out
+
+
+def _same_run(a, b):
+    (sa, ra, ta, xa), (sb, rb, tb, xb) = a, b
+    assert sa == sb
+    for p, q in zip(ra, rb):
+        assert (p.status, p.newton_iterations, p.linear_iterations, p.halvings) == \
+               (q.status, q.newton_iterations, q.linear_iterations, q.halvings)
+        assert p.dt == q.dt and p.error == q.error
+    assert (ta.rounds, ta.linear_iterations, ta.cell_iterations, ta.supersteps) == \
+           (tb.rounds, tb.linear_iterations, tb.cell_iterations, tb.supersteps)
+    for (a0, a1), (b0, b1) in zip(xa, xb):
+        assert np.array_equal(a0.view(np.uint64), b0.view(np.uint64))
+        assert np.array_equal(a1.view(np.uint64), b1.view(np.uint64))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_scheduled_advance_is_bit_identical(ewg_mod, precision):
+    """ewg_ensemble_advance_device (every decision on the device, supersteps inside one CUDA graph
+    WHILE node) gives the host-scheduled advance's reports, stats and fields bit for bit."""
+    cases = _cases(ewg_mod)
+    if precision == "fp64":
+        prec, so = ewg_mod.PRECISION_FP64, _fp64_opts(ewg_mod)
+    else:
+        prec = ewg_mod.PRECISION_MIXED
+        so = ewg_mod.default_solve_opts(precision=prec, linear_solver_tolerance=1e-3, verify_true_residual=0)
+    host, dev = _advance_pair(ewg_mod, cases, DTS, 3, prec, so)
+    assert host[0] == 0 and all(r.status == 0 for r in host[1])
+    assert host[2].supersteps > 3
+    _same_run(host, dev)
+
+
+def test_device_scheduled_halving_and_failure(ewg_mod):
+    """Step halving and a member that fails after its allowed halvings take the same course on the
+    device: with Newton limited to 2 iterations the 4000 s step of member 0 is halved until it is
+    accepted (10 divisions allowed), or the advance fails with that member's status (1 allowed)."""
+    cases = _cases(ewg_mod)[:2]
+    so = _fp64_opts(ewg_mod)
+    no = ewg_mod.default_newton_opts(newton_max_iterations=2)
+    dts = [4000.0, 250.0]
+    host, dev = _advance_pair(ewg_mod, cases, dts, 2, ewg_mod.PRECISION_FP64, so, no=no)
+    assert host[0] == 0 and host[1][0].halvings >= 1
+    _same_run(host, dev)
+    host, dev = _advance_pair(ewg_mod, cases, dts, 2, ewg_mod.PRECISION_FP64, so, no=no, max_divisions=1)
+    assert host[0] == ewg_mod.EWG_ERR_NOT_CONVERGED and host[1][0].status != 0 and host[1][1].status == 0
+    _same_run(host, dev)
