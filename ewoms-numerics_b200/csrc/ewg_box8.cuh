@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
                                                            const typename V2T<TV>::type* __restrict__ d,
                                                            typename V2T<TV>::type* __restrict__ w,
                                                            const int* __restrict__ status) {
+    pdl_enter();
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
     __shared__ double2 S[8][32];
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
@@ -420,6 +421,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(c
                                                             const typename V2T<TV>::type* __restrict__ wv,
                                                             typename V2T<TV>::type* __restrict__ y,
                                                             const int* __restrict__ status, double w) {
+    pdl_enter();
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
     __shared__ double2 S[8][32];
     const double winv = 1.0 / w;

@@ -274,6 +274,33 @@ void prof_flush(ewg_ctx* ctx);  // call after the stream is synchronised
         ::ewg::prof_end((ctx), (id));                                    \
     } while (0)
 
+// Launch with programmatic stream serialization (the kernel must start with pdl_enter): the
+// kernel's launch and block setup overlap the end of the previous kernel in the stream. EWG_PDL=0
+// at compile time launches these kernels like EWG_LAUNCH.
+#ifndef EWG_PDL
+#define EWG_PDL 1
+#endif
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(cudaStream_t stream, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = EWG_PDL;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#define EWG_LAUNCH_PDL(ctx, id, kernel, grid, block, ...)                          \
+    do {                                                                         \
+        ::ewg::prof_begin((ctx), (id));                                          \
+        ::ewg::launch_pdl((ctx)->stream, kernel, (grid), (block), __VA_ARGS__);  \
+        ::ewg::prof_end((ctx), (id));                                            \
+    } while (0)
+
 void build_phys(Phys& P, const ewg_grid* g, const ewg_problem* p);
 ewg_status cuda_fail(ewg_ctx* ctx, cudaError_t e, const char* what);
 int grid_size_for(ewg_ctx* ctx, const void* kernel, int block, size_t smem = 0);

@@ -15,6 +15,17 @@
 namespace ewg {
 
 constexpr int kSolBlock = 256;
+
+// Programmatic dependent launch. A kernel launched with EWG_LAUNCH_PDL may be scheduled while the
+// kernel before it in the stream is still finishing; its first statement, pdl_enter, waits until
+// that kernel has completed with its writes visible and then lets the next kernel be scheduled.
+// So a PDL kernel completes only after its predecessor did, and nothing it reads or writes can
+// race with an earlier kernel; what overlaps is the launch and block setup with the tail of the
+// previous kernel. In a kernel launched without the attribute both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 constexpr int kMaxRed = 4;
 
 enum BiStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_FAILED = 2, ST_BREAKDOWN = 3, ST_MAXITER = 4 };

@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(kSolBlock) k_ilu_black_apply(const __grid_cons
                                                                 const typename V2T<TV>::type* __restrict__ d,
                                                                 typename V2T<TV>::type* __restrict__ y,
                                                                 const int* __restrict__ status, double w) {
+    pdl_enter();
     if (status && *status != ST_RUNNING) return;
     for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < P.Nh;
          h += (int64_t)gridDim.x * blockDim.x)
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(kSolBlock) k_ilu_red_apply(const __grid_consta
                                                               const typename V2T<TV>::type* __restrict__ d,
                                                               typename V2T<TV>::type* __restrict__ y,
                                                               const int* __restrict__ status, double w) {
+    pdl_enter();
     if (status && *status != ST_RUNNING) return;
     const double winv = 1.0 / w;
     for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < P.Nh;
@@ -147,6 +149,7 @@ __global__ void __launch_bounds__(kSolBlock) k_jacobi_apply(const __grid_constan
                                                              const typename V2T<TV>::type* __restrict__ d,
                                                              typename V2T<TV>::type* __restrict__ y,
                                                              const int* __restrict__ status, double w) {
+    pdl_enter();
     if (status && *status != ST_RUNNING) return;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
          s += (int64_t)gridDim.x * blockDim.x) {
@@ -248,6 +251,7 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_p(const __g
                                                        typename V2T<TV>::type* __restrict__ v,
                                                        typename V2T<TV>::type* __restrict__ p,
                                                        const BiState* __restrict__ st) {
+    pdl_enter();
     if (st->status != ST_RUNNING) return;
     const bool restart = st->restartPending != 0;
     const double beta = st->beta, omega = st->omega;
@@ -279,6 +283,7 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_spmv_alpha(
                                                                 typename V2T<TV>::type* __restrict__ v,
                                                                 BiState* st, double* partials, unsigned* counter,
                                                                 const SpmvExtra ex) {
+    pdl_enter();
     if (st->status != ST_RUNNING) return;
     double red[1] = {0.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
@@ -310,6 +315,7 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_hs(const __
                                                         typename V2T<TV>::type* __restrict__ r,
                                                         const typename V2T<TV>::type* __restrict__ v,
                                                         BiState* st, double* partials, unsigned* counter) {
+    pdl_enter();
     if (st->status != ST_RUNNING) return;
     const double alpha = st->alpha;
     double red[2] = {0.0, 0.0};  // max |s|, any y != 0
@@ -343,6 +349,7 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_spmv_omega(
                                                                 typename V2T<TV>::type* __restrict__ t,
                                                                 BiState* st, double* partials, unsigned* counter,
                                                                 const SpmvExtra ex) {
+    pdl_enter();
     if (st->status != ST_RUNNING) return;
     double red[2] = {0.0, 0.0};
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
@@ -376,6 +383,7 @@ __global__ void __launch_bounds__(kSolBlock, kRedBlocksPerSM) k_bicg_xr(const __
                                                         const typename V2T<TV>::type* __restrict__ t,
                                                         const typename V2T<TV>::type* __restrict__ r0,
                                                         BiState* st, double* partials, unsigned* counter) {
+    pdl_enter();
     if (st->status != ST_RUNNING) return;
     const double omega = st->omega;
     double red[4] = {0.0, 0.0, 0.0, 0.0};  // sum r0.r', sum r'.r', max |s|, any z != 0
@@ -872,18 +880,18 @@ static void launch_precond(ewg_ctx* ctx, KrylovWs<T>& w, int kind, double relax,
         int g = grid_size_for(ctx, (const void*)k_jacobi_apply<T, T>, kSolBlock);
         {
             auto kfn = k_jacobi_apply<T, T>;
-            EWG_LAUNCH(ctx, K_JACOBI_APPLY, kfn, g, kSolBlock, P, w.Dinv, d, y, status, relax);
+            EWG_LAUNCH_PDL(ctx, K_JACOBI_APPLY, kfn, g, kSolBlock, P, w.Dinv, d, y, status, relax);
         }
     } else {
         int g = grid_size_for(ctx, (const void*)k_ilu_black_apply<T, T>, kSolBlock);
         {
             auto kfn = k_ilu_black_apply<T, T>;
-            EWG_LAUNCH(ctx, K_ILU_BLACK_APPLY, kfn, g, kSolBlock, P, w.Dinv, w.L, d, y, status, relax);
+            EWG_LAUNCH_PDL(ctx, K_ILU_BLACK_APPLY, kfn, g, kSolBlock, P, w.Dinv, w.L, d, y, status, relax);
         }
         int g2 = grid_size_for(ctx, (const void*)k_ilu_red_apply<T, T>, kSolBlock);
         {
             auto kfn = k_ilu_red_apply<T, T>;
-            EWG_LAUNCH(ctx, K_ILU_RED_APPLY, kfn, g2, kSolBlock, P, A, w.Dinv, d, y, status, relax);
+            EWG_LAUNCH_PDL(ctx, K_ILU_RED_APPLY, kfn, g2, kSolBlock, P, A, w.Dinv, d, y, status, relax);
         }
     }
 }
@@ -993,21 +1001,21 @@ static ewg_status bicgstab(ewg_ctx* ctx, KrylovWs<T>& w, const ewg_solve_opts* o
     int guard = 0;
     for (;;) {
         for (int k = 0; k < interval; ++k) {
-            EWG_LAUNCH(ctx, K_BICG_P, k_bicg_p<T>, G, kSolBlock, P, w.r, w.r0, w.v, w.p, sw->st);
+            EWG_LAUNCH_PDL(ctx, K_BICG_P, k_bicg_p<T>, G, kSolBlock, P, w.r, w.r0, w.v, w.p, sw->st);
             if (b8) launch_precond_b8<T>(ctx, w, relax, w.p, w.y, status);
             else launch_precond<T>(ctx, w, o->precond, relax, w.p, w.y, status);
             {
                 auto kfn = b8 ? k_bicg_spmv_alpha<T, T, 2> : k_bicg_spmv_alpha<T, T, 0>;
-                EWG_LAUNCH(ctx, K_BICG_SPMV_ALPHA, kfn, G, kSolBlock, P, A, w.y, w.r0, w.v, sw->st, part, cnt, ex);
+                EWG_LAUNCH_PDL(ctx, K_BICG_SPMV_ALPHA, kfn, G, kSolBlock, P, A, w.y, w.r0, w.v, sw->st, part, cnt, ex);
             }
-            EWG_LAUNCH(ctx, K_BICG_HS, k_bicg_hs<T>, G, kSolBlock, P, w.x, w.y, w.r, w.v, sw->st, part, cnt);
+            EWG_LAUNCH_PDL(ctx, K_BICG_HS, k_bicg_hs<T>, G, kSolBlock, P, w.x, w.y, w.r, w.v, sw->st, part, cnt);
             if (b8) launch_precond_b8<T>(ctx, w, relax, w.r, w.z, status);
             else launch_precond<T>(ctx, w, o->precond, relax, w.r, w.z, status);
             {
                 auto kfn = b8 ? k_bicg_spmv_omega<T, T, 2> : k_bicg_spmv_omega<T, T, 0>;
-                EWG_LAUNCH(ctx, K_BICG_SPMV_OMEGA, kfn, G, kSolBlock, P, A, w.z, w.r, w.y, sw->st, part, cnt, ex);
+                EWG_LAUNCH_PDL(ctx, K_BICG_SPMV_OMEGA, kfn, G, kSolBlock, P, A, w.z, w.r, w.y, sw->st, part, cnt, ex);
             }
-            EWG_LAUNCH(ctx, K_BICG_XR, k_bicg_xr<T>, G, kSolBlock, P, w.x, w.z, w.r, w.y, w.r0, sw->st, part, cnt);
+            EWG_LAUNCH_PDL(ctx, K_BICG_XR, k_bicg_xr<T>, G, kSolBlock, P, w.x, w.z, w.r, w.y, w.r0, sw->st, part, cnt);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "bicgstab launch");
         if ((e = cudaMemcpyAsync(sw->h_st, sw->st, sizeof(BiState), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
