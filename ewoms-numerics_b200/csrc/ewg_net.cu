@@ -10,10 +10,13 @@
 // x fastest), Cin padded to 16 or 32, the last layer's 2 outputs padded to 8 (16 for gradients).
 //
 // Kernels
-//   k_conv3d       implicit-GEMM convolution on the tensor cores (mma.sync m16n8k16 BF16 ->
-//                  FP32): one warp computes 16 voxels x Cout; K = 27 taps x Cin. Used for the
-//                  forward pass (bias, ReLU) and for input gradients (flipped, transposed
-//                  weights; epilogue multiplies by the ReLU mask of the layer below).
+//   k_conv3d_tc    implicit-GEMM convolution on the 5th-generation tensor cores (tcgen05.mma
+//                  BF16 -> FP32 in tensor memory, TMA loads of the shifted input boxes; see
+//                  ewg_conv_tc.cuh): the three 32-channel layers of the forward pass (bias, ReLU)
+//                  and the three input-gradient convolutions (flipped, transposed weights;
+//                  epilogue multiplies by the ReLU mask of the layer below).
+//   k_conv3d       warp-level implicit-GEMM convolution (mma.sync m16n8k16 BF16 -> FP32): one
+//                  warp computes 16 voxels x Cout; K = 27 taps x Cin. The 2-output last layer.
 //   k_conv3d_wgrad weight and bias gradients on FP32 CUDA cores, one block per (tap, voxel chunk).
 //   k_adam         Adam update of the FP32 master weights, then BF16 working copies.
 #include <cuda_bf16.h>
@@ -26,6 +29,7 @@
 #include <vector>
 
 #include "ewg_internal.cuh"
+#include "ewg_conv_tc.cuh"
 
 namespace ewg {
 
@@ -340,6 +344,123 @@ ewg_status ensure_capacity(ewg_net* n, int64_t V) {
     return EWG_OK;
 }
 
+// ---- tensor-core convolution: tensor maps and launches ----------------------------------------
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver the runtime uses (no link against libcuda)
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// channels-last activations [B][D][H][W][C] as the 5-D map (C, x, y, z, volume), box (C, 32, 4, 1, 1)
+bool tc_map_activations(CUtensorMap* m, const __nv_bfloat16* p, int C, const VolDims& d) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t row = (cuuint64_t)C * 2;
+    const cuuint64_t dims[5] = {(cuuint64_t)C, (cuuint64_t)d.W, (cuuint64_t)d.H, (cuuint64_t)d.D, (cuuint64_t)d.B};
+    const cuuint64_t strides[4] = {row, row * d.W, row * d.W * d.H, row * d.W * d.H * d.D};
+    const cuuint32_t box[5] = {(cuuint32_t)C, (cuuint32_t)kTcTileX, (cuuint32_t)kTcTileY, 1, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, C == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// weights [27][COUT][CIN] as the 2-D map (CIN, 27 COUT), box (CIN, COUT): one tap per box
+bool tc_map_weights(CUtensorMap* m, const __nv_bfloat16* p, int cin, int cout) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cin, (cuuint64_t)kTaps * cout};
+    const cuuint64_t strides[1] = {(cuuint64_t)cin * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)cin, (cuuint32_t)cout};
+    const cuuint32_t es[2] = {1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, cin == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the device word the tensor-core convolution records a failed wait in (0: none)
+static __device__ int g_convTcErr;
+
+int* conv_tc_err_ptr() {
+    int* p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_convTcErr) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+template <int CIN, int COUT, int EPI>
+cudaError_t conv_tc_attr() {
+    return cudaFuncSetAttribute(k_conv3d_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcShape<CIN, COUT>::smemBytes);
+}
+
+cudaError_t conv_tc_attrs() {
+    cudaError_t e = conv_tc_attr<16, 32, EPI_BIAS_RELU>();
+    if (!e) e = conv_tc_attr<32, 32, EPI_BIAS_RELU>();
+    if (!e) e = conv_tc_attr<16, 32, EPI_MASK>();
+    if (!e) e = conv_tc_attr<32, 32, EPI_MASK>();
+    return e;
+}
+
+// One 3x3x3 convolution (CIN -> COUT = 32, epilogue bias + ReLU or ReLU mask) on the tensor cores;
+// false when a tensor map cannot be built.
+template <int CIN, int COUT, int EPI>
+bool launch_conv_tc(cudaStream_t st, const VolDims& d, const __nv_bfloat16* in, const __nv_bfloat16* W,
+                    const float* bias, const __nv_bfloat16* mask, int maskC, __nv_bfloat16* out, int outC) {
+    static_assert(EPI == EPI_BIAS_RELU || EPI == EPI_MASK, "tensor-core epilogues");
+    CUtensorMap mi, mw;
+    int* err = conv_tc_err_ptr();
+    if (!err || !tc_map_activations(&mi, in, CIN, d) || !tc_map_weights(&mw, W, CIN, COUT)) return false;
+    const int64_t nTiles = (int64_t)d.B * d.D * ((d.H + kTcTileY - 1) / kTcTileY) * ((d.W + kTcTileX - 1) / kTcTileX);
+    static int perSM = 0, sms = 0;
+    if (perSM == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_conv3d_tc<CIN, COUT, EPI>, kTcThreads,
+                                                          TcShape<CIN, COUT>::smemBytes) != cudaSuccess || perSM < 1)
+            perSM = 1;
+        cudaGetLastError();
+    }
+    const int64_t full = (int64_t)sms * perSM;
+    const int grid = (int)(nTiles < full ? nTiles : full);
+    k_conv3d_tc<CIN, COUT, EPI><<<grid, kTcThreads, TcShape<CIN, COUT>::smemBytes, st>>>(
+        mi, mw, d.D, d.H, d.W, nTiles, bias, mask, maskC, out, outC, err);
+    return true;
+}
+
+// After a synchronization: EWG_ERR_TIMEOUT if a tensor-core convolution gave up a wait since the
+// last check (the word is cleared).
+ewg_status conv_tc_check(std::string* errText) {
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_convTcErr, sizeof(int));
+    if (e != cudaSuccess) {
+        if (errText) *errText = std::string("read convolution status: ") + cudaGetErrorString(e);
+        return EWG_ERR_CUDA;
+    }
+    if (v == 0) return EWG_OK;
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_convTcErr, &zero, sizeof(int));
+    if (errText) *errText = "tensor-core convolution: a bounded wait gave up (stage " + std::to_string(v) + ")";
+    return EWG_ERR_TIMEOUT;
+}
+
 // The dynamic shared-memory limit of one k_conv3d instance (its weights, up to 55,296 B, are above
 // the 48 KB default). The attribute belongs to the current device, so ewg_net_create sets it for
 // the device the net lives on.
@@ -355,6 +476,7 @@ cudaError_t conv_smem_attrs() {
     if (!e) e = conv_smem_attr<32, 8, EPI_BIAS>();
     if (!e) e = conv_smem_attr<16, 32, EPI_MASK>();
     if (!e) e = conv_smem_attr<32, 32, EPI_MASK>();
+    if (!e) e = conv_tc_attrs();
     return e;
 }
 
@@ -369,13 +491,22 @@ void launch_conv(ewg_net* n, const VolDims& d, const __nv_bfloat16* in, const __
     k<<<(int)blocks, 128, smem, n->stream>>>(d, in, W, bias, mask, maskC, out, outC);
 }
 
-// forward pass over the features already in act[0]
-void forward(ewg_net* n, const VolDims& d) {
+// forward pass over the features already in act[0]: the three 32-channel layers on the
+// tensor cores (tcgen05), the 2-output layer with the warp-level kernel
+ewg_status forward(ewg_net* n, const VolDims& d) {
     const float* p = n->params;
-    launch_conv<16, 32, EPI_BIAS_RELU>(n, d, n->act[0], n->wf[0], p + n->bOff[0], nullptr, 0, n->act[1], 32);
-    launch_conv<32, 32, EPI_BIAS_RELU>(n, d, n->act[1], n->wf[1], p + n->bOff[1], nullptr, 0, n->act[2], 32);
-    launch_conv<32, 32, EPI_BIAS_RELU>(n, d, n->act[2], n->wf[2], p + n->bOff[2], nullptr, 0, n->act[3], 32);
+    bool ok = launch_conv_tc<16, 32, EPI_BIAS_RELU>(n->stream, d, n->act[0], n->wf[0], p + n->bOff[0], nullptr, 0,
+                                                    n->act[1], 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_BIAS_RELU>(n->stream, d, n->act[1], n->wf[1], p + n->bOff[1], nullptr, 0,
+                                                     n->act[2], 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_BIAS_RELU>(n->stream, d, n->act[2], n->wf[2], p + n->bOff[2], nullptr, 0,
+                                                     n->act[3], 32);
+    if (!ok) {
+        n->err = "tensor map of a convolution could not be built";
+        return EWG_ERR_CUDA;
+    }
     launch_conv<32, 8, EPI_BIAS>(n, d, n->act[3], n->wf[3], p + n->bOff[3], nullptr, 0, n->out, 2);
+    return EWG_OK;
 }
 
 template <int CIN, int COUT>
@@ -387,17 +518,23 @@ void launch_wgrad(ewg_net* n, const VolDims& d, const __nv_bfloat16* X, const __
                                                                         n->grads + n->bOff[l], chunk);
 }
 
-// backward pass after forward(); dY of the last layer in grad16; gradients accumulate in grads
-void backward(ewg_net* n, const VolDims& d) {
+// backward pass after forward(); dY of the last layer in grad16; gradients accumulate in grads.
+// The input gradients are convolutions with the flipped, transposed weights on the tensor cores.
+ewg_status backward(ewg_net* n, const VolDims& d) {
     // layer 4: X = H3 (32), dY (16 wide, 8 used)
     launch_wgrad<32, 8>(n, d, n->act[3], n->grad16, 16, 3);
     // dH3 = conv(dY, W4t) * (H3 > 0): Cin' = 16 (8 real + 8 zero), Cout' = 32
-    launch_conv<16, 32, EPI_MASK>(n, d, n->grad16, n->wt[3], nullptr, n->act[3], 32, n->gradA, 32);
+    bool ok = launch_conv_tc<16, 32, EPI_MASK>(n->stream, d, n->grad16, n->wt[3], nullptr, n->act[3], 32, n->gradA, 32);
     launch_wgrad<32, 32>(n, d, n->act[2], n->gradA, 32, 2);
-    launch_conv<32, 32, EPI_MASK>(n, d, n->gradA, n->wt[2], nullptr, n->act[2], 32, n->gradB, 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_MASK>(n->stream, d, n->gradA, n->wt[2], nullptr, n->act[2], 32, n->gradB, 32);
     launch_wgrad<32, 32>(n, d, n->act[1], n->gradB, 32, 1);
-    launch_conv<32, 32, EPI_MASK>(n, d, n->gradB, n->wt[1], nullptr, n->act[1], 32, n->gradA, 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_MASK>(n->stream, d, n->gradB, n->wt[1], nullptr, n->act[1], 32, n->gradA, 32);
     launch_wgrad<16, 32>(n, d, n->act[0], n->gradA, 32, 0);
+    if (!ok) {
+        n->err = "tensor map of a convolution could not be built";
+        return EWG_ERR_CUDA;
+    }
+    return EWG_OK;
 }
 
 ewg_status refresh_weights(ewg_net* n) {
@@ -543,7 +680,7 @@ ewg_status ewg_net_eval_host(ewg_net* n, int32_t B, int32_t D, int32_t H, int32_
         for (int k = 0; k < 16; ++k) f16[v * 16 + k] = __float2bfloat16(k < 5 ? feat[v * 5 + k] : 0.f);
     cudaError_t e = cudaMemcpyAsync(n->act[0], f16.data(), sizeof(__nv_bfloat16) * V * 16, cudaMemcpyHostToDevice, n->stream);
     if (e) return net_fail(n, e, "upload features");
-    forward(n, d);
+    if ((st = forward(n, d))) return st;
     if (target) {
         e = cudaMemcpyAsync(n->target, target, sizeof(float) * V * 2, cudaMemcpyHostToDevice, n->stream);
         if (!e) e = cudaMemsetAsync(n->dLoss, 0, sizeof(float), n->stream);
@@ -551,7 +688,7 @@ ewg_status ewg_net_eval_host(ewg_net* n, int32_t B, int32_t D, int32_t H, int32_
         k_mse<<<256, 256, 0, n->stream>>>(V, n->out, n->target, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
         if (grads) {
             if ((e = cudaMemsetAsync(n->grads, 0, sizeof(float) * n->nParams, n->stream))) return net_fail(n, e, "zero grads");
-            backward(n, d);
+            if ((st = backward(n, d))) return st;
         }
     }
     if ((e = cudaGetLastError())) return net_fail(n, e, "net kernels");
@@ -559,7 +696,38 @@ ewg_status ewg_net_eval_host(ewg_net* n, int32_t B, int32_t D, int32_t H, int32_
     if (target && loss && (e = cudaMemcpyAsync(loss, n->dLoss, sizeof(float), cudaMemcpyDeviceToHost, n->stream))) return net_fail(n, e, "read loss");
     if (target && grads && (e = cudaMemcpyAsync(grads, n->grads, sizeof(float) * n->nParams, cudaMemcpyDeviceToHost, n->stream)))
         return net_fail(n, e, "read grads");
-    return net_fail(n, cudaStreamSynchronize(n->stream), "sync net");
+    if ((st = net_fail(n, cudaStreamSynchronize(n->stream), "sync net"))) return st;
+    return conv_tc_check(&n->err);
+}
+
+// One 3x3x3 convolution layer on the tensor cores, synchronous on the stream (declared in ewg.h).
+ewg_status ewg_net_conv3d(int32_t cin, int32_t epilogue, int32_t B, int32_t D, int32_t H, int32_t W, const void* in,
+                          const void* w, const float* bias, const void* mask, void* out, void* stream) {
+    if ((cin != 16 && cin != 32) || (epilogue != EPI_BIAS_RELU && epilogue != EPI_MASK) || B < 1 || D < 1 || H < 1 ||
+        W < 1 || !in || !w || !out || (epilogue == EPI_BIAS_RELU && !bias) || (epilogue == EPI_MASK && !mask))
+        return EWG_ERR_INVALID;
+    for (const void* p : {in, w, (const void*)out, mask})
+        if (p && (reinterpret_cast<uintptr_t>(p) & 15)) return EWG_ERR_INVALID;
+    if (conv_tc_attrs() != cudaSuccess) { cudaGetLastError(); return EWG_ERR_CUDA; }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const VolDims d{D, H, W, B};
+    const auto* x = static_cast<const __nv_bfloat16*>(in);
+    const auto* wt = static_cast<const __nv_bfloat16*>(w);
+    const auto* mk = static_cast<const __nv_bfloat16*>(mask);
+    auto* y = static_cast<__nv_bfloat16*>(out);
+    bool ok;
+    if (cin == 16) {
+        ok = epilogue == EPI_BIAS_RELU ? launch_conv_tc<16, 32, EPI_BIAS_RELU>(st, d, x, wt, bias, nullptr, 0, y, 32)
+                                       : launch_conv_tc<16, 32, EPI_MASK>(st, d, x, wt, nullptr, mk, 32, y, 32);
+    } else {
+        ok = epilogue == EPI_BIAS_RELU ? launch_conv_tc<32, 32, EPI_BIAS_RELU>(st, d, x, wt, bias, nullptr, 0, y, 32)
+                                       : launch_conv_tc<32, 32, EPI_MASK>(st, d, x, wt, nullptr, mk, 32, y, 32);
+    }
+    if (!ok) return EWG_ERR_CUDA;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return EWG_ERR_CUDA;
+    return conv_tc_check(nullptr);
 }
 
 // Record one training sample from a context after a converged step: features of solution(1)
@@ -601,9 +769,9 @@ ewg_status ewg_net_train(ewg_net* n, const int64_t* sampleIdx, int32_t steps, fl
         if (!e) e = cudaMemsetAsync(n->dLoss, 0, sizeof(float), n->stream);
         if (!e) e = cudaMemsetAsync(n->grads, 0, sizeof(float) * n->nParams, n->stream);
         if (e) return net_fail(n, e, "train setup");
-        forward(n, d);
+        if ((st = forward(n, d))) return st;
         k_mse<<<256, 256, 0, n->stream>>>(V, n->out, s.t, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
-        backward(n, d);
+        if ((st = backward(n, d))) return st;
         n->adamStep += 1;
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = 1.f - std::pow(b1, (float)n->adamStep), c2 = 1.f - std::pow(b2, (float)n->adamStep);
@@ -613,6 +781,7 @@ ewg_status ewg_net_train(ewg_net* n, const int64_t* sampleIdx, int32_t steps, fl
         float l = 0.f;
         if ((e = cudaMemcpyAsync(&l, n->dLoss, sizeof(float), cudaMemcpyDeviceToHost, n->stream))) return net_fail(n, e, "loss");
         if ((e = cudaStreamSynchronize(n->stream))) return net_fail(n, e, "train sync");
+        if ((st = conv_tc_check(&n->err))) return st;
         acc += l;
     }
     if (meanLoss) *meanLoss = (float)(acc / steps);
@@ -630,12 +799,13 @@ ewg_status ewg_net_eval_samples(ewg_net* n, const int64_t* sampleIdx, int32_t co
         if (st) return st;
         cudaMemcpyAsync(n->act[0], s.f, sizeof(__nv_bfloat16) * d.V() * 16, cudaMemcpyDeviceToDevice, n->stream);
         cudaMemsetAsync(n->dLoss, 0, sizeof(float), n->stream);
-        forward(n, d);
+        if ((st = forward(n, d))) return st;
         k_mse<<<256, 256, 0, n->stream>>>(d.V(), n->out, s.t, n->grad16, n->dLoss, n->lossW[0], n->lossW[1], n->act[0], n->wFront);
         float l = 0.f;
         cudaMemcpyAsync(&l, n->dLoss, sizeof(float), cudaMemcpyDeviceToHost, n->stream);
         cudaError_t e = cudaStreamSynchronize(n->stream);
         if (e) return net_fail(n, e, "eval samples");
+        if ((st = conv_tc_check(&n->err))) return st;
         acc += l;
     }
     if (meanLoss) *meanLoss = (float)(acc / count);
@@ -656,10 +826,11 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* n, double dt, int32_t* usedG
     // both the context and the network stream run this sequence; order them by synchronising
     if ((e = cudaStreamSynchronize(ctx->stream))) return cuda_fail(ctx, e, "sync ctx");
     k_features<<<512, 256, 0, n->stream>>>(P, ctx->x1, ctx->perm, dt, n->fs, n->act[0]);
-    forward(n, d);
+    if ((st = forward(n, d))) return st;
     k_apply_guess<<<512, 256, 0, n->stream>>>(P, ctx->x1, n->out, n->tp, n->ts, n->applyPressure, n->snThreshold, ctx->x0);
     if ((e = cudaGetLastError())) return cuda_fail(ctx, e, "guess kernels");
     if ((e = cudaStreamSynchronize(n->stream))) return cuda_fail(ctx, e, "sync guess");
+    if ((st = conv_tc_check(&n->err))) return st;
     double rg = 0.0, rp = 0.0;
     int bad = 0;
     // residual-only evaluations (the old-time storage is that of solution(1) in both)
@@ -683,8 +854,9 @@ ewg_status ewg_predict_guess(ewg_ctx* ctx, ewg_net* n, double dt, int32_t* usedG
 
 // ---- forward pass that allocates nothing ----------------------------------------------------
 //
-// ewg_net_forward_noalloc runs the same four k_conv3d launches as the forward pass of
-// ewg_net_eval_host, for callers that must not allocate device memory: a host simulator that
+// ewg_net_forward_noalloc runs the same four convolution launches as the forward pass of
+// ewg_net_eval_host (three on the tensor cores, whose tensor maps are host-side descriptors, and
+// the 2-output layer), for callers that must not allocate device memory: a host simulator that
 // hands all of the device's memory to its own arena up front, and time-step loops that cannot
 // afford the device-wide synchronisation of cudaMalloc / cudaFree. The caller
 // passes the FP32 parameters, the features and the output on the device; the BF16 weights, the
@@ -748,6 +920,7 @@ ewg_status noalloc_setup(int dev, unsigned char** out, char* msg, int32_t len) {
         if (e == cudaSuccess) e = noalloc_conv_attr<16, 32, EPI_BIAS_RELU>();
         if (e == cudaSuccess) e = noalloc_conv_attr<32, 32, EPI_BIAS_RELU>();
         if (e == cudaSuccess) e = noalloc_conv_attr<32, 8, EPI_BIAS>();
+        if (e == cudaSuccess) e = conv_tc_attrs();
         if (e != cudaSuccess) {
             char text[256];
             std::snprintf(text, sizeof(text), "no-allocation scratch set-up: %s", cudaGetErrorString(e));
@@ -799,9 +972,10 @@ extern "C" ewg_status ewg_net_forward_noalloc(const float* params, int32_t B, in
     __nv_bfloat16* actA = reinterpret_cast<__nv_bfloat16*>(base + kNoAllocOffActA);
     __nv_bfloat16* actB = reinterpret_cast<__nv_bfloat16*>(base + kNoAllocOffActB);
     k_pack_features<<<256, 256, 0, s>>>(V, features, feat);
-    noalloc_conv<16, 32, EPI_BIAS_RELU>(s, d, feat, wf[0], params + boff[0], actA, 32);
-    noalloc_conv<32, 32, EPI_BIAS_RELU>(s, d, actA, wf[1], params + boff[1], actB, 32);
-    noalloc_conv<32, 32, EPI_BIAS_RELU>(s, d, actB, wf[2], params + boff[2], actA, 32);
+    bool ok = launch_conv_tc<16, 32, EPI_BIAS_RELU>(s, d, feat, wf[0], params + boff[0], nullptr, 0, actA, 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_BIAS_RELU>(s, d, actA, wf[1], params + boff[1], nullptr, 0, actB, 32);
+    ok = ok && launch_conv_tc<32, 32, EPI_BIAS_RELU>(s, d, actB, wf[2], params + boff[2], nullptr, 0, actA, 32);
+    if (!ok) return noalloc_fail(message, message_len, EWG_ERR_CUDA, "tensor map of a convolution could not be built");
     noalloc_conv<32, 8, EPI_BIAS>(s, d, actA, wf[3], params + boff[3], outputs, 2);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(message, message_len, EWG_ERR_CUDA, cudaGetErrorString(e));
     return EWG_OK;

@@ -417,6 +417,17 @@ ewg_status ewg_net_forward_noalloc(const float* params, int32_t B, int32_t D, in
                                    const float* features, float* outputs, void* stream, char* message,
                                    int32_t message_len);
 
+/* One 3x3x3 convolution layer of the guess network on the tensor cores (tcgen05.mma, TMA),
+ * synchronous on `stream` (a cudaStream_t; NULL: the default stream). With v a voxel and the
+ * taps t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1) over the 27 neighbours (zero outside the volume):
+ *   acc[v][o] = sum_t sum_c in[nbr(v, t)][c] w[t][o][c]              (FP32 accumulation)
+ *   epilogue 0: out[v][o] = max(acc + bias[o], 0)    epilogue 2: out[v][o] = acc * (mask[v][o] > 0)
+ * in: [B][D][H][W][cin] BF16 channels-last, cin 16 or 32; w: [27][32][cin] BF16; bias: 32 FP32
+ * (epilogue 0); mask: [B][D][H][W][32] BF16 (epilogue 2); out: [B][D][H][W][32] BF16. Device
+ * pointers, 16-byte aligned. EWG_ERR_TIMEOUT: a bounded wait in the kernel gave up. */
+ewg_status ewg_net_conv3d(int32_t cin, int32_t epilogue, int32_t B, int32_t D, int32_t H, int32_t W, const void* in,
+                          const void* w, const float* bias, const void* mask, void* out, void* stream);
+
 /* ---- batched ensemble (no reference counterpart: the reference runs one lens problem per
  * Simulator; an ensemble of permeability realizations is many such runs of
  * NewtonMethod::apply, newtonmethod.hh:308-517, with FvBaseProblem::timeIntegration's step
