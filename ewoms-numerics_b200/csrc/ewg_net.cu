@@ -379,6 +379,21 @@ bool tc_map_activations(CUtensorMap* m, const __nv_bfloat16* p, int C, const Vol
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// the same activations for row tiles: box (8, 130, 3, 1, 1), 8 channels x 130 x-positions x 3 rows,
+// no swizzle (one 16-byte row per position)
+bool tc_map_activation_rows(CUtensorMap* m, const __nv_bfloat16* p, int C, const VolDims& d) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t row = (cuuint64_t)C * 2;
+    const cuuint64_t dims[5] = {(cuuint64_t)C, (cuuint64_t)d.W, (cuuint64_t)d.H, (cuuint64_t)d.D, (cuuint64_t)d.B};
+    const cuuint64_t strides[4] = {row, row * d.W, row * d.W * d.H, row * d.W * d.H * d.D};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kTcRowX, (cuuint32_t)kTcRowY, 1, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // weights [27][COUT][CIN] as the 2-D map (CIN, 27 COUT), box (CIN, COUT): one tap per box
 bool tc_map_weights(CUtensorMap* m, const __nv_bfloat16* p, int cin, int cout) {
     EncodeTiledFn f = encode_tiled();
@@ -406,8 +421,20 @@ int* conv_tc_err_ptr() {
 
 template <int CIN, int COUT, int EPI>
 cudaError_t conv_tc_attr() {
-    return cudaFuncSetAttribute(k_conv3d_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                TcShape<CIN, COUT>::smemBytes);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcShape<CIN, COUT>::smemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv3d_tc_rows<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcRowShape<CIN, COUT>::smemBytes);
+    return e;
+}
+
+// resident CTAs per SM of a kernel at its dynamic shared memory (queried once per instance)
+int tc_resident(const void* k, int smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kTcThreads, smem) != cudaSuccess || n < 1) n = 1;
+    cudaGetLastError();
+    return n;
 }
 
 cudaError_t conv_tc_attrs() {
@@ -418,30 +445,42 @@ cudaError_t conv_tc_attrs() {
     return e;
 }
 
-// One 3x3x3 convolution (CIN -> COUT = 32, epilogue bias + ReLU or ReLU mask) on the tensor cores;
-// false when a tensor map cannot be built.
+// One 3x3x3 convolution (CIN -> COUT = 32, epilogue bias + ReLU or ReLU mask) on the tensor cores:
+// row tiles (one input box per z-tap feeds nine taps) for volumes at least kTcRowMinW wide, 32 x 4
+// patches otherwise; false when a tensor map cannot be built.
 template <int CIN, int COUT, int EPI>
 bool launch_conv_tc(cudaStream_t st, const VolDims& d, const __nv_bfloat16* in, const __nv_bfloat16* W,
                     const float* bias, const __nv_bfloat16* mask, int maskC, __nv_bfloat16* out, int outC) {
     static_assert(EPI == EPI_BIAS_RELU || EPI == EPI_MASK, "tensor-core epilogues");
     CUtensorMap mi, mw;
     int* err = conv_tc_err_ptr();
-    if (!err || !tc_map_activations(&mi, in, CIN, d) || !tc_map_weights(&mw, W, CIN, COUT)) return false;
-    const int64_t nTiles = (int64_t)d.B * d.D * ((d.H + kTcTileY - 1) / kTcTileY) * ((d.W + kTcTileX - 1) / kTcTileX);
-    static int perSM = 0, sms = 0;
-    if (perSM == 0) {
+    const bool rows = d.W >= kTcRowMinW;
+    if (!err || !tc_map_weights(&mw, W, CIN, COUT)) return false;
+    if (!(rows ? tc_map_activation_rows(&mi, in, CIN, d) : tc_map_activations(&mi, in, CIN, d))) return false;
+    static int sms = 0, perSM = 0, perSMRows = 0;
+    if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_conv3d_tc<CIN, COUT, EPI>, kTcThreads,
-                                                          TcShape<CIN, COUT>::smemBytes) != cudaSuccess || perSM < 1)
-            perSM = 1;
-        cudaGetLastError();
+        perSM = tc_resident((const void*)k_conv3d_tc<CIN, COUT, EPI>, TcShape<CIN, COUT>::smemBytes);
+        perSMRows = tc_resident((const void*)k_conv3d_tc_rows<CIN, COUT, EPI>, TcRowShape<CIN, COUT>::smemBytes);
     }
-    const int64_t full = (int64_t)sms * perSM;
-    const int grid = (int)(nTiles < full ? nTiles : full);
-    k_conv3d_tc<CIN, COUT, EPI><<<grid, kTcThreads, TcShape<CIN, COUT>::smemBytes, st>>>(
-        mi, mw, d.D, d.H, d.W, nTiles, bias, mask, maskC, out, outC, err);
+    if (rows) {
+        // row tiles: 128 consecutive voxels of one x-row
+        const int64_t nTiles = (int64_t)d.B * d.D * d.H * ((d.W + kTcRows - 1) / kTcRows);
+        const int64_t full = (int64_t)sms * perSMRows;
+        const int grid = (int)(nTiles < full ? nTiles : full);
+        k_conv3d_tc_rows<CIN, COUT, EPI><<<grid, kTcThreads, TcRowShape<CIN, COUT>::smemBytes, st>>>(
+            mi, mw, d.D, d.H, d.W, nTiles, bias, mask, maskC, out, outC, err);
+    } else {
+        // 32 x 4 patches of one z-plane
+        const int64_t nTiles =
+            (int64_t)d.B * d.D * ((d.H + kTcTileY - 1) / kTcTileY) * ((d.W + kTcTileX - 1) / kTcTileX);
+        const int64_t full = (int64_t)sms * perSM;
+        const int grid = (int)(nTiles < full ? nTiles : full);
+        k_conv3d_tc<CIN, COUT, EPI><<<grid, kTcThreads, TcShape<CIN, COUT>::smemBytes, st>>>(
+            mi, mw, d.D, d.H, d.W, nTiles, bias, mask, maskC, out, outC, err);
+    }
     return true;
 }
 
