@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
                                                            const int* __restrict__ status) {
     pdl_enter();
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
-    __shared__ double2 S[8][32];
+    __shared__ double2 SB[2][8][32];  // two tiles' box values (a tile's levels order its own)
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
     const int level = __popc(q);
     const int64_t nTiles = (P.Nb + 31) >> 5;
@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
         const int64_t b = tile * 32 + lane;
         const bool valid = b < P.Nb;
         const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+        double2 (&S)[8][32] = SB[((tile - blockIdx.x) / gridDim.x) & 1];
         double r0 = 0.0, r1 = 0.0, Lin[3][4];
         if (valid) {
             const auto ds = d[pos];
@@ -346,7 +347,8 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
                 S[q][lane] = make_double2((double)o.x, (double)o.y);
             }
         }
-        __syncthreads();  // S is reused by the next tile
+        // no barrier here: the next tile writes the other buffer, and the tile after it can only
+        // start once every warp has passed the next tile's first level barrier
     }
 }
 
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(c
                                                             const int* __restrict__ status, double w) {
     pdl_enter();
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
-    __shared__ double2 S[8][32];
+    __shared__ double2 SB[2][8][32];  // two tiles' box values (a tile's levels order its own)
     const double winv = 1.0 / w;
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
     const int level = 3 - __popc(q);
@@ -432,6 +434,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(c
         const int64_t b = tile * 32 + lane;
         const bool valid = b < P.Nb;
         const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+        double2 (&S)[8][32] = SB[((tile - blockIdx.x) / gridDim.x) & 1];
         double r0 = 0.0, r1 = 0.0, Ain[3][4], Di[4] = {0.0, 0.0, 0.0, 0.0};
         if (valid) {
             const auto ws = wv[pos];
@@ -459,7 +462,8 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(c
                 else S[q][lane] = make_double2((double)o.x * winv, (double)o.y * winv);
             }
         }
-        __syncthreads();  // S is reused by the next tile
+        // no barrier here: the next tile writes the other buffer, and the tile after it can only
+        // start once every warp has passed the next tile's first level barrier
     }
 }
 

@@ -382,63 +382,74 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3d_tc(const __grid_consta
     }
 }
 
-// ---- row tiles: one box per z-tap serves the nine (x, y) taps ------------------------------------
+// ---- row tiles ------------------------------------------------------------------------------
 //
-// For volumes at least kTcRowMinW wide, a tile is 128 consecutive voxels of one x-row (b, z, y,
-// x0 .. x0 + 127). For each z-tap dz the producer loads, per group of 8 channels, one TMA box of
-// 8 channels x 130 x-positions (x0 - 1 .. x0 + 128) x 3 rows (y - 1 .. y + 1) into one stage, with
-// no swizzle: every (x, y) position is one 16-byte row, x-positions of one row are consecutive,
-// the three rows follow each other (130 x 16 B apart) and the channel groups follow the rows. The
-// A operand of the tap (dx, dy) is then the 128 consecutive 16-byte rows starting at row
-// (dy + 1) 130 + dx + 1 of each channel group -- a K-major operand without swizzle whose 8-row
-// core matrices are 128 B apart (SBO) and whose two 8-channel halves of a K = 16 step are one
-// channel group apart (LBO; groups sit 6272 B apart so every box starts 128-byte aligned). One
-// stage thus feeds nine taps: 3 loads of (CIN / 8) x 6240 B per tile instead of 27 of
-// 128 x 2 CIN B.
+// For volumes at least kTcRowMinW wide a tile is 128 consecutive voxels of one x-row; its input
+// boxes are 130 x-positions (x0 - 1 .. x0 + 128) of one row, unswizzled: every position is one
+// 16-byte row of 8 channels, so the A operand of tap dx is the same box read from position dx + 1
+// (a K-major operand without swizzle whose 8-row core matrices are 128 B apart).
 constexpr int kTcRowMinW = 96;
-constexpr int kTcRowX = 130, kTcRowY = 3;
-constexpr int kTcBoxBytes = kTcRowX * kTcRowY * 16;     // one channel group's box (6240 B)
-constexpr int kTcGroupBytes = (kTcBoxBytes + 127) / 128 * 128;  // its place in a stage (128-byte aligned)
+constexpr int kTcRowX = 130;
+
+// ---- row tiles with a ring of input rows -----------------------------------------------------------
+//
+// A CTA walks segments of kTcSegRows consecutive output rows of one (x-tile, z, volume) column.
+// Output row y needs the input rows y - 1, y, y + 1 of the planes z - 1, z, z + 1; consecutive
+// output rows share two of the three, so the producer loads each input row once per segment: an
+// "item" is one input row y' of the three planes (3 x CIN / 8 boxes of 8 channels x 130
+// x-positions x 1 row, unswizzled) into one slot of a ring of kTcRingSlots. The MMA issuer runs
+// output row y from the items of y - 1, y, y + 1 (the A operand of tap (dx, dy, dz) is the slot of
+// row y + dy, plane z + dz, at x-offset dx + 1) and frees the item of row y - 1 after the row (a
+// segment's last row frees all three). Per 128 output voxels the shared-memory fill is one item
+// (3 x CIN / 8 x 2080 B, 25 KB for 32 channels) plus the segment's two extra rows.
+constexpr int kTcSegRows = 16;
+constexpr int kTcRingSlots = 4;
+constexpr int kTcLineBytes = kTcRowX * 16;                         // one box: 130 positions x 16 B
+constexpr int kTcLineStride = (kTcLineBytes + 127) / 128 * 128;    // 2176: boxes 128-byte aligned
 
 template <int CIN, int COUT>
-struct TcRowShape {
+struct TcRingShape {
     using S = TcShape<CIN, COUT>;
     static constexpr int groups = CIN / 8;
-    static constexpr int stages = CIN == 32 ? 2 : 4;
-    static constexpr int txBytes = groups * kTcBoxBytes;     // bytes the stage's boxes deliver
-    static constexpr int aRegion = (groups * kTcGroupBytes + 1023) / 1024 * 1024;
-    static constexpr int barOff = S::wRegion + stages * aRegion;
+    static constexpr int planeBytes = groups * kTcLineStride;      // one input row of one plane
+    static constexpr int slotBytes = 3 * planeBytes;               // one item: the row in 3 planes
+    static constexpr int txBytes = 3 * groups * kTcLineBytes;      // bytes an item's boxes deliver
+    static constexpr int barOff = S::wRegion + kTcRingSlots * slotBytes;
     static constexpr int smemBytes = barOff + 256 + 1024;
 };
 
-// descriptor of an A operand without swizzle (layout type 0): LBO = one channel group, SBO = 8 rows
-__device__ __forceinline__ uint64_t tc_smem_desc_rows(uint32_t saddr) {
-    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(kTcGroupBytes >> 4) << 16) | ((uint64_t)(128 >> 4) << 32) |
-           (1ull << 46);
+// descriptor of an A operand in a ring slot: no swizzle, LBO = one 8-channel box, SBO = 8 rows
+__device__ __forceinline__ uint64_t tc_smem_desc_line(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(kTcLineStride >> 4) << 16) |
+           ((uint64_t)(128 >> 4) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ TcTile tc_row_tile(const int D, const int H, const int W, int64_t t) {
-    const int nx = (W + kTcRows - 1) / kTcRows;
-    TcTile r;
-    r.x0 = (int)(t % nx) * kTcRows;
-    t /= nx;
-    r.y0 = (int)(t % H);
-    t /= H;
-    r.z = (int)(t % D);
-    r.b = (int)(t / D);
+struct TcSeg {
+    int b, z, y0, y1, x0;  // output rows y0 .. y1 - 1 of the column (b, z, x0 .. x0 + 127)
+};
+__device__ __forceinline__ TcSeg tc_seg(const int D, const int H, const int W, int64_t sIdx) {
+    const int nx = (W + kTcRows - 1) / kTcRows, ns = (H + kTcSegRows - 1) / kTcSegRows;
+    TcSeg r;
+    r.x0 = (int)(sIdx % nx) * kTcRows;
+    sIdx /= nx;
+    r.y0 = (int)(sIdx % ns) * kTcSegRows;
+    sIdx /= ns;
+    r.z = (int)(sIdx % D);
+    r.b = (int)(sIdx / D);
+    r.y1 = r.y0 + kTcSegRows < H ? r.y0 + kTcSegRows : H;
     return r;
 }
 
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kTcThreads, 1) k_conv3d_tc_rows(const __grid_constant__ CUtensorMap mapIn,
+__global__ void __launch_bounds__(kTcThreads, 1) k_conv3d_tc_ring(const __grid_constant__ CUtensorMap mapIn,
                                                                   const __grid_constant__ CUtensorMap mapW, int D, int H,
-                                                                  int W, int64_t nTiles, const float* __restrict__ bias,
+                                                                  int W, int64_t nSegs, const float* __restrict__ bias,
                                                                   const __nv_bfloat16* __restrict__ mask, int maskC,
                                                                   __nv_bfloat16* __restrict__ out, int outC,
                                                                   int* __restrict__ err) {
     using S = TcShape<CIN, COUT>;
-    using R = TcRowShape<CIN, COUT>;
-    constexpr int NS = R::stages;
+    using R = TcRingShape<CIN, COUT>;
+    constexpr int NS = kTcRingSlots;
     extern __shared__ unsigned char smemRaw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
     unsigned char* wS = smem;
@@ -475,16 +486,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3d_tc_rows(const __grid_c
     const uint32_t tmem = *tmemSlot;
 
     if (warp == 4 && lane == 0) {
-        // ---- TMA producer: weights, then per tile and z-tap one stage of CIN / 8 boxes
+        // ---- TMA producer: weights, then per segment the input rows y0 - 1 .. y1 as items
         tc_prefetch_map(&mapIn);
         tc_prefetch_map(&mapW);
         tc_bar_expect_tx(wBar, S::wBytes);
         for (int tap = 0; tap < 27; ++tap) tc_tma_load_2d(wS + tap * S::wTapBytes, &mapW, wBar, 0, tap * COUT);
         uint32_t it = 0;
-        for (int64_t t = blockIdx.x; t < nTiles && !tc_dead(dead); t += gridDim.x) {
-            const TcTile tl = tc_row_tile(D, H, W, t);
-            bool stop = false;
-            for (int dz = -1; dz <= 1; ++dz, ++it) {
+        bool stop = false;
+        for (int64_t sg = blockIdx.x; sg < nSegs && !stop && !tc_dead(dead); sg += gridDim.x) {
+            const TcSeg seg = tc_seg(D, H, W, sg);
+            for (int yi = seg.y0 - 1; yi <= seg.y1; ++yi, ++it) {
                 const uint32_t st = it % NS, ph = (it / NS) & 1;
                 if (it >= (uint32_t)NS && !tc_bar_wait(&empty[st], ph ^ 1)) {
                     tc_fail(err, dead, TC_ERR_EMPTY);
@@ -492,108 +503,132 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3d_tc_rows(const __grid_c
                     break;
                 }
                 tc_bar_expect_tx(&full[st], R::txBytes);
-                unsigned char* dst = aS + st * R::aRegion;
+                unsigned char* slot = aS + st * R::slotBytes;
 #pragma unroll
-                for (int g = 0; g < R::groups; ++g)
-                    tc_tma_load_5d(dst + g * kTcGroupBytes, &mapIn, &full[st], 8 * g, tl.x0 - 1, tl.y0 - 1, tl.z + dz,
-                                   tl.b);
+                for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+                    for (int g = 0; g < R::groups; ++g)
+                        tc_tma_load_5d(slot + pz * R::planeBytes + g * kTcLineStride, &mapIn, &full[st], 8 * g,
+                                       seg.x0 - 1, yi, seg.z + pz - 1, seg.b);
             }
-            if (stop) break;
         }
         const uint32_t issued = it;
         for (uint32_t k = issued > (uint32_t)NS ? issued - NS : 0; k < issued; ++k)
             if (!tc_bar_wait(&full[k % NS], (k / NS) & 1)) { tc_fail(err, dead, TC_ERR_DRAIN); break; }
         if (!tc_bar_wait(wBar, 0)) tc_fail(err, dead, TC_ERR_DRAIN);
     } else if (warp == 5 && lane == 0) {
-        // ---- MMA issuer: per stage (z-tap) the nine (x, y) taps
+        // ---- MMA issuer: output row y from the items of rows y - 1, y, y + 1
         constexpr uint32_t idesc = tc_instr_desc<COUT>();
         const uint32_t wBase = tc_smem_u32(wS), aBase = tc_smem_u32(aS);
         bool ok = tc_bar_wait(wBar, 0);
         if (!ok) tc_fail(err, dead, TC_ERR_WEIGHTS);
         tc_fence_after();
-        uint32_t it = 0, local = 0;
-        for (int64_t t = blockIdx.x; ok && t < nTiles && !tc_dead(dead); t += gridDim.x, ++local) {
-            const uint32_t acc = local & 1, accPh = (local >> 1) & 1;
-            if (local >= 2 && !tc_bar_wait(&accEmpty[acc], accPh ^ 1)) {
-                tc_fail(err, dead, TC_ERR_ACC_EMPTY);
-                break;
+        uint32_t item0 = 0, local = 0;  // first item of the segment, output rows done
+        for (int64_t sg = blockIdx.x; ok && sg < nSegs && !tc_dead(dead); sg += gridDim.x) {
+            const TcSeg seg = tc_seg(D, H, W, sg);
+            const int rows = seg.y1 - seg.y0;
+            // the segment's first two items
+            for (uint32_t k = item0; k < item0 + 2 && ok; ++k) {
+                if (!tc_bar_wait(&full[k % NS], (k / NS) & 1)) { tc_fail(err, dead, TC_ERR_FULL); ok = false; }
             }
-            tc_fence_after();
-            const uint32_t d = tmem + acc * 32;
-            for (int zt = 0; zt < 3; ++zt, ++it) {
-                const uint32_t st = it % NS, ph = (it / NS) & 1;
-                if (!tc_bar_wait(&full[st], ph)) {
+            for (int j = 0; j < rows && ok; ++j, ++local) {
+                const uint32_t acc = local & 1, accPh = (local >> 1) & 1;
+                if (local >= 2 && !tc_bar_wait(&accEmpty[acc], accPh ^ 1)) {
+                    tc_fail(err, dead, TC_ERR_ACC_EMPTY);
+                    ok = false;
+                    break;
+                }
+                const uint32_t knew = item0 + j + 2;  // input row y + 1
+                if (!tc_bar_wait(&full[knew % NS], (knew / NS) & 1)) {
                     tc_fail(err, dead, TC_ERR_FULL);
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t stage = aBase + st * R::aRegion;
+                const uint32_t d = tmem + acc * 32;
 #pragma unroll
-                for (int yx = 0; yx < 9; ++yx) {
-                    const int tap = zt * 9 + yx;         // tap = 9 (dz + 1) + 3 (dy + 1) + dx + 1
-                    const int row = (yx / 3) * kTcRowX + (yx % 3);
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint32_t slot = aBase + ((item0 + j + dy) % NS) * R::slotBytes;
 #pragma unroll
-                    for (int k = 0; k < S::kSteps; ++k) {
-                        const uint64_t ad = tc_smem_desc_rows(stage + 2 * k * kTcGroupBytes + row * 16);
-                        const uint64_t bd = tc_smem_desc<CIN, COUT>(wBase + tap * S::wTapBytes + k * 32);
-                        tc_mma_f16(d, ad, bd, idesc, tap > 0 || k > 0);
-                    }
+                    for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+                        for (int dx = 0; dx < 3; ++dx) {
+                            const int tap = pz * 9 + dy * 3 + dx;  // 9 (dz + 1) + 3 (dy + 1) + dx + 1
+#pragma unroll
+                            for (int k = 0; k < S::kSteps; ++k) {
+                                const uint64_t ad =
+                                    tc_smem_desc_line(slot + pz * R::planeBytes + 2 * k * kTcLineStride + dx * 16);
+                                const uint64_t bd = tc_smem_desc<CIN, COUT>(wBase + tap * S::wTapBytes + k * 32);
+                                tc_mma_f16(d, ad, bd, idesc, tap > 0 || k > 0);
+                            }
+                        }
                 }
-                tc_commit(&empty[st]);
+                tc_commit(&accFull[acc]);
+                // input row y - 1 is done; after the segment's last row, rows y and y + 1 too
+                tc_commit(&empty[(item0 + j) % NS]);
+                if (j == rows - 1) {
+                    tc_commit(&empty[(item0 + j + 1) % NS]);
+                    tc_commit(&empty[(item0 + j + 2) % NS]);
+                }
             }
-            if (!ok) break;
-            tc_commit(&accFull[acc]);
+            item0 += rows + 2;
         }
         tc_commit(drain);
         if (!tc_bar_wait(drain, 0)) tc_fail(err, dead, TC_ERR_DRAIN);
     } else if (warp < 4) {
-        // ---- epilogue: thread = voxel x0 + 32 warp + lane of the row
+        // ---- epilogue: thread = voxel x0 + 32 warp + lane of the output row
         float bv[COUT];
 #pragma unroll
         for (int c = 0; c < COUT; ++c) bv[c] = EPI == 0 ? bias[c] : 0.f;
         const int row = warp * 32 + lane;
         uint32_t local = 0;
-        for (int64_t t = blockIdx.x; t < nTiles; t += gridDim.x, ++local) {
-            const uint32_t acc = local & 1, accPh = (local >> 1) & 1;
-            int stop = 0;
-            if (lane == 0) stop = tc_dead(dead) ? 1 : (tc_bar_wait(&accFull[acc], accPh) ? 0 : 2);
-            stop = __shfl_sync(0xffffffffu, stop, 0);
-            if (stop == 2 && lane == 0) tc_fail(err, dead, TC_ERR_ACC_FULL);
-            if (stop) break;
-            tc_fence_after();
-            float v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + acc * 32;
-            if (COUT == 32) tc_tmem_ld32(taddr, v);
-            else tc_tmem_ld16(taddr, v);
-            tc_fence_before();
-            tc_bar_arrive(&accEmpty[acc]);
-            const TcTile tl = tc_row_tile(D, H, W, t);
-            const int x = tl.x0 + row;
-            if (x >= W) continue;
-            const int64_t vox = (((int64_t)tl.b * D + tl.z) * H + tl.y0) * W + x;
-            if (EPI == 2) {
-                const uint4* mp = reinterpret_cast<const uint4*>(mask + vox * maskC);
+        bool go = true;
+        for (int64_t sg = blockIdx.x; go && sg < nSegs; sg += gridDim.x) {
+            const TcSeg seg = tc_seg(D, H, W, sg);
+            for (int y = seg.y0; y < seg.y1; ++y, ++local) {
+                const uint32_t acc = local & 1, accPh = (local >> 1) & 1;
+                int stop = 0;
+                if (lane == 0) stop = tc_dead(dead) ? 1 : (tc_bar_wait(&accFull[acc], accPh) ? 0 : 2);
+                stop = __shfl_sync(0xffffffffu, stop, 0);
+                if (stop == 2 && lane == 0) tc_fail(err, dead, TC_ERR_ACC_FULL);
+                if (stop) {
+                    go = false;
+                    break;
+                }
+                tc_fence_after();
+                float v[32];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + acc * 32;
+                if (COUT == 32) tc_tmem_ld32(taddr, v);
+                else tc_tmem_ld16(taddr, v);
+                tc_fence_before();
+                tc_bar_arrive(&accEmpty[acc]);
+                const int x = seg.x0 + row;
+                if (x >= W) continue;
+                const int64_t vox = (((int64_t)seg.b * D + seg.z) * H + y) * W + x;
+                if (EPI == 2) {
+                    const uint4* mp = reinterpret_cast<const uint4*>(mask + vox * maskC);
+#pragma unroll
+                    for (int q = 0; q < COUT / 8; ++q) {
+                        const uint4 m4 = mp[q];
+                        const __nv_bfloat16* mb = reinterpret_cast<const __nv_bfloat16*>(&m4);
+#pragma unroll
+                        for (int jj = 0; jj < 8; ++jj)
+                            if (!(__bfloat162float(mb[jj]) > 0.f)) v[q * 8 + jj] = 0.f;
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) v[c] = fmaxf(v[c] + bv[c], 0.f);
+                }
+                uint4* op = reinterpret_cast<uint4*>(out + vox * outC);
 #pragma unroll
                 for (int q = 0; q < COUT / 8; ++q) {
-                    const uint4 m4 = mp[q];
-                    const __nv_bfloat16* mb = reinterpret_cast<const __nv_bfloat16*>(&m4);
+                    uint4 o;
+                    __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        if (!(__bfloat162float(mb[j]) > 0.f)) v[q * 8 + j] = 0.f;
+                    for (int jj = 0; jj < 4; ++jj)
+                        ob[jj] = __floats2bfloat162_rn(v[q * 8 + 2 * jj], v[q * 8 + 2 * jj + 1]);
+                    op[q] = o;
                 }
-            } else {
-#pragma unroll
-                for (int c = 0; c < COUT; ++c) v[c] = fmaxf(v[c] + bv[c], 0.f);
-            }
-            uint4* op = reinterpret_cast<uint4*>(out + vox * outC);
-#pragma unroll
-            for (int q = 0; q < COUT / 8; ++q) {
-                uint4 o;
-                __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) ob[j] = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
-                op[q] = o;
             }
         }
     }

@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_bicg_init(ENS_ARGS
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_PENDING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         double red[2] = {0.0, 0.0};  // sum b.b, max |b|
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_bicg_p(ENS_ARGS, c
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
             const bool restart = st[m].restartPending != 0;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_ilu_black_apply(EN
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
             const int64_t off = sm.off;
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_ilu_red_apply(ENS_
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
             const int64_t off = sm.off;
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_alpha(ENS_AR
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         const int64_t off = sm.off;
         double red[1] = {0.0};
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_hs(ENS_ARGS, typen
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         const double alpha = st[m].alpha;
         double red[2] = {0.0, 0.0};  // max |s|, any y != 0
@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_omega(ENS_AR
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         const int64_t off = sm.off;
         double red[2] = {0.0, 0.0};
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_xr(ENS_ARGS, typen
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
         if (m < 0) continue;
-        const Phys& P = sm.P;
+        const Phys P = sm.P;  // the fields the rows use, in registers
         const int64_t hEnd = tile_end(P, sh[1]);
         const double omega = st[m].omega;
         double red[4] = {0.0, 0.0, 0.0, 0.0};  // sum r0.r', sum r'.r', max |s|, any z != 0

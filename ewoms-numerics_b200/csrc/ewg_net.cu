@@ -379,15 +379,15 @@ bool tc_map_activations(CUtensorMap* m, const __nv_bfloat16* p, int C, const Vol
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// the same activations for row tiles: box (8, 130, 3, 1, 1), 8 channels x 130 x-positions x 3 rows,
-// no swizzle (one 16-byte row per position)
-bool tc_map_activation_rows(CUtensorMap* m, const __nv_bfloat16* p, int C, const VolDims& d) {
+// the same activations for the ring of input rows: box (8, 130, 1, 1, 1), 8 channels x 130
+// x-positions of one row, no swizzle
+bool tc_map_activation_lines(CUtensorMap* m, const __nv_bfloat16* p, int C, const VolDims& d) {
     EncodeTiledFn f = encode_tiled();
     if (!f) return false;
     const cuuint64_t row = (cuuint64_t)C * 2;
     const cuuint64_t dims[5] = {(cuuint64_t)C, (cuuint64_t)d.W, (cuuint64_t)d.H, (cuuint64_t)d.D, (cuuint64_t)d.B};
     const cuuint64_t strides[4] = {row, row * d.W, row * d.W * d.H, row * d.W * d.H * d.D};
-    const cuuint32_t box[5] = {8, (cuuint32_t)kTcRowX, (cuuint32_t)kTcRowY, 1, 1};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kTcRowX, 1, 1, 1};
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
     return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -419,22 +419,43 @@ int* conv_tc_err_ptr() {
     return p;
 }
 
+// the dynamic shared-memory limit of both tilings and the largest shared-memory carveout, so that
+// two CTAs (their 55 KB of weights and the TMA ring each) share an SM
 template <int CIN, int COUT, int EPI>
 cudaError_t conv_tc_attr() {
     cudaError_t e = cudaFuncSetAttribute(k_conv3d_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcShape<CIN, COUT>::smemBytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_conv3d_tc_rows<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TcRowShape<CIN, COUT>::smemBytes);
+        e = cudaFuncSetAttribute(k_conv3d_tc<CIN, COUT, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv3d_tc_ring<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcRingShape<CIN, COUT>::smemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv3d_tc_ring<CIN, COUT, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return e;
 }
 
-// resident CTAs per SM of a kernel at its dynamic shared memory (queried once per instance)
+// CTAs of a tensor-core convolution that fit on one SM: by shared memory (the SM's shared memory
+// over the CTA's dynamic size plus the per-block reservation) and by registers (64 K in four
+// sub-partitions of 16 K, a CTA's six warps spread two per sub-partition at most), at most 4.
+// (cudaOccupancyMaxActiveBlocksPerMultiprocessor reports 1 for these kernels although the profiler
+// shows two resident.)
 int tc_resident(const void* k, int smem) {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kTcThreads, smem) != cudaSuccess || n < 1) n = 1;
-    cudaGetLastError();
-    return n;
+    cudaFuncAttributes fa;
+    int dev = 0, smemSM = 0, resv = 0;
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smemSM, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const int bySmem = smemSM / (smem + resv);
+    const int regs = (fa.numRegs + 7) / 8 * 8;
+    const int warpsPerSubpartition = 16384 / (regs * 32);
+    const int byRegs = warpsPerSubpartition / ((kTcThreads / 32 + 3) / 4);
+    int n = bySmem < byRegs ? bySmem : byRegs;
+    if (n > 4) n = 4;
+    return n < 1 ? 1 : n;
 }
 
 cudaError_t conv_tc_attrs() {
@@ -456,22 +477,23 @@ bool launch_conv_tc(cudaStream_t st, const VolDims& d, const __nv_bfloat16* in, 
     int* err = conv_tc_err_ptr();
     const bool rows = d.W >= kTcRowMinW;
     if (!err || !tc_map_weights(&mw, W, CIN, COUT)) return false;
-    if (!(rows ? tc_map_activation_rows(&mi, in, CIN, d) : tc_map_activations(&mi, in, CIN, d))) return false;
-    static int sms = 0, perSM = 0, perSMRows = 0;
+    if (!(rows ? tc_map_activation_lines(&mi, in, CIN, d) : tc_map_activations(&mi, in, CIN, d))) return false;
+    static int sms = 0, perSM = 0, perSMRing = 0;
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         perSM = tc_resident((const void*)k_conv3d_tc<CIN, COUT, EPI>, TcShape<CIN, COUT>::smemBytes);
-        perSMRows = tc_resident((const void*)k_conv3d_tc_rows<CIN, COUT, EPI>, TcRowShape<CIN, COUT>::smemBytes);
+        perSMRing = tc_resident((const void*)k_conv3d_tc_ring<CIN, COUT, EPI>, TcRingShape<CIN, COUT>::smemBytes);
     }
     if (rows) {
-        // row tiles: 128 consecutive voxels of one x-row
-        const int64_t nTiles = (int64_t)d.B * d.D * d.H * ((d.W + kTcRows - 1) / kTcRows);
-        const int64_t full = (int64_t)sms * perSMRows;
-        const int grid = (int)(nTiles < full ? nTiles : full);
-        k_conv3d_tc_rows<CIN, COUT, EPI><<<grid, kTcThreads, TcRowShape<CIN, COUT>::smemBytes, st>>>(
-            mi, mw, d.D, d.H, d.W, nTiles, bias, mask, maskC, out, outC, err);
+        // row tiles of 128 voxels in segments of kTcSegRows rows, input rows reused through a ring
+        const int64_t nSegs = (int64_t)d.B * d.D * ((d.H + kTcSegRows - 1) / kTcSegRows) *
+                              ((d.W + kTcRows - 1) / kTcRows);
+        const int64_t full = (int64_t)sms * perSMRing;
+        const int grid = (int)(nSegs < full ? nSegs : full);
+        k_conv3d_tc_ring<CIN, COUT, EPI><<<grid, kTcThreads, TcRingShape<CIN, COUT>::smemBytes, st>>>(
+            mi, mw, d.D, d.H, d.W, nSegs, bias, mask, maskC, out, outC, err);
     } else {
         // 32 x 4 patches of one z-plane
         const int64_t nTiles =

@@ -5,8 +5,10 @@ the layer's output scale (the BF16 rounding of an FP32 sum of at most 864 produc
 input widths (16 and 32 channels), both epilogues (bias + ReLU, ReLU mask of the layer below), and
 volumes whose x / y extents are not multiples of the 32 x 4 voxel tile, where the TMA boxes reach past
 the volume and the convolution's zero padding is the copy's zero fill; volumes at least 96 wide, which
-take the row-tile kernel (one 130 x 3 box per z-tap feeding nine taps), with and without a partial last
-row tile; a batch of two volumes checks that no tap reads across volumes."""
+take the ring kernel (rows of 128 voxels in segments of 16 rows, each input row loaded once per segment
+into a ring and shared by three output rows), with and without a partial last row tile, with several
+segments per column and a last segment of one row; a batch of two volumes checks that no tap reads
+across volumes."""
 import ctypes as C
 
 import numpy as np
@@ -65,7 +67,7 @@ def _conv(lib, torch, cin, epilogue, shape, seed):
 @pytest.mark.parametrize("cin", [16, 32])
 @pytest.mark.parametrize("epilogue", [0, 2])
 @pytest.mark.parametrize("shape", [(1, 4, 8, 32), (1, 3, 5, 40), (2, 4, 7, 33), (1, 3, 5, 130), (2, 2, 3, 128),
-                                   (1, 2, 4, 200)])
+                                   (1, 2, 4, 200), (1, 2, 19, 100), (2, 1, 17, 128), (1, 3, 33, 96)])
 def test_tensor_core_conv_matches_fp64(ewg_mod, cin, epilogue, shape):
     import torch
     lib = ewg_mod.load()
