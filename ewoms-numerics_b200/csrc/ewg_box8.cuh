@@ -306,6 +306,43 @@ __device__ __forceinline__ void b8_fwd_near_all(const double2 (&S)[8][32], int l
     default: CALL(7); break;         \
     }
 
+// Forward sweep of colour C over the 32 boxes of superblocks b0 .. b0 + 31 (boxes past P.Nb are
+// idle): warp q = place q, lane = box. Every thread of the block calls it; S holds the box values.
+template <typename TM, typename TV, int C>
+__device__ __forceinline__ void b8_forward_tile(const Phys& P, const TM* __restrict__ L,
+                                                const typename V2T<TV>::type* __restrict__ d,
+                                                typename V2T<TV>::type* __restrict__ w, int64_t b0,
+                                                double2 (&S)[8][32], int lane, int q) {
+    const int level = __popc(q);
+    const int64_t b = b0 + lane;
+    const bool valid = b < P.Nb;
+    const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+    double r0 = 0.0, r1 = 0.0, Lin[3][4];
+    if (valid) {
+        const auto ds = d[pos];
+        r0 = (double)ds.x;
+        r1 = (double)ds.y;
+#define EWG_B8_CALL(Q) b8_fwd_far_all<TM, TV, C, Q>(P, L, w, b, pos, r0, r1, Lin)
+        EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+    }
+#pragma unroll
+    for (int lev = 0; lev < 4; ++lev) {
+        if (lev > 0) __syncthreads();
+        if (lev == level) {
+#define EWG_B8_CALL(Q) b8_fwd_near_all<C, Q>(S, lane, Lin, r0, r1)
+            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+            typename V2T<TV>::type o;
+            o.x = (TV)r0;
+            o.y = (TV)r1;
+            if (valid) w[pos] = o;
+            // later places read the stored (rounded) value, as the reference's vector holds it
+            S[q][lane] = make_double2((double)o.x, (double)o.y);
+        }
+    }
+}
+
 // forward sweep of colour C: w_c = d_c - sum_{k earlier} L_ck w_k
 template <typename TM, typename TV, int C>
 __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
@@ -316,40 +353,12 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
     __shared__ double2 SB[2][8][32];  // two tiles' box values (a tile's levels order its own)
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
-    const int level = __popc(q);
     const int64_t nTiles = (P.Nb + 31) >> 5;
-    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
-        const int64_t b = tile * 32 + lane;
-        const bool valid = b < P.Nb;
-        const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
-        double2 (&S)[8][32] = SB[((tile - blockIdx.x) / gridDim.x) & 1];
-        double r0 = 0.0, r1 = 0.0, Lin[3][4];
-        if (valid) {
-            const auto ds = d[pos];
-            r0 = (double)ds.x;
-            r1 = (double)ds.y;
-#define EWG_B8_CALL(Q) b8_fwd_far_all<TM, TV, C, Q>(P, L, w, b, pos, r0, r1, Lin)
-            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
-#undef EWG_B8_CALL
-        }
-#pragma unroll
-        for (int lev = 0; lev < 4; ++lev) {
-            if (lev > 0) __syncthreads();
-            if (lev == level) {
-#define EWG_B8_CALL(Q) b8_fwd_near_all<C, Q>(S, lane, Lin, r0, r1)
-                EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
-#undef EWG_B8_CALL
-                typename V2T<TV>::type o;
-                o.x = (TV)r0;
-                o.y = (TV)r1;
-                if (valid) w[pos] = o;
-                // later places read the stored (rounded) value, as the reference's vector holds it
-                S[q][lane] = make_double2((double)o.x, (double)o.y);
-            }
-        }
-        // no barrier here: the next tile writes the other buffer, and the tile after it can only
-        // start once every warp has passed the next tile's first level barrier
-    }
+    int k = 0;
+    // no barrier between tiles: the next tile writes the other buffer, and the tile after it can
+    // only start once every warp has passed the next tile's first level barrier
+    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++k)
+        b8_forward_tile<TM, TV, C>(P, L, d, w, tile * 32, SB[k & 1], lane, q);
 }
 
 // backward, before the levels: the terms of later colours, and the blocks of the same box
@@ -413,6 +422,45 @@ __device__ __forceinline__ void b8_bwd_near_all(const double2 (&S)[8][32], int l
     b8_bwd_near<C, Q, 0>(S, lane, Ain, r0, r1);
 }
 
+// Backward sweep of colour C over the 32 boxes of superblocks b0 .. b0 + 31 (as b8_forward_tile).
+template <typename TM, typename TV, int C>
+__device__ __forceinline__ void b8_backward_tile(const Phys& P, const TM* __restrict__ A, const TM* __restrict__ Dinv,
+                                                 const typename V2T<TV>::type* __restrict__ wv,
+                                                 typename V2T<TV>::type* __restrict__ y, double w, double winv,
+                                                 int64_t b0, double2 (&S)[8][32], int lane, int q) {
+    const int level = 3 - __popc(q);
+    const int64_t b = b0 + lane;
+    const bool valid = b < P.Nb;
+    const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
+    double r0 = 0.0, r1 = 0.0, Ain[3][4], Di[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+        const auto ws = wv[pos];
+        r0 = (double)ws.x;
+        r1 = (double)ws.y;
+#define EWG_B8_CALL(Q) b8_bwd_far_all<TM, TV, C, Q>(P, A, y, b, pos, winv, r0, r1, Ain)
+        EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+        load_block(Dinv, P.N, 0, pos, Di);
+    }
+#pragma unroll
+    for (int lev = 0; lev < 4; ++lev) {
+        if (lev > 0) __syncthreads();
+        if (lev == level) {
+#define EWG_B8_CALL(Q) b8_bwd_near_all<C, Q>(S, lane, Ain, r0, r1)
+            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
+#undef EWG_B8_CALL
+            const double u0 = Di[0] * r0 + Di[1] * r1, u1 = Di[2] * r0 + Di[3] * r1;
+            typename V2T<TV>::type o;
+            o.x = (TV)(w * u0);
+            o.y = (TV)(w * u1);
+            if (valid) y[pos] = o;
+            // the unscaled value as a later-colour reader recovers it from the stored one
+            if (w == 1.0) S[q][lane] = make_double2((double)o.x, (double)o.y);
+            else S[q][lane] = make_double2((double)o.x * winv, (double)o.y * winv);
+        }
+    }
+}
+
 // backward sweep of colour C: y_c = inv(D'_c) (w_c - sum_{k later} A_ck y_k), output relax * y.
 // w stays in its own vector (the preconditioned SpMV reads it again). The stored outputs of later
 // colours are relax * y; the coupling term works on unscaled y, as the reference's backward solve
@@ -425,46 +473,13 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(c
                                                             const int* __restrict__ status, double w) {
     pdl_enter();
     if (status && *status != ST_RUNNING) return;  // uniform over the grid
-    __shared__ double2 SB[2][8][32];  // two tiles' box values (a tile's levels order its own)
+    __shared__ double2 SB[2][8][32];
     const double winv = 1.0 / w;
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
-    const int level = 3 - __popc(q);
     const int64_t nTiles = (P.Nb + 31) >> 5;
-    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
-        const int64_t b = tile * 32 + lane;
-        const bool valid = b < P.Nb;
-        const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
-        double2 (&S)[8][32] = SB[((tile - blockIdx.x) / gridDim.x) & 1];
-        double r0 = 0.0, r1 = 0.0, Ain[3][4], Di[4] = {0.0, 0.0, 0.0, 0.0};
-        if (valid) {
-            const auto ws = wv[pos];
-            r0 = (double)ws.x;
-            r1 = (double)ws.y;
-#define EWG_B8_CALL(Q) b8_bwd_far_all<TM, TV, C, Q>(P, A, y, b, pos, winv, r0, r1, Ain)
-            EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
-#undef EWG_B8_CALL
-            load_block(Dinv, P.N, 0, pos, Di);
-        }
-#pragma unroll
-        for (int lev = 0; lev < 4; ++lev) {
-            if (lev > 0) __syncthreads();
-            if (lev == level) {
-#define EWG_B8_CALL(Q) b8_bwd_near_all<C, Q>(S, lane, Ain, r0, r1)
-                EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
-#undef EWG_B8_CALL
-                const double u0 = Di[0] * r0 + Di[1] * r1, u1 = Di[2] * r0 + Di[3] * r1;
-                typename V2T<TV>::type o;
-                o.x = (TV)(w * u0);
-                o.y = (TV)(w * u1);
-                if (valid) y[pos] = o;
-                // the unscaled value as a later-colour reader recovers it from the stored one
-                if (w == 1.0) S[q][lane] = make_double2((double)o.x, (double)o.y);
-                else S[q][lane] = make_double2((double)o.x * winv, (double)o.y * winv);
-            }
-        }
-        // no barrier here: the next tile writes the other buffer, and the tile after it can only
-        // start once every warp has passed the next tile's first level barrier
-    }
+    int k = 0;
+    for (int64_t tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++k)
+        b8_backward_tile<TM, TV, C>(P, A, Dinv, wv, y, w, winv, tile * 32, SB[k & 1], lane, q);
 }
 
 #undef EWG_B8_PLACE_SWITCH

@@ -25,9 +25,13 @@
 //     class, the number of resident blocks (multiples of the SM count) and, for the assembly,
 //     the register budget variant, and keeps the fastest. Sum reductions do not depend on the
 //     launch shape, so results do not depend on the tuning.
-//   * Newton runs per member on the host in lockstep rounds: each round linearizes the members
-//     still iterating, solves the ones that need a correction and updates them; a member whose
-//     step fails is restored and restarts with half the step size.
+//   * ILU(0) order: red-black, or the single problem's box-8-colour order (ewg_box8.cuh) when every
+//     member's grid has it; the box-8 solve keeps each member's BiCGStab vectors in its box-8 order.
+//   * Newton runs per member in supersteps: each superstep linearizes the members still iterating,
+//     solves the ones that need a correction and updates them; a member whose step fails is
+//     restored and restarts with half the step size. The decisions are taken either on the host
+//     between supersteps (ewg_ensemble_advance) or on the device, with whole supersteps replayed by
+//     a CUDA graph WHILE node (ewg_ensemble_advance_device).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +39,7 @@
 #include <vector>
 
 #include "ewg_assemble.cuh"
+#include "ewg_box8.cuh"
 #include "ewg_krylov.cuh"
 
 namespace {
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(kEnsTile, MINB) ke_assemble(
 }
 
 // x0 -= dx for the members in mask (newtonmethod.hh:743-809); a non-finite dx sets flags[m] bit 2
-template <typename T>
+template <typename T, bool B8>
 __global__ void __launch_bounds__(kEnsTile) ke_update(ENS_ARGS, const int* __restrict__ mask, double2* __restrict__ x0,
                                                       const typename V2T<T>::type* __restrict__ dx,
                                                       int* __restrict__ flags) {
@@ -281,13 +286,14 @@ __global__ void __launch_bounds__(kEnsTile) ke_update(ENS_ARGS, const int* __res
             int bad = 0;
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = sm.off + col * P.Nh + h;
+                const int64_t sx = B8 ? sm.off + b8_to_split_pos(P, col * P.Nh + h) : s;  // dx is in solver order
                 const auto d = dx[s];
                 const double d0 = (double)d.x, d1 = (double)d.y;
                 if (!isfinite(d0) || !isfinite(d1)) bad = 1;
-                double2 v = x0[s];
+                double2 v = x0[sx];
                 v.x -= d0;
                 v.y -= d1;
-                x0[s] = v;
+                x0[sx] = v;
             }
             if (bad) atomicOr(&flags[m], 2);
         }
@@ -332,8 +338,8 @@ __global__ void __launch_bounds__(kEnsTile) ke_ilu_black_factor(ENS_ARGS, const 
     }
 }
 
-// b = (T) r for the members in mask
-template <typename T>
+// b = (T) r for the members in mask (B8: b in box-8 order)
+template <typename T, bool B8>
 __global__ void __launch_bounds__(kEnsTile) ke_rhs(ENS_ARGS, const int* __restrict__ mask, const double2* __restrict__ r,
                                                    typename V2T<T>::type* __restrict__ b) {
     __shared__ EnsMember sm;
@@ -345,7 +351,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_rhs(ENS_ARGS, const int* __restri
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = sm.off + col * P.Nh + h;
-                const double2 v = r[s];
+                const double2 v = r[B8 ? sm.off + b8_to_split_pos(P, col * P.Nh + h) : s];
                 typename V2T<T>::type o;
                 o.x = (T)v.x;
                 o.y = (T)v.y;
@@ -492,11 +498,15 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_ilu_red_apply(ENS_
 }
 
 // v = A y; alpha = rho_i / (r0hat . v)
-template <typename T>
+// B8: box-8 order, v = A y from the sweeps' intermediate w (spmv_row_b8_precond: J is the box-8
+// copy A8, E8 = A_cc - D', W the forward sweep's output)
+template <typename T, bool B8>
 __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_alpha(ENS_ARGS, const T* __restrict__ J,
                                                           const typename V2T<T>::type* __restrict__ y,
                                                           const typename V2T<T>::type* __restrict__ r0,
-                                                          typename V2T<T>::type* __restrict__ v, ENS_BICG_ARGS) {
+                                                          typename V2T<T>::type* __restrict__ v,
+                                                          const T* __restrict__ E8,
+                                                          const typename V2T<T>::type* __restrict__ W, ENS_BICG_ARGS) {
     __shared__ EnsMember sm;
     __shared__ int sh[2];
     ENS_TILE_LOOP {
@@ -510,7 +520,9 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_alpha(ENS_AR
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = col * P.Nh + h;
                 double a0, a1;
-                spmv_row<T, T>(P, J + kEnsBands * 4 * off, y + off, s, a0, a1);
+                if (B8) spmv_row_b8_precond<T, T>(P, J + kEnsBands * 4 * off, E8 + 4 * off, W + off, st[m].w, y + off, s,
+                                                  a0, a1);
+                else spmv_row<T, T>(P, J + kEnsBands * 4 * off, y + off, s, a0, a1);
                 typename V2T<T>::type o;
                 o.x = (T)a0; o.y = (T)a1;
                 v[off + s] = o;
@@ -571,11 +583,13 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_hs(ENS_ARGS, typen
 }
 
 // t = A z; omega = (t . s) / (t . t)
-template <typename T>
+template <typename T, bool B8>
 __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_omega(ENS_ARGS, const T* __restrict__ J,
                                                           const typename V2T<T>::type* __restrict__ z,
                                                           const typename V2T<T>::type* __restrict__ sres,
-                                                          typename V2T<T>::type* __restrict__ tv, ENS_BICG_ARGS) {
+                                                          typename V2T<T>::type* __restrict__ tv,
+                                                          const T* __restrict__ E8,
+                                                          const typename V2T<T>::type* __restrict__ W, ENS_BICG_ARGS) {
     __shared__ EnsMember sm;
     __shared__ int sh[2];
     ENS_TILE_LOOP {
@@ -589,7 +603,9 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_spmv_omega(ENS_AR
             for (int col = 0; col < 2; ++col) {
                 const int64_t s = col * P.Nh + h;
                 double a0, a1;
-                spmv_row<T, T>(P, J + kEnsBands * 4 * off, z + off, s, a0, a1);
+                if (B8) spmv_row_b8_precond<T, T>(P, J + kEnsBands * 4 * off, E8 + 4 * off, W + off, st[m].w, z + off, s,
+                                                  a0, a1);
+                else spmv_row<T, T>(P, J + kEnsBands * 4 * off, z + off, s, a0, a1);
                 typename V2T<T>::type o;
                 o.x = (T)a0; o.y = (T)a1;
                 tv[off + s] = o;
@@ -654,6 +670,114 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_xr(ENS_ARGS, typen
             s->iter += 1;
             iteration_top(s, out[0], out[1]);
         }
+    }
+}
+
+// ---- box-8-colour ILU(0) for ensembles whose members all have that order -------------------------
+//
+// The single-problem box-8 factorization and sweeps (ewg_box8.cuh) per member: each member's
+// Jacobian is copied into its box-8 order (stride N_m, the member's block of planes), and during
+// the solve every BiCGStab vector of a member is in that order (the right-hand side is converted
+// on the way in, the correction on the way out). A tile of kEnsTileH half indices of a member is
+// kEnsTileH / 32 superblocks of it, so the sweeps take a tile as kEnsTileH / 1024 blocks of 32
+// boxes and the factorization as one thread per superblock.
+
+constexpr int kEnsB8Sub = kEnsTileH / 1024;  // 32-box sub-tiles of a tile
+
+// A8 = J in box-8 order (28 planes per member)
+template <typename T>
+__global__ void __launch_bounds__(kEnsTile) ke_b8_matrix(ENS_ARGS, const int* __restrict__ mask, const T* __restrict__ J,
+                                                         T* __restrict__ A8) {
+    __shared__ EnsMember sm;
+    __shared__ int sh[2];
+    ENS_TILE_LOOP {
+        if (begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh) < 0) continue;
+        const Phys P = sm.P;
+        const int64_t hEnd = tile_end(P, sh[1]);
+        const T* Jm = J + kEnsBands * 4 * sm.off;
+        T* Am = A8 + kEnsBands * 4 * sm.off;
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
+            for (int col = 0; col < 2; ++col) {
+                const int64_t s8 = col * P.Nh + h, sp = b8_to_split_pos(P, s8);
+                for (int pl = 0; pl < kEnsBands * 4; ++pl) Am[(int64_t)pl * P.N + s8] = Jm[(int64_t)pl * P.N + sp];
+            }
+    }
+}
+
+// factorization of colour C: one thread per superblock of the tile; a singular pivot sets bit 4
+template <typename T, int C>
+__global__ void __launch_bounds__(kEnsTile) ke_b8_factor(ENS_ARGS, const int* __restrict__ mask, const T* __restrict__ A8,
+                                                         T* __restrict__ Dinv8, T* __restrict__ L8, T* __restrict__ E8,
+                                                         int* __restrict__ flags) {
+    __shared__ EnsMember sm;
+    __shared__ int sh[2];
+    ENS_TILE_LOOP {
+        const int m = begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh);
+        if (m < 0) continue;
+        const Phys P = sm.P;
+        const int64_t b = sh[1] / 32 + threadIdx.x;
+        if (threadIdx.x >= kEnsTileH / 32 || b >= P.Nb) continue;
+        const int64_t off = sm.off;
+        const T* A = A8 + kEnsBands * 4 * off;
+        T* Di = Dinv8 + 4 * off;
+        T* L = L8 + 24 * off;
+        T* E = E8 + 4 * off;
+        const Box8Pos bp = b8_box(P, (uint32_t)b);
+        double dinvBox[8][4];
+        bool ok = true;
+        ok &= b8_factor_cell<T, C, 0>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 1>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 2>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 3>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 4>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 5>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 6>(P, A, Di, L, E, b, bp, dinvBox);
+        ok &= b8_factor_cell<T, C, 7>(P, A, Di, L, E, b, bp, dinvBox);
+        if (!ok) atomicOr(&flags[m], 4);
+    }
+}
+
+// forward sweep of colour C for the running members: w = (D' + L_A)^-1 d, colour C's cells
+template <typename T, int C>
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_forward(ENS_ARGS, const T* __restrict__ L8,
+                                                                         const typename V2T<T>::type* __restrict__ d,
+                                                                         typename V2T<T>::type* __restrict__ w,
+                                                                         const BiState* __restrict__ st) {
+    __shared__ EnsMember sm;
+    __shared__ int sh[2];
+    __shared__ double2 SB[2][8][32];
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    int k = 0;
+    ENS_TILE_LOOP {
+        if (begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh) < 0) continue;
+        const Phys P = sm.P;
+        const int64_t off = sm.off;
+        for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k)
+            b8_forward_tile<T, T, C>(P, L8 + 24 * off, d + off, w + off, sh[1] / 32 + sub * 32, SB[k & 1], lane, q);
+    }
+}
+
+// backward sweep of colour C: y = relax (D')^-1 (w - U_A y / relax), colour C's cells
+template <typename T, int C>
+__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_backward(ENS_ARGS, const T* __restrict__ A8,
+                                                                          const T* __restrict__ Dinv8,
+                                                                          const typename V2T<T>::type* __restrict__ wv,
+                                                                          typename V2T<T>::type* __restrict__ y,
+                                                                          const BiState* __restrict__ st) {
+    __shared__ EnsMember sm;
+    __shared__ int sh[2];
+    __shared__ double2 SB[2][8][32];
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    int k = 0;
+    ENS_TILE_LOOP {
+        const int m = begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh);
+        if (m < 0) continue;
+        const Phys P = sm.P;
+        const int64_t off = sm.off;
+        const double w = st[m].w;
+        for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k)
+            b8_backward_tile<T, T, C>(P, A8 + kEnsBands * 4 * off, Dinv8 + 4 * off, wv + off, y + off, w, 1.0 / w,
+                                      sh[1] / 32 + sub * 32, SB[k & 1], lane, q);
     }
 }
 
@@ -746,6 +870,10 @@ struct ewg_ensemble {
     // BiCGStab chunk graph
     cudaGraphExec_t graphExec = nullptr;
     double relaxation = 1.0;
+    // box-8-colour ILU(0) (every member's grid has the order): the solve runs in box-8 order
+    bool b8 = false;
+    bool b8ok = false;         // every member has the order
+    void *A8 = nullptr, *L8 = nullptr, *Dinv8 = nullptr, *E8 = nullptr, *W8 = nullptr;
     // device scheduler of ewg_ensemble_advance_device (allocated on its first call)
     ewg::RunD* dRun = nullptr;
     ewg::SchedD* dSched = nullptr;
@@ -792,16 +920,45 @@ struct Ops {
         ke_intensive<<<e->grid[EC_INTENSIVE], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->x0,
                                                                         e->lens, e->iq);
     }
+    template <int C>
+    static void b8_factor_colour(ewg_ensemble* e, int g) {
+        ke_b8_factor<T, C><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->A8), m(e->Dinv8),
+                                                         m(e->L8), m(e->E8), e->flagsF);
+    }
     static void factor(ewg_ensemble* e) {
         const int g = e->grid[EC_FACTOR];
+        if (e->b8) {
+            ke_b8_matrix<T><<<e->grid[EC_CELL], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J),
+                                                                         m(e->A8));
+            b8_factor_colour<0>(e, g);
+            b8_factor_colour<1>(e, g);
+            b8_factor_colour<2>(e, g);
+            b8_factor_colour<3>(e, g);
+            b8_factor_colour<4>(e, g);
+            b8_factor_colour<5>(e, g);
+            b8_factor_colour<6>(e, g);
+            b8_factor_colour<7>(e, g);
+            return;
+        }
         ke_diag_inverse_red<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J), m(e->Dinv),
                                                              e->flagsF);
         ke_ilu_black_factor<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J), m(e->Dinv),
                                                              m(e->L), e->flagsF);
     }
+    // box-8 sweeps of all colours for the running members: W = forward(d), y = backward(W)
+    template <int C>
+    static void b8_fwd(ewg_ensemble* e, int g, const VT<T>* d) {
+        ke_b8_forward<T, C><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlB.d, e->tlB.dn, m(e->L8), d, v(e->W8), e->st);
+    }
+    template <int C>
+    static void b8_bwd(ewg_ensemble* e, int g, VT<T>* y) {
+        ke_b8_backward<T, C><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlB.d, e->tlB.dn, m(e->A8), m(e->Dinv8), v(e->W8), y,
+                                                           e->st);
+    }
     static void rhs_init(ewg_ensemble* e) {
         const int g = e->grid[EC_CELL];
-        ke_rhs<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->r, v(e->kb));
+        if (e->b8) ke_rhs<T, true><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->r, v(e->kb));
+        else ke_rhs<T, false><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->r, v(e->kb));
         ke_bicg_init<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, v(e->kb), v(e->kx), v(e->kr),
                                                       v(e->kr0), v(e->kv), v(e->kp), e->st, e->partials, e->counters);
     }
@@ -815,18 +972,36 @@ struct Ops {
                                                            v(E->kp), E->st);
                 break;
             case EC_ILU_BLACK:
+                if (E->b8) {  // the forward sweeps (d = p or s, into W)
+                    const VT<T>* d = which ? v(E->kr) : v(E->kp);
+                    b8_fwd<0>(E, g, d); b8_fwd<1>(E, g, d); b8_fwd<2>(E, g, d); b8_fwd<3>(E, g, d);
+                    b8_fwd<4>(E, g, d); b8_fwd<5>(E, g, d); b8_fwd<6>(E, g, d); b8_fwd<7>(E, g, d);
+                    break;
+                }
                 ke_ilu_black_apply<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->Dinv), m(E->L),
                                                                     which ? v(E->kr) : v(E->kp),
                                                                     which ? v(E->kz) : v(E->ky), E->st);
                 break;
             case EC_ILU_RED:
+                if (E->b8) {  // the backward sweeps (from W into y or z)
+                    VT<T>* y = which ? v(E->kz) : v(E->ky);
+                    b8_bwd<7>(E, g, y); b8_bwd<6>(E, g, y); b8_bwd<5>(E, g, y); b8_bwd<4>(E, g, y);
+                    b8_bwd<3>(E, g, y); b8_bwd<2>(E, g, y); b8_bwd<1>(E, g, y); b8_bwd<0>(E, g, y);
+                    break;
+                }
                 ke_ilu_red_apply<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->J), m(E->Dinv),
                                                                   which ? v(E->kr) : v(E->kp),
                                                                   which ? v(E->kz) : v(E->ky), E->st);
                 break;
             case EC_SPMV_ALPHA:
-                ke_spmv_alpha<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->J), v(E->ky),
-                                                               v(E->kr0), v(E->kv), E->st, E->partials, E->counters);
+                if (E->b8)
+                    ke_spmv_alpha<T, true><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->A8), v(E->ky),
+                                                                         v(E->kr0), v(E->kv), m(E->E8), v(E->W8), E->st,
+                                                                         E->partials, E->counters);
+                else
+                    ke_spmv_alpha<T, false><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->J), v(E->ky),
+                                                                          v(E->kr0), v(E->kv), nullptr, nullptr, E->st,
+                                                                          E->partials, E->counters);
                 break;
             case EC_HS:
                 ke_hs<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, v(E->kx), v(E->ky), v(E->kr),
@@ -834,8 +1009,14 @@ struct Ops {
                 break;
             case EC_SPMV_OMEGA:
                 // t is stored in y (free after h)
-                ke_spmv_omega<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->J), v(E->kz),
-                                                               v(E->kr), v(E->ky), E->st, E->partials, E->counters);
+                if (E->b8)
+                    ke_spmv_omega<T, true><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->A8), v(E->kz),
+                                                                         v(E->kr), v(E->ky), m(E->E8), v(E->W8), E->st,
+                                                                         E->partials, E->counters);
+                else
+                    ke_spmv_omega<T, false><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->J), v(E->kz),
+                                                                          v(E->kr), v(E->ky), nullptr, nullptr, E->st,
+                                                                          E->partials, E->counters);
                 break;
             case EC_XR:
                 ke_xr<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, v(E->kx), v(E->kz), v(E->kr),
@@ -857,8 +1038,12 @@ struct Ops {
         kernel(e, EC_XR, 0);
     }
     static void update(ewg_ensemble* e) {
-        ke_update<T><<<e->grid[EC_CELL], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->x0, v(e->kx),
-                                                                  e->flagsU);
+        if (e->b8)
+            ke_update<T, true><<<e->grid[EC_CELL], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->x0,
+                                                                            v(e->kx), e->flagsU);
+        else
+            ke_update<T, false><<<e->grid[EC_CELL], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->x0,
+                                                                             v(e->kx), e->flagsU);
     }
 };
 
@@ -874,7 +1059,7 @@ void default_grids(ewg_ensemble* e) {
     const void* ks[EC_NUM] = {
         (const void*)ke_intensive, (const void*)ke_assemble<T, true, 3>, (const void*)ke_ilu_black_factor<T>,
         (const void*)ke_bicg_init<T>, (const void*)ke_ilu_black_apply<T>, (const void*)ke_ilu_red_apply<T>,
-        (const void*)ke_spmv_alpha<T>, (const void*)ke_spmv_omega<T>, (const void*)ke_bicg_p<T>, (const void*)ke_hs<T>,
+        (const void*)ke_spmv_alpha<T, false>, (const void*)ke_spmv_omega<T, false>, (const void*)ke_bicg_p<T>, (const void*)ke_hs<T>,
         (const void*)ke_xr<T>};
     for (int c = 0; c < EC_NUM; ++c) {
         int g = e->numSMs * resident_blocks(ks[c]);
@@ -966,6 +1151,33 @@ ewg_status build_graph(ewg_ensemble* e) {
     c = cudaGraphInstantiate(&e->graphExec, g, 0);
     cudaGraphDestroy(g);
     return ens_fail(e, c, "instantiate graph");
+}
+
+// The ILU(0) order of the solves: box-8-colour when every member's grid has it (ilu_ordering AUTO or
+// BOX8; BOX8 on an ensemble where some member lacks it is an error), else red-black. A change of
+// order drops the captured BiCGStab graph; the box-8 copies of the matrix are allocated on first use.
+ewg_status ens_set_order(ewg_ensemble* e, const ewg_solve_opts* o) {
+    if (o->ilu_ordering == EWG_ILU_ORDER_BOX8 && !e->b8ok) {
+        e->err = "box-8 ILU ordering needs every member's nx, ny, nz to be multiples of 4";
+        return EWG_ERR_INVALID;
+    }
+    const bool want = e->b8ok && (o->ilu_ordering == EWG_ILU_ORDER_AUTO || o->ilu_ordering == EWG_ILU_ORDER_BOX8);
+    if (want && !e->A8) {
+        const size_t sT = e->precision == EWG_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+        const int64_t n = e->total;
+        cudaError_t c = cudaMalloc(&e->A8, sT * kEnsBands * 4 * n);
+        if (c == cudaSuccess) c = cudaMalloc(&e->L8, sT * 24 * n);
+        if (c == cudaSuccess) c = cudaMalloc(&e->Dinv8, sT * 4 * n);
+        if (c == cudaSuccess) c = cudaMalloc(&e->E8, sT * 4 * n);
+        if (c == cudaSuccess) c = cudaMalloc(&e->W8, sT * 2 * n);
+        if (c != cudaSuccess) return ens_fail(e, c, "allocate box-8 ILU");
+    }
+    if (want != e->b8 && e->graphExec) {
+        cudaGraphExecDestroy(e->graphExec);
+        e->graphExec = nullptr;
+    }
+    e->b8 = want;
+    return EWG_OK;
 }
 
 BiState bicg_template(const ewg_solve_opts* o) {
@@ -1075,6 +1287,7 @@ ewg_status ensemble_advance(ewg_ensemble* e, int steps, const double* dt, const 
                             const ewg_solve_opts* so, ewg_ensemble_report* rep, ewg_ensemble_stats* stats) {
     const int M = e->M;
     const int maxDiv = e->maxDiv;
+    if (ewg_status o = ens_set_order(e, so)) return o;
     std::vector<MemberRun> mr(M);
     for (int m = 0; m < M; ++m) {
         if (!(dt[m] > 0)) { e->err = "dt must be positive"; return EWG_ERR_INVALID; }
@@ -1581,6 +1794,7 @@ ewg_status ensemble_advance_device(ewg_ensemble* e, int steps, const double* dt,
     const int M = e->M;
     for (int m = 0; m < M; ++m)
         if (!(dt[m] > 0)) { e->err = "dt must be positive"; return EWG_ERR_INVALID; }
+    if (ewg_status o = ens_set_order(e, so)) return o;
     ewg_status s = ensure_sched(e);
     if (s) return s;
     cudaError_t c;
@@ -1662,6 +1876,7 @@ ewg_status ensemble_advance_device(ewg_ensemble* e, int steps, const double* dt,
 // Time every launch shape of each kernel class on the current state and keep the fastest.
 template <typename T>
 ewg_status autotune(ewg_ensemble* e, const double* dt, const ewg_solve_opts* so) {
+    if (ewg_status o = ens_set_order(e, so)) return o;
     std::vector<int> all(e->M);
     for (int m = 0; m < e->M; ++m) {
         all[m] = m;
@@ -1771,7 +1986,8 @@ void ewg_ensemble_destroy(ewg_ensemble* e) {
     void* ps[] = {e->dm, e->x0, e->x1, e->sold, e->r, e->stage, e->perm, e->lens, e->iq, e->geo, e->J,
                   e->Dinv, e->L, e->kx, e->kr, e->kr0, e->kv, e->kp, e->ky, e->kz, e->kb, e->partials, e->counters,
                   e->st, e->stSave, e->mask, e->errmax, e->flags, e->flagsF, e->flagsU, e->dtArr,
-                  e->dRun, e->dSched, e->dPrefix, e->dTilesAll, e->maskF, e->maskA, e->maskS};
+                  e->dRun, e->dSched, e->dPrefix, e->dTilesAll, e->maskF, e->maskA, e->maskS,
+                  e->A8, e->L8, e->Dinv8, e->E8, e->W8};
     for (void* p : ps)
         if (p) cudaFree(p);
     void* hs[] = {e->hSt, e->hMask, e->hErr, e->hFlags, e->hFlagsF, e->hFlagsU, e->hDt, e->hRun, e->hSched};
@@ -1877,6 +2093,8 @@ ewg_status ewg_ensemble_create(int32_t members, const ewg_grid* grids, const ewg
         off += em.P.N;
     }
     e->nTiles = (int)e->hTiles.size();
+    e->b8ok = true;
+    for (int m = 0; m < members; ++m) e->b8ok = e->b8ok && e->hm[m].P.b8ok;
     const bool mixed = e->precision == EWG_PRECISION_MIXED;
     const size_t sT = mixed ? sizeof(float) : sizeof(double);
     const size_t sV = 2 * sT;

@@ -229,3 +229,67 @@ def test_device_scheduled_halving_and_failure(ewg_mod):
     host, dev = _advance_pair(ewg_mod, cases, dts, 2, ewg_mod.PRECISION_FP64, so, no=no, max_divisions=1)
     assert host[0] == ewg_mod.EWG_ERR_NOT_CONVERGED and host[1][0].status != 0 and host[1][1].status == 0
     _same_run(host, dev)
+
+
+SIZES8 = [(8, 8, 4), (12, 8, 8), (16, 12, 8)]  # every extent a multiple of 4: box-8-colour ILU(0)
+
+
+def _cases8(ewg):
+    return [ewg.lens3d_case(nx, ny, nz, seed=20 + k, sigma=0.5 + 0.5 * k, corr_cells=2.0 + k)
+            for k, (nx, ny, nz) in enumerate(SIZES8)]
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_box8_ensemble_matches_single_problems(ewg_mod, device):
+    """With every member's grid in box-8 order the ensemble solves with the box-8-colour ILU(0)
+    (ilu_ordering AUTO), as the single problem does on those grids: three FP64 steps give the same
+    Newton iteration counts per member as the single-problem runs, BiCGStab counts within 15 %, and
+    fields within 1e-8; the red-black order stays selectable and needs more BiCGStab iterations."""
+    cases = _cases8(ewg_mod)
+    so = _fp64_opts(ewg_mod)
+    ens = ewg_mod.Ensemble(cases, precision=ewg_mod.PRECISION_FP64, check_interval=4)
+    ens.apply_initial_solution()
+    st, reps, _ = ens.advance(3, DTS, sopts=so, device=device)
+    assert st == 0
+    rb = ewg_mod.Ensemble(cases, precision=ewg_mod.PRECISION_FP64, check_interval=4)
+    rb.apply_initial_solution()
+    st2, reps_rb, _ = rb.advance(3, DTS, sopts=_fp64_opts(ewg_mod, ilu_ordering=ewg_mod.ILU_ORDER_REDBLACK),
+                                 device=device)
+    assert st2 == 0
+    for m, c in enumerate(cases):
+        sreps, x = _run_single(ewg_mod, c, DTS[m], 3, so)
+        assert reps[m].newton_iterations == sum(r.iterations for r in sreps), m
+        lin = sum(r.linear_iterations for r in sreps)
+        assert abs(reps[m].linear_iterations - lin) <= max(3, 0.15 * lin), (reps[m].linear_iterations, lin)
+        xe = ens.get_solution(m, 0)
+        assert rel_close(xe[:, 0], x[:, 0], 1e-8)[0]
+        assert np.max(np.abs(xe[:, 1] - x[:, 1])) <= 1e-8
+        assert reps[m].linear_iterations < reps_rb[m].linear_iterations, (m, reps[m].linear_iterations,
+                                                                          reps_rb[m].linear_iterations)
+    ens.close()
+    rb.close()
+
+
+def test_box8_ensemble_mixed_and_rejection(ewg_mod):
+    """The mixed-precision box-8 ensemble reaches the Newton tolerance with S_w within 1e-6 of the
+    FP64 single problem, the host and device schedulers give the same bits, and requesting the box-8
+    order on an ensemble with a member that lacks it is rejected."""
+    cases = _cases8(ewg_mod)
+    so = ewg_mod.default_solve_opts(precision=ewg_mod.PRECISION_MIXED, linear_solver_tolerance=1e-3,
+                                    verify_true_residual=0)
+    host, dev = _advance_pair(ewg_mod, cases, DTS, 3, ewg_mod.PRECISION_MIXED, so)
+    assert host[0] == 0 and all(r.status == 0 and r.error <= 1e-8 for r in host[1])
+    _same_run(host, dev)
+    for m, c in enumerate(cases):
+        _, x = _run_single(ewg_mod, c, DTS[m], 3, _fp64_opts(ewg_mod))
+        xe = host[3][m][0]
+        assert rel_close(xe[:, 0], x[:, 0], 1e-8)[0]
+        assert np.max(np.abs(xe[:, 1] - x[:, 1])) <= 1e-6
+    mixed_cases = _cases8(ewg_mod)[:2] + [_cases(ewg_mod)[1]]  # 12x8x6 lacks the order
+    ens = ewg_mod.Ensemble(mixed_cases, precision=ewg_mod.PRECISION_FP64)
+    ens.apply_initial_solution()
+    st, _, _ = ens.advance(1, DTS, sopts=_fp64_opts(ewg_mod, ilu_ordering=ewg_mod.ILU_ORDER_BOX8), check=False)
+    assert st == ewg_mod.EWG_ERR_INVALID
+    st, reps, _ = ens.advance(1, DTS, sopts=_fp64_opts(ewg_mod))  # AUTO: red-black for all
+    assert st == 0 and all(r.status == 0 for r in reps)
+    ens.close()
