@@ -30,6 +30,16 @@ import numpy as np  # noqa: E402
 
 METRIC = "s per implicit time step, plain FP64 vs learned+mixed (same Newton tol); Mcells/s"
 FALLBACK_HBM_GBS = 6650.0
+# The reference's own CPU step on the 256x256x128 workload is composed from timed phases (an
+# 8.39 M-cell implicit step of the sequential natural-order ILU(0) BiCGStab takes over an hour).
+# Its iteration counts: Newton per step as measured on the device for this workload (steps 4-6 of
+# the plain path: 11, 11, 10; the oracle takes the same Newton counts as the device in every
+# parity test), and BiCGStab per step = the device's box-8-colour count (3556, 3512, 3133) times
+# the natural order's share of it, 2163 / 2461 = 0.879 (the oracle's first implicit step of the
+# 128x128x64 lens in both orders).
+NATURAL_OVER_BOX8 = 2163.0 / 2461.0
+REF_NEWTON_PER_STEP = (11 + 11 + 10) / 3.0
+REF_BICGSTAB_PER_STEP = (3556 + 3512 + 3133) / 3.0 * NATURAL_OVER_BOX8
 
 
 def parse():
@@ -51,6 +61,8 @@ def parse():
     ap.add_argument("--ensemble-scheduler", default="device", choices=["device", "host"],
                     help="device: Newton / step decisions on the device, supersteps in a CUDA graph WHILE node")
     ap.add_argument("--no-vcfv", action="store_true")
+    ap.add_argument("--no-conv", action="store_true")
+    ap.add_argument("--conv", action="store_true", help="time only the guess network's tensor-core convolutions")
     return ap.parse_args()
 
 
@@ -335,7 +347,8 @@ def cpu_baseline_block(case, x, gpu, steps_its):
     N = case.n_cells
     ph = cpu_phases_full(case, x)
     n_newton = float(np.mean([a for a, _ in steps_its]))
-    n_bicg = float(np.mean([b for _, b in steps_its]))
+    # the timed steps ran the box-8-colour ILU(0); the reference's natural order needs fewer
+    n_bicg = float(np.mean([b for _, b in steps_its])) * NATURAL_OVER_BOX8
     # a step: one linearization and one ILU(0) factorization per Newton iteration, one BiCGStab
     # iteration per counted iteration (the last linearization of a step is not solved)
     s_step = n_newton * ph["s_per_linearization"] + (n_newton - 1) * ph["s_ilu_factorization"] + \
@@ -359,7 +372,8 @@ def cpu_baseline_block(case, x, gpu, steps_its):
                        f"natural-order block-ILU(0) BiCGStab iterations (sequential, as one reference rank); "
                        f"value = cells / composed step time, the step composed of {n_newton:.1f} "
                        f"linearizations, {n_newton - 1:.1f} ILU(0) factorizations and {n_bicg:.0f} BiCGStab "
-                       f"iterations (the means of the timed GPU steps, red-black ILU(0))"),
+                       f"iterations (the means of the timed GPU steps; their box-8-colour BiCGStab count times "
+                       f"{NATURAL_OVER_BOX8:.3f}, the natural order's share measured by the oracle at 128x128x64)"),
             "s_per_step_composed": s_step, "phases": ph, "gpu_over_cpu": phases,
             "vcfv_linearization": cpu_vcfv_linearization()}
 
@@ -368,39 +382,66 @@ def cpu_baseline_block(case, x, gpu, steps_its):
 
 
 def run_reference(args, rank, world, pg):
-    """The reference's CPU path: the oracle restatement on the host cores (the reference itself
-    needs DUNE / ewoms-material, absent here)."""
+    """The reference's CPU path on the bench's own workload (the 256x256x128 lens, seed 0): the
+    oracle restatement on the host cores (the reference itself needs DUNE / ewoms-material, absent
+    here). A timed step is a bounded sample of an implicit step: one AD linearization with the element
+    loop on all cores (the reference's ThreadsPerProcess tasklets) and one natural-order block-ILU(0)
+    factorization + BiCGStab iteration (sequential, as one reference rank runs dune-istl); the step
+    time is composed from the sampled phase times with REF_NEWTON_PER_STEP linearizations and
+    factorizations and REF_BICGSTAB_PER_STEP iterations, the per-iteration time measured once
+    before the timed steps on a solve capped at 1 + 8 iterations."""
     if rank != 0:
         return
-    nx, ny, nz = 48, 48, 24
     import ewg
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()
-    case = ewg.lens3d_case(nx, ny, nz, seed=0)
+    case = ewg.lens3d_case(args.nx, args.ny, args.nz, seed=0)
     cores = os.cpu_count() or 1
+    dt = 250.0
     o = oracle.Oracle(case, nthreads=cores)
     o.apply_initial_solution()
-    for _ in range(args.warmup):
-        o.run(1, 250.0)
+    o.linearize(dt, 0)  # the first iteration of a step fills the storage cache of solution(1)
+    capped = dict(linear_solver_tolerance=1e-30, linear_solver_abs_tolerance=0.0, restart_on_breakdown=1,
+                  verify_true_residual=0)
+    its = 8
     t0 = time.perf_counter()
-    its = o.run(args.steps, 250.0)
-    el = time.perf_counter() - t0
-    value = case.n_cells * args.steps / el / 1e6
+    o.solve(ewg.default_solve_opts(linear_solver_max_iterations=1, **capped))
+    t_1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.solve(ewg.default_solve_opts(linear_solver_max_iterations=1 + its, **capped))
+    t_it = (time.perf_counter() - t0 - t_1) / its
+    for _ in range(args.warmup):
+        o.linearize(dt, 1)
+    samples = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.linearize(dt, 1)
+        t_lin = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        o.solve(ewg.default_solve_opts(linear_solver_max_iterations=1, **capped))
+        t_fact = max(time.perf_counter() - t0 - t_it, 0.0)
+        samples.append(REF_NEWTON_PER_STEP * t_lin + (REF_NEWTON_PER_STEP - 1) * t_fact + REF_BICGSTAB_PER_STEP * t_it)
+    o.close()
+    s_step = float(np.mean(samples))
+    value = case.n_cells / s_step / 1e6
+    sample = (f"oracle (CPU restatement of the reference path) on the {args.nx}x{args.ny}x{args.nz} lens, hydrostatic "
+              f"initial state: per timed step one AD linearization (element loop on {cores} threads) and one "
+              f"natural-order block-ILU(0) factorization + BiCGStab iteration (sequential, as one reference rank); "
+              f"step = {REF_NEWTON_PER_STEP:.2f} x (linearization + factorization) - 1 factorization + "
+              f"{REF_BICGSTAB_PER_STEP:.0f} x {t_it:.3f} s per BiCGStab iteration")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mcells/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": el / args.steps * 1e3, "s_per_step": el / args.steps,
+        "ms_per_step": s_step * 1e3, "s_per_step": s_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"lens3d {nx}x{ny}x{nz} sample of the 256x256x128 lens problem "
-                                                    f"(the CPU restatement cannot run 256x256x128 implicit steps in "
-                                                    f"minutes; the main line's cpu_baseline times its phases there)",
-                                        "dt": 250.0, "newton_tol": 1e-8, "linear_tol": 1e-10,
-                                        "ilu_ordering": "natural (the reference's)"},
-        "newton_its": [a for a, _ in its], "linear_its": [b for _, b in its],
-        "cpu_baseline": {"value": value, "unit": "Mcells/s", "cores": cores, "kind": "port",
-                         "sample": f"oracle restatement on a {nx}x{ny}x{nz} sub-grid, {args.steps} implicit steps after "
-                                   f"{args.warmup} warm-up steps, element loop on {cores} threads"},
+        "data": "synthetic (seeded log-normal permeability, hydrostatic initial state)",
+        "config": {"workload": f"lens3d {args.nx}x{args.ny}x{args.nz} ({case.n_cells} cells) plain FP64 path, implicit "
+                               f"Euler dt=250 s, Newton tol 1e-8, BiCGStab+ILU0 rel 1e-10",
+                   "cells": case.n_cells, "precision": "fp64", "ilu_ordering": "natural (the reference's)"},
+        "phases": {"s_per_bicgstab_iteration": t_it, "s_per_step_samples": samples,
+                   "newton_per_step": REF_NEWTON_PER_STEP, "bicgstab_per_step": REF_BICGSTAB_PER_STEP},
+        "cpu_baseline": {"value": value, "unit": "Mcells/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -554,6 +595,51 @@ def run_ensemble(args, rank, pg, torch, ewg):
         "launch_shapes": shapes, "autotune_s": tune_s,
     }
     ens.close()
+    return out
+
+
+def run_conv(torch, ewg, shape=(1, 128, 256, 256), reps=10):
+    """The guess network's tensor-core convolution (ewg_net_conv3d, tcgen05.mma + TMA) on a volume
+    of the bench grid's size: both layer widths (16 -> 32 and 32 -> 32 channels, bias + ReLU), CUDA
+    events around reps calls after 3 warm-up calls; FLOPs = 2 x 27 x Cin x 32 per voxel."""
+    import ctypes as C
+    lib = ewg.load()
+    fn = lib.ewg_net_conv3d
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_int32] * 6 + [C.c_void_p] * 6
+    B, D, H, W = shape
+    V = B * D * H * W
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        pass
+    out = {"volume": list(shape), "voxels": V, "peak_bf16_tflops": peak,
+           "peak_kind": "measured burst (MEASURED_PEAKS.json bf16_tflops)" if peak else None}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for cin in (16, 32):
+        x = torch.randn(V * cin, device="cuda", generator=g).to(torch.bfloat16)
+        w = (torch.randn(27 * 32 * cin, device="cuda", generator=g) * 0.05).to(torch.bfloat16)
+        b = torch.zeros(32, device="cuda")
+        y = torch.empty(V * 32, dtype=torch.bfloat16, device="cuda")
+        s = torch.cuda.current_stream()
+        args = (cin, 0, B, D, H, W, C.c_void_p(x.data_ptr()), C.c_void_p(w.data_ptr()), C.c_void_p(b.data_ptr()),
+                None, C.c_void_p(y.data_ptr()), C.c_void_p(s.cuda_stream))
+        for _ in range(3):
+            if fn(*args) != 0:
+                raise RuntimeError("ewg_net_conv3d failed")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            if fn(*args) != 0:
+                raise RuntimeError("ewg_net_conv3d failed")
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = 2.0 * 27 * cin * 32 * V / (ms * 1e-3) / 1e12
+        out[f"cin{cin}"] = {"ms": ms, "tflops": tf, "frac": tf / peak if peak else None}
+        del x, w, y
     return out
 
 
@@ -738,6 +824,10 @@ def run_ours(args, rank, world, local, pg):
     if not args.no_vcfv:
         vcfv = run_vcfv(args, rank, pg, torch, ewg)
 
+    conv = None
+    if not args.no_conv:
+        conv = run_conv(torch, ewg, (1, nz, ny, nx))
+
     if rank != 0:
         ctx.close()
         return
@@ -801,7 +891,8 @@ def run_ours(args, rank, world, local, pg):
                     "update": sum(r.t_update for r in reps) / len(reps)},
         "roofline": roofline, "linearization": lin, "linearizers": linearizers, "bicgstab": bicg,
         "kernels": {k: {"ms": v[0], "launches": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "vcfv": vcfv, "cpu_baseline": cpu,
+        "gpu_launches": launches, "e2e": e2e, "forms": forms, "ensemble": ensemble, "vcfv": vcfv,
+        "guess_conv": conv, "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -814,6 +905,11 @@ def main():
         # the host-core reference arm: rank 0 alone runs it, other ranks exit without work
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")), None)
+        return
+    if args.conv:
+        import torch
+        import ewg
+        print(json.dumps({"guess_conv": run_conv(torch, ewg, (1, args.nz, args.ny, args.nx))}), flush=True)
         return
     rank, world, local, pg = dist_init(args)
     try:
