@@ -276,6 +276,19 @@ NCU_TRAFFIC = {
     "ilu_red_apply": (133.50e6 + 4.21e6) * 8,
     "bicg_xr": (83.93e6 + 3.81e6) * 8,
 }
+# with the box-8-colour ILU(0): ncu dram__bytes_read.sum + dram__bytes_write.sum of the 192x192x96
+# case (3,538,944 cells; profiles/traffic_lens3d_192x192x96_fp64_box8.md) scaled by the cell count
+# (x 2.370); the sweeps' figures are per launch averaged over the 8 colours, like their
+# algorithmic bytes (their written colour stays in L2 for the next launches to read)
+NCU_TRAFFIC_B8 = {
+    "b8_backward": 74.25e6 * 2.370,
+    "b8_forward": 59.92e6 * 2.370,
+    "bicg_spmv_alpha": 734.6e6 * 2.370,
+    "bicg_spmv_omega": 737.1e6 * 2.370,
+    "bicg_xr": 358.1e6 * 2.370,
+    "bicg_hs": 285.6e6 * 2.370,
+    "bicg_p": 195.7e6 * 2.370,
+}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -841,7 +854,7 @@ def run_ours(args, rank, world, local, pg):
     db = kernel_bytes(dname, N, F, s_mat=s, s_vec=s, b8=b8, Fx=Fx)
     avg_ms = dms / dn
     achieved = db / (avg_ms * 1e-3) / 1e9 if db else None
-    traffic = NCU_TRAFFIC.get(dname) if not mixed else None
+    traffic = (NCU_TRAFFIC_B8 if b8 else NCU_TRAFFIC).get(dname) if not mixed else None
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic,
                 "algorithmic_bytes_per_launch": db, "avg_launch_ms": avg_ms, "launches": dn,
