@@ -26,37 +26,13 @@ namespace ewg {
 
 constexpr int kLinBlock = 256;
 
-// Four cells per pass of the grid-stride loop, their loads issued before any of them is
-// evaluated: one thread keeps four loads of S_w and the lens flag in flight instead of one.
-constexpr int kIntensiveUnroll = 4;
 __global__ void __launch_bounds__(kLinBlock) k_intensive(const __grid_constant__ Phys P,
                                                          const double2* __restrict__ x,
                                                          const uint8_t* __restrict__ lens,
                                                          double* __restrict__ iq) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t N = P.N;
-    for (int64_t s0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s0 < N; s0 += kIntensiveUnroll * stride) {
-        double sw[kIntensiveUnroll];
-        int lf[kIntensiveUnroll];
-#pragma unroll
-        for (int u = 0; u < kIntensiveUnroll; ++u) {
-            const int64_t s = s0 + u * stride;
-            sw[u] = s < N ? x[s].y : 1.0;
-            lf[u] = s < N ? lens[s] : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < kIntensiveUnroll; ++u) {
-            const int64_t s = s0 + u * stride;
-            if (s >= N) break;
-            const IqVals o = intensive_values(P, sw[u], lf[u]);
-            iq[s] = o.pc;
-            iq[N + s] = o.dpc;
-            iq[2 * N + s] = o.lw;
-            iq[3 * N + s] = o.dlw;
-            iq[4 * N + s] = o.ln;
-            iq[5 * N + s] = o.dln;
-        }
-    }
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x)
+        intensive_cell(P, x, lens, iq, s);
 }
 
 // Non-negative doubles compare like their bit patterns as unsigned integers.
