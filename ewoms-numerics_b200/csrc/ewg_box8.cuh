@@ -42,6 +42,33 @@
 
 namespace ewg {
 
+// The box-8 copies of the matrix (A8, 7 bands), its L factors (L8, 6 bands), inverted pivots and
+// E = A_cc - D' (1 band each) are solver-internal and block-packed: the 2x2 block of band b of the
+// cell at box-8 position s is the four consecutive values at element offset 4 (b N + s), so a
+// block is one 16-byte load in FP32 and two in FP64 (the linearizer's planes keep one entry per
+// plane).
+template <typename T>
+__device__ __forceinline__ void load_pb(const T* __restrict__ A, int64_t N, int band, int64_t s, double b[4]);
+template <>
+__device__ __forceinline__ void load_pb<float>(const float* __restrict__ A, int64_t N, int band, int64_t s, double b[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(A) + ((int64_t)band * N + s));
+    b[0] = v.x; b[1] = v.y; b[2] = v.z; b[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void load_pb<double>(const double* __restrict__ A, int64_t N, int band, int64_t s, double b[4]) {
+    const double2* p = reinterpret_cast<const double2*>(A) + 2 * ((int64_t)band * N + s);
+    const double2 v0 = __ldg(p), v1 = __ldg(p + 1);
+    b[0] = v0.x; b[1] = v0.y; b[2] = v1.x; b[3] = v1.y;
+}
+__device__ __forceinline__ void store_pb(float* __restrict__ A, int64_t N, int band, int64_t s, const double b[4]) {
+    reinterpret_cast<float4*>(A)[(int64_t)band * N + s] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
+}
+__device__ __forceinline__ void store_pb(double* __restrict__ A, int64_t N, int band, int64_t s, const double b[4]) {
+    double2* p = reinterpret_cast<double2*>(A) + 2 * ((int64_t)band * N + s);
+    p[0] = make_double2(b[0], b[1]);
+    p[1] = make_double2(b[2], b[3]);
+}
+
 struct Box8Pos {
     int bx, by, bz;
 };
@@ -144,19 +171,19 @@ __device__ __forceinline__ void b8_factor_face(const Phys& P, const TM* __restri
     if (n < 0) return;
     const int band = band_of(AXIS, SIDE);
     double Ack[4], Dk[4], Akc[4], Lb[4], B[4];
-    load_block(A, P.N, band, pos, Ack);
+    load_pb(A, P.N, band, pos, Ack);
     if (NB::inBox) {
 #pragma unroll
         for (int t = 0; t < 4; ++t) Dk[t] = dinvBox[NB::nQ][t];
     } else {
-        load_block(Dinv, P.N, 0, n, Dk);
+        load_pb(Dinv, P.N, 0, n, Dk);
     }
     mul2(Ack, Dk, Lb);
-    load_block(A, P.N, opposite_band(band), n, Akc);
+    load_pb(A, P.N, opposite_band(band), n, Akc);
     mul2(Lb, Akc, B);
 #pragma unroll
     for (int t = 0; t < 4; ++t) D[t] -= B[t];
-    store4(L, P.N, band - 1, pos, Lb);
+    store_pb(L, P.N, band - 1, pos, Lb);
 }
 
 template <typename TM, int C, int Q>
@@ -165,7 +192,7 @@ __device__ __forceinline__ bool b8_factor_cell(const Phys& P, const TM* __restri
                                                double (&dinvBox)[8][4]) {
     const int64_t pos = (int64_t)(C * 8 + Q) * P.Nb + b;
     double D[4];
-    load_block(A, P.N, 0, pos, D);
+    load_pb(A, P.N, 0, pos, D);
     // every earlier neighbour updates only D (no two neighbours are adjacent), in ascending
     // column order of the permuted row, as bilu0_decomposition's k loop
     using O = B8FaceOrder<C, Q>;
@@ -177,16 +204,16 @@ __device__ __forceinline__ bool b8_factor_cell(const Phys& P, const TM* __restri
     b8_factor_face<TM, C, Q, (O::dir(5) >> 1), (O::dir(5) & 1)>(P, A, Dinv, L, b, bp, pos, dinvBox, D);
     // E = A_cc - D' (what the pivot lost to the earlier neighbours), for the preconditioned SpMV
     double Ad[4], Ec[4];
-    load_block(A, P.N, 0, pos, Ad);
+    load_pb(A, P.N, 0, pos, Ad);
 #pragma unroll
     for (int t = 0; t < 4; ++t) Ec[t] = Ad[t] - D[t];
-    store4(E, P.N, 0, pos, Ec);
+    store_pb(E, P.N, 0, pos, Ec);
     double o[4];
     const bool ok = inv2(D, o);
     if (!ok) o[0] = o[1] = o[2] = o[3] = 0.0;
 #pragma unroll
     for (int t = 0; t < 4; ++t) dinvBox[Q][t] = o[t];
-    store4(Dinv, P.N, 0, pos, o);
+    store_pb(Dinv, P.N, 0, pos, o);
     return ok;
 }
 
@@ -244,13 +271,13 @@ __device__ __forceinline__ void b8_fwd_far(const Phys& P, const TM* __restrict__
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
     if (!NB::earlier) return;
     if (NB::inBox) {
-        load_block(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lin[AXIS]);
+        load_pb(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lin[AXIS]);
         return;
     }
     const int64_t n = b8_nbr_pos<C, Q, AXIS, SIDE>(P, b, bp);
     if (n < 0) return;
     double Lb[4];
-    load_block(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lb);
+    load_pb(L, P.N, band_of(AXIS, SIDE) - 1, pos, Lb);
     const auto wk = w[n];
     const double x0 = (double)wk.x, x1 = (double)wk.y;
     r0 -= Lb[0] * x0; r0 -= Lb[1] * x1;
@@ -371,13 +398,13 @@ __device__ __forceinline__ void b8_bwd_far(const Phys& P, const TM* __restrict__
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
     if (NB::earlier) return;
     if (NB::inBox) {
-        load_block(A, P.N, band_of(AXIS, SIDE), pos, Ain[AXIS]);
+        load_pb(A, P.N, band_of(AXIS, SIDE), pos, Ain[AXIS]);
         return;
     }
     const int64_t n = b8_nbr_pos<C, Q, AXIS, SIDE>(P, b, bp);
     if (n < 0) return;
     double Ab[4];
-    load_block(A, P.N, band_of(AXIS, SIDE), pos, Ab);
+    load_pb(A, P.N, band_of(AXIS, SIDE), pos, Ab);
     const auto yk = y[n];
     double x0 = (double)yk.x, x1 = (double)yk.y;
     if (winv != 1.0) { x0 *= winv; x1 *= winv; }
@@ -440,7 +467,7 @@ __device__ __forceinline__ void b8_backward_tile(const Phys& P, const TM* __rest
 #define EWG_B8_CALL(Q) b8_bwd_far_all<TM, TV, C, Q>(P, A, y, b, pos, winv, r0, r1, Ain)
         EWG_B8_PLACE_SWITCH(q, EWG_B8_CALL)
 #undef EWG_B8_CALL
-        load_block(Dinv, P.N, 0, pos, Di);
+        load_pb(Dinv, P.N, 0, pos, Di);
     }
 #pragma unroll
     for (int lev = 0; lev < 4; ++lev) {
@@ -531,7 +558,7 @@ __device__ __forceinline__ void spmv_row_b8(const Phys& P, const TM* __restrict_
     for (int q = 0; q < 7; ++q) {
         const int band = bands[q];
         double B[4];
-        load_block(A, P.N, band, s, B);
+        load_pb(A, P.N, band, s, B);
         double x0 = 0.0, x1 = 0.0;
         if (band == 0) {
             const auto xk = x[s];
@@ -569,7 +596,7 @@ __device__ __forceinline__ void spmv_row_b8_precond(const Phys& P, const TM* __r
     a1 = relax * (double)wc.y;
     {
         double B[4];
-        load_block(E, P.N, 0, s, B);
+        load_pb(E, P.N, 0, s, B);
         const auto yc = y[s];
         const double x0 = (double)yc.x, x1 = (double)yc.y;
         a0 += B[0] * x0; a0 += B[1] * x1;
@@ -586,7 +613,7 @@ __device__ __forceinline__ void spmv_row_b8_precond(const Phys& P, const TM* __r
         const B8Step st = b8_step(P, g, b, bp, axis, side);
         if (!st.exists) continue;
         double B[4];
-        load_block(A, P.N, band, s, B);
+        load_pb(A, P.N, band, s, B);
         const auto yk = y[st.pos];
         const double x0 = (double)yk.x, x1 = (double)yk.y;
         a0 += B[0] * x0; a0 += B[1] * x1;
@@ -610,13 +637,14 @@ __device__ __forceinline__ int64_t b8_to_split_pos(const Phys& P, int64_t s) {
     return (int64_t)col * P.Nh + (c >> 1);
 }
 
-// matrix planes (nPlanes planes of N values): out[plane][s8] = in[plane][split(s8)], converting TI -> TO
+// matrix planes (nPlanes = 4 x bands planes of N values) into the block-packed box-8 copy:
+// out block (band, s8) = in planes (4 band .. 4 band + 3)[split(s8)], converting TI -> TO
 template <typename TI, typename TO>
 __global__ void k_b8_matrix_from_split(const __grid_constant__ Phys P, int nPlanes, const TI* __restrict__ in,
                                        TO* __restrict__ out) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
         const int64_t sp = b8_to_split_pos(P, s);
-        for (int p = 0; p < nPlanes; ++p) out[(int64_t)p * P.N + s] = (TO)in[(int64_t)p * P.N + sp];
+        for (int p = 0; p < nPlanes; ++p) out[4 * ((int64_t)(p >> 2) * P.N + s) + (p & 3)] = (TO)in[(int64_t)p * P.N + sp];
     }
 }
 

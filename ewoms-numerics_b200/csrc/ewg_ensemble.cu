@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksVec) ke_xr(ENS_ARGS, typen
 
 constexpr int kEnsB8Sub = kEnsTileH / 1024;  // 32-box sub-tiles of a tile
 
-// A8 = J in box-8 order (28 planes per member)
+// A8 = J in box-8 order, block-packed (7 bands of 2x2 blocks per member)
 template <typename T>
 __global__ void __launch_bounds__(kEnsTile) ke_b8_matrix(ENS_ARGS, const int* __restrict__ mask, const T* __restrict__ J,
                                                          T* __restrict__ A8) {
@@ -699,7 +699,8 @@ __global__ void __launch_bounds__(kEnsTile) ke_b8_matrix(ENS_ARGS, const int* __
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
             for (int col = 0; col < 2; ++col) {
                 const int64_t s8 = col * P.Nh + h, sp = b8_to_split_pos(P, s8);
-                for (int pl = 0; pl < kEnsBands * 4; ++pl) Am[(int64_t)pl * P.N + s8] = Jm[(int64_t)pl * P.N + sp];
+                for (int pl = 0; pl < kEnsBands * 4; ++pl)
+                    Am[4 * ((int64_t)(pl >> 2) * P.N + s8) + (pl & 3)] = Jm[(int64_t)pl * P.N + sp];
             }
     }
 }
