@@ -210,11 +210,12 @@ def kernel_bytes(name, N, F, s_mat=8, s_vec=8, b8=False, Fx=None):
     if b8:
         Fx = F // 2 if Fx is None else Fx
         table8 = {
-            # forward, per colour: L blocks of the earlier neighbours, d in, w out, the earlier
-            # neighbours' w across box faces (within a box they stay in registers)
+            # forward, per launch (a sweep is 8 colour launches): L blocks of the earlier
+            # neighbours, d in, w out, the earlier neighbours' w across box faces (within a box they
+            # stay in registers)
             "b8_forward": (F * blk + N * vec * 2 + Fx * vec) / 8,
-            # backward, per colour: blocks of the later neighbours, inverted pivots, w in, y out,
-            # the later neighbours' y across box faces
+            # backward, per launch: blocks of the later neighbours, inverted pivots, w in, y out, the
+            # later neighbours' y across box faces
             "b8_backward": (F * blk + N * blk + N * vec * 2 + Fx * vec) / 8,
             # v = relax w + E y + sum of the earlier neighbours' blocks times y; r0hat (or s) for
             # the dot products
@@ -278,11 +279,11 @@ NCU_TRAFFIC = {
 }
 # with the box-8-colour ILU(0): ncu dram__bytes_read.sum + dram__bytes_write.sum of the 192x192x96
 # case (3,538,944 cells; profiles/traffic_lens3d_192x192x96_fp64_box8.md) scaled by the cell count
-# (x 2.370); the sweeps' figures are per launch averaged over the 8 colours, like their
-# algorithmic bytes (their written colour stays in L2 for the next launches to read)
+# (x 2.370); the sweeps' figures are a sweep's traffic over its 8 colour launches, like their
+# algorithmic bytes (a written colour stays in L2 for the next launches to read)
 NCU_TRAFFIC_B8 = {
-    "b8_backward": 74.25e6 * 2.370,
-    "b8_forward": 59.92e6 * 2.370,
+    "b8_backward": 594.6e6 / 8 * 2.370,
+    "b8_forward": 479.6e6 / 8 * 2.370,
     "bicg_spmv_alpha": 734.6e6 * 2.370,
     "bicg_spmv_omega": 737.1e6 * 2.370,
     "bicg_xr": 358.1e6 * 2.370,
@@ -707,7 +708,7 @@ def run_ours(args, rank, world, local, pg):
     torch.cuda.synchronize()
     ctx.profile_reset()
     # every 7th launch of each kernel class is bracketed by CUDA events (all launches counted); 7 is
-    # prime to the 8 colour phases of a box-8 sweep, so every colour is sampled alike
+    # prime to the 8 colour launches of a box-8 sweep, so every colour is sampled alike
     ctx.profile_enable(True, period=7)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)

@@ -35,8 +35,8 @@ template <typename T, int C>
 void backward_colour(ewg_ctx* ctx, const T* A8, const T* Dinv8, const typename V2T<T>::type* w,
                      typename V2T<T>::type* y, const int* status, double relax) {
     auto kfn = k_b8_backward<T, T, C>;
-    EWG_LAUNCH_PDL(ctx, K_B8_BACKWARD, kfn, b8_sweep_grid(ctx, (const void*)kfn), kB8Block, ctx->P, A8, Dinv8, w, y, status,
-               relax);
+    EWG_LAUNCH_PDL(ctx, K_B8_BACKWARD, kfn, b8_sweep_grid(ctx, (const void*)kfn), kB8Block, ctx->P, A8, Dinv8, w, y,
+                   status, relax);
 }
 
 }  // namespace

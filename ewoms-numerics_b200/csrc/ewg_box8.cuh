@@ -217,24 +217,53 @@ __device__ __forceinline__ bool b8_factor_cell(const Phys& P, const TM* __restri
     return ok;
 }
 
+// Colour levels. Adjacent boxes differ in exactly one colour bit, so boxes whose colours have the
+// same number of set bits never share a face: colours 1, 2, 4 depend only on colour 0 and colours
+// 3, 5, 6 only on 1, 2, 4. A phase of the factorization or the sweeps can therefore run one launch
+// per level -- {0}, {1, 2, 4}, {3, 5, 6}, {7} (the backward sweep in the reverse order) -- with the
+// same results as one launch per colour in colour order: a cell's values depend only on its
+// finished neighbours, and the terms of its row are summed in the same order. The batched ensemble
+// does (its launches are the cost there); the single problem keeps one launch per colour.
+template <int LEVEL>
+struct B8Level {
+    static constexpr int count = (LEVEL == 0 || LEVEL == 3) ? 1 : 3;
+    __host__ __device__ static constexpr int colour(int i) {
+        return LEVEL == 0 ? 0 : (LEVEL == 3 ? 7 : (LEVEL == 1 ? (1 << i) : (7 ^ (1 << i))));
+    }
+};
+// calls F::template run<C>() for colour i of the level (i uniform over the block)
+#define EWG_B8_LEVEL_DISPATCH(LEVEL, i, CALL)                              \
+    do {                                                                   \
+        if (B8Level<LEVEL>::count == 1) { CALL(B8Level<LEVEL>::colour(0)); } \
+        else if ((i) == 0) { CALL(B8Level<LEVEL>::colour(0)); }            \
+        else if ((i) == 1) { CALL(B8Level<LEVEL>::colour(1)); }            \
+        else { CALL(B8Level<LEVEL>::colour(2)); }                          \
+    } while (0)
+
+template <typename TM, int C>
+__device__ __forceinline__ bool b8_factor_box(const Phys& P, const TM* __restrict__ A, TM* __restrict__ Dinv,
+                                              TM* __restrict__ L, TM* __restrict__ E, int64_t b) {
+    const Box8Pos bp = b8_box(P, (uint32_t)b);
+    double dinvBox[8][4];
+    bool ok = true;
+    ok &= b8_factor_cell<TM, C, 0>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 1>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 2>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 3>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 4>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 5>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 6>(P, A, Dinv, L, E, b, bp, dinvBox);
+    ok &= b8_factor_cell<TM, C, 7>(P, A, Dinv, L, E, b, bp, dinvBox);
+    return ok;
+}
+
+// factorization of colour C: one thread per box
 template <typename TM, int C>
 __global__ void __launch_bounds__(kSolBlock) k_b8_factor(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                           TM* __restrict__ Dinv, TM* __restrict__ L, TM* __restrict__ E,
                                                           int* bad) {
-    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < P.Nb; b += (int64_t)gridDim.x * blockDim.x) {
-        const Box8Pos bp = b8_box(P, (uint32_t)b);
-        double dinvBox[8][4];
-        bool ok = true;
-        ok &= b8_factor_cell<TM, C, 0>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 1>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 2>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 3>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 4>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 5>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 6>(P, A, Dinv, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<TM, C, 7>(P, A, Dinv, L, E, b, bp, dinvBox);
-        if (!ok) atomicOr(bad, 1);
-    }
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < P.Nb; b += (int64_t)gridDim.x * blockDim.x)
+        if (!b8_factor_box<TM, C>(P, A, Dinv, L, E, b)) atomicOr(bad, 1);
 }
 
 // ---- sweeps: one warp per place, one lane per box ---------------------------------------------------
@@ -370,7 +399,8 @@ __device__ __forceinline__ void b8_forward_tile(const Phys& P, const TM* __restr
     }
 }
 
-// forward sweep of colour C: w_c = d_c - sum_{k earlier} L_ck w_k
+// forward sweep of colour C: w_c = d_c - sum_{k earlier} L_ck w_k. (One launch per colour: a
+// launch per colour level, with the three colours' code in one kernel, ran 10 % slower here.)
 template <typename TM, typename TV, int C>
 __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
                                                            const typename V2T<TV>::type* __restrict__ d,

@@ -705,69 +705,73 @@ __global__ void __launch_bounds__(kEnsTile) ke_b8_matrix(ENS_ARGS, const int* __
     }
 }
 
-// factorization of colour C: one thread per superblock of the tile; a singular pivot sets bit 4
-template <typename T, int C>
+// factorization of one colour level: one thread per superblock of the tile and colour of the level;
+// a singular pivot sets bit 4
+template <typename T, int LEVEL>
 __global__ void __launch_bounds__(kEnsTile) ke_b8_factor(ENS_ARGS, const int* __restrict__ mask, const T* __restrict__ A8,
                                                          T* __restrict__ Dinv8, T* __restrict__ L8, T* __restrict__ E8,
                                                          int* __restrict__ flags) {
     __shared__ EnsMember sm;
     __shared__ int sh[2];
+    constexpr int NC = B8Level<LEVEL>::count;
+    static_assert(NC * (kEnsTileH / 32) <= kEnsTile, "one thread per (superblock, colour) of a tile");
     ENS_TILE_LOOP {
         const int m = begin_tile(mem, tiles, t, mask, nullptr, 0, sm, sh);
         if (m < 0) continue;
         const Phys P = sm.P;
-        const int64_t b = sh[1] / 32 + threadIdx.x;
-        if (threadIdx.x >= kEnsTileH / 32 || b >= P.Nb) continue;
+        const int ci = threadIdx.x / (kEnsTileH / 32);
+        const int64_t b = sh[1] / 32 + threadIdx.x % (kEnsTileH / 32);
+        if (ci >= NC || b >= P.Nb) continue;
         const int64_t off = sm.off;
         const T* A = A8 + kEnsBands * 4 * off;
         T* Di = Dinv8 + 4 * off;
         T* L = L8 + 24 * off;
         T* E = E8 + 4 * off;
-        const Box8Pos bp = b8_box(P, (uint32_t)b);
-        double dinvBox[8][4];
         bool ok = true;
-        ok &= b8_factor_cell<T, C, 0>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 1>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 2>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 3>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 4>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 5>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 6>(P, A, Di, L, E, b, bp, dinvBox);
-        ok &= b8_factor_cell<T, C, 7>(P, A, Di, L, E, b, bp, dinvBox);
+#define EWG_B8_CALL(C) ok = b8_factor_box<T, C>(P, A, Di, L, E, b)
+        EWG_B8_LEVEL_DISPATCH(LEVEL, ci, EWG_B8_CALL);
+#undef EWG_B8_CALL
         if (!ok) atomicOr(&flags[m], 4);
     }
 }
 
-// forward sweep of colour C for the running members: w = (D' + L_A)^-1 d, colour C's cells
-template <typename T, int C>
+// forward sweep of one colour level for the running members: w = (D' + L_A)^-1 d on its cells
+template <typename T, int LEVEL>
 __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_forward(ENS_ARGS, const T* __restrict__ L8,
-                                                                         const typename V2T<T>::type* __restrict__ d,
-                                                                         typename V2T<T>::type* __restrict__ w,
-                                                                         const BiState* __restrict__ st) {
+                                                                          const typename V2T<T>::type* __restrict__ d,
+                                                                          typename V2T<T>::type* __restrict__ w,
+                                                                          const BiState* __restrict__ st) {
     __shared__ EnsMember sm;
     __shared__ int sh[2];
     __shared__ double2 SB[2][8][32];
+    constexpr int NC = B8Level<LEVEL>::count;
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
     int k = 0;
     ENS_TILE_LOOP {
         if (begin_tile(mem, tiles, t, nullptr, st, ST_RUNNING, sm, sh) < 0) continue;
         const Phys P = sm.P;
         const int64_t off = sm.off;
-        for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k)
-            b8_forward_tile<T, T, C>(P, L8 + 24 * off, d + off, w + off, sh[1] / 32 + sub * 32, SB[k & 1], lane, q);
+        for (int ci = 0; ci < NC; ++ci)
+            for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k) {
+#define EWG_B8_CALL(C) \
+    b8_forward_tile<T, T, C>(P, L8 + 24 * off, d + off, w + off, sh[1] / 32 + sub * 32, SB[k & 1], lane, q)
+                EWG_B8_LEVEL_DISPATCH(LEVEL, ci, EWG_B8_CALL);
+#undef EWG_B8_CALL
+            }
     }
 }
 
-// backward sweep of colour C: y = relax (D')^-1 (w - U_A y / relax), colour C's cells
-template <typename T, int C>
+// backward sweep of one colour level: y = relax (D')^-1 (w - U_A y / relax) on its cells
+template <typename T, int LEVEL>
 __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_backward(ENS_ARGS, const T* __restrict__ A8,
-                                                                          const T* __restrict__ Dinv8,
-                                                                          const typename V2T<T>::type* __restrict__ wv,
-                                                                          typename V2T<T>::type* __restrict__ y,
-                                                                          const BiState* __restrict__ st) {
+                                                                           const T* __restrict__ Dinv8,
+                                                                           const typename V2T<T>::type* __restrict__ wv,
+                                                                           typename V2T<T>::type* __restrict__ y,
+                                                                           const BiState* __restrict__ st) {
     __shared__ EnsMember sm;
     __shared__ int sh[2];
     __shared__ double2 SB[2][8][32];
+    constexpr int NC = B8Level<LEVEL>::count;
     const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
     int k = 0;
     ENS_TILE_LOOP {
@@ -776,9 +780,14 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_backward(ENS_A
         const Phys P = sm.P;
         const int64_t off = sm.off;
         const double w = st[m].w;
-        for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k)
-            b8_backward_tile<T, T, C>(P, A8 + kEnsBands * 4 * off, Dinv8 + 4 * off, wv + off, y + off, w, 1.0 / w,
-                                      sh[1] / 32 + sub * 32, SB[k & 1], lane, q);
+        for (int ci = 0; ci < NC; ++ci)
+            for (int sub = 0; sub < kEnsB8Sub; ++sub, ++k) {
+#define EWG_B8_CALL(C)                                                                                      \
+    b8_backward_tile<T, T, C>(P, A8 + kEnsBands * 4 * off, Dinv8 + 4 * off, wv + off, y + off, w, 1.0 / w, \
+                              sh[1] / 32 + sub * 32, SB[k & 1], lane, q)
+                EWG_B8_LEVEL_DISPATCH(LEVEL, ci, EWG_B8_CALL);
+#undef EWG_B8_CALL
+            }
     }
 }
 
@@ -921,24 +930,20 @@ struct Ops {
         ke_intensive<<<e->grid[EC_INTENSIVE], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, e->x0,
                                                                         e->lens, e->iq);
     }
-    template <int C>
-    static void b8_factor_colour(ewg_ensemble* e, int g) {
-        ke_b8_factor<T, C><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->A8), m(e->Dinv8),
-                                                         m(e->L8), m(e->E8), e->flagsF);
+    template <int LEVEL>
+    static void b8_factor_level(ewg_ensemble* e, int g) {
+        ke_b8_factor<T, LEVEL><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->A8),
+                                                             m(e->Dinv8), m(e->L8), m(e->E8), e->flagsF);
     }
     static void factor(ewg_ensemble* e) {
         const int g = e->grid[EC_FACTOR];
         if (e->b8) {
             ke_b8_matrix<T><<<e->grid[EC_CELL], kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J),
                                                                          m(e->A8));
-            b8_factor_colour<0>(e, g);
-            b8_factor_colour<1>(e, g);
-            b8_factor_colour<2>(e, g);
-            b8_factor_colour<3>(e, g);
-            b8_factor_colour<4>(e, g);
-            b8_factor_colour<5>(e, g);
-            b8_factor_colour<6>(e, g);
-            b8_factor_colour<7>(e, g);
+            b8_factor_level<0>(e, g);
+            b8_factor_level<1>(e, g);
+            b8_factor_level<2>(e, g);
+            b8_factor_level<3>(e, g);
             return;
         }
         ke_diag_inverse_red<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J), m(e->Dinv),
@@ -946,7 +951,7 @@ struct Ops {
         ke_ilu_black_factor<T><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlA.d, e->tlA.dn, e->mask, m(e->J), m(e->Dinv),
                                                              m(e->L), e->flagsF);
     }
-    // box-8 sweeps of all colours for the running members: W = forward(d), y = backward(W)
+    // box-8 sweeps of all colour levels for the running members: W = forward(d), y = backward(W)
     template <int C>
     static void b8_fwd(ewg_ensemble* e, int g, const VT<T>* d) {
         ke_b8_forward<T, C><<<g, kEnsTile, 0, e->stream>>>(e->dm, e->tlB.d, e->tlB.dn, m(e->L8), d, v(e->W8), e->st);
@@ -976,7 +981,6 @@ struct Ops {
                 if (E->b8) {  // the forward sweeps (d = p or s, into W)
                     const VT<T>* d = which ? v(E->kr) : v(E->kp);
                     b8_fwd<0>(E, g, d); b8_fwd<1>(E, g, d); b8_fwd<2>(E, g, d); b8_fwd<3>(E, g, d);
-                    b8_fwd<4>(E, g, d); b8_fwd<5>(E, g, d); b8_fwd<6>(E, g, d); b8_fwd<7>(E, g, d);
                     break;
                 }
                 ke_ilu_black_apply<T><<<g, kEnsTile, 0, E->stream>>>(E->dm, E->tlB.d, E->tlB.dn, m(E->Dinv), m(E->L),
@@ -986,7 +990,6 @@ struct Ops {
             case EC_ILU_RED:
                 if (E->b8) {  // the backward sweeps (from W into y or z)
                     VT<T>* y = which ? v(E->kz) : v(E->ky);
-                    b8_bwd<7>(E, g, y); b8_bwd<6>(E, g, y); b8_bwd<5>(E, g, y); b8_bwd<4>(E, g, y);
                     b8_bwd<3>(E, g, y); b8_bwd<2>(E, g, y); b8_bwd<1>(E, g, y); b8_bwd<0>(E, g, y);
                     break;
                 }
