@@ -707,9 +707,11 @@ def run_ours(args, rank, world, local, pg):
     barrier(pg)
     torch.cuda.synchronize()
     ctx.profile_reset()
-    # every 7th launch of each kernel class is bracketed by CUDA events (all launches counted); 7 is
-    # prime to the 8 colour launches of a box-8 sweep, so every colour is sampled alike
-    ctx.profile_enable(True, period=7)
+    # every 31st launch of each kernel class is bracketed by CUDA events (all launches counted): 31
+    # is prime to the 8 colour launches of a box-8 sweep, so every colour is sampled alike, and an
+    # event pair (which also ends the programmatic launch overlap of its kernel) lands on one in
+    # 31 launches, so the sampling costs the timed steps little
+    ctx.profile_enable(True, period=31)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     reps = []
