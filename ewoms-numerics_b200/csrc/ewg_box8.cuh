@@ -39,6 +39,11 @@
 #ifndef EWG_B8_SWEEP_BLOCKS
 #define EWG_B8_SWEEP_BLOCKS 4
 #endif
+// ... for FP32 matrices, whose blocks take half the registers
+#ifndef EWG_B8_SWEEP_BLOCKS_F32
+#define EWG_B8_SWEEP_BLOCKS_F32 5
+#endif
+#define EWG_B8_SWEEP_MINB(TM) (sizeof(TM) == 4 ? EWG_B8_SWEEP_BLOCKS_F32 : EWG_B8_SWEEP_BLOCKS)
 
 namespace ewg {
 
@@ -59,6 +64,11 @@ __device__ __forceinline__ void load_pb<double>(const double* __restrict__ A, in
     const double2* p = reinterpret_cast<const double2*>(A) + 2 * ((int64_t)band * N + s);
     const double2 v0 = __ldg(p), v1 = __ldg(p + 1);
     b[0] = v0.x; b[1] = v0.y; b[2] = v1.x; b[3] = v1.y;
+}
+// the FP32 blocks kept as FP32 in registers (converted exactly where they are used)
+__device__ __forceinline__ void load_pb(const float* __restrict__ A, int64_t N, int band, int64_t s, float b[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(A) + ((int64_t)band * N + s));
+    b[0] = v.x; b[1] = v.y; b[2] = v.z; b[3] = v.w;
 }
 __device__ __forceinline__ void store_pb(float* __restrict__ A, int64_t N, int band, int64_t s, const double b[4]) {
     reinterpret_cast<float4*>(A)[(int64_t)band * N + s] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
@@ -294,7 +304,7 @@ constexpr int kB8Block = 256;  // 8 places x 32 boxes
 template <typename TM, typename TV, int C, int Q, int R>
 __device__ __forceinline__ void b8_fwd_far(const Phys& P, const TM* __restrict__ L,
                                            const typename V2T<TV>::type* __restrict__ w, int64_t b, const Box8Pos& bp,
-                                           int64_t pos, double& r0, double& r1, double (&Lin)[3][4]) {
+                                           int64_t pos, double& r0, double& r1, TM (&Lin)[3][4]) {
     using O = B8FaceOrder<C, Q>;
     constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
@@ -316,7 +326,7 @@ __device__ __forceinline__ void b8_fwd_far(const Phys& P, const TM* __restrict__
 template <typename TM, typename TV, int C, int Q>
 __device__ __forceinline__ void b8_fwd_far_all(const Phys& P, const TM* __restrict__ L,
                                                const typename V2T<TV>::type* __restrict__ w, int64_t b, int64_t pos,
-                                               double& r0, double& r1, double (&Lin)[3][4]) {
+                                               double& r0, double& r1, TM (&Lin)[3][4]) {
     const Box8Pos bp = b8_box(P, (uint32_t)b);
     b8_fwd_far<TM, TV, C, Q, 0>(P, L, w, b, bp, pos, r0, r1, Lin);
     b8_fwd_far<TM, TV, C, Q, 1>(P, L, w, b, bp, pos, r0, r1, Lin);
@@ -327,8 +337,8 @@ __device__ __forceinline__ void b8_fwd_far_all(const Phys& P, const TM* __restri
 }
 
 // forward, in its level: the terms of the same box, ascending
-template <int C, int Q, int R>
-__device__ __forceinline__ void b8_fwd_near(const double2 (&S)[8][32], int lane, const double (&Lin)[3][4], double& r0,
+template <int C, int Q, int R, typename MT>
+__device__ __forceinline__ void b8_fwd_near(const double2 (&S)[8][32], int lane, const MT (&Lin)[3][4], double& r0,
                                             double& r1) {
     using O = B8FaceOrder<C, Q>;
     constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
@@ -339,8 +349,8 @@ __device__ __forceinline__ void b8_fwd_near(const double2 (&S)[8][32], int lane,
     r1 -= Lin[AXIS][2] * v.x; r1 -= Lin[AXIS][3] * v.y;
 }
 
-template <int C, int Q>
-__device__ __forceinline__ void b8_fwd_near_all(const double2 (&S)[8][32], int lane, const double (&Lin)[3][4],
+template <int C, int Q, typename MT>
+__device__ __forceinline__ void b8_fwd_near_all(const double2 (&S)[8][32], int lane, const MT (&Lin)[3][4],
                                                 double& r0, double& r1) {
     b8_fwd_near<C, Q, 0>(S, lane, Lin, r0, r1);
     b8_fwd_near<C, Q, 1>(S, lane, Lin, r0, r1);
@@ -373,7 +383,8 @@ __device__ __forceinline__ void b8_forward_tile(const Phys& P, const TM* __restr
     const int64_t b = b0 + lane;
     const bool valid = b < P.Nb;
     const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
-    double r0 = 0.0, r1 = 0.0, Lin[3][4];
+    double r0 = 0.0, r1 = 0.0;
+    TM Lin[3][4];
     if (valid) {
         const auto ds = d[pos];
         r0 = (double)ds.x;
@@ -402,7 +413,7 @@ __device__ __forceinline__ void b8_forward_tile(const Phys& P, const TM* __restr
 // forward sweep of colour C: w_c = d_c - sum_{k earlier} L_ck w_k. (One launch per colour: a
 // launch per colour level, with the three colours' code in one kernel, ran 10 % slower here.)
 template <typename TM, typename TV, int C>
-__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
+__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_MINB(TM)) k_b8_forward(const __grid_constant__ Phys P, const TM* __restrict__ L,
                                                            const typename V2T<TV>::type* __restrict__ d,
                                                            typename V2T<TV>::type* __restrict__ w,
                                                            const int* __restrict__ status) {
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_forward(co
 template <typename TM, typename TV, int C, int Q, int R>
 __device__ __forceinline__ void b8_bwd_far(const Phys& P, const TM* __restrict__ A,
                                            const typename V2T<TV>::type* __restrict__ y, int64_t b, const Box8Pos& bp,
-                                           int64_t pos, double winv, double& r0, double& r1, double (&Ain)[3][4]) {
+                                           int64_t pos, double winv, double& r0, double& r1, TM (&Ain)[3][4]) {
     using O = B8FaceOrder<C, Q>;
     constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
     using NB = B8Nbr<C, Q, AXIS, SIDE>;
@@ -446,7 +457,7 @@ __device__ __forceinline__ void b8_bwd_far(const Phys& P, const TM* __restrict__
 template <typename TM, typename TV, int C, int Q>
 __device__ __forceinline__ void b8_bwd_far_all(const Phys& P, const TM* __restrict__ A,
                                                const typename V2T<TV>::type* __restrict__ y, int64_t b, int64_t pos,
-                                               double winv, double& r0, double& r1, double (&Ain)[3][4]) {
+                                               double winv, double& r0, double& r1, TM (&Ain)[3][4]) {
     const Box8Pos bp = b8_box(P, (uint32_t)b);
     b8_bwd_far<TM, TV, C, Q, 5>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
     b8_bwd_far<TM, TV, C, Q, 4>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
@@ -456,8 +467,8 @@ __device__ __forceinline__ void b8_bwd_far_all(const Phys& P, const TM* __restri
     b8_bwd_far<TM, TV, C, Q, 0>(P, A, y, b, bp, pos, winv, r0, r1, Ain);
 }
 
-template <int C, int Q, int R>
-__device__ __forceinline__ void b8_bwd_near(const double2 (&S)[8][32], int lane, const double (&Ain)[3][4], double& r0,
+template <int C, int Q, int R, typename MT>
+__device__ __forceinline__ void b8_bwd_near(const double2 (&S)[8][32], int lane, const MT (&Ain)[3][4], double& r0,
                                             double& r1) {
     using O = B8FaceOrder<C, Q>;
     constexpr int dir = O::dir(R), AXIS = dir >> 1, SIDE = dir & 1;
@@ -468,8 +479,8 @@ __device__ __forceinline__ void b8_bwd_near(const double2 (&S)[8][32], int lane,
     r1 -= Ain[AXIS][2] * v.x; r1 -= Ain[AXIS][3] * v.y;
 }
 
-template <int C, int Q>
-__device__ __forceinline__ void b8_bwd_near_all(const double2 (&S)[8][32], int lane, const double (&Ain)[3][4],
+template <int C, int Q, typename MT>
+__device__ __forceinline__ void b8_bwd_near_all(const double2 (&S)[8][32], int lane, const MT (&Ain)[3][4],
                                                 double& r0, double& r1) {
     b8_bwd_near<C, Q, 5>(S, lane, Ain, r0, r1);
     b8_bwd_near<C, Q, 4>(S, lane, Ain, r0, r1);
@@ -489,7 +500,8 @@ __device__ __forceinline__ void b8_backward_tile(const Phys& P, const TM* __rest
     const int64_t b = b0 + lane;
     const bool valid = b < P.Nb;
     const int64_t pos = (int64_t)(C * 8 + q) * P.Nb + b;
-    double r0 = 0.0, r1 = 0.0, Ain[3][4], Di[4] = {0.0, 0.0, 0.0, 0.0};
+    double r0 = 0.0, r1 = 0.0;
+    TM Ain[3][4], Di[4] = {(TM)0, (TM)0, (TM)0, (TM)0};
     if (valid) {
         const auto ws = wv[pos];
         r0 = (double)ws.x;
@@ -523,7 +535,7 @@ __device__ __forceinline__ void b8_backward_tile(const Phys& P, const TM* __rest
 // colours are relax * y; the coupling term works on unscaled y, as the reference's backward solve
 // runs before its final scaling.
 template <typename TM, typename TV, int C>
-__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_BLOCKS) k_b8_backward(const __grid_constant__ Phys P, const TM* __restrict__ A,
+__global__ void __launch_bounds__(kB8Block, EWG_B8_SWEEP_MINB(TM)) k_b8_backward(const __grid_constant__ Phys P, const TM* __restrict__ A,
                                                             const TM* __restrict__ Dinv,
                                                             const typename V2T<TV>::type* __restrict__ wv,
                                                             typename V2T<TV>::type* __restrict__ y,
