@@ -41,7 +41,7 @@
 #endif
 // ... for FP32 matrices, whose blocks take half the registers
 #ifndef EWG_B8_SWEEP_BLOCKS_F32
-#define EWG_B8_SWEEP_BLOCKS_F32 5
+#define EWG_B8_SWEEP_BLOCKS_F32 6
 #endif
 #define EWG_B8_SWEEP_MINB(TM) (sizeof(TM) == 4 ? EWG_B8_SWEEP_BLOCKS_F32 : EWG_B8_SWEEP_BLOCKS)
 

@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(kEnsTile) ke_b8_factor(ENS_ARGS, const int* __
 
 // forward sweep of one colour level for the running members: w = (D' + L_A)^-1 d on its cells
 template <typename T, int LEVEL>
-__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_forward(ENS_ARGS, const T* __restrict__ L8,
+__global__ void __launch_bounds__(kEnsTile, sizeof(T) == 4 ? kEnsBlocksSpmv + 2 : kEnsBlocksSpmv) ke_b8_forward(ENS_ARGS, const T* __restrict__ L8,
                                                                           const typename V2T<T>::type* __restrict__ d,
                                                                           typename V2T<T>::type* __restrict__ w,
                                                                           const BiState* __restrict__ st) {
@@ -763,7 +763,7 @@ __global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_forward(ENS_AR
 
 // backward sweep of one colour level: y = relax (D')^-1 (w - U_A y / relax) on its cells
 template <typename T, int LEVEL>
-__global__ void __launch_bounds__(kEnsTile, kEnsBlocksSpmv) ke_b8_backward(ENS_ARGS, const T* __restrict__ A8,
+__global__ void __launch_bounds__(kEnsTile, sizeof(T) == 4 ? kEnsBlocksSpmv + 2 : kEnsBlocksSpmv) ke_b8_backward(ENS_ARGS, const T* __restrict__ A8,
                                                                            const T* __restrict__ Dinv8,
                                                                            const typename V2T<T>::type* __restrict__ wv,
                                                                            typename V2T<T>::type* __restrict__ y,
