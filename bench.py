@@ -227,10 +227,12 @@ def kernel_bytes(name, N, F, s_mat=8, s_vec=8, b8=False, Fx=None):
         if name in table8:
             return table8[name]
     table = {
-        # linearization: x, storage(old), K, lens flag in; the iq cache out (6 doubles)
-        "intensive": N * (16 + 1) + N * 48,
-        # x, S_old, K, lens, iq (6) in; r and the Jacobian column (diag + 2 per face) out
-        "assemble": N * (16 + 16 + 8 + 1 + 48) + N * (16 + 32) + F * 64,
+        # linearization: x, lens flag in; the neighbours' intensive quantities out (p_c, lambda_w,
+        # lambda_n); the 3D assembly evaluates its own cell's
+        "intensive": N * (16 + 1) + N * 24,
+        # x, S_old, K, lens, the cached p_c / lambda_w / lambda_n in; r and the Jacobian column
+        # (diag + 2 per face) out
+        "assemble": N * (16 + 16 + 8 + 1 + 24) + N * (16 + 32) + F * 64,
         # black rows: own d, red d, L blocks (one per face), Dinv; y_b out
         "ilu_black_apply": Nh * (vec + blk + vec) + Nh * vec + F * blk,
         # red rows: own d, black y, A_rb blocks (one per face), Dinv; y_r out

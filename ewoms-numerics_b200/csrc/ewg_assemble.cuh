@@ -16,7 +16,7 @@ namespace ewg {
 struct IqVals {
     double pc, dpc, lw, dlw, ln, dln;
 };
-__device__ __forceinline__ IqVals intensive_values(const Phys& P, double Sw, int lensFlag) {
+__device__ __forceinline__ IqVals intensive_values_full(const Phys& P, double Sw, int lensFlag) {
     const LawDev& L = P.law[lensFlag];
     MatOut m = material(L, Sw);
     // mobility = kr / mu as an AD quotient with a constant denominator
@@ -30,19 +30,32 @@ __device__ __forceinline__ IqVals intensive_values(const Phys& P, double Sw, int
     o.dln = (mun * m.krn.d) / (mun * mun);
     return o;
 }
+// The same with the state of all cells the DNAPL has not reached, S_w = 1, taken from the values
+// intensive_values_full gave for it at context creation (P.sat1): the same bits without the
+// material-law evaluation.
+__device__ __forceinline__ IqVals intensive_values(const Phys& P, double Sw, int lensFlag) {
+    if (Sw == 1.0) {
+        const double* c = P.sat1[lensFlag];
+        return IqVals{c[0], c[1], c[2], c[3], c[4], c[5]};
+    }
+    return intensive_values_full(P, Sw, lensFlag);
+}
 
-// the same, written to the cache in 6 planes (pc, dpc, lw, dlw, ln, dln)
+// the same, written to the cache in 6 planes (pc, dpc, lw, dlw, ln, dln); without `deriv` only the
+// values a neighbour reads (planes 0, 2, 4), for kernels that evaluate their own cell's quantities
 __device__ __forceinline__ void intensive_cell(const Phys& P, const double2* __restrict__ x,
                                                const uint8_t* __restrict__ lens, double* __restrict__ iq,
-                                               int64_t s) {
+                                               int64_t s, bool deriv = true) {
     const int64_t N = P.N;
     const IqVals o = intensive_values(P, x[s].y, lens[s]);
     iq[s] = o.pc;
-    iq[N + s] = o.dpc;
     iq[2 * N + s] = o.lw;
-    iq[3 * N + s] = o.dlw;
     iq[4 * N + s] = o.ln;
-    iq[5 * N + s] = o.dln;
+    if (deriv) {
+        iq[N + s] = o.dpc;
+        iq[3 * N + s] = o.dlw;
+        iq[5 * N + s] = o.dln;
+    }
 }
 
 __device__ __forceinline__ void store_block(double* J, int64_t N, int band, int64_t s, const double b[4]) {
@@ -132,7 +145,8 @@ __device__ __forceinline__ void boundary_face(const Phys& P, int side, const int
     if (left || right) {
         const double g1 = -P.g;
         const double depth = P.L[1] - xf[1];
-        const double pw = left ? P.pRef - P.leftScale * P.rho[0] * g1 * depth : P.pRef - P.rho[0] * g1 * depth;
+        const double pw = left ? __dsub_rn(P.pRef, P.leftScale * P.rho[0] * g1 * depth)
+                               : __dsub_rn(P.pRef, P.rho[0] * g1 * depth);
         const double pB[2] = {pw, pw + P.bndPc[in_lens(P, xf) ? 1 : 0] - 0.0};
         const double dA = xf[AXIS] - xc[AXIS];
         const double distSq = dA * dA;
@@ -149,24 +163,24 @@ __device__ __forceinline__ void boundary_face(const Phys& P, int side, const int
             const double dgS = a == 0 ? 0.0 : -dpcI * coef;
             const double rho = P.rho[a];
             const double pStatIn = -gTimesDist * rho;
-            grad = grad + distIn * (pStatIn / absDistSq);
+            grad = __dadd_rn(grad, __dmul_rn(distIn, pStatIn / absDistSq));
             const bool upB = grad * nA > 0;
             const double lamU = upB ? P.bndLam[lensI][a] : lam[a];
             const double dlamU = upB ? 0.0 : dlam[a];
             const double sK = Ki * grad;
             const double vel = sK * (-lamU);
             const double dvelP = (Ki * dgP) * (-lamU);
-            const double dvelS = (Ki * dgS) * (-lamU) + (-dlamU) * sK;
-            R[a] += vel * nA * rho * area;
-            D[a][0] += dvelP * nA * rho * area;
-            D[a][1] += dvelS * nA * rho * area;
+            const double dvelS = __dadd_rn((Ki * dgS) * (-lamU), (-dlamU) * sK);
+            R[a] = __dadd_rn(R[a], vel * nA * rho * area);
+            D[a][0] = __dadd_rn(D[a][0], dvelP * nA * rho * area);
+            D[a][1] = __dadd_rn(D[a][1], dvelS * nA * rho * area);
         }
         return;
     }
     const bool upper = xf[1] > P.L[1] - P.eps;
     bool inlet = upper && xf[0] > P.inletXlo && xf[0] < P.inletXhi;
     if (DIM == 3) inlet = inlet && xf[2] > P.inletZlo && xf[2] < P.inletZhi;
-    if (inlet) R[1] += P.inletRate * area;
+    if (inlet) R[1] = __dadd_rn(R[1], P.inletRate * area);
 }
 
 // ---- 3D interior cells --------------------------------------------------------------------------
@@ -176,7 +190,8 @@ __device__ __forceinline__ void boundary_face(const Phys& P, int side, const int
 // correction) comes from a small table instead of being recomputed from cell positions, and the
 // scalings by 1/V are multiplications. The two-point gradient is formed with explicitly rounded
 // products and sums (no fused multiply-add) so that its sign, which selects the upstream cell,
-// is the one an unfused CPU evaluation gets.
+// is the one an unfused CPU evaluation gets; the sums into the residual and the Jacobian blocks are
+// explicitly rounded too, so that every kernel inlining these functions gets the same bits.
 
 template <int AXIS>
 __device__ __forceinline__ void interior_face_tab(const Phys& P, const FaceGeo& G, int side, double Ki,
@@ -201,15 +216,15 @@ __device__ __forceinline__ void interior_face_tab(const Phys& P, const FaceGeo& 
         const double sK = Kf * grad;
         const double vel = sK * (-lamU);
         const double dvelP = (Kf * dgP) * (-lamU);
-        const double dvelS = (Kf * dgS) * (-lamU) + (-dlamU) * sK;
+        const double dvelS = __dadd_rn((Kf * dgS) * (-lamU), (-dlamU) * sK);
         // mass flux (v . n) rho A; the neighbour's block is divided by its volume
         const double ra = side ? P.rhoArea[AXIS][a] : -P.rhoArea[AXIS][a];
         const double F = vel * ra;
         const double dFP = dvelP * ra;
         const double dFS = dvelS * ra;
-        R[a] += F;
-        D[a][0] += dFP;
-        D[a][1] += dFS;
+        R[a] = __dadd_rn(R[a], F);
+        D[a][0] = __dadd_rn(D[a][0], dFP);
+        D[a][1] = __dadd_rn(D[a][1], dFS);
         Dj[2 * a] = dFP * -P.invVol;
         Dj[2 * a + 1] = dFS * -P.invVol;
     }
@@ -282,10 +297,10 @@ __device__ __forceinline__ double assemble_core3(const Phys& P, const FaceGeo* _
         const double fac = V / dt;
         const double sw0 = P.porosity * Sw * P.rho[0];
         const double sn0 = P.porosity * (1.0 - (0.0 + Sw)) * P.rho[1];
-        R[0] += (sw0 - so.x) * fac;
-        R[1] += (sn0 - so.y) * fac;
-        D[0][1] += (P.porosity * P.rho[0]) * fac;
-        D[1][1] += (-P.porosity * P.rho[1]) * fac;
+        R[0] = __dadd_rn(R[0], __dmul_rn(sw0 - so.x, fac));
+        R[1] = __dadd_rn(R[1], __dmul_rn(sn0 - so.y, fac));
+        D[0][1] = __dadd_rn(D[0][1], __dmul_rn(P.porosity * P.rho[0], fac));
+        D[1][1] = __dadd_rn(D[1][1], __dmul_rn(-P.porosity * P.rho[1], fac));
     }
     // boundary faces (warp-uniform except at the two ends of each x-row)
 #pragma unroll
@@ -312,15 +327,15 @@ __device__ __forceinline__ double assemble_core3(const Phys& P, const FaceGeo* _
     return fmax(fabs(R[0]), fabs(R[1]));
 }
 
-// One cell of a 3D grid at split-order position s with its own and its neighbours' values read
-// from the global arrays and the intensive-quantity cache.
+// One cell of a 3D grid at split-order position s: its own intensive quantities evaluated here
+// (for the S_w = 1 cells a table read, intensive_values), the neighbours' read from the global
+// arrays and the cache (planes 0, 2, 4).
 template <typename JT, bool WITH_J, class NB>
 __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* __restrict__ geo,
                                                  const double2* __restrict__ x, const double2* __restrict__ sold,
                                                  const double* __restrict__ perm, const uint8_t* __restrict__ lens,
                                                  const double* __restrict__ iq, double dt, double2* __restrict__ rOut,
                                                  JT* __restrict__ J, int64_t s, int& bad, const NB& nbr) {
-    const int64_t N = P.N;
     const int s32 = (int)s;  // N < 2^31: 32-bit cell indices
     const int Nh32 = (int)P.Nh;
     const int col = s32 >= Nh32 ? 1 : 0;
@@ -329,16 +344,17 @@ __device__ __forceinline__ double assemble_cell3(const Phys& P, const FaceGeo* _
     const int idx[3] = {ci.i, ci.j, ci.k};
     const bool has[6] = {ci.i > 0, ci.i < P.nx - 1, ci.j > 0, ci.j < P.ny - 1, ci.k > 0, ci.k < P.nz - 1};
     const double2 xi = x[s32];
+    const IqVals q = intensive_values(P, xi.y, lens[s32]);
     OwnVals o;
     o.pw = xi.x;
     o.Sw = xi.y;
     o.K = perm[s32];
-    o.pc = iq[s32];
-    o.dpc = iq[N + s32];
-    o.lam[0] = iq[2 * N + s32];
-    o.lam[1] = iq[4 * N + s32];
-    o.dlam[0] = iq[3 * N + s32];
-    o.dlam[1] = iq[5 * N + s32];
+    o.pc = q.pc;
+    o.dpc = q.dpc;
+    o.lam[0] = q.lw;
+    o.lam[1] = q.ln;
+    o.dlam[0] = q.dlw;
+    o.dlam[1] = q.dln;
     const int base = (col ^ 1) * Nh32;
     const int nxh = P.nxh, planeh = (int)P.planeh;
     const int nb[6] = {base + h - 1 + ci.b, base + h + ci.b, base + h - nxh, base + h + nxh, base + h - planeh,

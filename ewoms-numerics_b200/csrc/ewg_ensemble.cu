@@ -235,8 +235,8 @@ __global__ void __launch_bounds__(kEnsTile) ke_intensive(ENS_ARGS, const int* __
         const int64_t off = sm.off;
         const int64_t hEnd = tile_end(P, sh[1]);
         for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
-            intensive_cell(P, x + off, lens + off, iq + 6 * off, h);
-            intensive_cell(P, x + off, lens + off, iq + 6 * off, P.Nh + h);
+            intensive_cell(P, x + off, lens + off, iq + 6 * off, h, false);
+            intensive_cell(P, x + off, lens + off, iq + 6 * off, P.Nh + h, false);
         }
     }
 }

@@ -88,6 +88,9 @@ struct Phys {
     // p_cnw and the phase mobilities k_r / mu
     double bndPc[2];
     double bndLam[2][2];
+    // intensive quantities at S_w = 1 per region (p_c, dp_c, lambda_w, dlambda_w, lambda_n,
+    // dlambda_n with d/dS_w), evaluated on the device by the same function at context creation
+    double sat1[2][6];
     FastDiv fdNxh, fdNy;     // divisions by nx / 2 and ny in cell_of (N < 2^31)
     double rhoArea[3][2];    // rho_alpha * face area per axis (mass flux per unit velocity)
     double invVol;           // 1 / cell volume

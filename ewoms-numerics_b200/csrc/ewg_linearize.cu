@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kLinBlock) k_intensive(const __grid_constant__
                                                          double* __restrict__ iq) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N;
          s += (int64_t)gridDim.x * blockDim.x)
-        intensive_cell(P, x, lens, iq, s);
+        intensive_cell(P, x, lens, iq, s, P.dim == 2);  // 3D kernels evaluate their own cell
 }
 
 // Non-negative doubles compare like their bit patterns as unsigned integers.
@@ -371,7 +371,8 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble_fd(
     block_max_publish(localMax, errmax);
 }
 
-// S_w = 1 state of the free-flow boundary per region: p_cnw and k_r / mu of both phases
+// S_w = 1 state per region: p_cnw and k_r / mu of both phases for the free-flow boundary
+// (out[0..5]), and the intensive quantities with their derivatives (out[6..17])
 __global__ void k_boundary_constants(const __grid_constant__ Phys P, double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     for (int r = 0; r < 2; ++r) {
@@ -379,6 +380,9 @@ __global__ void k_boundary_constants(const __grid_constant__ Phys P, double* out
         out[3 * r] = m.pc.v;
         out[3 * r + 1] = m.krw.v / P.mu[0];
         out[3 * r + 2] = m.krn.v / P.mu[1];
+        const IqVals q = intensive_values_full(P, 1.0, r);
+        const double v[6] = {q.pc, q.dpc, q.lw, q.dlw, q.ln, q.dln};
+        for (int c = 0; c < 6; ++c) out[6 + 6 * r + c] = v[c];
     }
 }
 
@@ -412,10 +416,10 @@ ewg_status launch_storage(ewg_ctx* ctx, const double2* x, double2* sold) {
 
 cudaError_t boundary_constants(Phys& P, cudaStream_t stream) {
     double* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, sizeof(double) * 6);
+    cudaError_t e = cudaMalloc(&d, sizeof(double) * 18);
     if (e != cudaSuccess) return e;
     k_boundary_constants<<<1, 32, 0, stream>>>(P, d);
-    double h[6] = {0, 0, 0, 0, 0, 0};
+    double h[18] = {0};
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -425,6 +429,7 @@ cudaError_t boundary_constants(Phys& P, cudaStream_t stream) {
         P.bndPc[r] = h[3 * r];
         P.bndLam[r][0] = h[3 * r + 1];
         P.bndLam[r][1] = h[3 * r + 2];
+        for (int c = 0; c < 6; ++c) P.sat1[r][c] = h[6 + 6 * r + c];
     }
     return cudaSuccess;
 }

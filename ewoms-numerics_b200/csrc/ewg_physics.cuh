@@ -5,6 +5,10 @@
 // respect to S_w (struct VD) and add the trivial p_w derivatives by hand. The arithmetic follows
 // the forward-mode rules of DenseAd::Evaluation (product rule, pow(x, e)' = pow(x, e)/x*e with the
 // x == 0 special case, sqrt' = 0.5/sqrt) so values agree with an AD evaluation to rounding.
+// Sums of products are written with explicitly rounded operations (no fused multiply-add): the
+// compiler's choice of which product to fuse may differ between the kernels that inline these
+// functions, and explicit rounding makes every kernel get the same bits (also the bits of an
+// unfused CPU evaluation).
 //
 // Material laws (ewoms-material, restated from their published form):
 //   EffToAbsLaw: S_e = (S - S_r) / (1 - (S_wr + S_nr)); k_rn reads 1 - S_n,e
@@ -26,11 +30,13 @@ struct VD {
     double v, d;
 };
 
-__device__ __forceinline__ VD vd_mul(VD a, VD b) { return {a.v * b.v, a.d * b.v + b.d * a.v}; }
-__device__ __forceinline__ VD vd_add(VD a, VD b) { return {a.v + b.v, a.d + b.d}; }
-__device__ __forceinline__ VD vd_sub(VD a, VD b) { return {a.v - b.v, a.d - b.d}; }
-__device__ __forceinline__ VD vd_scale(VD a, double s) { return {a.v * s, a.d * s}; }
-__device__ __forceinline__ VD vd_rsub(double s, VD a) { return {s - a.v, -a.d}; }  // s - a
+__device__ __forceinline__ VD vd_mul(VD a, VD b) {
+    return {__dmul_rn(a.v, b.v), __dadd_rn(__dmul_rn(a.d, b.v), __dmul_rn(b.d, a.v))};
+}
+__device__ __forceinline__ VD vd_add(VD a, VD b) { return {__dadd_rn(a.v, b.v), __dadd_rn(a.d, b.d)}; }
+__device__ __forceinline__ VD vd_sub(VD a, VD b) { return {__dsub_rn(a.v, b.v), __dsub_rn(a.d, b.d)}; }
+__device__ __forceinline__ VD vd_scale(VD a, double s) { return {__dmul_rn(a.v, s), __dmul_rn(a.d, s)}; }
+__device__ __forceinline__ VD vd_rsub(double s, VD a) { return {__dsub_rn(s, a.v), -a.d}; }  // s - a
 __device__ __forceinline__ VD vd_pow(VD x, double e) {
     if (x.v == 0.0) return {0.0, 0.0};
     double px = pow(x.v, e);
@@ -76,10 +82,11 @@ __device__ __forceinline__ VD hermite(const LawDev& L, VD x) {
     return y;
 }
 __device__ __forceinline__ VD reg_vg_pcnw(const LawDev& L, VD Se) {
-    if (Se.v < L.pcLowSw) return {L.pcLow + L.pcSlopeLow * (Se.v - L.pcLowSw), L.pcSlopeLow * Se.d};
+    if (Se.v < L.pcLowSw)
+        return {__dadd_rn(L.pcLow, __dmul_rn(L.pcSlopeLow, Se.v - L.pcLowSw)), L.pcSlopeLow * Se.d};
     if (Se.v > L.pcHighSw) {
         if (Se.v < 1.0) return hermite(L, Se);
-        return {L.m1High * (Se.v - 1.0) + 0.0, L.m1High * Se.d};
+        return {__dadd_rn(__dmul_rn(L.m1High, Se.v - 1.0), 0.0), L.m1High * Se.d};
     }
     return vg_pcnw(L, Se);
 }
@@ -94,8 +101,9 @@ __device__ __forceinline__ VD reg_vg_krn(const LawDev& L, VD Sw) {
     return vg_krn(L, Sw);
 }
 __device__ __forceinline__ VD reg_bc_pcnw(const LawDev& L, VD Se) {
-    if (Se.v <= L.bcLowSw) return {L.bcPcLow + L.bcSlopeLow * (Se.v - L.bcLowSw), L.bcSlopeLow * Se.d};
-    if (Se.v >= 1.0) return {L.pe + L.bcSlopeOne * (Se.v - 1.0), L.bcSlopeOne * Se.d};
+    if (Se.v <= L.bcLowSw)
+        return {__dadd_rn(L.bcPcLow, __dmul_rn(L.bcSlopeLow, Se.v - L.bcLowSw)), L.bcSlopeLow * Se.d};
+    if (Se.v >= 1.0) return {__dadd_rn(L.pe, __dmul_rn(L.bcSlopeOne, Se.v - 1.0)), L.bcSlopeOne * Se.d};
     return vd_scale(vd_pow(Se, L.negInvLambda), L.pe);
 }
 __device__ __forceinline__ VD reg_bc_krw(const LawDev& L, VD Se) {
