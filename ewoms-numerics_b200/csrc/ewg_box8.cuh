@@ -680,13 +680,35 @@ __device__ __forceinline__ int64_t b8_to_split_pos(const Phys& P, int64_t s) {
 }
 
 // matrix planes (nPlanes = 4 x bands planes of N values) into the block-packed box-8 copy:
-// out block (band, s8) = in planes (4 band .. 4 band + 3)[split(s8)], converting TI -> TO
+// out block (band, s8) = in planes (4 band .. 4 band + 3)[split(s8)], converting TI -> TO.
+// One thread per pair of cells two apart in x (colour bit 0 clear and set, same place and box):
+// they are neighbours in the split order (split positions sp and sp + 1, sp even), so each plane
+// is read as one aligned pair and every sector read is used whole; each block is written as one
+// 16- or 32-byte packed store.
 template <typename TI, typename TO>
 __global__ void k_b8_matrix_from_split(const __grid_constant__ Phys P, int nPlanes, const TI* __restrict__ in,
                                        TO* __restrict__ out) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.N; s += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t sp = b8_to_split_pos(P, s);
-        for (int p = 0; p < nPlanes; ++p) out[4 * ((int64_t)(p >> 2) * P.N + s) + (p & 3)] = (TO)in[(int64_t)p * P.N + sp];
+    using TI2 = typename V2T<TI>::type;
+    const TI2* __restrict__ in2 = reinterpret_cast<const TI2*>(in);
+    const int64_t half = P.N / 2;
+    const int bands = nPlanes / 4;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < half; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = t / P.Nb;                            // 32 groups with colour bit 0 clear
+        const int64_t b = t - gi * P.Nb;
+        const int64_t g = ((gi >> 3) << 4) | (gi & 7);          // colour = g >> 3, place = g & 7
+        const int64_t s = g * P.Nb + b, s2 = s + 8 * P.Nb;      // colour bit 0 clear / set
+        const int64_t sp = b8_to_split_pos(P, s);              // even; s2 sits at sp + 1
+        for (int band = 0; band < bands; ++band) {
+            double v[4], w[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const TI2 a = in2[((int64_t)(4 * band + c) * P.N + sp) >> 1];
+                v[c] = (double)a.x;
+                w[c] = (double)a.y;
+            }
+            store_pb(out, P.N, band, s, v);
+            store_pb(out, P.N, band, s2, w);
+        }
     }
 }
 
