@@ -10,8 +10,10 @@
 //
 // Two kernels per linearization:
 //   k_intensive  one thread per cell: the intensive quantities of immiscibleintensivequantities.hh
-//                :87-145 that neighbours need (p_c, lambda_w, lambda_n with d/dS_w), written once
-//                per cell like the reference's intensive-quantity cache (lensproblem.hh:166).
+//                :87-145 that neighbours need (p_c, lambda_w, lambda_n; on 2D grids also their
+//                d/dS_w), written once per cell like the reference's intensive-quantity cache
+//                (lensproblem.hh:166). The 3D assembly evaluates its own cell's quantities with
+//                their derivatives itself; cells at S_w = 1 take them from a per-region table.
 //   k_assemble   one thread per cell: fluxes over its faces (darcyfluxmodule.hh:185-527,
 //                immisciblelocalresidual.hh:123-149), the implicit-Euler storage term
 //                (fvbaselocalresidual.hh:494-629), the lens boundary conditions
