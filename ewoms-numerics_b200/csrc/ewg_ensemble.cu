@@ -696,12 +696,26 @@ __global__ void __launch_bounds__(kEnsTile) ke_b8_matrix(ENS_ARGS, const int* __
         const int64_t hEnd = tile_end(P, sh[1]);
         const T* Jm = J + kEnsBands * 4 * sm.off;
         T* Am = A8 + kEnsBands * 4 * sm.off;
-        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x)
-            for (int col = 0; col < 2; ++col) {
-                const int64_t s8 = col * P.Nh + h, sp = b8_to_split_pos(P, s8);
-                for (int pl = 0; pl < kEnsBands * 4; ++pl)
-                    Am[4 * ((int64_t)(pl >> 2) * P.N + s8) + (pl & 3)] = Jm[(int64_t)pl * P.N + sp];
+        // half index h -> the pair of cells two apart in x (colour bit 0 clear / set, same place and
+        // box), neighbours in the split order: aligned pair loads, packed block stores
+        const typename V2T<T>::type* __restrict__ Jm2 = reinterpret_cast<const typename V2T<T>::type*>(Jm);
+        for (int64_t h = sh[1] + threadIdx.x; h < hEnd; h += blockDim.x) {
+            const int64_t gi = h / P.Nb, b = h - gi * P.Nb;
+            const int64_t g = ((gi >> 3) << 4) | (gi & 7);
+            const int64_t s8 = g * P.Nb + b, s8b = s8 + 8 * P.Nb;
+            const int64_t sp = b8_to_split_pos(P, s8);  // even; s8b sits at sp + 1
+            for (int band = 0; band < kEnsBands; ++band) {
+                double v[4], w[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const typename V2T<T>::type a = Jm2[((int64_t)(4 * band + c) * P.N + sp) >> 1];
+                    v[c] = (double)a.x;
+                    w[c] = (double)a.y;
+                }
+                store_pb(Am, P.N, band, s8, v);
+                store_pb(Am, P.N, band, s8b, w);
             }
+        }
     }
 }
 
