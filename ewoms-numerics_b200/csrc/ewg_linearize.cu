@@ -498,7 +498,7 @@ ewg_status build_interior_tables(ewg_ctx* ctx) {
 
 // resident blocks per SM the interior kernel is compiled for (register budget 65536 / (256 x it))
 #ifndef EWG_INTERIOR_MIN_BLOCKS
-#define EWG_INTERIOR_MIN_BLOCKS 3
+#define EWG_INTERIOR_MIN_BLOCKS 2
 #endif
 constexpr int kInteriorMinBlocks = EWG_INTERIOR_MIN_BLOCKS;
 
