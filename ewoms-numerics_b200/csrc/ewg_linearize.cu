@@ -192,8 +192,15 @@ __global__ void __launch_bounds__(kLinBlock) k_assemble(
 
 
 // 3D grids: every cell through assemble_cell3 (face geometry from the table)
+// threads per block of the 3D assembly (with EWG_INTERIOR_MIN_BLOCKS below: 256 threads, two
+// blocks per SM, 99 registers without spills measured fastest against 128 x 4-5 and 192 x 3)
+#ifndef EWG_ASSEMBLE3_BLOCK
+#define EWG_ASSEMBLE3_BLOCK 256
+#endif
+constexpr int kAsm3Block = EWG_ASSEMBLE3_BLOCK;
+
 template <typename JT, bool WITH_J, int MINB>
-__global__ void __launch_bounds__(kLinBlock, MINB) k_assemble3(
+__global__ void __launch_bounds__(kAsm3Block, MINB) k_assemble3(
     const __grid_constant__ Phys P, const FaceGeo* __restrict__ geo, const double2* __restrict__ x,
     const double2* __restrict__ sold, const double* __restrict__ perm, const uint8_t* __restrict__ lens,
     const double* __restrict__ iq, double dt, double2* __restrict__ rOut, JT* __restrict__ J,
@@ -505,8 +512,8 @@ constexpr int kInteriorMinBlocks = EWG_INTERIOR_MIN_BLOCKS;
 template <typename JT, bool WITH_J>
 static void launch_assemble3(ewg_ctx* ctx, double dt, const double2* x, double2* r, JT* J) {
     auto k = k_assemble3<JT, WITH_J, kInteriorMinBlocks>;
-    int g = grid_size_for(ctx, (const void*)k, kLinBlock);
-    EWG_LAUNCH(ctx, K_ASSEMBLE, k, g, kLinBlock, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
+    int g = grid_size_for(ctx, (const void*)k, kAsm3Block);
+    EWG_LAUNCH(ctx, K_ASSEMBLE, k, g, kAsm3Block, ctx->P, ctx->geo, x, ctx->sold, ctx->perm, ctx->lens, ctx->iq, dt,
                r, J, ctx->d_errmax, ctx->d_flags);
 }
 
